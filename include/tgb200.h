@@ -1,0 +1,177 @@
+/*
+ * tgb200.h -- C-ABI of the B200 SOAP-GAP backend (libtgb200.so).
+ *
+ * The reference (TurboGAP, Fortran) selects its backend at link time: a module
+ * named gap_backend / gpu_context with identical public procedures is compiled
+ * from either the CPU or the GPU source (src/gap_backend_cpu.f90:6-17,
+ * src/gpu_context.f90:1-24). This header is the C side of that seam: every
+ * entry point is callable from Fortran through ISO_C_BINDING (all arguments are
+ * plain pointers and sizes, arrays column-major with the Fortran shapes named
+ * below, neighbour indices 1-based).
+ *
+ * Conventions
+ *   - Every call returns TG_OK (0) or a negative TG_ERR_* code; tg_last_error()
+ *     returns the text of the last failure on the calling thread.
+ *   - (3, n) arrays are contiguous x,y,z triples (Fortran column-major).
+ *   - Host pointers are only read/written during the call; the backend owns
+ *     every device buffer, stream and cached sparse set.
+ *   - Not re-entrant: one host thread per context (one MPI rank per GPU in the
+ *     reference's model, src/gpu_context.f90:41-58).
+ */
+#ifndef TGB200_H
+#define TGB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TG_OK = 0,
+    TG_ERR_ARG = -1,          /* invalid argument or unsupported hyperparameter */
+    TG_ERR_CUDA = -2,         /* CUDA runtime/driver error                      */
+    TG_ERR_CAPACITY = -3,     /* caller buffer too small; required size returned */
+    TG_ERR_STATE = -4,        /* call out of order (no context, no open block)  */
+    TG_ERR_DEVICE = -5,       /* device-side error word set (see message)       */
+    TG_ERR_TIMEOUT = -6,      /* a bounded device wait expired                  */
+    TG_ERR_NOMEM = -7         /* device allocation failed                       */
+};
+
+/* Arithmetic of the GAP kernel GEMMs. */
+enum {
+    TG_PREC_BF16X3 = 3,       /* plain form: bf16 hi/lo split, 3 products, fp32 accumulate */
+    TG_PREC_BF16 = 1          /* mixed form: single bf16 product, fp32 accumulate          */
+};
+
+/* One soap_turbo block's hyperparameters (type soap_turbo, src/types.f90:75-134,
+ * as filled by read_gap_hypers, src/read_files.f90:4633-5236). Per-species arrays
+ * hold n_species entries; rcut_soft is rcut_hard - buffer (read_files.f90:5101-5108).
+ * species_z[s] is the global species id (1-based position in the input deck's
+ * species_types) that descriptor species s stands for. */
+typedef struct {
+    int32_t n_species;
+    int32_t l_max;
+    int32_t radial_enhancement;
+    int32_t central_species;        /* 1-based descriptor species index; 0 = all */
+    const int32_t *alpha_max;
+    const int32_t *species_z;
+    const double *rcut_hard;
+    const double *rcut_soft;
+    const double *nf;
+    const double *global_scaling;
+    const double *atom_sigma_r;
+    const double *atom_sigma_r_scaling;
+    const double *atom_sigma_t;
+    const double *atom_sigma_t_scaling;
+    const double *amplitude_scaling;
+    const double *central_weight;
+} tg_soap_hypers;
+
+/* ---- device context: gpu_context_init / gpu_context_finalize
+ *      (src/gpu_context.f90:41-58). n_omp is set to 1 as on the CPU path. */
+int tg_context_init(int32_t rank, int32_t device, int32_t *n_omp);
+int tg_context_finalize(void);
+
+/* gpu_memory_budget_init (src/gpu_context.f90:100-162): the batch budget in GB
+ * the driver uses for max_Gbytes_per_process, from the device's free memory. */
+int tg_memory_budget(double *max_gbytes);
+
+const char *tg_last_error(void);
+
+/* ---- sparse set of one block: soap_backend_begin(hypers) / soap_backend_end()
+ *      (src/gap.f90:49-64). Uploads Qs(dim, n_sparse) (column-major, one sparse
+ *      point per column, src/read_files.f90:707-720) and alphas(n_sparse), builds
+ *      the radial/angular tables, and makes the block current. The upload is
+ *      cached by block_key: a later begin with the same key and n_sparse reuses
+ *      the device copy (the GPU branch of the reference uploads per call). */
+int tg_soap_begin(int32_t block_key, const tg_soap_hypers *hypers, int32_t n_sparse,
+                  const double *Qs, const double *alphas, double delta, double zeta,
+                  int32_t precision);
+int tg_soap_end(void);
+
+/* ---- get_gap_soap (src/gap_interface.f90:41-57, live body :178-431) for the
+ *      current block, prediction with forces: the remap to central sites and
+ *      kept pairs, get_soap, get_soap_energy_and_forces (src/gap.f90:66-259) and
+ *      the scatter to global indices.
+ *   n_total_sites            atoms in the unit cell (first argument of the reference)
+ *   n_sites0                 sites in this batch (this_i_end - this_i_beg + 1)
+ *   n_neigh0(n_sites0), neighbors_list0(P) (1-based supercell indices),
+ *   rjs0(P), xyz0(3, P)       the batch slices of build_neighbors_list's output
+ *   species_batch(n_sites0)  global species id of each batch site
+ *   species_all(n_total_sites) global species id of every unit-cell atom
+ *   energies0(n_total_sites), forces0(3, n_total_sites): ASSIGNED for the sites
+ *     this block touches, left unchanged elsewhere (gap_interface.f90:422-431);
+ *   virial(3, 3): overwritten. */
+int tg_get_gap_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                    const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                    const int32_t *species_batch, const int32_t *species_all,
+                    double *energies0, double *forces0, double *virial);
+
+/* Descriptor only (soap_turbo get_soap as called at gap_interface.f90:320-325,
+ * through the same remap): soap(dim, n_central) of the current block's central
+ * sites in batch order. The Cartesian derivative array soap_cart_der is never
+ * formed on the device; forces come from the fused adjoint contraction. */
+int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                const int32_t *species_batch, const int32_t *species_all, double *soap,
+                int32_t *n_central);
+
+/* ---- build_neighbors_list (src/neighbors.f90:243-605) with
+ *      rebuild_neighbors_list = .true.: self pair first, cell list for
+ *      orthorhombic boxes of at least 2 rcut, O(N * N_supercell) search
+ *      otherwise; per pair rjs, xyz (MIC), thetas, phis, neighbor_species.
+ *   positions(3, n_sites_supercell), species_supercell(n_sites_supercell),
+ *   do_list(n_sites) (logical as int32), a/b/c_box(3) (orthorhombic boxes are
+ *   snapped as the reference does). cap = capacity of the per-pair arrays; if
+ *   smaller than needed, returns TG_ERR_CAPACITY with *n_pairs = required.
+ *   Lists, rjs and xyz are bit-identical to the reference arithmetic; thetas
+ *   and phis are within a few ulp (device acos/atan2). */
+int tg_build_neighbors_list(int32_t n_sites_supercell, const double *positions,
+                            int32_t n_sites, double *a_box, double *b_box, double *c_box,
+                            double rcut_max, const int32_t *indices,
+                            const int32_t *species_supercell, const int32_t *do_list,
+                            int64_t cap, int32_t *n_neigh, int32_t *neighbors_list,
+                            double *rjs, double *thetas, double *phis, double *xyz,
+                            int32_t *neighbor_species, int64_t *n_pairs);
+
+/* ---- velocity_verlet (src/md.f90:226-283), no fixed atoms, arrays (3, n). */
+int tg_velocity_verlet(int32_t n, double *positions, double *positions_prev,
+                       double *velocities, const double *forces, double *forces_prev,
+                       const double *masses, double dt, double *dt_prev, int32_t first_step);
+
+/* ---- device-resident MD engine: the hot loop of the driver (turbogap.f90:664,
+ *      neighbours :896-997, SOAP blocks :1274-1378, totals :1941/2009) and of
+ *      compute_md's NVE path (src/turbogap_md.f90:161-297): neighbour list, every
+ *      registered block, energies/forces/virial, wrap_pbc, remove_cm_vel and
+ *      velocity_verlet, all on the GPU without host round trips. Each block is
+ *      one tg_soap_begin'ed block_key (captured at engine creation). */
+typedef struct tg_engine tg_engine;
+
+int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *species,
+                     const double *masses, const double *a_box, const double *b_box,
+                     const double *c_box, int32_t n_blocks, const int32_t *block_keys,
+                     const double *e0_by_species, int32_t n_species_total,
+                     double neighbors_buffer, tg_engine **out);
+int tg_engine_destroy(tg_engine *e);
+/* Replace positions (3, n) and velocities (3, n) (velocities may be NULL). */
+int tg_engine_set_state(tg_engine *e, const double *positions, const double *velocities);
+/* Energies (n), forces (3, n), virial (3, 3) at the current positions. */
+int tg_engine_compute(tg_engine *e, double *energies, double *forces, double *virial);
+/* n_steps of NVE velocity-Verlet with time step dt (fs); graph-captured after
+ * the first step. Optional outputs (NULL to skip) are read after the last step:
+ * potential energy and kinetic energy (eV). */
+int tg_engine_md(tg_engine *e, int32_t n_steps, double dt, double *e_pot, double *e_kin);
+int tg_engine_get_state(tg_engine *e, double *positions, double *velocities, double *forces);
+/* Pairs in the current neighbour list. */
+int tg_engine_n_pairs(tg_engine *e, int64_t *n_pairs);
+/* CUDA stream the engine launches on (cudaStream_t), for timing with events. */
+int tg_engine_stream(tg_engine *e, void **stream);
+/* Evaluate energies+forces on the device without copying results out; the
+ * bench uses this for device-resident timing. */
+int tg_engine_compute_device(tg_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

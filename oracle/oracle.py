@@ -1,0 +1,325 @@
+"""ctypes front-end of the FP64 CPU oracle (oracle/tg_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: it is the checker the CUDA backend is compared with.
+Arrays follow the Fortran layout of the reference: ``(3, n)`` arrays are passed
+as numpy ``(n, 3)`` C-order (identical memory), neighbour indices are 1-based.
+
+Parity status: geometry, neighbour lists, get_gap_soap remap, GAP kernel and
+velocity-Verlet restate the reference Fortran; the SOAP descriptor restates the
+published method because the soap_turbo submodule is absent from the
+reference tree -- descriptor values are parity unpinned (see tg_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "_build", "libtg_oracle.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++, OpenMP)."""
+    if force or not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(
+            os.path.join(_HERE, "tg_oracle.cpp")):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _SO
+
+
+class _Hypers(C.Structure):
+    _fields_ = [
+        ("n_species", C.c_int), ("l_max", C.c_int), ("radial_enhancement", C.c_int),
+        ("central_species", C.c_int),
+        ("alpha_max", C.POINTER(C.c_int)), ("species_z", C.POINTER(C.c_int)),
+        ("rcut_hard", C.POINTER(C.c_double)), ("rcut_soft", C.POINTER(C.c_double)),
+        ("nf", C.POINTER(C.c_double)), ("global_scaling", C.POINTER(C.c_double)),
+        ("atom_sigma_r", C.POINTER(C.c_double)), ("atom_sigma_r_scaling", C.POINTER(C.c_double)),
+        ("atom_sigma_t", C.POINTER(C.c_double)), ("atom_sigma_t_scaling", C.POINTER(C.c_double)),
+        ("amplitude_scaling", C.POINTER(C.c_double)), ("central_weight", C.POINTER(C.c_double)),
+    ]
+
+
+class _Block(C.Structure):
+    _fields_ = [("hypers", _Hypers), ("n_sparse", C.c_int), ("Qs", C.POINTER(C.c_double)),
+                ("alphas", C.POINTER(C.c_double)), ("delta", C.c_double), ("zeta", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        L = _lib
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_get_distance.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]
+        L.orc_number_of_unit_cells.argtypes = [_dp, _dp, _dp, C.c_double, _ip]
+        L.orc_make_supercell.argtypes = [C.c_int, _dp, _ip, _dp, _dp, _dp, _ip, _dp, _ip]
+        L.orc_build_neighbors_list.restype = C.c_int64
+        L.orc_build_neighbors_list.argtypes = [C.c_int, _dp, C.c_int, _dp, _dp, _dp, C.c_double,
+                                               _ip, _ip, _ip, C.c_int64, _ip, _ip, _dp, _dp, _dp,
+                                               _dp, _ip]
+        L.orc_soap_dim.argtypes = [C.POINTER(_Hypers)]
+        L.orc_poly3_W.argtypes = [C.c_int, _dp]
+        L.orc_radial.argtypes = [C.POINTER(_Hypers), C.c_int, C.c_double, C.c_int, _dp, _dp]
+        L.orc_angular.argtypes = [C.POINTER(_Hypers), C.c_int, C.c_double, _dp, _dp]
+        L.orc_real_ylm.argtypes = [C.c_int, _dp, _dp, C.c_void_p]
+        L.orc_get_soap.argtypes = [C.POINTER(_Hypers), C.c_int, _ip, C.c_int, _ip, _dp, _dp, _dp,
+                                   C.c_void_p, C.c_void_p]
+        L.orc_soap_energy_and_forces.argtypes = [C.c_int, C.c_int, _dp, C.c_void_p, C.c_int, _dp,
+                                                 _dp, C.c_double, C.c_double, C.c_double, _ip, _ip,
+                                                 _dp, C.c_int, C.c_int, _dp, _dp, _dp]
+        L.orc_get_gap_soap.argtypes = [C.POINTER(_Hypers), C.c_int, C.c_int, _ip, _ip, _dp, _dp,
+                                       _ip, _ip, C.c_int, _dp, _dp, C.c_double, C.c_double,
+                                       C.c_int, _dp, _dp, _dp]
+        L.orc_atom_pair_batches.argtypes = [C.c_int, _ip, _dp, C.c_double, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, C.c_double, _ip, _ip, _ip, _ip]
+        L.orc_velocity_verlet.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double,
+                                          _dp, C.c_int]
+        L.orc_remove_cm_vel.argtypes = [C.c_int, _dp, _dp]
+        L.orc_wrap_pbc.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_evaluate.argtypes = [C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int, C.POINTER(_Block),
+                                   C.c_void_p, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp,
+                                   C.POINTER(C.c_int64)]
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return lib().orc_set_threads(int(n))
+
+
+def _f64(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _i32(x):
+    return np.ascontiguousarray(x, dtype=np.int32)
+
+
+class HypersC:
+    """Keeps the numpy buffers behind an ``orc_soap_hypers`` alive.
+
+    ``h`` is any object with the soap_turbo hyperparameter attributes
+    (``n_species, l_max, radial_enhancement, central_species, alpha_max,
+    species_z, rcut_hard, rcut_soft, nf, global_scaling, atom_sigma_r,
+    atom_sigma_r_scaling, atom_sigma_t, atom_sigma_t_scaling,
+    amplitude_scaling, central_weight``)."""
+
+    _dfields = ("rcut_hard", "rcut_soft", "nf", "global_scaling", "atom_sigma_r",
+                "atom_sigma_r_scaling", "atom_sigma_t", "atom_sigma_t_scaling",
+                "amplitude_scaling", "central_weight")
+
+    def __init__(self, h):
+        self.keep = {}
+        s = _Hypers()
+        s.n_species = int(h.n_species)
+        s.l_max = int(h.l_max)
+        s.radial_enhancement = int(h.radial_enhancement)
+        s.central_species = int(h.central_species)
+        for name in ("alpha_max", "species_z"):
+            a = _i32(getattr(h, name))
+            self.keep[name] = a
+            setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_int)))
+        for name in self._dfields:
+            a = _f64(getattr(h, name))
+            self.keep[name] = a
+            setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        self.struct = s
+        self.dim = lib().orc_soap_dim(C.byref(s))
+
+    @property
+    def ref(self):
+        return C.byref(self.struct)
+
+
+def get_distance(posi, posj, a, b, c):
+    dist = np.zeros(3)
+    d = np.zeros(1)
+    ish = np.zeros(3, np.int32)
+    lib().orc_get_distance(_f64(posi), _f64(posj), _f64(a), _f64(b), _f64(c), dist, d, ish)
+    return dist, float(d[0]), ish
+
+
+def number_of_unit_cells(a, b, c, rcut):
+    ind = np.zeros(3, np.int32)
+    lib().orc_number_of_unit_cells(_f64(a), _f64(b), _f64(c), float(rcut), ind)
+    return ind
+
+
+def make_supercell(positions, species, a, b, c, indices):
+    n = positions.shape[0]
+    nrep = int(np.prod(indices))
+    pos = np.zeros((n * nrep, 3))
+    spc = np.zeros(n * nrep, np.int32)
+    lib().orc_make_supercell(n, _f64(positions), _i32(species), _f64(a), _f64(b), _f64(c),
+                             _i32(indices), pos, spc)
+    return pos, spc
+
+
+def build_neighbors_list(positions_sc, n_sites, a, b, c, rcut_max, indices, species_sc,
+                         do_list=None):
+    """neighbors.f90:243-605. Returns dict of n_neigh, neighbors_list (1-based),
+    rjs, thetas, phis, xyz (P,3), neighbor_species."""
+    nsc = positions_sc.shape[0]
+    if do_list is None:
+        do_list = np.ones(n_sites, np.int32)
+    a, b, c = _f64(a).copy(), _f64(b).copy(), _f64(c).copy()
+    cap = n_sites * 48
+    while True:
+        n_neigh = np.zeros(n_sites, np.int32)
+        nl = np.zeros(cap, np.int32)
+        rjs = np.zeros(cap)
+        th = np.zeros(cap)
+        ph = np.zeros(cap)
+        xyz = np.zeros((cap, 3))
+        ns = np.zeros(cap, np.int32)
+        np_ = lib().orc_build_neighbors_list(nsc, _f64(positions_sc), n_sites, a, b, c,
+                                             float(rcut_max), _i32(indices), _i32(species_sc),
+                                             _i32(do_list), cap, n_neigh, nl, rjs, th, ph, xyz, ns)
+        if np_ >= 0:
+            break
+        cap = -np_
+    P = int(np_)
+    return dict(n_neigh=n_neigh, neighbors_list=nl[:P], rjs=rjs[:P], thetas=th[:P],
+                phis=ph[:P], xyz=xyz[:P], neighbor_species=ns[:P])
+
+
+def poly3_W(alpha_max):
+    W = np.zeros((alpha_max, alpha_max))
+    lib().orc_poly3_W(int(alpha_max), W)
+    return W
+
+
+def radial(hc: HypersC, s, r, self_pair=False):
+    am = int(hc.keep["alpha_max"][s])
+    R = np.zeros(am)
+    dR = np.zeros(am)
+    lib().orc_radial(hc.ref, int(s), float(r), int(self_pair), R, dR)
+    return R, dR
+
+
+def angular(hc: HypersC, s, r):
+    L = hc.struct.l_max
+    a = np.zeros(L + 1)
+    da = np.zeros(L + 1)
+    lib().orc_angular(hc.ref, int(s), float(r), a, da)
+    return a, da
+
+
+def real_ylm(l_max, u, with_grad=False):
+    L2 = (l_max + 1) ** 2
+    Y = np.zeros(L2)
+    dY = np.zeros((L2, 3)) if with_grad else None
+    lib().orc_real_ylm(int(l_max), _f64(u), Y, dY.ctypes.data if with_grad else None)
+    return (Y, dY) if with_grad else Y
+
+
+def get_soap(hc: HypersC, n_neigh, mask, rjs, xyz, derivatives=True):
+    """soap(n_sites, dim) [row per site], soap_cart_der(P, dim, 3), |p|(n_sites)."""
+    n_sites = len(n_neigh)
+    P = len(rjs)
+    dim = hc.dim
+    soap = np.zeros((n_sites, dim))
+    sdp = np.zeros(n_sites)
+    der = np.zeros((P, dim, 3)) if derivatives else None
+    mask_cm = _i32(np.asarray(mask, dtype=np.int32).T.copy())  # (n_species, P) = Fortran (P, ns)
+    lib().orc_get_soap(hc.ref, n_sites, _i32(n_neigh), P, mask_cm, _f64(rjs), _f64(xyz), soap,
+                       der.ctypes.data if derivatives else None, sdp.ctypes.data)
+    return soap, der, sdp
+
+
+def soap_energy_and_forces(soap, soap_der, Qs, alphas, delta, zeta, e0, n_neigh,
+                           neighbors_list, xyz, n_sites0, do_forces=True):
+    """gap.f90:66-259. soap (n_sites, D), Qs (M, D), soap_der (P, D, 3)."""
+    n_sites, D = soap.shape
+    M = Qs.shape[0]
+    en = np.zeros(n_sites)
+    f = np.zeros((n_sites0, 3))
+    vir = np.zeros(9)
+    sd = _f64(soap_der) if do_forces else None
+    lib().orc_soap_energy_and_forces(D, n_sites, _f64(soap), sd.ctypes.data if do_forces else None,
+                                     M, _f64(Qs), _f64(alphas), float(delta), float(zeta),
+                                     float(e0), _i32(n_neigh), _i32(neighbors_list), _f64(xyz),
+                                     int(n_sites0), int(do_forces), en, f, vir)
+    return en, f, vir.reshape(3, 3).T
+
+
+def get_gap_soap(hc: HypersC, n_total_sites, n_neigh0, neighbors_list0, rjs0, xyz0,
+                 species_batch, species_all, Qs, alphas, delta, zeta, do_forces=True):
+    """gap_interface.f90:41-480; energies0/forces0 assigned for touched sites."""
+    e = np.zeros(n_total_sites)
+    f = np.zeros((n_total_sites, 3))
+    vir = np.zeros(9)
+    lib().orc_get_gap_soap(hc.ref, int(n_total_sites), len(n_neigh0), _i32(n_neigh0),
+                           _i32(neighbors_list0), _f64(rjs0), _f64(xyz0), _i32(species_batch),
+                           _i32(species_all), Qs.shape[0], _f64(Qs), _f64(alphas), float(delta),
+                           float(zeta), int(do_forces), e, f, vir)
+    return e, f, vir.reshape(3, 3).T
+
+
+def atom_pair_batches(n_neigh, rjs, rcut, l_max, n_max, n_soap, n_species, max_gbytes):
+    n = len(n_neigh)
+    ib, ie, jb, je = (np.zeros(max(n, 1), np.int32) for _ in range(4))
+    k = lib().orc_atom_pair_batches(n, _i32(n_neigh), _f64(rjs), float(rcut), int(l_max),
+                                    int(n_max), int(n_soap), int(n_species), float(max_gbytes),
+                                    ib, ie, jb, je)
+    return ib[:k], ie[:k], jb[:k], je[:k]
+
+
+def velocity_verlet(positions, positions_prev, velocities, forces, forces_prev, masses, dt,
+                    dt_prev, first_step):
+    """md.f90:226-283, in place on the (n,3) arrays; returns new dt_prev."""
+    dtp = np.array([dt_prev], dtype=np.float64)
+    lib().orc_velocity_verlet(len(masses), positions, positions_prev, velocities, _f64(forces),
+                              forces_prev, _f64(masses), float(dt), dtp, int(first_step))
+    return float(dtp[0])
+
+
+def remove_cm_vel(vel, masses):
+    lib().orc_remove_cm_vel(len(masses), vel, _f64(masses))
+
+
+def wrap_pbc(positions, a, b, c):
+    lib().orc_wrap_pbc(positions.shape[0], positions, _f64(a), _f64(b), _f64(c))
+
+
+def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max_gbytes=1.0):
+    """Energies (n), forces (n,3), virial (3,3) of one periodic structure.
+
+    ``blocks``: sequence of objects with ``hypers`` (attributes as HypersC),
+    ``Qs`` (M, D), ``alphas`` (M), ``delta``, ``zeta``."""
+    n = positions.shape[0]
+    box = _f64(box)
+    keep = []
+    arr = (_Block * len(blocks))()
+    for i, b in enumerate(blocks):
+        hc = HypersC(b.hypers)
+        Qs = _f64(b.Qs)
+        al = _f64(b.alphas)
+        keep += [hc, Qs, al]
+        arr[i].hypers = hc.struct
+        arr[i].n_sparse = Qs.shape[0]
+        arr[i].Qs = Qs.ctypes.data_as(C.POINTER(C.c_double))
+        arr[i].alphas = al.ctypes.data_as(C.POINTER(C.c_double))
+        arr[i].delta = float(b.delta)
+        arr[i].zeta = float(b.zeta)
+    e0a = _f64(e0) if e0 is not None else None
+    en = np.zeros(n)
+    f = np.zeros((n, 3))
+    vir = np.zeros(9)
+    npairs = C.c_int64(0)
+    rc = lib().orc_evaluate(n, _f64(positions), _i32(species), _f64(box[0]), _f64(box[1]),
+                            _f64(box[2]), len(blocks), arr,
+                            e0a.ctypes.data if e0a is not None else None,
+                            len(e0a) if e0a is not None else 0, float(neighbors_buffer),
+                            float(max_gbytes), en, f, vir, C.byref(npairs))
+    if rc != 0:
+        raise RuntimeError(f"oracle evaluate failed: {rc}")
+    return en, f, vir.reshape(3, 3).T, int(npairs.value)

@@ -1,0 +1,265 @@
+"""Host-side mirror of TurboGAP's backend seam, running on the CUDA backend.
+
+The procedure names and argument meanings follow the reference modules this
+backend replaces (procedure -> reference):
+
+  gpu_context_init / gpu_context_finalize   src/gpu_context.f90:41-58
+  gpu_memory_budget_init                    src/gpu_context.f90:100-162
+  soap_backend_begin / soap_backend_end     src/gap.f90:49-64
+  get_gap_soap                              src/gap_interface.f90:41-480
+  get_soap                                  soap_turbo get_soap, called at gap_interface.f90:320-325
+  build_neighbors_list                      src/neighbors.f90:243-605
+  velocity_verlet                           src/md.f90:226-283
+  Engine (device-resident MD step)          turbogap.f90:664-2196 + turbogap_md.f90:161-297
+
+Arrays use the reference's shapes with numpy row-major equivalents: Fortran
+(3, n) is numpy (n, 3); Fortran (dim, n) is numpy (n, dim); neighbour indices
+are 1-based supercell indices. Errors raise BackendError (the reference stops
+or calls turbogap_abort).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import TG_PREC_BF16, TG_PREC_BF16X3, BackendError, check, lib  # noqa: F401
+from .hypers import GapBlock, SoapTurboHypers
+
+
+def _f64(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _i32(x):
+    return np.ascontiguousarray(x, dtype=np.int32)
+
+
+# --------------------------------------------------------------------- context
+def gpu_context_init(rank: int = 0, device: int = 0) -> int:
+    """Bind this process to ``device``; returns n_omp (1, as on the CPU path)."""
+    n = C.c_int32(0)
+    check(lib().tg_context_init(int(rank), int(device), C.byref(n)))
+    return int(n.value)
+
+
+def gpu_context_finalize() -> None:
+    check(lib().tg_context_finalize())
+
+
+def gpu_memory_budget_init() -> float:
+    """max_Gbytes_per_process for the SOAP batch planner."""
+    g = C.c_double(0.0)
+    check(lib().tg_memory_budget(C.byref(g)))
+    return float(g.value)
+
+
+# --------------------------------------------------------------------- blocks
+class _HypersC:
+    def __init__(self, h: SoapTurboHypers):
+        self.keep = []
+        s = _lib.TgSoapHypers()
+        s.n_species = h.n_species
+        s.l_max = h.l_max
+        s.radial_enhancement = h.radial_enhancement
+        s.central_species = h.central_species
+
+        def iarr(v):
+            a = _i32(v)
+            self.keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+        def darr(v):
+            a = _f64(v)
+            self.keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+
+        s.alpha_max = iarr(h.alpha_max)
+        s.species_z = iarr(h.species_z)
+        s.rcut_hard = darr(h.rcut_hard)
+        s.rcut_soft = darr(h.rcut_soft)
+        s.nf = darr(h.nf)
+        s.global_scaling = darr(h.global_scaling)
+        s.atom_sigma_r = darr(h.atom_sigma_r)
+        s.atom_sigma_r_scaling = darr(h.atom_sigma_r_scaling)
+        s.atom_sigma_t = darr(h.atom_sigma_t)
+        s.atom_sigma_t_scaling = darr(h.atom_sigma_t_scaling)
+        s.amplitude_scaling = darr(h.amplitude_scaling)
+        s.central_weight = darr(h.central_weight)
+        self.struct = s
+
+
+def soap_backend_begin(block: GapBlock, key: int, precision: int = TG_PREC_BF16X3) -> None:
+    """Make ``block`` current; its sparse set is uploaded once per ``key``."""
+    hc = _HypersC(block.hypers)
+    # Qs(dim, n_sparse) column-major == numpy (n_sparse, dim) row-major
+    check(lib().tg_soap_begin(int(key), C.byref(hc.struct), block.n_sparse, _f64(block.Qs),
+                              _f64(block.alphas), float(block.delta), float(block.zeta),
+                              int(precision)))
+
+
+def soap_backend_end() -> None:
+    check(lib().tg_soap_end())
+
+
+def get_gap_soap(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_batch,
+                 species_all, energies0: Optional[np.ndarray] = None,
+                 forces0: Optional[np.ndarray] = None):
+    """Energies, forces and virial of the current block for one batch.
+
+    ``energies0`` (n_total_sites) and ``forces0`` (n_total_sites, 3) are assigned
+    for the sites the block touches and left unchanged elsewhere, as in the
+    reference; fresh zero arrays are used when not given. Returns
+    (energies0, forces0, virial(3,3))."""
+    if energies0 is None:
+        energies0 = np.zeros(n_total_sites)
+    if forces0 is None:
+        forces0 = np.zeros((n_total_sites, 3))
+    assert energies0.dtype == np.float64 and energies0.flags.c_contiguous
+    assert forces0.dtype == np.float64 and forces0.flags.c_contiguous
+    vir = np.zeros(9)
+    nn = _i32(n_neigh0)
+    check(lib().tg_get_gap_soap(int(n_total_sites), len(nn), nn, _i32(neighbors_list0),
+                                _f64(rjs0), _f64(xyz0), _i32(species_batch), _i32(species_all),
+                                energies0, forces0, vir))
+    return energies0, forces0, vir.reshape(3, 3).T.copy()
+
+
+def get_soap(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_batch,
+             species_all, dim: int):
+    """Descriptors (n_central, dim) of the current block's central sites."""
+    nn = _i32(n_neigh0)
+    out = np.zeros((len(nn), dim))
+    nc = C.c_int32(0)
+    check(lib().tg_get_soap(int(n_total_sites), len(nn), nn, _i32(neighbors_list0), _f64(rjs0),
+                            _f64(xyz0), _i32(species_batch), _i32(species_all), out,
+                            C.byref(nc)))
+    return out[: nc.value].copy()
+
+
+# --------------------------------------------------------------------- geometry / MD
+def build_neighbors_list(positions_sc, n_sites: int, a, b, c, rcut_max: float, indices,
+                         species_sc, do_list=None, cap: Optional[int] = None):
+    """Full neighbour lists (self first) as build_neighbors_list returns them."""
+    pos = _f64(positions_sc)
+    nsc = pos.shape[0]
+    a, b, c = _f64(a).copy(), _f64(b).copy(), _f64(c).copy()
+    dl = _i32(do_list) if do_list is not None else None
+    cap = int(cap) if cap else n_sites * 48
+    while True:
+        nn = np.zeros(n_sites, np.int32)
+        nl = np.zeros(max(cap, 1), np.int32)
+        rjs = np.zeros(max(cap, 1))
+        th = np.zeros(max(cap, 1))
+        ph = np.zeros(max(cap, 1))
+        xyz = np.zeros((max(cap, 1), 3))
+        ns = np.zeros(max(cap, 1), np.int32)
+        P = C.c_int64(0)
+        rc = lib().tg_build_neighbors_list(nsc, pos, int(n_sites), a, b, c, float(rcut_max),
+                                           _i32(indices), _i32(species_sc),
+                                           dl.ctypes.data if dl is not None else None, cap, nn, nl,
+                                           rjs, th, ph, xyz, ns, C.byref(P))
+        if rc == -3 and P.value > cap:
+            cap = int(P.value)
+            continue
+        check(rc)
+        break
+    P = int(P.value)
+    return dict(n_neigh=nn, neighbors_list=nl[:P], rjs=rjs[:P], thetas=th[:P], phis=ph[:P],
+                xyz=xyz[:P], neighbor_species=ns[:P], a_box=a, b_box=b, c_box=c)
+
+
+def velocity_verlet(positions, positions_prev, velocities, forces, forces_prev, masses, dt,
+                    dt_prev, first_step):
+    """In place on (n,3) float64 arrays; returns the new dt_prev."""
+    dtp = C.c_double(dt_prev)
+    check(lib().tg_velocity_verlet(len(masses), positions, positions_prev, velocities,
+                                   _f64(forces), forces_prev, _f64(masses), float(dt),
+                                   C.byref(dtp), int(first_step)))
+    return float(dtp.value)
+
+
+class Engine:
+    """Device-resident SOAP-GAP evaluator and NVE integrator for one structure.
+
+    All blocks must have been opened with soap_backend_begin under the keys
+    given here. Positions/velocities live on the GPU between calls."""
+
+    def __init__(self, positions, species, masses, box, block_keys: Sequence[int],
+                 e0_by_species=None, neighbors_buffer: float = 0.0):
+        box = _f64(box)
+        self.n = int(np.asarray(positions).shape[0])
+        keys = _i32(block_keys)
+        e0 = _f64(e0_by_species) if e0_by_species is not None else None
+        h = C.c_void_p()
+        check(lib().tg_engine_create(self.n, _f64(positions), _i32(species), _f64(masses),
+                                     _f64(box[0]), _f64(box[1]), _f64(box[2]), len(keys), keys,
+                                     e0.ctypes.data if e0 is not None else None,
+                                     len(e0) if e0 is not None else 0, float(neighbors_buffer),
+                                     C.byref(h)))
+        self._h = h
+        self._keep = e0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tg_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, positions=None, velocities=None):
+        p = _f64(positions) if positions is not None else None
+        v = _f64(velocities) if velocities is not None else None
+        check(lib().tg_engine_set_state(self._h, p.ctypes.data if p is not None else None,
+                                        v.ctypes.data if v is not None else None))
+
+    def compute(self):
+        """(energies (n), forces (n,3), virial (3,3)) at the current positions."""
+        e = np.zeros(self.n)
+        f = np.zeros((self.n, 3))
+        v = np.zeros(9)
+        check(lib().tg_engine_compute(self._h, e.ctypes.data, f.ctypes.data, v.ctypes.data))
+        return e, f, v.reshape(3, 3).T.copy()
+
+    def compute_device(self):
+        check(lib().tg_engine_compute_device(self._h))
+
+    def md(self, n_steps: int, dt: float):
+        """n_steps NVE velocity-Verlet steps; returns (E_pot, E_kin) after them."""
+        ep = C.c_double(0.0)
+        ek = C.c_double(0.0)
+        check(lib().tg_engine_md(self._h, int(n_steps), float(dt), C.byref(ep), C.byref(ek)))
+        return float(ep.value), float(ek.value)
+
+    def get_state(self):
+        p = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        f = np.zeros((self.n, 3))
+        check(lib().tg_engine_get_state(self._h, p.ctypes.data, v.ctypes.data, f.ctypes.data))
+        return p, v, f
+
+    def n_pairs(self) -> int:
+        n = C.c_int64(0)
+        check(lib().tg_engine_n_pairs(self._h, C.byref(n)))
+        return int(n.value)
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().tg_engine_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+
+def gemm_bf16_tn(A_bf16: np.ndarray, B_bf16: np.ndarray) -> np.ndarray:
+    """Test hook: C = A . B^T through the tcgen05 GEMM (uint16 bf16 bit patterns)."""
+    M, K = A_bf16.shape
+    N = B_bf16.shape[0]
+    out = np.zeros((M, N), np.float32)
+    check(lib().tgx_gemm_bf16_tn(M, N, K, np.ascontiguousarray(A_bf16, np.uint16),
+                                 np.ascontiguousarray(B_bf16, np.uint16), out))
+    return out

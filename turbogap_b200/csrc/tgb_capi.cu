@@ -1,0 +1,1124 @@
+// tgb_capi.cu -- context, sparse-set blocks, the get_gap_soap path, the neighbour
+// list entry point and the device-resident MD engine behind include/tgb200.h.
+
+#include "tgb_common.cuh"
+#include "tgb_gemm.cuh"
+#include "tgb_neighbors.cuh"
+#include "tgb_soap.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+namespace tgb {
+
+// ---------------------------------------------------------------- errors
+static thread_local char g_err[2048] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+const char *last_error() { return g_err; }
+
+int init_soap_constants();
+
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    int ensure(size_t m) {
+        if (m <= n && p) return TG_OK;
+        dev_free(p);
+        n = 0;
+        TGB_TRY(dev_alloc(&p, m));
+        n = m;
+        return TG_OK;
+    }
+    void release() {
+        dev_free(p);
+        n = 0;
+    }
+    ~DBuf() { release(); }
+};
+
+static int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// ---------------------------------------------------------------- blocks
+struct Block {
+    int key = 0, precision = TG_PREC_BF16X3;
+    SoapHostHypers hh{};
+    int ns = 0, amax = 0, lmax = 0, ntot = 0, nlm = 0, dim = 0;
+    int M = 0, Mpad = 0, K1 = 0, K2 = 0, nsplit = 3, n_tiles = 0, tw = 0;
+    double delta = 1.0, zeta = 1.0, rcut_max = 0.0;
+    int zeta_int = 0;
+    signed char zmap[kMaxZ];
+    DBuf<float> table, selfR;
+    DBuf<__nv_bfloat16> QsA, QsT;
+    DBuf<double> alpha, kcoef, mu, aoff, g0;
+    TmaMap tmB1{}, tmB2{};
+
+    SoapParams params(int n_atoms) const {
+        SoapParams P{};
+        P.ns = ns; P.amax = amax; P.lmax = lmax; P.ntot = ntot; P.nlm = nlm; P.dim = dim;
+        P.nsplit = nsplit; P.K1 = K1; P.tw = tw; P.n_atoms = n_atoms;
+        std::memcpy(P.zmap, zmap, sizeof(zmap));
+        for (int s = 0; s < ns; ++s) {
+            P.rcut[s] = (float)hh.rcut_hard[s];
+            P.tab_h[s] = (float)(hh.rcut_hard[s] / kTableIntervals);
+            P.tab_inv_h[s] = (float)(kTableIntervals / hh.rcut_hard[s]);
+        }
+        P.table = table.p;
+        P.self_R = selfR.p;
+        P.mu = mu.p;
+        P.g0 = g0.p;
+        return P;
+    }
+};
+
+// Per-block evaluation buffers, sized by the number of central sites.
+struct Workspace {
+    int cap = 0;
+    DBuf<__nv_bfloat16> qsplit, kd;
+    DBuf<float> q, c, g;
+    DBuf<double> pnorm, epart, kdsum, qoff, vpart;
+    TmaMap tmA1{}, tmA2{};
+    int tm_rows = -1;
+    const void *tm_p1 = nullptr, *tm_p2 = nullptr;
+
+    int ensure(const Block &b, int n_sites) {
+        const int n = n_sites > 0 ? n_sites : 1;
+        if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.K2 ||
+            qsplit.n < (size_t)n * b.K1 || c.n < (size_t)n * b.ntot * b.nlm ||
+            epart.n < (size_t)n * b.n_tiles || kdsum.n < (size_t)n * b.n_tiles) {
+            const int nc = n > cap ? n : cap;
+            TGB_TRY(qsplit.ensure((size_t)nc * b.K1));
+            TGB_TRY(kd.ensure((size_t)nc * b.K2));
+            TGB_TRY(q.ensure((size_t)nc * b.dim));
+            TGB_TRY(g.ensure((size_t)nc * b.dim));
+            TGB_TRY(c.ensure((size_t)nc * b.ntot * b.nlm));
+            TGB_TRY(pnorm.ensure(nc));
+            TGB_TRY(epart.ensure((size_t)nc * b.n_tiles));
+            TGB_TRY(kdsum.ensure((size_t)nc * b.n_tiles));
+            TGB_TRY(qoff.ensure(nc));
+            TGB_TRY(vpart.ensure((size_t)9 * ((nc + 3) / 4 + 1)));
+            cap = nc;
+        }
+        if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p) {
+            TGB_TRY(make_tma_bf16(&tmA1, qsplit.p, n, b.K1, b.K1, kGemmBM));
+            TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.K2, b.K2, kGemmBM));
+            tm_rows = n;
+            tm_p1 = qsplit.p;
+            tm_p2 = kd.p;
+        }
+        return TG_OK;
+    }
+};
+
+namespace {
+
+__global__ void k_prep_sparse(const double *__restrict__ Qs, const double *__restrict__ mu, int M,
+                              int Mpad, int dim, int K1, int K2, int nsplit,
+                              __nv_bfloat16 *__restrict__ QsA, __nv_bfloat16 *__restrict__ QsT) {
+    // Operands hold q_s - mu. B-side pattern per segment: [hi | lo | hi] (nsplit 3)
+    // or [hi] (nsplit 1); the A side is [hi | hi | lo], so the three products are
+    // hi.hi + hi.lo + lo.hi.
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nA = (int64_t)Mpad * K1, nT = (int64_t)dim * K2;
+    if (t < nA) {
+        const int s = (int)(t / K1), k = (int)(t % K1);
+        float v = 0.f;
+        int seg = k / dim, d = k % dim;
+        if (s < M && seg < nsplit) {
+            const float x = (float)(Qs[(size_t)s * dim + d] - mu[d]);
+            __nv_bfloat16 hi, lo;
+            bf16_split(x, hi, lo);
+            v = __bfloat162float(seg == 1 ? lo : hi);
+        }
+        QsA[t] = __float2bfloat16_rn(v);
+    } else if (t < nA + nT) {
+        const int64_t u = t - nA;
+        const int d = (int)(u / K2), k = (int)(u % K2);
+        const int seg = k / Mpad, s = k % Mpad;
+        float v = 0.f;
+        if (s < M && seg < nsplit) {
+            const float x = (float)(Qs[(size_t)s * dim + d] - mu[d]);
+            __nv_bfloat16 hi, lo;
+            bf16_split(x, hi, lo);
+            v = __bfloat162float(seg == 1 ? lo : hi);
+        }
+        QsT[u] = __float2bfloat16_rn(v);
+    }
+}
+
+__global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad, double coef,
+                             double *__restrict__ alpha, double *__restrict__ kcoef) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= Mpad) return;
+    const double a = s < M ? al[s] : 0.0;
+    alpha[s] = a;
+    kcoef[s] = coef * a;
+}
+
+}  // namespace
+
+// Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces.
+int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
+                   double *energies, double *virial, unsigned *err, cudaStream_t st) {
+    if (S.n_sites <= 0) return TG_OK;
+    TGB_TRY(w.ensure(b, S.n_sites));
+    const SoapParams P = b.params(n_atoms);
+    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
+    TGB_TRY(launch_soap_expand(P, S, O, st));
+    GemmEpi e1{};
+    e1.mode = EPI_GAP_KERNEL;
+    e1.rows = S.n_sites;
+    e1.cols = b.Mpad;
+    e1.alpha = b.alpha.p;
+    e1.kcoef = b.kcoef.p;
+    e1.zeta_int = b.zeta_int;
+    e1.zeta_f = b.zeta;
+    e1.epart = w.epart.p;
+    e1.kdsum = w.kdsum.p;
+    e1.aoff = b.aoff.p;
+    e1.qoff = w.qoff.p;
+    e1.kd = w.kd.p;
+    e1.K2 = b.K2;
+    e1.Mpad = b.Mpad;
+    e1.nsplit = b.nsplit;
+    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st));
+    GemmEpi e2{};
+    e2.mode = EPI_STORE_F32;
+    e2.rows = S.n_sites;
+    e2.cols = b.dim;
+    e2.out = w.g.p;
+    e2.ldo = b.dim;
+    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
+    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_tiles, b.delta * b.delta};
+    ForceOut FO{forces, energies, w.vpart.p, err};
+    int nblk = 0;
+    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
+    TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
+    return TG_OK;
+}
+
+// ---------------------------------------------------------------- context
+struct Engine;
+
+struct Context {
+    int device = -1;
+    cudaStream_t st = nullptr;
+    std::map<int, std::unique_ptr<Block>> blocks;
+    std::map<int, std::unique_ptr<Workspace>> ws;
+    Block *current = nullptr;
+    DBuf<unsigned> err;
+    // staging of the get_gap_soap path
+    DBuf<int> nn, nl, nbr, spb, spa, flag, site_row, site_atom, seen, cnt;
+    DBuf<int64_t> pstart;
+    DBuf<double> rjs, xyz, en, fo, vir;
+    DBuf<char> scan;
+};
+
+static Context *g_ctx = nullptr;
+
+static int need_ctx() {
+    TGB_CHECK(g_ctx != nullptr, TG_ERR_STATE, "tg_context_init has not been called");
+    return TG_OK;
+}
+
+static int check_err_word(Context &c, unsigned *err_dev) {
+    unsigned e = 0;
+    TGB_CUDA(cudaMemcpyAsync(&e, err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c.st));
+    TGB_CUDA(cudaStreamSynchronize(c.st));
+    if (e) {
+        TGB_CUDA(cudaMemsetAsync(err_dev, 0, sizeof(unsigned), c.st));
+        if (e & (DEV_ERR_TIMEOUT_TMA | DEV_ERR_TIMEOUT_MMA | DEV_ERR_TIMEOUT_EPI)) {
+            set_error("device wait timed out (error word 0x%x)", e);
+            return TG_ERR_TIMEOUT;
+        }
+        set_error("device error word 0x%x%s", e,
+                  (e & DEV_ERR_NEIGH_CAPACITY) ? " (neighbour pair capacity exceeded)" : "");
+        return TG_ERR_DEVICE;
+    }
+    return TG_OK;
+}
+
+}  // namespace tgb
+
+using namespace tgb;
+
+// ============================================================== C-ABI
+extern "C" {
+
+const char *tg_last_error(void) { return tgb::last_error(); }
+
+int tg_context_init(int32_t rank, int32_t device, int32_t *n_omp) {
+    (void)rank;
+    if (n_omp) *n_omp = 1;
+    if (g_ctx) return TG_OK;
+    int ndev = 0;
+    TGB_CUDA(cudaGetDeviceCount(&ndev));
+    TGB_CHECK(device >= 0 && device < ndev, TG_ERR_ARG, "device %d not present (%d devices)", device,
+              ndev);
+    TGB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    TGB_CUDA(cudaGetDeviceProperties(&prop, device));
+    TGB_CHECK(prop.major == 10 && prop.minor == 0, TG_ERR_ARG,
+              "this backend is built for sm_100a (B200); device %d is sm_%d%d", device, prop.major,
+              prop.minor);
+    auto *c = new Context();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        set_error("cudaStreamCreate failed");
+        return TG_ERR_CUDA;
+    }
+    int r = init_soap_constants();
+    if (r == TG_OK) r = c->err.ensure(1);
+    if (r == TG_OK && cudaMemset(c->err.p, 0, sizeof(unsigned)) != cudaSuccess) r = TG_ERR_CUDA;
+    if (r != TG_OK) {
+        cudaStreamDestroy(c->st);
+        delete c;
+        return r;
+    }
+    g_ctx = c;
+    return TG_OK;
+}
+
+int tg_context_finalize(void) {
+    if (!g_ctx) return TG_OK;
+    cudaStreamSynchronize(g_ctx->st);
+    cudaStream_t st = g_ctx->st;
+    delete g_ctx;
+    g_ctx = nullptr;
+    cudaStreamDestroy(st);
+    return TG_OK;
+}
+
+int tg_memory_budget(double *max_gbytes) {
+    TGB_TRY(need_ctx());
+    size_t fr = 0, tot = 0;
+    TGB_CUDA(cudaMemGetInfo(&fr, &tot));
+    // Batches are a host-memory device in the reference; on the device the whole
+    // step is resident, so the budget is what is free, less a 10 % reserve.
+    if (max_gbytes) *max_gbytes = 0.9 * (double)fr / (1024.0 * 1024.0 * 1024.0);
+    return TG_OK;
+}
+
+int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, const double *Qs,
+                  const double *alphas, double delta, double zeta, int32_t precision) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    auto it = C.blocks.find(block_key);
+    if (it != C.blocks.end() && it->second->M == n_sparse && it->second->precision == precision) {
+        C.current = it->second.get();
+        return TG_OK;
+    }
+    TGB_CHECK(h && Qs && alphas, TG_ERR_ARG, "null hypers/Qs/alphas");
+    TGB_CHECK(h->n_species >= 1 && h->n_species <= kMaxSpecies, TG_ERR_ARG,
+              "n_species %d outside 1..%d", h->n_species, kMaxSpecies);
+    TGB_CHECK(precision == TG_PREC_BF16X3 || precision == TG_PREC_BF16, TG_ERR_ARG,
+              "precision must be TG_PREC_BF16X3 or TG_PREC_BF16");
+    TGB_CHECK(n_sparse >= 1, TG_ERR_ARG, "n_sparse must be positive");
+    auto b = std::make_unique<Block>();
+    b->key = block_key;
+    b->precision = precision;
+    SoapHostHypers &hh = b->hh;
+    hh.ns = h->n_species;
+    hh.lmax = h->l_max;
+    hh.radial_enhancement = h->radial_enhancement;
+    hh.central_species = h->central_species;
+    TGB_CHECK(hh.radial_enhancement >= 0 && hh.radial_enhancement <= 2, TG_ERR_ARG,
+              "radial_enhancement must be 0..2");
+    TGB_CHECK(hh.central_species >= 0 && hh.central_species <= hh.ns, TG_ERR_ARG,
+              "central_species out of range");
+    for (int s = 0; s < hh.ns; ++s) {
+        hh.alpha_max[s] = h->alpha_max[s];
+        hh.species_z[s] = h->species_z[s];
+        hh.rcut_hard[s] = h->rcut_hard[s];
+        hh.rcut_soft[s] = h->rcut_soft[s];
+        hh.nf[s] = h->nf[s];
+        hh.global_scaling[s] = h->global_scaling[s];
+        hh.sigma_r[s] = h->atom_sigma_r[s];
+        hh.sigma_r_scaling[s] = h->atom_sigma_r_scaling[s];
+        hh.sigma_t[s] = h->atom_sigma_t[s];
+        hh.sigma_t_scaling[s] = h->atom_sigma_t_scaling[s];
+        hh.amplitude_scaling[s] = h->amplitude_scaling[s];
+        hh.central_weight[s] = h->central_weight[s];
+        TGB_CHECK(hh.alpha_max[s] == hh.alpha_max[0], TG_ERR_ARG,
+                  "the device path needs the same alpha_max for every species");
+        TGB_CHECK(hh.species_z[s] >= 1 && hh.species_z[s] < kMaxZ, TG_ERR_ARG,
+                  "species id %d outside 1..%d", hh.species_z[s], kMaxZ - 1);
+        TGB_CHECK(hh.rcut_hard[s] > 0.0 && hh.sigma_r[s] > 0.0 && hh.sigma_t[s] > 0.0, TG_ERR_ARG,
+                  "rcut and atom sigmas must be positive");
+        for (int s2 = 0; s2 < s; ++s2)
+            TGB_CHECK(hh.species_z[s2] != hh.species_z[s], TG_ERR_ARG,
+                      "repeated species in one block (multiplicity > 1) is not supported on the device");
+    }
+    b->ns = hh.ns;
+    b->amax = hh.alpha_max[0];
+    b->lmax = hh.lmax;
+    TGB_CHECK(soap_shape_supported(b->ns, b->amax, b->lmax), TG_ERR_ARG,
+              "unsupported SOAP shape: n_species %d alpha_max %d l_max %d", b->ns, b->amax, b->lmax);
+    b->ntot = b->ns * b->amax;
+    b->nlm = (b->lmax + 1) * (b->lmax + 1);
+    b->dim = b->ntot * (b->ntot + 1) / 2 * (b->lmax + 1);
+    b->nsplit = precision == TG_PREC_BF16X3 ? 3 : 1;
+    b->M = n_sparse;
+    b->Mpad = round_up(n_sparse, 64);
+    b->K1 = round_up(b->nsplit * b->dim, kGemmBK);
+    b->K2 = b->nsplit * b->Mpad;
+    b->n_tiles = gemm_n_tiles(b->Mpad);
+    b->tw = ((3 * b->amax + 3 * (b->lmax + 1)) + 3) / 4 * 4;
+    b->delta = delta;
+    b->rcut_max = 0.0;
+    for (int s = 0; s < hh.ns; ++s) b->rcut_max = std::max(b->rcut_max, hh.rcut_hard[s]);
+    // gap.f90:115-121: zeta within 1e-5 of an integer is snapped to it
+    if (std::fabs(zeta - (double)(int)zeta) < 1.e-5 && (int)zeta >= 1) {
+        b->zeta_int = (int)zeta;
+        b->zeta = (double)b->zeta_int;
+    } else {
+        b->zeta_int = 0;
+        b->zeta = zeta;
+    }
+    for (int z = 0; z < kMaxZ; ++z) b->zmap[z] = -1;
+    for (int s = hh.ns - 1; s >= 0; --s) b->zmap[hh.species_z[s]] = (signed char)s;
+    TGB_TRY(b->table.ensure((size_t)hh.ns * (kTableIntervals + 1) * b->tw));
+    TGB_TRY(b->selfR.ensure((size_t)hh.ns * b->amax));
+    TGB_TRY(b->QsA.ensure((size_t)b->Mpad * b->K1));
+    TGB_TRY(b->QsT.ensure((size_t)b->dim * b->K2));
+    TGB_TRY(b->alpha.ensure(b->Mpad));
+    TGB_TRY(b->kcoef.ensure(b->Mpad));
+    TGB_TRY(b->mu.ensure(b->dim));
+    TGB_TRY(b->aoff.ensure(b->Mpad));
+    TGB_TRY(b->g0.ensure(b->dim));
+    // Centre of the sparse set (FP64): the GEMMs run on q - mu and q_s - mu, the
+    // exact rank-1 terms mu.q_s and (q - mu).mu are added in the epilogue.
+    {
+        std::vector<double> mu(b->dim, 0.0), aoff(b->Mpad, 0.0);
+        for (int s = 0; s < n_sparse; ++s)
+            for (int d = 0; d < b->dim; ++d) mu[d] += Qs[(size_t)s * b->dim + d];
+        for (int d = 0; d < b->dim; ++d) mu[d] /= (double)n_sparse;
+        for (int s = 0; s < n_sparse; ++s) {
+            double a = 0.0;
+            for (int d = 0; d < b->dim; ++d) a += mu[d] * Qs[(size_t)s * b->dim + d];
+            aoff[s] = a;
+        }
+        // g0 = sum_s zeta delta^2 alpha_s (q_s - mu): dE/dq of an atom with K = 1 to
+        // every sparse point; GEMM 2 only carries the deviation from it.
+        std::vector<double> g0(b->dim, 0.0);
+        const double zd2 = b->zeta * delta * delta;
+        for (int s = 0; s < n_sparse; ++s) {
+            const double c = zd2 * alphas[s];
+            for (int d = 0; d < b->dim; ++d) g0[d] += c * (Qs[(size_t)s * b->dim + d] - mu[d]);
+        }
+        TGB_CUDA(cudaMemcpy(b->g0.p, g0.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
+        TGB_CUDA(cudaMemcpy(b->mu.p, mu.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
+        TGB_CUDA(cudaMemcpy(b->aoff.p, aoff.data(), sizeof(double) * b->Mpad, cudaMemcpyHostToDevice));
+    }
+    DBuf<double> tq, ta;
+    TGB_TRY(tq.ensure((size_t)n_sparse * b->dim));
+    TGB_TRY(ta.ensure(n_sparse));
+    TGB_CUDA(cudaMemcpyAsync(tq.p, Qs, sizeof(double) * n_sparse * b->dim, cudaMemcpyHostToDevice, C.st));
+    TGB_CUDA(cudaMemcpyAsync(ta.p, alphas, sizeof(double) * n_sparse, cudaMemcpyHostToDevice, C.st));
+    const int64_t tot = (int64_t)b->Mpad * b->K1 + (int64_t)b->dim * b->K2;
+    k_prep_sparse<<<(unsigned)((tot + 255) / 256), 256, 0, C.st>>>(tq.p, b->mu.p, b->M, b->Mpad,
+                                                                   b->dim, b->K1, b->K2, b->nsplit,
+                                                                   b->QsA.p, b->QsT.p);
+    k_prep_alpha<<<(b->Mpad + 255) / 256, 256, 0, C.st>>>(ta.p, b->M, b->Mpad,
+                                                          b->zeta * delta * delta, b->alpha.p,
+                                                          b->kcoef.p);
+    TGB_CUDA(cudaGetLastError());
+    TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st));
+    TGB_TRY(make_tma_bf16(&b->tmB1, b->QsA.p, b->Mpad, b->K1, b->K1, kGemmBN));
+    TGB_TRY(make_tma_bf16(&b->tmB2, b->QsT.p, b->dim, b->K2, b->K2, kGemmBN));
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    C.current = b.get();
+    C.blocks[block_key] = std::move(b);
+    return TG_OK;
+}
+
+int tg_soap_end(void) {
+    TGB_TRY(need_ctx());
+    g_ctx->current = nullptr;
+    return TG_OK;
+}
+
+}  // extern "C"
+
+namespace tgb {
+namespace {
+
+__global__ void k_central_flags(int n, const int *__restrict__ spb, const signed char *zfirst,
+                                int cs, int *__restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int z = spb[i];
+    int first = (z >= 0 && z < kMaxZ) ? zfirst[z] + 1 : 0;   // 1-based, 0 if absent
+    flag[i] = (cs == 0 || first == cs) ? 1 : 0;
+}
+
+__global__ void k_sites(int n, const int *__restrict__ flag, const int *__restrict__ incl,
+                        const int64_t *__restrict__ pstart, const int *__restrict__ nl1,
+                        int n_total, int *__restrict__ site_row, int *__restrict__ site_atom) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i]) return;
+    const int idx = incl[i] - 1;
+    site_row[idx] = i;
+    site_atom[idx] = (nl1[pstart[i]] - 1) % n_total;
+}
+
+__global__ void k_to0(int64_t P, const int *__restrict__ nl1, int *__restrict__ nbr) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < P) nbr[p] = nl1[p] - 1;
+}
+
+// Atoms a block "sees" (gap_interface.f90:204-232): kept pairs of central sites.
+__global__ void k_seen(int n_sites, const int *__restrict__ site_row, const int64_t *__restrict__ pstart,
+                       const int *__restrict__ nbr, const double *__restrict__ rjs,
+                       const int *__restrict__ spa, const signed char *zfirst, double rcut_max,
+                       int n_total, int *__restrict__ seen) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_sites) return;
+    const int row = site_row[i];
+    for (int64_t p = pstart[row]; p < pstart[row + 1]; ++p) {
+        const int j = nbr[p] % n_total;
+        const int z = spa[j];
+        if (rjs[p] < rcut_max && z >= 0 && z < kMaxZ && zfirst[z] >= 0) seen[j] = 1;
+    }
+}
+
+// q = mu + delta (rows of dim)
+__global__ void k_d2f(int64_t n, int dim, const float *__restrict__ a, const double *__restrict__ mu,
+                      double *__restrict__ b) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = mu[i % dim] + (double)a[i];
+}
+
+__global__ void k_gather_species(int64_t P, const int *__restrict__ nbr, const int *__restrict__ sp,
+                                 int *__restrict__ out) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < P) out[p] = sp[nbr[p]];
+}
+
+__global__ void k_is_self(int n, const int64_t *__restrict__ pstart, int *__restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && pstart[i + 1] > pstart[i]) flag[pstart[i]] = 1;
+}
+
+__global__ void k_add1(int64_t P, int *__restrict__ v) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p < P) v[p] += 1;
+}
+
+// energies(i) = e0(species(i)) (turbogap.f90:1253-1261)
+__global__ void k_energy_e0(int n, const int *__restrict__ sp, const double *__restrict__ e0, int nz,
+                            double *__restrict__ en) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int z = sp[i];
+    en[i] = (z >= 1 && z <= nz) ? e0[z - 1] : 0.0;
+}
+
+}  // namespace
+
+static unsigned grid_for(int64_t n, int tb = 256) { return (unsigned)((n + tb - 1) / tb); }
+
+// Shared front half of tg_get_gap_soap / tg_get_soap: uploads the batch and
+// builds the central-site list (gap_interface.f90:178-309 semantics).
+static int stage_batch(Context &C, Block &b, int n_total, int n_sites0, const int32_t *n_neigh0,
+                       const int32_t *nl0, const double *rjs0, const double *xyz0,
+                       const int32_t *spb, const int32_t *spa, int64_t *P_out, int *n_central,
+                       DBuf<signed char> &zf) {
+    int64_t P = 0;
+    for (int i = 0; i < n_sites0; ++i) {
+        TGB_CHECK(n_neigh0[i] >= 1, TG_ERR_ARG, "site %d has no self pair (n_neigh0 = %d)", i,
+                  n_neigh0[i]);
+        P += n_neigh0[i];
+    }
+    for (int64_t p = 0; p < P; ++p)
+        TGB_CHECK(nl0[p] >= 1, TG_ERR_ARG, "neighbors_list0(%lld) = %d is not a 1-based index",
+                  (long long)(p + 1), nl0[p]);
+    *P_out = P;
+    cudaStream_t st = C.st;
+    TGB_TRY(C.nn.ensure(n_sites0));
+    TGB_TRY(C.pstart.ensure((size_t)n_sites0 + 1));
+    TGB_TRY(C.nl.ensure(P));
+    TGB_TRY(C.nbr.ensure(P));
+    TGB_TRY(C.rjs.ensure(P));
+    TGB_TRY(C.xyz.ensure(3 * P));
+    TGB_TRY(C.spb.ensure(n_sites0));
+    TGB_TRY(C.spa.ensure(n_total));
+    TGB_TRY(C.flag.ensure(n_sites0));
+    TGB_TRY(C.cnt.ensure((size_t)n_sites0 + 1));
+    TGB_TRY(C.site_row.ensure(n_sites0));
+    TGB_TRY(C.site_atom.ensure(n_sites0));
+    TGB_CUDA(cudaMemcpyAsync(C.nn.p, n_neigh0, sizeof(int) * n_sites0, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(C.nl.p, nl0, sizeof(int) * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(C.rjs.p, rjs0, sizeof(double) * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(C.xyz.p, xyz0, sizeof(double) * 3 * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(C.spb.p, spb, sizeof(int) * n_sites0, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(C.spa.p, spa, sizeof(int) * n_total, cudaMemcpyHostToDevice, st));
+    signed char zfirst[kMaxZ];
+    for (int z = 0; z < kMaxZ; ++z) zfirst[z] = b.zmap[z];
+    TGB_TRY(zf.ensure(kMaxZ));
+    TGB_CUDA(cudaMemcpyAsync(zf.p, zfirst, kMaxZ, cudaMemcpyHostToDevice, st));
+    size_t need = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, need, C.nn.p, C.pstart.p + 1, n_sites0);
+    size_t need2 = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, need2, C.flag.p, C.cnt.p, n_sites0);
+    TGB_TRY(C.scan.ensure(std::max(need, need2)));
+    TGB_CUDA(cudaMemsetAsync(C.pstart.p, 0, sizeof(int64_t), st));
+    size_t bytes = C.scan.n;
+    TGB_CUDA(cub::DeviceScan::InclusiveSum(C.scan.p, bytes, C.nn.p, C.pstart.p + 1, n_sites0, st));
+    k_central_flags<<<grid_for(n_sites0), 256, 0, st>>>(n_sites0, C.spb.p, zf.p, b.hh.central_species,
+                                                        C.flag.p);
+    bytes = C.scan.n;
+    TGB_CUDA(cub::DeviceScan::InclusiveSum(C.scan.p, bytes, C.flag.p, C.cnt.p, n_sites0, st));
+    k_sites<<<grid_for(n_sites0), 256, 0, st>>>(n_sites0, C.flag.p, C.cnt.p, C.pstart.p, C.nl.p,
+                                                n_total, C.site_row.p, C.site_atom.p);
+    k_to0<<<grid_for(P), 256, 0, st>>>(P, C.nl.p, C.nbr.p);
+    TGB_CUDA(cudaGetLastError());
+    int nc = 0;
+    TGB_CUDA(cudaMemcpyAsync(&nc, C.cnt.p + (n_sites0 - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    *n_central = nc;
+    return TG_OK;
+}
+
+}  // namespace tgb
+
+extern "C" {
+
+int tg_get_gap_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                    const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                    const int32_t *species_batch, const int32_t *species_all, double *energies0,
+                    double *forces0, double *virial) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
+    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0, TG_ERR_ARG, "bad site counts");
+    if (virial)
+        for (int q = 0; q < 9; ++q) virial[q] = 0.0;
+    if (n_sites0 == 0) return TG_OK;
+    Block &b = *C.current;
+    DBuf<signed char> zf;
+    int64_t P = 0;
+    int nc = 0;
+    TGB_TRY(stage_batch(C, b, n_total_sites, n_sites0, n_neigh0, neighbors_list0, rjs0, xyz0,
+                        species_batch, species_all, &P, &nc, zf));
+    cudaStream_t st = C.st;
+    TGB_TRY(C.en.ensure(n_total_sites));
+    TGB_TRY(C.fo.ensure(3 * (size_t)n_total_sites));
+    TGB_TRY(C.vir.ensure(9));
+    TGB_TRY(C.seen.ensure(n_total_sites));
+    TGB_CUDA(cudaMemsetAsync(C.en.p, 0, sizeof(double) * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(C.fo.p, 0, sizeof(double) * 3 * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(C.vir.p, 0, sizeof(double) * 9, st));
+    TGB_CUDA(cudaMemsetAsync(C.seen.p, 0, sizeof(int) * n_total_sites, st));
+    auto &wp = C.ws[b.key];
+    if (!wp) wp = std::make_unique<Workspace>();
+    SiteArgs S{nc, C.site_row.p, C.site_atom.p, C.pstart.p, C.nbr.p, C.xyz.p, C.spa.p};
+    TGB_TRY(evaluate_block(b, *wp, S, n_total_sites, C.fo.p, C.en.p, C.vir.p, C.err.p, st));
+    k_seen<<<grid_for(nc), 256, 0, st>>>(nc, C.site_row.p, C.pstart.p, C.nbr.p, C.rjs.p, C.spa.p,
+                                          zf.p, b.rcut_max, n_total_sites, C.seen.p);
+    TGB_CUDA(cudaGetLastError());
+    TGB_TRY(check_err_word(C, C.err.p));
+    std::vector<double> en(n_total_sites), fo(3 * (size_t)n_total_sites), vr(9);
+    std::vector<int> seen(n_total_sites), rows(nc), atoms(nc);
+    TGB_CUDA(cudaMemcpyAsync(en.data(), C.en.p, sizeof(double) * n_total_sites, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(fo.data(), C.fo.p, sizeof(double) * 3 * n_total_sites, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(vr.data(), C.vir.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(seen.data(), C.seen.p, sizeof(int) * n_total_sites, cudaMemcpyDeviceToHost, st));
+    if (nc > 0)
+        TGB_CUDA(cudaMemcpyAsync(atoms.data(), C.site_atom.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    // gap_interface.f90:422-431: assignment to the sites this block touched
+    if (energies0)
+        for (int i = 0; i < nc; ++i) energies0[atoms[i]] = en[atoms[i]];
+    if (forces0)
+        for (int j = 0; j < n_total_sites; ++j)
+            if (seen[j])
+                for (int q = 0; q < 3; ++q) forces0[3 * (size_t)j + q] = fo[3 * (size_t)j + q];
+    if (virial)
+        for (int q = 0; q < 9; ++q) virial[q] = vr[q];
+    return TG_OK;
+}
+
+int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                const int32_t *species_batch, const int32_t *species_all, double *soap,
+                int32_t *n_central) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
+    if (n_central) *n_central = 0;
+    if (n_sites0 == 0) return TG_OK;
+    Block &b = *C.current;
+    DBuf<signed char> zf;
+    int64_t P = 0;
+    int nc = 0;
+    TGB_TRY(stage_batch(C, b, n_total_sites, n_sites0, n_neigh0, neighbors_list0, rjs0, xyz0,
+                        species_batch, species_all, &P, &nc, zf));
+    if (n_central) *n_central = nc;
+    if (nc == 0) return TG_OK;
+    auto &wp = C.ws[b.key];
+    if (!wp) wp = std::make_unique<Workspace>();
+    TGB_TRY(wp->ensure(b, nc));
+    SiteArgs S{nc, C.site_row.p, C.site_atom.p, C.pstart.p, C.nbr.p, C.xyz.p, C.spa.p};
+    const SoapParams Pm = b.params(n_total_sites);
+    DescOut O{wp->qsplit.p, wp->q.p, wp->qoff.p, wp->pnorm.p, wp->c.p};
+    TGB_TRY(launch_soap_expand(Pm, S, O, C.st));
+    DBuf<double> out;
+    TGB_TRY(out.ensure((size_t)nc * b.dim));
+    k_d2f<<<grid_for((int64_t)nc * b.dim), 256, 0, C.st>>>((int64_t)nc * b.dim, b.dim, wp->q.p,
+                                                            b.mu.p, out.p);
+    TGB_CUDA(cudaGetLastError());
+    TGB_CUDA(cudaMemcpyAsync(soap, out.p, sizeof(double) * nc * b.dim, cudaMemcpyDeviceToHost, C.st));
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    return TG_OK;
+}
+
+int tg_build_neighbors_list(int32_t n_sites_supercell, const double *positions, int32_t n_sites,
+                            double *a_box, double *b_box, double *c_box, double rcut_max,
+                            const int32_t *indices, const int32_t *species_supercell,
+                            const int32_t *do_list, int64_t cap, int32_t *n_neigh,
+                            int32_t *neighbors_list, double *rjs, double *thetas, double *phis,
+                            double *xyz, int32_t *neighbor_species, int64_t *n_pairs) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(n_sites >= 1 && n_sites_supercell >= n_sites, TG_ERR_ARG, "bad site counts");
+    Box bx = make_box(a_box, b_box, c_box);
+    if (bx.ortho) {   // neighbors.f90:372-384: snap the off-diagonal noise to zero
+        a_box[1] = a_box[2] = b_box[0] = b_box[2] = c_box[0] = c_box[1] = 0.0;
+        bx = make_box(a_box, b_box, c_box);
+    }
+    bool use_cells = false;
+    const CellGrid g = plan_cells(bx, rcut_max, indices, &use_cells);
+    cudaStream_t st = C.st;
+    NeighborList nl;
+    DBuf<double> pos;
+    DBuf<int> dl, sp, nsp, selff;
+    TGB_TRY(pos.ensure(3 * (size_t)n_sites_supercell));
+    TGB_TRY(dl.ensure(n_sites));
+    TGB_TRY(sp.ensure(n_sites_supercell));
+    TGB_CUDA(cudaMemcpyAsync(pos.p, positions, sizeof(double) * 3 * n_sites_supercell, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(sp.p, species_supercell, sizeof(int) * n_sites_supercell, cudaMemcpyHostToDevice, st));
+    if (do_list) TGB_CUDA(cudaMemcpyAsync(dl.p, do_list, sizeof(int) * n_sites, cudaMemcpyHostToDevice, st));
+    int64_t pcap = std::max<int64_t>(cap, 1);
+    int rc = nl.reserve(n_sites, n_sites_supercell, pcap, g);
+    if (rc == TG_OK && cudaMemsetAsync(nl.err, 0, sizeof(unsigned), st) != cudaSuccess) rc = TG_ERR_CUDA;
+    if (rc == TG_OK)
+        rc = nl_build(nl, n_sites, n_sites_supercell, pos.p, bx, g, use_cells, rcut_max,
+                      do_list ? dl.p : nullptr, st);
+    int64_t P = 0;
+    if (rc == TG_OK) {
+        if (cudaMemcpyAsync(&P, nl.pstart + n_sites, sizeof(int64_t), cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            rc = TG_ERR_CUDA;
+    }
+    if (rc == TG_OK) {
+        if (n_pairs) *n_pairs = P;
+        if (P > cap) {
+            set_error("neighbour arrays hold %lld pairs, %lld needed", (long long)cap, (long long)P);
+            rc = TG_ERR_CAPACITY;
+        }
+    }
+    if (rc == TG_OK) {
+        rc = selff.ensure(P);
+        if (rc == TG_OK) rc = nsp.ensure(P);
+        DBuf<double> th, ph;
+        if (rc == TG_OK) rc = th.ensure(P);
+        if (rc == TG_OK) rc = ph.ensure(P);
+        if (rc == TG_OK && P > 0) {
+            cudaMemsetAsync(selff.p, 0, sizeof(int) * P, st);
+            k_is_self<<<grid_for(n_sites), 256, 0, st>>>(n_sites, nl.pstart, selff.p);
+            rc = launch_angles(P, nl.rjs, nl.xyz, selff.p, th.p, ph.p, st);
+            k_gather_species<<<grid_for(P), 256, 0, st>>>(P, nl.nbr, sp.p, nsp.p);
+            k_add1<<<grid_for(P), 256, 0, st>>>(P, nl.nbr);
+            if (cudaGetLastError() != cudaSuccess) rc = TG_ERR_CUDA;
+            if (rc == TG_OK) {
+                cudaMemcpyAsync(n_neigh, nl.n_neigh, sizeof(int) * n_sites, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(neighbors_list, nl.nbr, sizeof(int) * P, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(rjs, nl.rjs, sizeof(double) * P, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(xyz, nl.xyz, sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(thetas, th.p, sizeof(double) * P, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(phis, ph.p, sizeof(double) * P, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(neighbor_species, nsp.p, sizeof(int) * P, cudaMemcpyDeviceToHost, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) {
+                    set_error("copy-back of the neighbour list failed");
+                    rc = TG_ERR_CUDA;
+                }
+            }
+        } else if (rc == TG_OK) {
+            cudaMemcpyAsync(n_neigh, nl.n_neigh, sizeof(int) * n_sites, cudaMemcpyDeviceToHost, st);
+            cudaStreamSynchronize(st);
+        }
+    }
+    if (rc == TG_OK) rc = check_err_word(C, nl.err);
+    nl.release();
+    return rc;
+}
+
+int tg_velocity_verlet(int32_t n, double *positions, double *positions_prev, double *velocities,
+                       const double *forces, double *forces_prev, const double *masses, double dt,
+                       double *dt_prev, int32_t first_step) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    cudaStream_t st = C.st;
+    DBuf<double> p, pp, v, f, fp, m;
+    const size_t b3 = sizeof(double) * 3 * n;
+    TGB_TRY(p.ensure(3 * n)); TGB_TRY(pp.ensure(3 * n)); TGB_TRY(v.ensure(3 * n));
+    TGB_TRY(f.ensure(3 * n)); TGB_TRY(fp.ensure(3 * n)); TGB_TRY(m.ensure(n));
+    TGB_CUDA(cudaMemcpyAsync(p.p, positions, b3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(v.p, velocities, b3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(f.p, forces, b3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(fp.p, forces_prev, b3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(m.p, masses, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    TGB_TRY(launch_velocity_verlet(n, p.p, pp.p, v.p, f.p, fp.p, m.p, dt, dt_prev ? *dt_prev : dt,
+                                   first_step, st));
+    TGB_CUDA(cudaMemcpyAsync(positions, p.p, b3, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(positions_prev, pp.p, b3, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(velocities, v.p, b3, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(forces_prev, fp.p, b3, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    if (dt_prev) *dt_prev = dt;
+    return TG_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== engine
+namespace tgb {
+
+struct BlockRun {
+    Block *b = nullptr;
+    std::unique_ptr<Workspace> w;
+    DBuf<int> sites;
+    int n_sites = 0;
+};
+
+struct Engine {
+    int n = 0, nsc = 0, indices[3] = {1, 1, 1};
+    bool use_cells = false;
+    CellGrid g{1, 1, 1};
+    Box box{}, box_prim{};
+    double rcut = 0.0;
+    int nz = 0;
+    DBuf<double> pos, pos_sc, pos_prev, vel, f, f_prev, mass, en, vir, e0, acc4, ekin, abc;
+    DBuf<int> species;
+    DBuf<unsigned> err;
+    NeighborList nl;
+    std::vector<std::unique_ptr<BlockRun>> runs;
+    cudaGraphExec_t graph = nullptr;
+    double graph_dt = 0.0;
+    bool first_step = true;
+    double dt_prev = 0.0;
+    cudaStream_t st = nullptr;
+
+    ~Engine() {
+        if (graph) cudaGraphExecDestroy(graph);
+        nl.release();
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int compute_ef() {
+        const double *p = pos.p;
+        if (nsc > n) {
+            TGB_TRY(launch_supercell(n, pos.p, abc.p, indices, pos_sc.p, st));
+            p = pos_sc.p;
+        }
+        TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
+        TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
+        TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
+        for (auto &r : runs) {
+            SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
+        }
+        return TG_OK;
+    }
+
+    int md_step(double dt, bool first) {
+        TGB_TRY(compute_ef());
+        TGB_TRY(launch_wrap(n, pos.p, box_prim, st));
+        TGB_TRY(launch_remove_cm(n, vel.p, mass.p, acc4.p, st));
+        TGB_TRY(launch_velocity_verlet(n, pos.p, pos_prev.p, vel.p, f.p, f_prev.p, mass.p, dt,
+                                       first ? dt : dt_prev, first ? 1 : 0, st));
+        return TG_OK;
+    }
+};
+
+}  // namespace tgb
+
+struct tg_engine {
+    tgb::Engine e;
+};
+
+extern "C" {
+
+int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *species,
+                     const double *masses, const double *a_box, const double *b_box,
+                     const double *c_box, int32_t n_blocks, const int32_t *block_keys,
+                     const double *e0_by_species, int32_t n_species_total, double neighbors_buffer,
+                     tg_engine **out) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(out && n_atoms >= 1 && n_blocks >= 1, TG_ERR_ARG, "bad engine arguments");
+    Context &C = *g_ctx;
+    auto holder = std::make_unique<tg_engine>();
+    Engine &E = holder->e;
+    E.n = n_atoms;
+    TGB_CUDA(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    double rcut = 0.0;
+    for (int k = 0; k < n_blocks; ++k) {
+        auto it = C.blocks.find(block_keys[k]);
+        TGB_CHECK(it != C.blocks.end(), TG_ERR_STATE, "block key %d was never begun", block_keys[k]);
+        rcut = std::max(rcut, it->second->rcut_max);
+    }
+    rcut += neighbors_buffer;   // turbogap_setup.f90:284-285
+    E.rcut = rcut;
+    // read_files.f90:320-380: supercell when the box cannot hold a cutoff sphere
+    host_unit_cells(a_box, b_box, c_box, rcut, E.indices);
+    E.box_prim = make_box(a_box, b_box, c_box);
+    TGB_CHECK(E.box_prim.ortho, TG_ERR_ARG, "the device engine supports orthorhombic boxes");
+    double A[3], B[3], Cc[3];
+    for (int q = 0; q < 3; ++q) {
+        A[q] = a_box[q] * E.indices[0];
+        B[q] = b_box[q] * E.indices[1];
+        Cc[q] = c_box[q] * E.indices[2];
+    }
+    E.box = make_box(A, B, Cc);
+    E.nsc = n_atoms * E.indices[0] * E.indices[1] * E.indices[2];
+    E.g = plan_cells(E.box, rcut, E.indices, &E.use_cells);
+    const size_t n3 = 3 * (size_t)n_atoms;
+    TGB_TRY(E.pos.ensure(n3)); TGB_TRY(E.pos_prev.ensure(n3)); TGB_TRY(E.vel.ensure(n3));
+    TGB_TRY(E.f.ensure(n3)); TGB_TRY(E.f_prev.ensure(n3)); TGB_TRY(E.mass.ensure(n_atoms));
+    TGB_TRY(E.en.ensure(n_atoms)); TGB_TRY(E.vir.ensure(9)); TGB_TRY(E.acc4.ensure(4));
+    TGB_TRY(E.ekin.ensure(1)); TGB_TRY(E.species.ensure(n_atoms)); TGB_TRY(E.err.ensure(1));
+    TGB_TRY(E.abc.ensure(9));
+    E.nz = std::max(n_species_total, 1);
+    TGB_TRY(E.e0.ensure(E.nz));
+    std::vector<double> e0(E.nz, 0.0);
+    if (e0_by_species)
+        for (int z = 0; z < n_species_total; ++z) e0[z] = e0_by_species[z];
+    const double abc_h[9] = {a_box[0], a_box[1], a_box[2], b_box[0], b_box[1],
+                             b_box[2], c_box[0], c_box[1], c_box[2]};
+    if (E.nsc > E.n) TGB_TRY(E.pos_sc.ensure(3 * (size_t)E.nsc));
+    cudaStream_t st = E.st;
+    TGB_CUDA(cudaMemcpyAsync(E.pos.p, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemsetAsync(E.vel.p, 0, sizeof(double) * n3, st));
+    TGB_CUDA(cudaMemsetAsync(E.f_prev.p, 0, sizeof(double) * n3, st));
+    TGB_CUDA(cudaMemcpyAsync(E.mass.p, masses, sizeof(double) * n_atoms, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.species.p, species, sizeof(int) * n_atoms, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.e0.p, e0.data(), sizeof(double) * E.nz, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.abc.p, abc_h, sizeof(abc_h), cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemsetAsync(E.err.p, 0, sizeof(unsigned), st));
+    // central sites of each block (species never change during MD)
+    for (int k = 0; k < n_blocks; ++k) {
+        Block *b = C.blocks[block_keys[k]].get();
+        auto run = std::make_unique<BlockRun>();
+        run->b = b;
+        run->w = std::make_unique<Workspace>();
+        std::vector<int> sites;
+        for (int i = 0; i < n_atoms; ++i) {
+            const int z = species[i];
+            int first = 0;
+            for (int s = 0; s < b->ns; ++s)
+                if (b->hh.species_z[s] == z) { first = s + 1; break; }
+            if (b->hh.central_species == 0 || first == b->hh.central_species) sites.push_back(i);
+        }
+        run->n_sites = (int)sites.size();
+        TGB_TRY(run->sites.ensure(sites.size()));
+        if (!sites.empty())
+            TGB_CUDA(cudaMemcpyAsync(run->sites.p, sites.data(), sizeof(int) * sites.size(),
+                                     cudaMemcpyHostToDevice, st));
+        TGB_TRY(run->w->ensure(*b, run->n_sites));
+        E.runs.push_back(std::move(run));
+    }
+    // size the pair arrays from a first build, with 40 % headroom for MD
+    const double *p0 = E.pos.p;
+    if (E.nsc > E.n) {
+        TGB_TRY(launch_supercell(E.n, E.pos.p, E.abc.p, E.indices, E.pos_sc.p, st));
+        p0 = E.pos_sc.p;
+    }
+    TGB_TRY(E.nl.reserve(E.n, E.nsc, (int64_t)E.n * 48, E.g));
+    TGB_CUDA(cudaMemsetAsync(E.nl.err, 0, sizeof(unsigned), st));
+    TGB_TRY(nl_build(E.nl, E.n, E.nsc, p0, E.box, E.g, E.use_cells, rcut, nullptr, st));
+    int64_t P = 0;
+    TGB_CUDA(cudaMemcpyAsync(&P, E.nl.pstart + E.n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    TGB_TRY(E.nl.reserve(E.n, E.nsc, (int64_t)(P * 1.4) + 64, E.g));
+    TGB_CUDA(cudaMemsetAsync(E.nl.err, 0, sizeof(unsigned), st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    *out = holder.release();
+    return TG_OK;
+}
+
+int tg_engine_destroy(tg_engine *e) {
+    if (!e) return TG_OK;
+    cudaStreamSynchronize(e->e.st);
+    delete e;
+    return TG_OK;
+}
+
+int tg_engine_set_state(tg_engine *eh, const double *positions, const double *velocities) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    const size_t b3 = sizeof(double) * 3 * E.n;
+    if (positions) TGB_CUDA(cudaMemcpyAsync(E.pos.p, positions, b3, cudaMemcpyHostToDevice, E.st));
+    if (velocities) TGB_CUDA(cudaMemcpyAsync(E.vel.p, velocities, b3, cudaMemcpyHostToDevice, E.st));
+    E.first_step = true;
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+static int engine_errors(Engine &E) {
+    unsigned e1 = 0, e2 = 0;
+    TGB_CUDA(cudaMemcpyAsync(&e1, E.err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaMemcpyAsync(&e2, E.nl.err, sizeof(unsigned), cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    const unsigned e = e1 | e2;
+    if (!e) return TG_OK;
+    TGB_CUDA(cudaMemsetAsync(E.err.p, 0, sizeof(unsigned), E.st));
+    TGB_CUDA(cudaMemsetAsync(E.nl.err, 0, sizeof(unsigned), E.st));
+    if (e & (DEV_ERR_TIMEOUT_TMA | DEV_ERR_TIMEOUT_MMA | DEV_ERR_TIMEOUT_EPI)) {
+        set_error("device wait timed out (error word 0x%x)", e);
+        return TG_ERR_TIMEOUT;
+    }
+    set_error("device error word 0x%x%s", e,
+              (e & DEV_ERR_NEIGH_CAPACITY) ? " (neighbour pair capacity exceeded)" : "");
+    return TG_ERR_DEVICE;
+}
+
+int tg_engine_compute_device(tg_engine *eh) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    return eh->e.compute_ef();
+}
+
+int tg_engine_compute(tg_engine *eh, double *energies, double *forces, double *virial) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    TGB_TRY(E.compute_ef());
+    if (energies)
+        TGB_CUDA(cudaMemcpyAsync(energies, E.en.p, sizeof(double) * E.n, cudaMemcpyDeviceToHost, E.st));
+    if (forces)
+        TGB_CUDA(cudaMemcpyAsync(forces, E.f.p, sizeof(double) * 3 * E.n, cudaMemcpyDeviceToHost, E.st));
+    if (virial) TGB_CUDA(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return engine_errors(E);
+}
+
+int tg_engine_md(tg_engine *eh, int32_t n_steps, double dt, double *e_pot, double *e_kin) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    for (int s = 0; s < n_steps; ++s) {
+        if (E.first_step) {
+            TGB_TRY(E.md_step(dt, true));
+            E.first_step = false;
+            E.dt_prev = dt;
+            TGB_TRY(engine_errors(E));
+            continue;
+        }
+        if (!E.graph || E.graph_dt != dt) {
+            if (E.graph) {
+                cudaGraphExecDestroy(E.graph);
+                E.graph = nullptr;
+            }
+            cudaGraph_t gr;
+            TGB_CUDA(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+            int r = E.md_step(dt, false);
+            cudaError_t ce = cudaStreamEndCapture(E.st, &gr);
+            TGB_TRY(r);
+            TGB_CUDA(ce);
+            ce = cudaGraphInstantiate(&E.graph, gr, 0);
+            cudaGraphDestroy(gr);
+            TGB_CUDA(ce);
+            E.graph_dt = dt;
+        }
+        TGB_CUDA(cudaGraphLaunch(E.graph, E.st));
+        E.dt_prev = dt;
+    }
+    TGB_TRY(engine_errors(E));
+    if (e_kin) {
+        TGB_TRY(launch_kinetic(E.n, E.vel.p, E.mass.p, E.ekin.p, E.st));
+        TGB_CUDA(cudaMemcpyAsync(e_kin, E.ekin.p, sizeof(double), cudaMemcpyDeviceToHost, E.st));
+    }
+    if (e_pot) {
+        std::vector<double> en(E.n);
+        TGB_CUDA(cudaMemcpyAsync(en.data(), E.en.p, sizeof(double) * E.n, cudaMemcpyDeviceToHost, E.st));
+        TGB_CUDA(cudaStreamSynchronize(E.st));
+        double s = 0.0;
+        for (double v : en) s += v;
+        *e_pot = s;
+    }
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+int tg_engine_get_state(tg_engine *eh, double *positions, double *velocities, double *forces) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    const size_t b3 = sizeof(double) * 3 * E.n;
+    if (positions) TGB_CUDA(cudaMemcpyAsync(positions, E.pos.p, b3, cudaMemcpyDeviceToHost, E.st));
+    if (velocities) TGB_CUDA(cudaMemcpyAsync(velocities, E.vel.p, b3, cudaMemcpyDeviceToHost, E.st));
+    if (forces) TGB_CUDA(cudaMemcpyAsync(forces, E.f.p, b3, cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {
+    TGB_CHECK(eh && n_pairs, TG_ERR_ARG, "null argument");
+    Engine &E = eh->e;
+    TGB_CUDA(cudaMemcpyAsync(n_pairs, E.nl.pstart + E.n, sizeof(int64_t), cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+int tg_engine_stream(tg_engine *eh, void **stream) {
+    TGB_CHECK(eh && stream, TG_ERR_ARG, "null argument");
+    *stream = (void *)eh->e.st;
+    return TG_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== test-only
+#include "../../include/tgb200_test.h"
+
+extern "C" int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t *A,
+                                const uint16_t *B, float *Cout) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(M > 0 && N > 0 && K > 0 && K % kGemmBK == 0, TG_ERR_ARG, "bad GEMM shape");
+    DBuf<__nv_bfloat16> a, b;
+    DBuf<float> c;
+    TGB_TRY(a.ensure((size_t)M * K));
+    TGB_TRY(b.ensure((size_t)N * K));
+    TGB_TRY(c.ensure((size_t)M * N));
+    TGB_CUDA(cudaMemcpyAsync(a.p, A, sizeof(uint16_t) * M * K, cudaMemcpyHostToDevice, C.st));
+    TGB_CUDA(cudaMemcpyAsync(b.p, B, sizeof(uint16_t) * N * K, cudaMemcpyHostToDevice, C.st));
+    TGB_CUDA(cudaMemsetAsync(c.p, 0, sizeof(float) * M * N, C.st));
+    TmaMap ta{}, tb{};
+    TGB_TRY(make_tma_bf16(&ta, a.p, M, K, K, kGemmBM));
+    TGB_TRY(make_tma_bf16(&tb, b.p, N, K, K, kGemmBN));
+    GemmEpi ep{};
+    ep.mode = EPI_STORE_F32;
+    ep.rows = M;
+    ep.cols = N;
+    ep.out = c.p;
+    ep.ldo = N;
+    TGB_TRY(launch_gemm_tn(ta, tb, M, N, K, ep, C.err.p, C.st));
+    TGB_TRY(check_err_word(C, C.err.p));
+    TGB_CUDA(cudaMemcpyAsync(Cout, c.p, sizeof(float) * M * N, cudaMemcpyDeviceToHost, C.st));
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    return TG_OK;
+}

@@ -1,0 +1,366 @@
+// tgb_gemm.cu -- Blackwell (sm_100a) GEMM for the GAP sparse-set kernel.
+//
+// One CTA computes one 128 x 256 tile of C = A . B^T:
+//   warp 0  : TMA producer (one lane) feeding a 4-stage shared-memory ring,
+//   warp 1  : allocates 256 TMEM columns; one lane issues tcgen05.mma
+//             (M=128, N=256, K=16, bf16 -> fp32) and tcgen05.commit,
+//   warps 2-5: epilogue, tcgen05.ld of the accumulator (warp w reads TMEM lanes
+//             32*(w%4) .. +31) and the fused GAP epilogue.
+// Operand tiles are [rows x 64] bf16 with the 128-byte swizzle, which is the
+// canonical K-major layout of the UMMA shared-memory descriptor.
+// Every mbarrier wait is bounded by wall time; on expiry the waiting role sets
+// an error bit, stops issuing and lets the CTA drain and free its TMEM.
+
+#include "tgb_gemm.cuh"
+
+#include <cudaTypedefs.h>
+
+namespace tgb {
+
+namespace {
+
+constexpr uint64_t kWaitLimitNs = 2000000000ull;   // 2 s per wait
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr unsigned kTimeoutBits = DEV_ERR_TIMEOUT_TMA | DEV_ERR_TIMEOUT_MMA | DEV_ERR_TIMEOUT_EPI;
+
+// Bounded wait: true when the phase with the given parity completed. Gives up
+// after kWaitLimitNs, or at once when another CTA has already timed out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const unsigned *err) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 0) {
+            if (*reinterpret_cast<const volatile unsigned *>(err) & kTimeoutBits) return false;
+            if (global_ns() - t0 > kWaitLimitNs) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: start address>>4,
+// leading byte offset 1 (unused for swizzled K-major), stride byte offset
+// 1024 B (8 rows x 128 B) >> 4, descriptor version 1, layout SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor: fp32 accumulator, bf16 A and B, both K-major, N>>3, M>>4.
+__host__ __device__ constexpr uint32_t make_idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32"
+        " {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ double ipow_d(double x, int e) {
+    double r = 1.0;
+    for (int k = 0; k < e; ++k) r *= x;
+    return r;
+}
+__device__ __forceinline__ float ipow_f(float x, int e) {
+    float r = 1.f;
+    for (int k = 0; k < e; ++k) r *= x;
+    return r;
+}
+
+constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK, STAGES = kGemmStages;
+constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256;
+
+__global__ void __launch_bounds__(192, 1)
+    k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              int num_kb, int n_tiles_n, GemmEpi ep, unsigned *err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t *gbase = smem_raw + (base - raw);
+    const uint32_t sA = base, sB = base + STAGES * A_BYTES;
+    const uint32_t bars = sB + STAGES * B_BYTES;   // full[STAGES], empty[STAGES], acc
+    const uint32_t full0 = bars, empty0 = bars + 8 * STAGES, accb = bars + 16 * STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + (bars - base) + 16 * STAGES + 8);
+    const uint32_t slot_addr = bars + 16 * STAGES + 8;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile_m = blockIdx.x / n_tiles_n, tile_n = blockIdx.x % n_tiles_n;
+    const int m0 = tile_m * BM, n0 = tile_n * BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(accb, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot_addr),
+                     "r"((uint32_t)BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer
+        int issued = 0;
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) {
+                atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_TMA);
+                break;
+            }
+            mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
+            tma_load_2d(sA + s * A_BYTES, &tmA, kb * BK, m0, full0 + 8 * s);
+            tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
+            issued = kb + 1;
+        }
+        // Drain: the last load of every stage has landed before the CTA may exit
+        // (already true on the normal path, where the MMA consumed them).
+        for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
+            (void)mbar_wait(full0 + 8 * (kb % STAGES), (uint32_t)(kb / STAGES) & 1u, err);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer
+        constexpr uint32_t idesc = make_idesc(BM, BN);
+        bool ok = true;
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (!mbar_wait(full0 + 8 * s, ph, err)) {
+                atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_MMA);
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = sA + s * A_BYTES, b0 = sB + s * B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+                tc_mma(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), idesc,
+                       (kb > 0 || kk > 0) ? 1u : 0u);
+            tc_commit(empty0 + 8 * s);
+        }
+        (void)ok;
+        tc_commit(accb);
+    } else if (warp >= 2) {
+        // ---- epilogue
+        const bool ready = mbar_wait(accb, 0, err);
+        if (!ready && lane == 0) atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_EPI);
+        tc_fence_after();
+        const int q = warp & 3;
+        const int row = m0 + q * 32 + lane;
+        const bool row_ok = ready && row < ep.rows;
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
+        if (ep.mode == EPI_GAP_KERNEL) {
+            double e = 0.0, ks = 0.0;
+            const double qo = row_ok ? ep.qoff[row] : 0.0;
+            for (int c = 0; c < BN / 16; ++c) {
+                float v[16];
+                __syncwarp();
+                tmem_ld16(taddr + c * 16, v);
+                const int col0 = n0 + c * 16;
+                if (!row_ok || col0 >= ep.Mpad) continue;
+                __align__(16) __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int s = col0 + j;
+                    const double K = (double)v[j] + ep.aoff[s] + qo;
+                    double kz, km1;
+                    if (ep.zeta_int > 0) {
+                        km1 = ipow_d(K, ep.zeta_int - 1);
+                        kz = km1 * K;
+                    } else {
+                        km1 = pow(K, ep.zeta_f - 1.0);
+                        kz = pow(K, ep.zeta_f);
+                    }
+                    e += ep.alpha[s] * kz;
+                    const double kd = ep.kcoef[s] * km1;
+                    ks += kd;
+                    bf16_split((float)(kd - ep.kcoef[s]), hi[j], lo[j]);
+                }
+                __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + col0;
+                const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
+                const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
+                uint4 *d0 = reinterpret_cast<uint4 *>(kr);
+                d0[0] = h4[0];
+                d0[1] = h4[1];
+                if (ep.nsplit == 3) {
+                    uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
+                    uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
+                    d1[0] = h4[0];
+                    d1[1] = h4[1];
+                    d2[0] = l4[0];
+                    d2[1] = l4[1];
+                }
+            }
+            if (row_ok) {
+                ep.epart[(size_t)row * n_tiles_n + tile_n] = e;
+                ep.kdsum[(size_t)row * n_tiles_n + tile_n] = ks;
+            }
+        } else {
+            for (int c = 0; c < BN / 16; ++c) {
+                float v[16];
+                __syncwarp();
+                tmem_ld16(taddr + c * 16, v);
+                const int col0 = n0 + c * 16;
+                if (!row_ok || col0 >= ep.cols) continue;
+                float *o = ep.out + (size_t)row * ep.ldo + col0;
+                if (col0 + 16 <= ep.cols) {
+                    float4 *o4 = reinterpret_cast<float4 *>(o);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        o4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                } else {
+                    for (int j = 0; j < 16 && col0 + j < ep.cols; ++j) o[j] = v[j];
+                }
+            }
+        }
+    }
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"((uint32_t)BN)
+                     : "memory");
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder() {
+    if (g_encode) return TG_OK;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+        set_error("cuTensorMapEncodeTiled not available from the driver");
+        return TG_ERR_CUDA;
+    }
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return TG_OK;
+}
+
+}  // namespace
+
+int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld,
+                  int box_rows) {
+    TGB_TRY(get_encoder());
+    TGB_CHECK(((uintptr_t)base & 15) == 0, TG_ERR_ARG, "TMA base address not 16-byte aligned");
+    TGB_CHECK((ld * 2) % 16 == 0, TG_ERR_ARG, "TMA row stride %lld B not a multiple of 16",
+              (long long)(ld * 2));
+    TGB_CHECK(rows >= 1 && cols >= 1, TG_ERR_ARG, "empty TMA extent");
+    cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {(cuuint32_t)kGemmBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(&m->map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base),
+                          gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TGB_CHECK(r == CUDA_SUCCESS, TG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return TG_OK;
+}
+
+int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
+                   unsigned *err, cudaStream_t st) {
+    TGB_CHECK(K % kGemmBK == 0, TG_ERR_ARG, "GEMM K=%d must be a multiple of %d", K, kGemmBK);
+    // 16-byte vector stores in the epilogues
+    TGB_CHECK(ep.mode != EPI_STORE_F32 || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
+              TG_ERR_ARG, "fp32 output rows must be 16-byte aligned (ldo %% 4 == 0)");
+    TGB_CHECK(ep.mode != EPI_GAP_KERNEL || (ep.K2 % 8 == 0 && ep.Mpad % 16 == 0 &&
+                                            ((uintptr_t)ep.kd & 15) == 0),
+              TG_ERR_ARG, "bf16 kernel-derivative rows must be 16-byte aligned");
+    if (M <= 0 || N <= 0) return TG_OK;
+    static bool attr = false;
+    if (!attr) {
+        TGB_CUDA(cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)SMEM_BYTES));
+        attr = true;
+    }
+    const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
+    k_gemm_tn<<<tm * tn, 192, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tn, ep, err);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+}  // namespace tgb

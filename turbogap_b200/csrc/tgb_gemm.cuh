@@ -1,0 +1,62 @@
+// tgb_gemm.cuh -- tcgen05/TMA GEMM for the GAP kernel (interfaces).
+#pragma once
+
+#include "tgb_common.cuh"
+
+#include <cuda.h>
+
+namespace tgb {
+
+// C[M x N] = A[M x K] . B[N x K]^T, A and B bf16 K-major (row-major, K
+// contiguous), fp32 accumulation in tensor memory, fused epilogue:
+//   EPI_GAP_KERNEL  (GEMM 1 on centred operands, C = (q - mu).(q_s - mu)):
+//       K = C + aoff[s] + qoff[row]                          (FP64; the exact rank-1 terms)
+//       epart[row][tile] = sum_s alpha_s K^zeta              (FP64)
+//       kdsum[row][tile] = sum_s kd_s                        (FP64)
+//       kd[row][s + t*Mpad] = split(kd_s - kcoef_s), kd_s = kcoef_s K^(zeta-1),
+//                             kcoef_s = zeta delta^2 alpha_s (the K = 1 value is
+//                             carried exactly by the caller)
+//   EPI_STORE_F32   (GEMM 2, sum_s (kd_s - kcoef_s)(q_s - mu)): out[row][col] = C
+enum EpiMode { EPI_GAP_KERNEL = 0, EPI_STORE_F32 = 1 };
+
+struct GemmEpi {
+    int mode;
+    int rows;             // valid rows of C
+    int cols;             // valid columns of C
+    // EPI_GAP_KERNEL
+    const double *alpha;  // [Mpad]
+    const double *kcoef;  // [Mpad] = zeta delta^2 alpha_s
+    int zeta_int;         // > 0: integer power; 0: use zeta_f
+    double zeta_f;
+    double *epart;        // [rows][n_tiles_n]
+    double *kdsum;        // [rows][n_tiles_n]
+    const double *aoff;   // [Mpad]: mu . q_s
+    const double *qoff;   // [rows]: (q - mu) . mu
+    __nv_bfloat16 *kd;    // [rows][K2]
+    int K2, Mpad, nsplit;
+    // EPI_STORE_F32
+    float *out;
+    int ldo;
+};
+
+constexpr int kGemmBM = 128;
+constexpr int kGemmBN = 256;
+constexpr int kGemmBK = 64;
+constexpr int kGemmStages = 4;
+
+struct TmaMap {
+    alignas(64) CUtensorMap map;
+};
+
+// 2-D bf16 tensor map over a row-major [rows x cols] matrix (row stride ld
+// elements), box [box_rows x 64], 128-byte swizzle, zero fill out of range.
+int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld,
+                  int box_rows);
+
+int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
+                   unsigned *err, cudaStream_t st);
+
+// Number of N tiles the energy partials are split into.
+inline int gemm_n_tiles(int N) { return (N + kGemmBN - 1) / kGemmBN; }
+
+}  // namespace tgb

@@ -1,0 +1,581 @@
+// tgb_neighbors.cu -- neighbour lists and FP64 MD kernels.
+//
+// Compiled with --fmad=false: every expression here must round exactly as the
+// reference's FP64 Fortran does (two roundings for a*b+c), so that neighbour
+// indices, rjs and xyz are bit-identical to build_neighbors_list
+// (src/neighbors.f90:243-605) and velocity_verlet (src/md.f90:226-283) matches
+// given identical inputs.
+
+#include "tgb_neighbors.cuh"
+
+#include <cub/device/device_scan.cuh>
+
+namespace tgb {
+
+// Fortran MODULO for reals as gfortran evaluates it: fmod, then shift into the
+// sign of p; an exact zero takes the sign of p. fmod(a, p) == a whenever |a| < |p|,
+// which skips the slow path for positions already inside the box.
+__device__ __forceinline__ double f_modulo(double a, double p) {
+    double r = (fabs(a) < fabs(p)) ? a : fmod(a, p);
+    if (r != 0.0) {
+        if ((a < 0.0) != (p < 0.0)) r = r + p;
+    } else {
+        r = copysign(0.0, p);
+    }
+    return r;
+}
+
+__device__ __forceinline__ double dot3(const double *x, const double *y) {
+    double s = x[0] * y[0];
+    s = s + x[1] * y[1];
+    s = s + x[2] * y[2];
+    return s;
+}
+
+// get_distance (src/neighbors.f90:47-163), all-periodic.
+__device__ void get_distance(const double *posi, const double *posj, const Box &bx, double *dist,
+                             double *d) {
+    if (bx.ortho) {
+        double d2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double L = bx.L[i];
+            double v = f_modulo(posj[i] - posi[i], L);
+            if (v > L / 2.0) v = v - L;
+            dist[i] = v;
+            d2 = d2 + v * v;
+        }
+        *d = sqrt(d2);
+        return;
+    }
+    double dd[3] = {posj[0] - posi[0], posj[1] - posi[1], posj[2] - posi[2]};
+    double v[3] = {-1.0 * dot3(dd, bx.a), -1.0 * dot3(dd, bx.b), -1.0 * dot3(dd, bx.c)};
+    double ir[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) s = s + bx.inv[i][j] * v[j];
+        ir[i] = s;
+    }
+    int idx[3];
+    for (int i = 0; i < 3; ++i) idx[i] = (int)llround(ir[i]);
+    double res_opt = 1.e10, opt[3] = {0, 0, 0};
+    for (int i = idx[0] - 1; i <= idx[0] + 1; ++i)
+        for (int j = idx[1] - 1; j <= idx[1] + 1; ++j)
+            for (int k = idx[2] - 1; k <= idx[2] + 1; ++k) {
+                double t[3];
+                for (int q = 0; q < 3; ++q)
+                    t[q] = dd[q] + (double)i * bx.a[q] + (double)j * bx.b[q] + (double)k * bx.c[q];
+                const double res = dot3(t, t);
+                if (res < res_opt) {
+                    res_opt = res;
+                    opt[0] = t[0]; opt[1] = t[1]; opt[2] = t[2];
+                }
+            }
+    dist[0] = opt[0]; dist[1] = opt[1]; dist[2] = opt[2];
+    *d = sqrt(dot3(dist, dist));
+}
+
+namespace {
+
+__device__ __forceinline__ int imod(int x, int m) {
+    int r = x % m;
+    return r < 0 ? r + m : r;
+}
+
+// Cell of atom i (neighbors.f90:398-408): MIC vector from the box centre,
+// shifted back by the centre, scaled by cells per length.
+__device__ __forceinline__ void cell_coords(const double *p, const Box &bx, const CellGrid &g,
+                                            int *ci) {
+    const double tol = 1.e-10;
+    const double ctr[3] = {bx.L[0] / 2.0, bx.L[1] / 2.0, bx.L[2] / 2.0};
+    double dist[3], d;
+    get_distance(ctr, p, bx, dist, &d);
+    const int m[3] = {g.mx, g.my, g.mz};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double v = dist[q] + ctr[q];
+        ci[q] = (int)(v / (bx.L[q] + tol) * (double)m[q]);
+    }
+}
+
+__global__ void k_cell_assign(int n, const double *__restrict__ pos, Box bx, CellGrid g,
+                              int *__restrict__ cell_xyz, int *__restrict__ cell_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[3];
+    cell_coords(pos + 3 * (size_t)i, bx, g, c);
+    cell_xyz[3 * i] = c[0];
+    cell_xyz[3 * i + 1] = c[1];
+    cell_xyz[3 * i + 2] = c[2];
+    const int id = imod(c[0], g.mx) + imod(c[1], g.my) * g.mx + imod(c[2], g.mz) * g.my * g.mx;
+    atomicAdd(&cell_count[id], 1);
+}
+
+__global__ void k_cell_fill(int n, const int *__restrict__ cell_xyz, CellGrid g,
+                            const int *__restrict__ cell_start, int *__restrict__ cell_fill,
+                            int *__restrict__ cell_atoms) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int id = imod(cell_xyz[3 * i], g.mx) + imod(cell_xyz[3 * i + 1], g.my) * g.mx +
+                   imod(cell_xyz[3 * i + 2], g.mz) * g.my * g.mx;
+    const int slot = atomicAdd(&cell_fill[id], 1);
+    cell_atoms[cell_start[id] + slot] = i;
+}
+
+// The reference links each cell's atoms by head insertion, so a cell is walked
+// in descending atom index (neighbors.f90:398-408, 460-463).
+__global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start,
+                            const int *__restrict__ cell_count, int *__restrict__ cell_atoms) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int *a = cell_atoms + cell_start[c];
+    const int n = cell_count[c];
+    for (int i = 1; i < n; ++i) {
+        const int v = a[i];
+        int j = i - 1;
+        while (j >= 0 && a[j] < v) {
+            a[j + 1] = a[j];
+            --j;
+        }
+        a[j + 1] = v;
+    }
+}
+
+struct PairSink {
+    // count mode when nbr == nullptr
+    int64_t base;
+    int64_t cap;
+    int *nbr;
+    double *rjs;
+    double *xyz;
+    unsigned *err;
+    int count;
+    __device__ __forceinline__ void emit(int j, double d, const double *dist) {
+        if (nbr) {
+            const int64_t p = base + count;
+            if (p < cap) {
+                nbr[p] = j;
+                rjs[p] = d;
+                xyz[3 * p] = dist[0];
+                xyz[3 * p + 1] = dist[1];
+                xyz[3 * p + 2] = dist[2];
+            } else {
+                atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+            }
+        }
+        ++count;
+    }
+};
+
+// Cell-list search (neighbors.f90:409-472): self first, then cells k3 (z)
+// outer, j3, i3 inner with the reference's skips for 1- and 2-cell axes.
+__global__ void k_nl_cells(int n_sites, const double *__restrict__ pos, Box bx, CellGrid g,
+                           double rcut, const int *__restrict__ do_list,
+                           const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
+                           const int *__restrict__ cell_count, const int *__restrict__ cell_atoms,
+                           int *__restrict__ n_neigh, const int64_t *__restrict__ pstart,
+                           int64_t cap, int *__restrict__ nbr, double *__restrict__ rjs,
+                           double *__restrict__ xyz, unsigned *err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_sites) return;
+    if (do_list && !do_list[i]) {
+        if (!pstart) n_neigh[i] = 0;
+        return;
+    }
+    PairSink sink{pstart ? pstart[i] : 0, cap, pstart ? nbr : nullptr, rjs, xyz, err, 0};
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    sink.emit(i, 0.0, zero3);
+    const double *pi = pos + 3 * (size_t)i;
+    const int i2 = 1 + cell_xyz[3 * i], j2 = 1 + cell_xyz[3 * i + 1], k2 = 1 + cell_xyz[3 * i + 2];
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    for (int k3 = k2 - 1; k3 <= k2 + 1; ++k3) {
+        if (mz == 1 && k3 != 1) continue;
+        if (mz == 2 && k2 == 1 && k3 == 0) continue;
+        if (mz == 2 && k2 == 2 && k3 == 3) continue;
+        for (int j3 = j2 - 1; j3 <= j2 + 1; ++j3) {
+            if (my == 1 && j3 != 1) continue;
+            if (my == 2 && j2 == 1 && j3 == 0) continue;
+            if (my == 2 && j2 == 2 && j3 == 3) continue;
+            for (int i3 = i2 - 1; i3 <= i2 + 1; ++i3) {
+                if (mx == 1 && i3 != 1) continue;
+                if (mx == 2 && i2 == 1 && i3 == 0) continue;
+                if (mx == 2 && i2 == 2 && i3 == 3) continue;
+                const int c = imod(i3 - 1, mx) + imod(j3 - 1, my) * mx + imod(k3 - 1, mz) * mx * my;
+                const int s = cell_start[c], e = s + cell_count[c];
+                for (int q = s; q < e; ++q) {
+                    const int k = cell_atoms[q];
+                    if (k == i) continue;
+                    double dist[3], d;
+                    get_distance(pi, pos + 3 * (size_t)k, bx, dist, &d);
+                    if (d < rcut) sink.emit(k, d, dist);
+                }
+            }
+        }
+    }
+    if (!pstart) n_neigh[i] = sink.count;
+}
+
+// O(N * N_supercell) search (neighbors.f90:474-514): ascending supercell index.
+__global__ void k_nl_brute(int n_sites, int n_sc, const double *__restrict__ pos, Box bx,
+                           double rcut, const int *__restrict__ do_list, int *__restrict__ n_neigh,
+                           const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
+                           double *__restrict__ rjs, double *__restrict__ xyz, unsigned *err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_sites) return;
+    if (do_list && !do_list[i]) {
+        if (!pstart) n_neigh[i] = 0;
+        return;
+    }
+    PairSink sink{pstart ? pstart[i] : 0, cap, pstart ? nbr : nullptr, rjs, xyz, err, 0};
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    sink.emit(i, 0.0, zero3);
+    const double *pi = pos + 3 * (size_t)i;
+    for (int j = 0; j < n_sc; ++j) {
+        if (j == i) continue;
+        double dist[3], d;
+        get_distance(pi, pos + 3 * (size_t)j, bx, dist, &d);
+        if (d < rcut) sink.emit(j, d, dist);
+    }
+    if (!pstart) n_neigh[i] = sink.count;
+}
+
+__global__ void k_pstart_zero(int64_t *pstart) { pstart[0] = 0; }
+
+__global__ void k_angles(int64_t P, const double *__restrict__ rjs, const double *__restrict__ xyz,
+                         const int *__restrict__ is_self, double *__restrict__ th,
+                         double *__restrict__ ph) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    if (is_self[p]) {
+        th[p] = 0.0;
+        ph[p] = 0.0;
+        return;
+    }
+    const double d = rjs[p];
+    const double x = xyz[3 * p], y = xyz[3 * p + 1], z = xyz[3 * p + 2];
+    if (fabs(z) >= d) th[p] = z > 0.0 ? 0.0 : acos(-1.0);
+    else th[p] = acos(z / d);
+    ph[p] = atan2(y, x);
+}
+
+// read_files.f90:347-363 supercell replicas: a-index, b, c, then atom.
+__global__ void k_supercell(int n, const double *__restrict__ pos, const double *a,
+                            const double *b, const double *c, int ia, int ib, int ic,
+                            double *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nrep = ia * ib * ic;
+    if (t >= n * nrep) return;
+    const int r = t / n, i = t % n;
+    const int i2 = r / (ib * ic), j2 = (r / ic) % ib, k2 = r % ic;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        out[3 * (size_t)t + q] = pos[3 * (size_t)i + q] + (double)i2 * a[q] + (double)j2 * b[q] +
+                                 (double)k2 * c[q];
+}
+
+// velocity_verlet (md.f90:226-283) on (3, n) arrays, no fixed atoms.
+__global__ void k_velocity_verlet(int n, double *__restrict__ pos, double *__restrict__ pos_prev,
+                                  double *__restrict__ vel, const double *__restrict__ f,
+                                  double *__restrict__ f_prev, const double *__restrict__ m,
+                                  double dt, double dt_prev, int first_step) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * n) return;
+    const int i = t / 3;
+    const double mi = m[i];
+    double v = vel[t];
+    if (!first_step) v = v + 0.5 * (f[t] + f_prev[t]) / mi * dt_prev;
+    vel[t] = v;
+    const double p = pos[t];
+    pos_prev[t] = p;
+    f_prev[t] = f[t];
+    pos[t] = p + v * dt + 0.5 * f[t] / mi * (dt * dt);
+}
+
+// wrap_pbc (md.f90:348-380), orthorhombic: i_shift = floor(x / L).
+__global__ void k_wrap_ortho(int n, double *__restrict__ pos, Box bx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *p = pos + 3 * (size_t)i;
+    const double s0 = floor(p[0] / bx.a[0]), s1 = floor(p[1] / bx.b[1]), s2 = floor(p[2] / bx.c[2]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        p[q] = p[q] - (double)(int)s0 * bx.a[q] - (double)(int)s1 * bx.b[q] -
+               (double)(int)s2 * bx.c[q];
+}
+
+// sum_i m_i v_i (3) and sum_i m_i (1) into acc[4] (FP64 atomics, then apply)
+__global__ void k_cm_accumulate(int n, const double *__restrict__ vel, const double *__restrict__ m,
+                                double *acc) {
+    double s[4] = {0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double mi = m[i];
+        s[0] += mi * vel[3 * (size_t)i];
+        s[1] += mi * vel[3 * (size_t)i + 1];
+        s[2] += mi * vel[3 * (size_t)i + 2];
+        s[3] += mi;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s[q] = warp_sum(s[q]);
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < 4; ++q) atomicAdd(&acc[q], s[q]);
+}
+
+__global__ void k_cm_apply(int n, double *__restrict__ vel, const double *__restrict__ acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * n) return;
+    vel[t] = vel[t] - acc[t % 3] / acc[3];
+}
+
+__global__ void k_kinetic(int n, const double *__restrict__ vel, const double *__restrict__ m,
+                          double *acc) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double *v = vel + 3 * (size_t)i;
+        s += 0.5 * m[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
+}
+
+}  // namespace
+
+Box make_box(const double *a, const double *b, const double *c) {
+    Box bx{};
+    for (int q = 0; q < 3; ++q) { bx.a[q] = a[q]; bx.b[q] = b[q]; bx.c[q] = c[q]; }
+    const double tol = 1.e-6;
+    bx.ortho = fabs(a[1]) < tol && fabs(a[2]) < tol && fabs(b[0]) < tol && fabs(b[2]) < tol &&
+               fabs(c[0]) < tol && fabs(c[1]) < tol;
+    bx.L[0] = a[0]; bx.L[1] = b[1]; bx.L[2] = c[2];
+    // Gram matrix inverse for the triclinic branch (neighbors.f90:107-134).
+    auto d3 = [](const double *x, const double *y) {
+        double s = x[0] * y[0];
+        s = s + x[1] * y[1];
+        s = s + x[2] * y[2];
+        return s;
+    };
+    double m[3][3];
+    m[0][0] = d3(a, a); m[0][1] = d3(a, b); m[0][2] = d3(a, c);
+    m[1][0] = m[0][1];  m[1][1] = d3(b, b); m[1][2] = d3(b, c);
+    m[2][0] = m[0][2];  m[2][1] = m[1][2];  m[2][2] = d3(c, c);
+    const double md = -m[0][2] * m[0][2] * m[1][1] + 2.0 * m[0][1] * m[0][2] * m[1][2] -
+                      m[0][0] * m[1][2] * m[1][2] - m[0][1] * m[0][1] * m[2][2] +
+                      m[0][0] * m[1][1] * m[2][2];
+    double inv[3][3];
+    inv[0][0] = m[1][1] * m[2][2] - m[1][2] * m[1][2];
+    inv[0][1] = m[0][2] * m[1][2] - m[0][1] * m[2][2];
+    inv[0][2] = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+    inv[1][0] = inv[0][1];
+    inv[1][1] = m[0][0] * m[2][2] - m[0][2] * m[0][2];
+    inv[1][2] = m[0][1] * m[0][2] - m[0][0] * m[1][2];
+    inv[2][0] = inv[0][2];
+    inv[2][1] = inv[1][2];
+    inv[2][2] = m[0][0] * m[1][1] - m[0][1] * m[0][1];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) bx.inv[i][j] = inv[i][j] / md;
+    return bx;
+}
+
+void host_unit_cells(const double *a, const double *b, const double *c, double rcut, int *indices) {
+    auto cross = [](const double *x, const double *y, double *z) {
+        z[0] = x[1] * y[2] - x[2] * y[1];
+        z[1] = x[2] * y[0] - x[0] * y[2];
+        z[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    auto d3 = [](const double *x, const double *y) {
+        double s = x[0] * y[0];
+        s = s + x[1] * y[1];
+        s = s + x[2] * y[2];
+        return s;
+    };
+    double axb[3], cxa[3], bxc[3];
+    cross(a, b, axb);
+    cross(c, a, cxa);
+    cross(b, c, bxc);
+    const double n1 = sqrt(d3(axb, axb)), n2 = sqrt(d3(cxa, cxa)), n3 = sqrt(d3(bxc, bxc));
+    for (int i = 0; i < 3; ++i) { axb[i] /= n1; cxa[i] /= n2; bxc[i] /= n3; }
+    const double m[3][3] = {{d3(axb, a), d3(axb, b), d3(axb, c)},
+                            {d3(cxa, a), d3(cxa, b), d3(cxa, c)},
+                            {d3(bxc, a), d3(bxc, b), d3(bxc, c)}};
+    const double md = -m[0][2] * m[1][1] * m[2][0] + m[0][1] * m[1][2] * m[2][0] +
+                      m[0][2] * m[1][0] * m[2][1] - m[0][0] * m[1][2] * m[2][1] -
+                      m[0][1] * m[1][0] * m[2][2] + m[0][0] * m[1][1] * m[2][2];
+    double inv[3][3];
+    inv[0][0] = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+    inv[0][1] = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+    inv[0][2] = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+    inv[1][0] = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+    inv[1][1] = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+    inv[1][2] = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+    inv[2][0] = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+    inv[2][1] = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+    inv[2][2] = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) s = s + (inv[i][j] / md) * (2.0 * rcut);
+        s = fabs(s);
+        int k = (int)s;
+        if (s > (double)k) k = k + 1;
+        indices[i] = k;
+    }
+}
+
+int NeighborList::reserve(int ns, int nsc, int64_t pair_cap, const CellGrid &g) {
+    if (ns > n_alloc_sites) {
+        dev_free(n_neigh); dev_free(pstart); dev_free(cell_xyz);
+        TGB_TRY(dev_alloc(&n_neigh, ns));
+        TGB_TRY(dev_alloc(&pstart, (size_t)ns + 1));
+        TGB_TRY(dev_alloc(&cell_xyz, 3 * (size_t)ns));
+        n_alloc_sites = ns;
+        size_t need = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, need, n_neigh, pstart + 1, ns);
+        if (need > scan_bytes) {
+            dev_free(scan_tmp);
+            TGB_TRY(dev_alloc(reinterpret_cast<char **>(&scan_tmp), need));
+            scan_bytes = need;
+        }
+    }
+    if (nsc > n_alloc_sc) {
+        dev_free(cell_atoms);
+        TGB_TRY(dev_alloc(&cell_atoms, nsc));
+        n_alloc_sc = nsc;
+    }
+    const int64_t ncells = (int64_t)g.mx * g.my * g.mz;
+    if (ncells > n_alloc_cells) {
+        dev_free(cell_count); dev_free(cell_start); dev_free(cell_fill);
+        TGB_TRY(dev_alloc(&cell_count, ncells));
+        TGB_TRY(dev_alloc(&cell_start, ncells + 1));
+        TGB_TRY(dev_alloc(&cell_fill, ncells));
+        n_alloc_cells = ncells;
+        size_t need = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, need, cell_count, cell_start, (int)ncells);
+        if (need > scan_bytes) {
+            dev_free(scan_tmp);
+            TGB_TRY(dev_alloc(reinterpret_cast<char **>(&scan_tmp), need));
+            scan_bytes = need;
+        }
+    }
+    if (pair_cap > cap) {
+        dev_free(nbr); dev_free(rjs); dev_free(xyz);
+        TGB_TRY(dev_alloc(&nbr, pair_cap));
+        TGB_TRY(dev_alloc(&rjs, pair_cap));
+        TGB_TRY(dev_alloc(&xyz, 3 * pair_cap));
+        cap = pair_cap;
+    }
+    if (!err) TGB_TRY(dev_alloc(&err, 1));
+    return TG_OK;
+}
+
+void NeighborList::release() {
+    dev_free(n_neigh); dev_free(pstart); dev_free(cell_xyz); dev_free(cell_atoms);
+    dev_free(cell_count); dev_free(cell_start); dev_free(cell_fill); dev_free(nbr);
+    dev_free(rjs); dev_free(xyz); dev_free(scan_tmp); dev_free(err);
+    *this = NeighborList{};
+}
+
+CellGrid plan_cells(const Box &bx, double rcut, const int *indices, bool *use_cells) {
+    CellGrid g{1, 1, 1};
+    const bool small = indices[0] > 1 || indices[1] > 1 || indices[2] > 1;
+    *use_cells = bx.ortho && !small;
+    if (*use_cells) {
+        g.mx = (int)(bx.L[0] / rcut);
+        g.my = (int)(bx.L[1] / rcut);
+        g.mz = (int)(bx.L[2] / rcut);
+        if (g.mx < 1 || g.my < 1 || g.mz < 1) *use_cells = false;
+    }
+    if (!*use_cells) g = CellGrid{1, 1, 1};
+    return g;
+}
+
+int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const Box &bx,
+             const CellGrid &g, bool use_cells, double rcut, const int *do_list,
+             cudaStream_t st) {
+    const int TB = 128;
+    const int gb = (n_sites + TB - 1) / TB;
+    if (use_cells) {
+        const int ncells = g.mx * g.my * g.mz;
+        TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
+        TGB_CUDA(cudaMemsetAsync(nl.cell_fill, 0, sizeof(int) * ncells, st));
+        k_cell_assign<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, nl.cell_xyz, nl.cell_count);
+        size_t bytes = nl.scan_bytes;
+        TGB_CUDA(cub::DeviceScan::ExclusiveSum(nl.scan_tmp, bytes, nl.cell_count, nl.cell_start,
+                                               ncells, st));
+        k_cell_fill<<<gb, TB, 0, st>>>(n_sites, nl.cell_xyz, g, nl.cell_start, nl.cell_fill,
+                                       nl.cell_atoms);
+        k_cell_sort<<<(ncells + TB - 1) / TB, TB, 0, st>>>(ncells, nl.cell_start, nl.cell_count,
+                                                           nl.cell_atoms);
+        k_nl_cells<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
+                                      nl.cell_start, nl.cell_count, nl.cell_atoms, nl.n_neigh,
+                                      nullptr, nl.cap, nullptr, nullptr, nullptr, nl.err);
+    } else {
+        k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nullptr,
+                                      nl.cap, nullptr, nullptr, nullptr, nl.err);
+    }
+    k_pstart_zero<<<1, 1, 0, st>>>(nl.pstart);
+    size_t bytes = nl.scan_bytes;
+    TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n_sites,
+                                           st));
+    if (use_cells) {
+        k_nl_cells<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
+                                      nl.cell_start, nl.cell_count, nl.cell_atoms, nl.n_neigh,
+                                      nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);
+    } else {
+        k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nl.pstart,
+                                      nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);
+    }
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_angles(int64_t P, const double *rjs, const double *xyz, const int *is_self, double *th,
+                  double *ph, cudaStream_t st) {
+    if (P == 0) return TG_OK;
+    k_angles<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(P, rjs, xyz, is_self, th, ph);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_supercell(int n, const double *pos, const double *abc_dev, const int *indices,
+                     double *out, cudaStream_t st) {
+    const int tot = n * indices[0] * indices[1] * indices[2];
+    k_supercell<<<(tot + 255) / 256, 256, 0, st>>>(n, pos, abc_dev, abc_dev + 3, abc_dev + 6,
+                                                   indices[0], indices[1], indices[2], out);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_velocity_verlet(int n, double *pos, double *pos_prev, double *vel, const double *f,
+                           double *f_prev, const double *m, double dt, double dt_prev, int first,
+                           cudaStream_t st) {
+    k_velocity_verlet<<<(3 * n + 255) / 256, 256, 0, st>>>(n, pos, pos_prev, vel, f, f_prev, m, dt,
+                                                           dt_prev, first);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_wrap(int n, double *pos, const Box &bx, cudaStream_t st) {
+    if (!bx.ortho) {
+        set_error("wrap_pbc on device supports orthorhombic boxes only");
+        return TG_ERR_ARG;
+    }
+    k_wrap_ortho<<<(n + 255) / 256, 256, 0, st>>>(n, pos, bx);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_remove_cm(int n, double *vel, const double *m, double *acc4, cudaStream_t st) {
+    TGB_CUDA(cudaMemsetAsync(acc4, 0, 4 * sizeof(double), st));
+    k_cm_accumulate<<<148, 256, 0, st>>>(n, vel, m, acc4);
+    k_cm_apply<<<(3 * n + 255) / 256, 256, 0, st>>>(n, vel, acc4);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_kinetic(int n, const double *vel, const double *m, double *acc, cudaStream_t st) {
+    TGB_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), st));
+    k_kinetic<<<148, 256, 0, st>>>(n, vel, m, acc);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+}  // namespace tgb

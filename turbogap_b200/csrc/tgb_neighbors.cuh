@@ -1,0 +1,88 @@
+// tgb_neighbors.cuh -- neighbour-list and FP64 MD kernel interfaces.
+#pragma once
+
+#include "tgb_common.cuh"
+
+namespace tgb {
+
+template <class T>
+int dev_alloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), n * sizeof(T));
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+        *p = nullptr;
+        return TG_ERR_NOMEM;
+    }
+    return TG_OK;
+}
+
+template <class T>
+void dev_free(T *&p) {
+    if (p) cudaFree(reinterpret_cast<void *>(p));
+    p = nullptr;
+}
+
+// Simulation box (rows a, b, c). ortho: the reference's orthorhombic test
+// (neighbors.f90:85-88, tolerance 1e-6 on the off-diagonal components).
+struct Box {
+    double a[3], b[3], c[3];
+    double L[3];
+    double inv[3][3];
+    int ortho;
+};
+
+struct CellGrid {
+    int mx, my, mz;
+};
+
+// Pairs in CSR order: site i owns [pstart[i], pstart[i+1]); the first pair of
+// every site is the site itself (rjs = 0, xyz = 0). nbr holds 0-based
+// supercell indices.
+struct NeighborList {
+    int n_alloc_sites = 0, n_alloc_sc = 0;
+    int64_t n_alloc_cells = 0;
+    int64_t cap = 0;
+    int *n_neigh = nullptr;
+    int64_t *pstart = nullptr;
+    int *cell_xyz = nullptr;
+    int *cell_atoms = nullptr;
+    int *cell_count = nullptr;
+    int *cell_start = nullptr;
+    int *cell_fill = nullptr;
+    int *nbr = nullptr;
+    double *rjs = nullptr;
+    double *xyz = nullptr;
+    void *scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    unsigned *err = nullptr;
+
+    int reserve(int n_sites, int n_sc, int64_t pair_cap, const CellGrid &g);
+    void release();
+};
+
+Box make_box(const double *a, const double *b, const double *c);
+
+// number_of_unit_cells_for_given_cutoff (neighbors.f90:175-236), on the host.
+void host_unit_cells(const double *a, const double *b, const double *c, double rcut, int *indices);
+CellGrid plan_cells(const Box &bx, double rcut, const int *indices, bool *use_cells);
+
+// Count, scan and fill. Pairs beyond nl.cap are dropped and flag
+// DEV_ERR_NEIGH_CAPACITY; pstart[n_sites] is the required capacity.
+int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const Box &bx,
+             const CellGrid &g, bool use_cells, double rcut, const int *do_list,
+             cudaStream_t st);
+
+int launch_angles(int64_t P, const double *rjs, const double *xyz, const int *is_self, double *th,
+                  double *ph, cudaStream_t st);
+int launch_supercell(int n, const double *pos, const double *abc_dev, const int *indices,
+                     double *out, cudaStream_t st);
+int launch_velocity_verlet(int n, double *pos, double *pos_prev, double *vel, const double *f,
+                           double *f_prev, const double *m, double dt, double dt_prev, int first,
+                           cudaStream_t st);
+int launch_wrap(int n, double *pos, const Box &bx, cudaStream_t st);
+int launch_remove_cm(int n, double *vel, const double *m, double *acc4, cudaStream_t st);
+int launch_kinetic(int n, const double *vel, const double *m, double *acc, cudaStream_t st);
+
+}  // namespace tgb

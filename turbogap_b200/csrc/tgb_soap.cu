@@ -1,0 +1,833 @@
+// tgb_soap.cu -- SOAP descriptor (expansion, power spectrum, normalisation)
+// and the fused adjoint force/virial kernel for one soap_turbo block.
+//
+// The descriptor follows the published method (Caro, PRB 100, 024112 (2019);
+// Bartok et al., PRB 87, 184115 (2013)) in the form restated by the FP64 oracle:
+//   c_{n,lm}(i) = sum_j w(r) R_n(r) a_l(r) Y_lm(u)   (real Y_lm, u = r_ij/r)
+//   p_{nn'l}    = mu_{nn'} sum_m c_{n,lm} c_{n',lm}, mu = sqrt2 off-diagonal
+//   q           = p / |p|
+// R_n (poly3, orthonormalised by the FP64 Jacobi matrix) and a_l (smeared
+// angular factor 4 pi e^{-k} i_l(k)) are tabulated per species in FP64 on the
+// GPU and interpolated in FP32 (cubic Hermite, derivative of the interpolant).
+// Forces contract dE/dq through the normalisation and the power spectrum back
+// to dE/dc on chip; the per-pair Cartesian derivative of q is never formed.
+
+#include "tgb_soap.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace tgb {
+
+constexpr int kMaxL = 12;
+__constant__ float cYn[kMaxL + 1][kMaxL + 1];   // N_l0, sqrt2 N_lm (m > 0)
+__constant__ float cRa[kMaxL + 1][kMaxL + 1];   // (2l-1)/(l-m)
+__constant__ float cRb[kMaxL + 1][kMaxL + 1];   // (l+m-1)/(l-m)
+__constant__ float cDf[kMaxL + 2];              // (2m-1)!!
+
+int init_soap_constants() {
+    float yn[kMaxL + 1][kMaxL + 1] = {}, ra[kMaxL + 1][kMaxL + 1] = {},
+          rb[kMaxL + 1][kMaxL + 1] = {}, df[kMaxL + 2] = {};
+    for (int l = 0; l <= kMaxL; ++l)
+        for (int m = 0; m <= l; ++m) {
+            double ratio = 1.0;
+            for (int k = l - m + 1; k <= l + m; ++k) ratio /= (double)k;
+            const double N = std::sqrt((2.0 * l + 1.0) / (4.0 * kPi) * ratio);
+            yn[l][m] = (float)(m == 0 ? N : std::sqrt(2.0) * N);
+            if (l >= m + 2) {
+                ra[l][m] = (float)((2.0 * l - 1.0) / (double)(l - m));
+                rb[l][m] = (float)((double)(l + m - 1) / (double)(l - m));
+            }
+        }
+    for (int m = 0; m <= kMaxL + 1; ++m) {
+        double d = 1.0;
+        for (int k = 1; k <= 2 * m - 1; k += 2) d *= k;
+        df[m] = (float)d;
+    }
+    TGB_CUDA(cudaMemcpyToSymbol(cYn, yn, sizeof(yn)));
+    TGB_CUDA(cudaMemcpyToSymbol(cRa, ra, sizeof(ra)));
+    TGB_CUDA(cudaMemcpyToSymbol(cRb, rb, sizeof(rb)));
+    TGB_CUDA(cudaMemcpyToSymbol(cDf, df, sizeof(df)));
+    return TG_OK;
+}
+
+// ===================== FP64 table construction ==============================
+
+namespace {
+
+struct TableHyper {
+    double rh, rs, nf, gs, sr, srs, st, sts, A, cw;
+    int amax, lmax, re;
+};
+
+__device__ void d_scaled_moments(double tr, double s, int kmax, double *m) {
+    const double g1 = exp(-(1.0 - tr) * (1.0 - tr) / (2.0 * s * s));
+    const double g0 = exp(-tr * tr / (2.0 * s * s));
+    m[0] = s * sqrt(kPi / 2.0) * (erf((1.0 - tr) / (sqrt(2.0) * s)) + erf(tr / (sqrt(2.0) * s)));
+    for (int k = 0; k < kmax; ++k)
+        m[k + 1] = tr * m[k] + s * s * ((k > 0 ? k * m[k - 1] : 0.0) - g1 + (k == 0 ? g0 : 0.0));
+}
+
+__device__ double d_e_of(const double *m, int k, int re) {
+    if (re == 0) return m[k];
+    if (re == 1) return m[k] - m[k + 1];
+    return m[k] - 2.0 * m[k + 1] + m[k + 2];
+}
+
+// R_n(r) (without the neighbour weight) and dR_n/dr for n < amax.
+__device__ void d_radial_basis(const TableHyper &h, const double *W, double r, double *R,
+                               double *dR) {
+    const int amax = h.amax, re = h.re;
+    const double sig = h.sr * (1.0 + h.srs * r), dsig = h.sr * h.srs;
+    const double tr = (h.rh - r) / h.rh, sc = sig / h.rh;
+    const int kmax = amax + 2 + re + 2;
+    double m[32], dm[32];
+    d_scaled_moments(tr, sc, kmax, m);
+    for (int k = 0; k + 2 <= kmax; ++k) {
+        const double j1 = m[k + 1] - tr * m[k];
+        const double j2 = m[k + 2] - 2.0 * tr * m[k + 1] + tr * tr * m[k];
+        dm[k] = (-1.0 / h.rh) * j1 / (sc * sc) + (dsig / h.rh) * j2 / (sc * sc * sc);
+    }
+    const double pre = pow(h.rh, 0.5 + re);
+    for (int n = 0; n < amax; ++n) {
+        double v = 0.0, dv = 0.0;
+        for (int j = 0; j < amax; ++j) {
+            const double c = W[n * amax + j];
+            if (c == 0.0) continue;
+            v += c * d_e_of(m, j + 3, re);
+            dv += c * d_e_of(dm, j + 3, re);
+        }
+        R[n] = v * pre;
+        dR[n] = dv * pre;
+    }
+}
+
+__device__ void d_weight(const TableHyper &h, double r, double *w, double *dw) {
+    if (r >= h.rh) { *w = 0.0; *dw = 0.0; return; }
+    double fa = 1.0, dfa = 0.0;
+    if (h.A != 0.0) {
+        const double x = r / h.rh;
+        const double P = 1.0 - 3.0 * x * x + 2.0 * x * x * x;
+        const double dP = (-6.0 * x + 6.0 * x * x) / h.rh;
+        fa = pow(P, h.A);
+        dfa = h.A * pow(P, h.A - 1.0) * dP;
+    }
+    double fc = 1.0, dfc = 0.0;
+    if (h.rs < h.rh && r > h.rs) {
+        const double wd = h.rh - h.rs;
+        const double t = (r - h.rs) / wd;
+        const double den = 1.0 - t * t;
+        fc = exp(-h.nf * t * t / den);
+        dfc = fc * (-h.nf) * (2.0 * t / (den * den)) / wd;
+    }
+    *w = h.gs * fa * fc;
+    *dw = h.gs * (dfa * fc + fa * dfc);
+}
+
+// e^{-k} i_l(k) for l = 0..lmax+1 (power series; positive terms only).
+__device__ void d_scaled_msbessel(double k, int lmax1, double *out) {
+    const double ek = exp(-k);
+    double pref = 1.0;
+    const double x = 0.5 * k * k;
+    for (int l = 0; l <= lmax1; ++l) {
+        if (l > 0) pref *= k / (double)(2 * l + 1);
+        double term = 1.0, sum = 1.0;
+        for (int j = 1; j < 400; ++j) {
+            term *= x / ((double)j * (double)(2 * l + 2 * j + 1));
+            sum += term;
+            if (term < 1e-18 * sum) break;
+        }
+        out[l] = ek * pref * sum;
+    }
+}
+
+// Neighbour functions of one species at r: R~_n = w R_n and a_l, with d/dr.
+__device__ void d_functions(const TableHyper &h, const double *W, double r, double *R, double *dR,
+                            double *a, double *da) {
+    double Rb[16], dRb[16], w, dw;
+    d_weight(h, r, &w, &dw);
+    d_radial_basis(h, W, r, Rb, dRb);
+    for (int n = 0; n < h.amax; ++n) {
+        R[n] = w * Rb[n];
+        dR[n] = dw * Rb[n] + w * dRb[n];
+    }
+    const double st = h.st * (1.0 + h.sts * r), dst = h.st * h.sts;
+    const double kk = r * r / (st * st);
+    const double dk = 2.0 * r / (st * st) - 2.0 * r * r * dst / (st * st * st);
+    double ei[kMaxL + 3];
+    d_scaled_msbessel(kk, h.lmax + 1, ei);
+    for (int l = 0; l <= h.lmax; ++l) {
+        const double dil =
+            (l == 0) ? ei[1] : ((double)l * ei[l - 1] + (double)(l + 1) * ei[l + 1]) / (2.0 * l + 1.0);
+        a[l] = 4.0 * kPi * ei[l];
+        da[l] = 4.0 * kPi * (dil - ei[l]) * dk;
+    }
+}
+
+// One node per thread. Per node: [R~ | R~' | R~'' | a | a' | a''] (fp32). Values
+// and first derivatives are analytic (FP64); second derivatives are the central
+// difference of the analytic first derivative (FP64, step 1e-5 A), used only to
+// interpolate the first derivative as a cubic Hermite function of its own.
+__global__ void k_build_table(TableHyper h, const double *__restrict__ W, int tw,
+                              float *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > kTableIntervals) return;
+    const double r = h.rh * (double)k / (double)kTableIntervals;
+    const double eps = 1e-5;
+    double R[16], dR[16], a[kMaxL + 1], da[kMaxL + 1];
+    double Rp[16], dRp[16], ap[kMaxL + 1], dap[kMaxL + 1];
+    double Rm[16], dRm[16], am[kMaxL + 1], dam[kMaxL + 1];
+    d_functions(h, W, r, R, dR, a, da);
+    d_functions(h, W, r + eps, Rp, dRp, ap, dap);
+    d_functions(h, W, r - eps, Rm, dRm, am, dam);
+    const int A = h.amax, nl = h.lmax + 1;
+    float *o = out + (size_t)k * tw;
+    for (int n = 0; n < A; ++n) {
+        o[n] = (float)R[n];
+        o[A + n] = (float)dR[n];
+        o[2 * A + n] = (float)((dRp[n] - dRm[n]) / (2.0 * eps));
+    }
+    for (int l = 0; l < nl; ++l) {
+        o[3 * A + l] = (float)a[l];
+        o[3 * A + nl + l] = (float)da[l];
+        o[3 * A + 2 * nl + l] = (float)((dap[l] - dam[l]) / (2.0 * eps));
+    }
+    for (int q = 3 * A + 3 * nl; q < tw; ++q) o[q] = 0.0f;
+}
+
+// Central atom: weight global_scaling * central_weight, Gaussian at r = 0,
+// a_0(0) = 4 pi and Y_00 = 1/sqrt(4 pi) folded in.
+__global__ void k_build_self(TableHyper h, const double *__restrict__ W, float *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double R[16], dR[16];
+    d_radial_basis(h, W, 0.0, R, dR);
+    for (int n = 0; n < h.amax; ++n)
+        out[n] = (float)(h.gs * h.cw * R[n] * 4.0 * kPi / sqrt(4.0 * kPi));
+}
+
+}  // namespace
+
+// Orthonormal poly3 basis: Gram-Schmidt of (rc - x)^(alpha+2) on [0, rc], which is
+// t^3 P_n^{(0,6)}(2t - 1), t = (rc - x)/rc, normalised by sqrt(2n + 7). W[n][j]
+// is sqrt(2n+7) times the integer coefficient of t^j in P_n^{(0,6)}(2t - 1).
+static void poly3_jacobi_W(int amax, double *W) {
+    auto binom = [](int n, int k) -> long long {
+        if (k < 0 || k > n) return 0;
+        long long r = 1;
+        for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+        return r;
+    };
+    for (int n = 0; n < amax; ++n) {
+        std::vector<long long> coef(amax, 0);
+        for (int s = 0; s <= n; ++s) {
+            const long long base = binom(n, n - s) * binom(n + 6, s);
+            for (int i = 0; i <= s; ++i) coef[n - s + i] += base * binom(s, i) * (((s - i) % 2) ? -1 : 1);
+        }
+        const double nrm = std::sqrt((double)(2 * n + 7));
+        for (int j = 0; j < amax; ++j) W[n * amax + j] = nrm * (double)coef[j];
+    }
+}
+
+int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st) {
+    const int amax = h.alpha_max[0];
+    const int nl = h.lmax + 1;
+    const int tw = ((3 * amax + 3 * nl) + 3) / 4 * 4;
+    std::vector<double> W(amax * amax);
+    poly3_jacobi_W(amax, W.data());
+    double *dW = nullptr;
+    TGB_CUDA(cudaMalloc(&dW, sizeof(double) * W.size()));
+    TGB_CUDA(cudaMemcpyAsync(dW, W.data(), sizeof(double) * W.size(), cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < h.ns; ++s) {
+        TableHyper th{h.rcut_hard[s], h.rcut_soft[s], h.nf[s], h.global_scaling[s], h.sigma_r[s],
+                      h.sigma_r_scaling[s], h.sigma_t[s], h.sigma_t_scaling[s],
+                      h.amplitude_scaling[s], h.central_weight[s], amax, h.lmax,
+                      h.radial_enhancement};
+        k_build_table<<<(kTableIntervals + 1 + 127) / 128, 128, 0, st>>>(
+            th, dW, tw, table + (size_t)s * (kTableIntervals + 1) * tw);
+        k_build_self<<<1, 32, 0, st>>>(th, dW, self_R + s * amax);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaFree(dW);
+    TGB_CUDA(e);
+    TGB_CUDA(e2);
+    return TG_OK;
+}
+
+// ===================== FP32 device math ======================================
+
+namespace {
+
+template <int AMAX, int NL>
+struct RadAng {
+    float R[AMAX], dR[AMAX], a[NL], da[NL];
+};
+
+// Cubic Hermite interpolation of the species table at r. Values use the node
+// values and first derivatives; first derivatives use the node first and
+// second derivatives (an O(h^4) derivative, where differentiating the value
+// interpolant would only be O(h^3)). WITH_D = false skips the derivatives.
+template <int AMAX, int NL, int TW, bool WITH_D>
+__device__ __forceinline__ void table_eval(const float *__restrict__ T, float r, float h,
+                                           float inv_h, RadAng<AMAX, NL> &o) {
+    float x = r * inv_h;
+    int k = (int)x;
+    if (k > kTableIntervals - 1) k = kTableIntervals - 1;
+    if (k < 0) k = 0;
+    const float t = x - (float)k;
+    const float t2 = t * t, t3 = t2 * t;
+    const float h00 = 2.f * t3 - 3.f * t2 + 1.f, h10 = (t3 - 2.f * t2 + t) * h;
+    const float h01 = -2.f * t3 + 3.f * t2, h11 = (t3 - t2) * h;
+    const float *n0 = T + (size_t)k * TW;
+    const float *n1 = n0 + TW;
+    float b0[TW], b1[TW];
+#pragma unroll
+    for (int q = 0; q < TW; q += 4) {
+        const float4 v0 = __ldg(reinterpret_cast<const float4 *>(n0 + q));
+        const float4 v1 = __ldg(reinterpret_cast<const float4 *>(n1 + q));
+        b0[q] = v0.x; b0[q + 1] = v0.y; b0[q + 2] = v0.z; b0[q + 3] = v0.w;
+        b1[q] = v1.x; b1[q + 1] = v1.y; b1[q + 2] = v1.z; b1[q + 3] = v1.w;
+    }
+    constexpr int cA = 3 * AMAX;
+#pragma unroll
+    for (int n = 0; n < AMAX; ++n) {
+        o.R[n] = h00 * b0[n] + h10 * b0[AMAX + n] + h01 * b1[n] + h11 * b1[AMAX + n];
+        if (WITH_D)
+            o.dR[n] = h00 * b0[AMAX + n] + h10 * b0[2 * AMAX + n] + h01 * b1[AMAX + n] +
+                      h11 * b1[2 * AMAX + n];
+    }
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        o.a[l] = h00 * b0[cA + l] + h10 * b0[cA + NL + l] + h01 * b1[cA + l] + h11 * b1[cA + NL + l];
+        if (WITH_D)
+            o.da[l] = h00 * b0[cA + NL + l] + h10 * b0[cA + 2 * NL + l] + h01 * b1[cA + NL + l] +
+                      h11 * b1[cA + 2 * NL + l];
+    }
+}
+
+// Associated Legendre derivative polynomials Q[l][m] = d^m P_l/dz^m for m <= l,
+// and Q[l][l+1] = 0, by the standard upward recurrence in l.
+template <int LMAX>
+__device__ __forceinline__ void legendre_q(float z, float (&Q)[LMAX + 1][LMAX + 2]) {
+#pragma unroll
+    for (int m = 0; m <= LMAX; ++m) {
+        Q[m][m] = cDf[m];
+        if (m + 1 <= LMAX) Q[m + 1][m] = (float)(2 * m + 1) * z * Q[m][m];
+#pragma unroll
+        for (int l = m + 2; l <= LMAX; ++l)
+            Q[l][m] = cRa[l][m] * z * Q[l - 1][m] - cRb[l][m] * Q[l - 2][m];
+    }
+#pragma unroll
+    for (int l = 0; l <= LMAX; ++l) Q[l][l + 1] = 0.f;
+}
+
+template <int LMAX>
+__device__ __forceinline__ void cos_sin_m(float x, float y, float (&C)[LMAX + 1], float (&S)[LMAX + 1]) {
+    C[0] = 1.f;
+    S[0] = 0.f;
+#pragma unroll
+    for (int m = 1; m <= LMAX; ++m) {
+        C[m] = x * C[m - 1] - y * S[m - 1];
+        S[m] = x * S[m - 1] + y * C[m - 1];
+    }
+}
+
+__device__ __forceinline__ int fold_index(int j, int n) {
+    return j < n ? j : j % n;
+}
+
+// Descriptor species of a global species id, -1 when the block does not see it.
+__device__ __forceinline__ int zlookup(const SoapParams &P, int z) {
+    return (z >= 0 && z < kMaxZ) ? (int)P.zmap[z] : -1;
+}
+
+}  // namespace
+
+// ===================== expansion + power spectrum ===========================
+
+template <int NS, int AMAX, int LMAX>
+struct DescShape {
+    static constexpr int NL = LMAX + 1;
+    static constexpr int NLM = NL * NL;
+    static constexpr int NT = NS * AMAX;
+    static constexpr int DIM = NT * (NT + 1) / 2 * NL;
+    static constexpr int SLOTS = (NLM + 31) / 32;
+    static constexpr int DSLOTS = (DIM + 31) / 32;
+    static constexpr int TW = ((3 * AMAX + 3 * NL) + 3) / 4 * 4;
+    static constexpr int RHO = AMAX * NL;          // per-pair radial*angular products
+    static constexpr int CHUNK = 32;
+    static constexpr int WARPS = 4;
+    // shared memory per warp (floats): Y rows + rho rows (+ reused for c)
+    static constexpr int YS = CHUNK * NLM;
+    static constexpr int RS = CHUNK * RHO;
+    static constexpr int WARP_FLOATS = YS + RS + CHUNK;
+    static_assert(2 * NT * NLM <= YS + RS, "FP64 c must fit in the per-warp staging area");
+    static_assert(AMAX % 4 == 0, "float4 reads of rho rows need alpha_max % 4 == 0");
+};
+
+template <int NS, int AMAX, int LMAX>
+__global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
+    using Sh = DescShape<NS, AMAX, LMAX>;
+    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, DIM = Sh::DIM;
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *Ys = smem + warp * Sh::WARP_FLOATS;
+    float *rho = Ys + Sh::YS;
+    int *pspec = reinterpret_cast<int *>(rho + Sh::RS);
+    __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
+    for (int t = threadIdx.x; t < NT * (NT + 1) / 2; t += blockDim.x) {
+        int n = 0, rem = t;
+        while (rem >= NT - n) { rem -= NT - n; ++n; }
+        pair_n[t] = (unsigned char)n;
+        pair_n2[t] = (unsigned char)(n + rem);
+    }
+    __syncthreads();
+    const int site = blockIdx.x * Sh::WARPS + warp;
+    if (site >= S.n_sites) return;
+    const int row = S.site_row[site];
+    const int catom = S.site_atom[site];
+    const int64_t p0 = S.pstart[row];
+    const int np = (int)(S.pstart[row + 1] - p0);
+
+    int lmk[Sh::SLOTS], lk[Sh::SLOTS];
+#pragma unroll
+    for (int k = 0; k < Sh::SLOTS; ++k) {
+        lmk[k] = lane + 32 * k;
+        int l = 0;
+        while ((l + 1) * (l + 1) <= lmk[k]) ++l;
+        lk[k] = l;
+    }
+    // c accumulates in FP64: FP32 sums of ~30 pair terms onto the large central
+    // contribution were the dominant descriptor error.
+    double acc[NT][Sh::SLOTS];
+#pragma unroll
+    for (int n = 0; n < NT; ++n)
+#pragma unroll
+        for (int k = 0; k < Sh::SLOTS; ++k) acc[n][k] = 0.0;
+
+    for (int base = 0; base < np; base += Sh::CHUNK) {
+        const int t = lane;
+        int s = -1;
+        if (base + t < np) {
+            float *Yr = Ys + t * NLM;
+            float *rr = rho + t * Sh::RHO;   // layout [l][n]
+            if (base + t == 0) {
+                s = zlookup(P, S.species[catom]);
+                if (s >= 0) {
+                    for (int lm = 0; lm < NLM; ++lm) Yr[lm] = (lm == 0) ? 1.f : 0.f;
+                    for (int l = 0; l < NL; ++l)
+                        for (int n = 0; n < AMAX; ++n)
+                            rr[l * AMAX + n] = (l == 0) ? P.self_R[s * AMAX + n] : 0.f;
+                }
+            } else {
+                const int64_t p = p0 + base + t;
+                const int ja = fold_index(S.nbr[p], P.n_atoms);
+                s = zlookup(P, S.species[ja]);
+                const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
+                            z = (float)S.xyz[3 * p + 2];
+                const float r = sqrtf(x * x + y * y + z * z);
+                if (s >= 0 && r < P.rcut[s] && r > 0.f) {
+                    RadAng<AMAX, NL> ra;
+                    table_eval<AMAX, NL, Sh::TW, false>(P.table + (size_t)s * (kTableIntervals + 1) * Sh::TW,
+                                                        r, P.tab_h[s], P.tab_inv_h[s], ra);
+                    const float ir = 1.f / r;
+                    const float ux = x * ir, uy = y * ir, uz = z * ir;
+                    float C[LMAX + 1], Sn[LMAX + 1];
+                    cos_sin_m<LMAX>(ux, uy, C, Sn);
+                    float Q[LMAX + 1][LMAX + 2];
+                    legendre_q<LMAX>(uz, Q);
+#pragma unroll
+                    for (int l = 0; l <= LMAX; ++l) {
+                        Yr[l * l + l] = cYn[l][0] * Q[l][0];
+#pragma unroll
+                        for (int m = 1; m <= l; ++m) {
+                            const float f = cYn[l][m] * Q[l][m];
+                            Yr[l * l + l + m] = f * C[m];
+                            Yr[l * l + l - m] = f * Sn[m];
+                        }
+                    }
+#pragma unroll
+                    for (int l = 0; l < NL; ++l)
+#pragma unroll
+                        for (int n = 0; n < AMAX; ++n) rr[l * AMAX + n] = ra.R[n] * ra.a[l];
+                } else {
+                    s = -1;
+                }
+            }
+        }
+        pspec[t] = s;
+        __syncwarp();
+        const int cnt = min(Sh::CHUNK, np - base);
+        for (int tt = 0; tt < cnt; ++tt) {
+            const int ss = pspec[tt];
+            if (ss < 0) continue;
+            const float *Yr = Ys + tt * NLM;
+            const float *rr = rho + tt * Sh::RHO;
+#pragma unroll
+            for (int k = 0; k < Sh::SLOTS; ++k) {
+                if (lmk[k] < NLM) {
+                    const float yv = Yr[lmk[k]];
+                    const float4 *r4 = reinterpret_cast<const float4 *>(rr + lk[k] * AMAX);
+                    float rv[AMAX];
+#pragma unroll
+                    for (int q = 0; q < AMAX / 4; ++q) {
+                        const float4 v = r4[q];
+                        rv[4 * q] = v.x; rv[4 * q + 1] = v.y; rv[4 * q + 2] = v.z; rv[4 * q + 3] = v.w;
+                    }
+#pragma unroll
+                    for (int sp = 0; sp < NS; ++sp) {
+                        if (ss == sp) {
+#pragma unroll
+                            for (int n = 0; n < AMAX; ++n)
+                                acc[sp * AMAX + n][k] += (double)(rv[n] * yv);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    // c to shared (FP64, layout [n][lm]) and to global (fp32) for the force pass
+    double *cs = reinterpret_cast<double *>(Ys);
+#pragma unroll
+    for (int n = 0; n < NT; ++n)
+#pragma unroll
+        for (int k = 0; k < Sh::SLOTS; ++k)
+            if (lmk[k] < NLM) {
+                cs[n * NLM + lmk[k]] = acc[n][k];
+                O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)acc[n][k];
+            }
+    __syncwarp();
+    auto power = [&](int d) -> double {
+        const int pi = d / NL, l = d - pi * NL;
+        const int n = pair_n[pi], n2 = pair_n2[pi];
+        const double *c1 = cs + n * NLM + l * l, *c2 = cs + n2 * NLM + l * l;
+        double v = 0.0;
+        for (int m = 0; m < 2 * l + 1; ++m) v += c1[m] * c2[m];
+        return n != n2 ? v * 1.4142135623730951 : v;
+    };
+    // pass 1: |p| (FP64)
+    double nrm2 = 0.0;
+    for (int d = lane; d < DIM; d += 32) {
+        const double v = power(d);
+        nrm2 += v * v;
+    }
+    nrm2 = warp_sum(nrm2);
+    const double nrm = sqrt(nrm2);
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    // pass 2: q = p/|p|, delta = q - mu, delta . mu; operand rows hold split(delta)
+    const int K1 = P.K1;
+    __nv_bfloat16 *qs = O.qsplit + (size_t)site * K1;
+    double off = 0.0;
+    for (int d = lane; d < DIM; d += 32) {
+        const double mu = P.mu[d];
+        const double dl = power(d) * inv - mu;
+        off += dl * mu;
+        const float df = (float)dl;
+        O.q[(size_t)site * DIM + d] = df;
+        __nv_bfloat16 hi, lo;
+        bf16_split(df, hi, lo);
+        qs[d] = hi;
+        if (P.nsplit == 3) {
+            qs[DIM + d] = hi;
+            qs[2 * DIM + d] = lo;
+        }
+    }
+    off = warp_sum(off);
+    for (int d = P.nsplit * DIM + lane; d < K1; d += 32) qs[d] = __float2bfloat16_rn(0.f);
+    if (lane == 0) {
+        O.pnorm[site] = nrm;
+        O.qoff[site] = off;
+    }
+}
+
+// ===================== adjoint force / virial ================================
+
+template <int NS, int AMAX, int LMAX>
+struct ForceShape {
+    static constexpr int NL = LMAX + 1;
+    static constexpr int NLM = NL * NL;
+    static constexpr int NT = NS * AMAX;
+    static constexpr int DIM = NT * (NT + 1) / 2 * NL;
+    static constexpr int SLOTS = (NLM + 31) / 32;
+    static constexpr int TW = ((3 * AMAX + 3 * NL) + 3) / 4 * 4;
+    static constexpr int WARPS = 4;
+    static constexpr int BSTRIDE = NT * NT + 1;    // per-l stride of the B matrices (bank spread)
+    static constexpr int BAREA = (NL * BSTRIDE + 3) / 4 * 4;   // keeps gam 16-byte aligned
+    static constexpr int WARP_FLOATS = BAREA + NLM * NT;
+    static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
+};
+
+template <int NS, int AMAX, int LMAX>
+__global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
+    using Sh = ForceShape<NS, AMAX, LMAX>;
+    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, DIM = Sh::DIM;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ double vred[Sh::WARPS][6];
+    __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t < NT * (NT + 1) / 2; t += blockDim.x) {
+        int n = 0, rem = t;
+        while (rem >= NT - n) { rem -= NT - n; ++n; }
+        pair_n[t] = (unsigned char)n;
+        pair_n2[t] = (unsigned char)(n + rem);
+    }
+    if (lane < 6) vred[warp][lane] = 0.0;
+    __syncthreads();
+    float *Bm = smem + warp * Sh::WARP_FLOATS;   // [l][n][n2] (stride BSTRIDE per l)
+    float *gam = Bm + Sh::BAREA;                 // [lm][n]
+    const int site = blockIdx.x * Sh::WARPS + warp;
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    if (site < S.n_sites) {
+        const int row = S.site_row[site];
+        const int catom = S.site_atom[site];
+        const int64_t p0 = S.pstart[row];
+        const int np = (int)(S.pstart[row + 1] - p0);
+        // dE/dq = ksum mu + g0 + g_delta: ksum = sum_s kd_s (FP64, GEMM-1 epilogue),
+        // g0 = sum_s kcoef_s (q_s - mu) (FP64, per block), g_delta from GEMM 2;
+        // q = mu + delta. dE/dp = (dE/dq - (dE/dq . q) q) / |p|, all in FP64.
+        const float *g = I.g + (size_t)site * DIM;
+        const float *q = I.q + (size_t)site * DIM;
+        double ksum = 0.0;
+        for (int t = 0; t < I.n_etiles; ++t) ksum += I.kdsum[(size_t)site * I.n_etiles + t];
+        double dot = 0.0;
+        for (int d = lane; d < DIM; d += 32) {
+            const double mu = P.mu[d];
+            dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
+        }
+        dot = warp_sum(dot);
+        const double nrm = I.pnorm[site];
+        const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+        for (int d = lane; d < DIM; d += 32) {
+            const double mu = P.mu[d];
+            const double gd = ksum * mu + P.g0[d] + (double)g[d], qd = mu + (double)q[d];
+            const float h = (float)((gd - dot * qd) * inv);
+            const int pi = d / NL, l = d - pi * NL;
+            const int n = pair_n[pi], n2 = pair_n2[pi];
+            float *Bl = Bm + l * Sh::BSTRIDE;
+            if (n == n2) {
+                Bl[n * NT + n] = 2.f * h;
+            } else {
+                const float v = 1.41421356237309515f * h;
+                Bl[n * NT + n2] = v;
+                Bl[n2 * NT + n] = v;
+            }
+        }
+        __syncwarp();
+        // Gamma_{n,lm} = dE/dc_{n,lm} = sum_n2 B_l(n, n2) c_{n2,lm}
+        int lmk[Sh::SLOTS], lk[Sh::SLOTS];
+#pragma unroll
+        for (int k = 0; k < Sh::SLOTS; ++k) {
+            lmk[k] = lane + 32 * k;
+            int l = 0;
+            while ((l + 1) * (l + 1) <= lmk[k]) ++l;
+            lk[k] = l;
+        }
+        const float *cg = I.c + (size_t)site * NT * NLM;
+#pragma unroll
+        for (int k = 0; k < Sh::SLOTS; ++k) {
+            if (lmk[k] >= NLM) continue;
+            float cr[NT];
+#pragma unroll
+            for (int n2 = 0; n2 < NT; ++n2) cr[n2] = cg[n2 * NLM + lmk[k]];
+            const float *Bl = Bm + lk[k] * Sh::BSTRIDE;
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                float v = 0.f;
+#pragma unroll
+                for (int n2 = 0; n2 < NT; ++n2) v += Bl[n * NT + n2] * cr[n2];
+                gam[lmk[k] * NT + n] = v;
+            }
+        }
+        __syncwarp();
+        // pairs: lane per pair
+        double fs[3] = {0, 0, 0};
+        for (int pp = 1 + lane; pp < np; pp += 32) {
+            const int64_t p = p0 + pp;
+            const int j = S.nbr[p];
+            const int ja = fold_index(j, P.n_atoms);
+            const int s = zlookup(P, S.species[ja]);
+            const double X = S.xyz[3 * p], Yy = S.xyz[3 * p + 1], Z = S.xyz[3 * p + 2];
+            const float x = (float)X, y = (float)Yy, z = (float)Z;
+            const float r = sqrtf(x * x + y * y + z * z);
+            if (s < 0 || !(r < P.rcut[s]) || !(r > 0.f)) continue;
+            RadAng<AMAX, NL> ra;
+            table_eval<AMAX, NL, Sh::TW, true>(P.table + (size_t)s * (kTableIntervals + 1) * Sh::TW,
+                                               r, P.tab_h[s], P.tab_inv_h[s], ra);
+            const float ir = 1.f / r;
+            const float u[3] = {x * ir, y * ir, z * ir};
+            float C[LMAX + 1], Sn[LMAX + 1];
+            cos_sin_m<LMAX>(u[0], u[1], C, Sn);
+            float Q[LMAX + 1][LMAX + 2];
+            legendre_q<LMAX>(u[2], Q);
+            float T1 = 0.f, T2x = 0.f, T2y = 0.f, T2z = 0.f;
+            const int ch = s * AMAX;
+#pragma unroll
+            for (int l = 0; l <= LMAX; ++l) {
+                const float al = ra.a[l], dal = ra.da[l];
+#pragma unroll
+                for (int m = 0; m <= l; ++m) {
+                    // G = sum_n Gamma R_n, G' = sum_n Gamma dR_n for +m (C) and -m (S)
+                    const int lmp = l * l + l + m, lmn = l * l + l - m;
+                    float Gp = 0.f, dGp = 0.f, Gn = 0.f, dGn = 0.f;
+                    const float4 *gp = reinterpret_cast<const float4 *>(gam + lmp * NT + ch);
+#pragma unroll
+                    for (int qd = 0; qd < AMAX / 4; ++qd) {
+                        const float4 v = gp[qd];
+                        Gp += v.x * ra.R[4 * qd] + v.y * ra.R[4 * qd + 1] + v.z * ra.R[4 * qd + 2] +
+                              v.w * ra.R[4 * qd + 3];
+                        dGp += v.x * ra.dR[4 * qd] + v.y * ra.dR[4 * qd + 1] +
+                               v.z * ra.dR[4 * qd + 2] + v.w * ra.dR[4 * qd + 3];
+                    }
+                    const float f = cYn[l][m];
+                    const float Qlm = Q[l][m], Qlm1 = Q[l][m + 1];
+                    if (m == 0) {
+                        const float yv = f * Qlm;
+                        T1 += yv * (al * dGp + dal * Gp);
+                        T2z += al * Gp * f * Qlm1;
+                    } else {
+                        const float4 *gn = reinterpret_cast<const float4 *>(gam + lmn * NT + ch);
+#pragma unroll
+                        for (int qd = 0; qd < AMAX / 4; ++qd) {
+                            const float4 v = gn[qd];
+                            Gn += v.x * ra.R[4 * qd] + v.y * ra.R[4 * qd + 1] +
+                                  v.z * ra.R[4 * qd + 2] + v.w * ra.R[4 * qd + 3];
+                            dGn += v.x * ra.dR[4 * qd] + v.y * ra.dR[4 * qd + 1] +
+                                   v.z * ra.dR[4 * qd + 2] + v.w * ra.dR[4 * qd + 3];
+                        }
+                        const float yc = f * Qlm * C[m], ys = f * Qlm * Sn[m];
+                        T1 += yc * (al * dGp + dal * Gp) + ys * (al * dGn + dal * Gn);
+                        const float wc = al * Gp, wsn = al * Gn;
+                        const float fm = f * Qlm * (float)m;
+                        // grad of sqrt2 N Q C_m: (m C_{m-1}, -m S_{m-1}, Q' C_m)
+                        T2x += wc * fm * C[m - 1] + wsn * fm * Sn[m - 1];
+                        T2y += -wc * fm * Sn[m - 1] + wsn * fm * C[m - 1];
+                        T2z += (wc * C[m] + wsn * Sn[m]) * f * Qlm1;
+                    }
+                }
+            }
+            const float ut2 = u[0] * T2x + u[1] * T2y + u[2] * T2z;
+            // f_pair = -dE_i/dr_j = -(T1 u + (T2 - (u.T2) u)/r)
+            const float fx = -(T1 * u[0] + (T2x - ut2 * u[0]) * ir);
+            const float fy = -(T1 * u[1] + (T2y - ut2 * u[1]) * ir);
+            const float fz = -(T1 * u[2] + (T2z - ut2 * u[2]) * ir);
+            atomicAdd(&O.forces[3 * (size_t)ja], (double)fx);
+            atomicAdd(&O.forces[3 * (size_t)ja + 1], (double)fy);
+            atomicAdd(&O.forces[3 * (size_t)ja + 2], (double)fz);
+            fs[0] -= fx; fs[1] -= fy; fs[2] -= fz;
+            // virial += 1/2 (f x + x f), packed xx yy zz xy xz yz
+            vir[0] += (double)fx * X;
+            vir[1] += (double)fy * Yy;
+            vir[2] += (double)fz * Z;
+            vir[3] += 0.5 * ((double)fx * Yy + (double)fy * X);
+            vir[4] += 0.5 * ((double)fx * Z + (double)fz * X);
+            vir[5] += 0.5 * ((double)fy * Z + (double)fz * Yy);
+        }
+#pragma unroll
+        for (int qd = 0; qd < 3; ++qd) fs[qd] = warp_sum(fs[qd]);
+        if (lane == 0) {
+            atomicAdd(&O.forces[3 * (size_t)catom], fs[0]);
+            atomicAdd(&O.forces[3 * (size_t)catom + 1], fs[1]);
+            atomicAdd(&O.forces[3 * (size_t)catom + 2], fs[2]);
+            double e = 0.0;
+            for (int t = 0; t < I.n_etiles; ++t) e += I.epart[(size_t)site * I.n_etiles + t];
+            O.energies[catom] += I.delta2 * e;
+        }
+    }
+#pragma unroll
+    for (int qd = 0; qd < 6; ++qd) vir[qd] = warp_sum(vir[qd]);
+    if (lane == 0)
+        for (int qd = 0; qd < 6; ++qd) vred[warp][qd] = vir[qd];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < Sh::WARPS; ++w)
+            for (int qd = 0; qd < 6; ++qd) v[qd] += vred[w][qd];
+        double *o = O.vpart + (size_t)blockIdx.x * 9;
+        o[0] = v[0]; o[4] = v[1]; o[8] = v[2];
+        o[1] = o[3] = v[3];
+        o[2] = o[6] = v[4];
+        o[5] = o[7] = v[5];
+    }
+}
+
+__global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, double *out) {
+    const int q = threadIdx.y;   // 9 components
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += 32) s += vpart[(size_t)b * 9 + q];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[q] += s;
+}
+
+// ===================== launchers ============================================
+
+#define TGB_SOAP_SHAPES(X) X(1, 8, 8) X(2, 8, 8) X(1, 8, 6) X(2, 8, 6) X(1, 4, 4) X(2, 4, 4)
+
+bool soap_shape_supported(int ns, int amax, int lmax) {
+#define X(a, b, c) if (ns == a && amax == b && lmax == c) return true;
+    TGB_SOAP_SHAPES(X)
+#undef X
+    return false;
+}
+
+template <int NS, int AMAX, int LMAX>
+static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
+    using Sh = DescShape<NS, AMAX, LMAX>;
+    const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
+    static bool attr = false;
+    if (!attr) {
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
+    if (grid > 0) k_soap_expand<NS, AMAX, LMAX><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+template <int NS, int AMAX, int LMAX>
+static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
+                      int *nblk, cudaStream_t st) {
+    using Sh = ForceShape<NS, AMAX, LMAX>;
+    const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
+    static bool attr = false;
+    if (!attr) {
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
+    *nblk = grid;
+    if (grid > 0) k_soap_force<NS, AMAX, LMAX><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
+#define X(a, b, c) \
+    if (P.ns == a && P.amax == b && P.lmax == c) return expand_impl<a, b, c>(P, S, O, st);
+    TGB_SOAP_SHAPES(X)
+#undef X
+    set_error("unsupported SOAP shape: n_species %d alpha_max %d l_max %d", P.ns, P.amax, P.lmax);
+    return TG_ERR_ARG;
+}
+
+int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
+                      int *nblk, cudaStream_t st) {
+#define X(a, b, c) \
+    if (P.ns == a && P.amax == b && P.lmax == c) return force_impl<a, b, c>(P, S, I, O, nblk, st);
+    TGB_SOAP_SHAPES(X)
+#undef X
+    set_error("unsupported SOAP shape: n_species %d alpha_max %d l_max %d", P.ns, P.amax, P.lmax);
+    return TG_ERR_ARG;
+}
+
+int launch_virial_reduce(const double *vpart, int nblk, double *virial_out, cudaStream_t st) {
+    if (nblk <= 0) return TG_OK;
+    k_virial_reduce<<<1, dim3(32, 9), 0, st>>>(vpart, nblk, virial_out);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+}  // namespace tgb

@@ -1,0 +1,85 @@
+// tgb_soap.cuh -- SOAP descriptor and adjoint force kernels (interfaces).
+#pragma once
+
+#include "tgb_common.cuh"
+
+namespace tgb {
+
+constexpr int kMaxZ = 32;  // global species ids 1..31 map through zmap
+
+// Everything the descriptor and force kernels need about one block.
+struct SoapParams {
+    int ns, amax, lmax, ntot, nlm, dim;
+    int nsplit;           // 3: [hi | hi | lo] operand rows, 1: [hi]
+    int K1;               // row length (elements) of the split-q GEMM operand
+    int tw;               // table width: 2*amax + 2*(lmax+1) floats per node
+    int n_atoms;          // unit-cell atoms (folding of supercell indices)
+    signed char zmap[kMaxZ];   // global species id -> descriptor species (first match) or -1
+    float rcut[kMaxSpecies];
+    float tab_h[kMaxSpecies];  // node spacing (A)
+    float tab_inv_h[kMaxSpecies];
+    const float *table;        // [ns][kTableIntervals + 1][tw]
+    const float *self_R;       // [ns][amax]: central-atom contribution to c_{n,00}
+    const double *mu;          // [dim]: mean of the sparse set; the GEMMs see q - mu
+    const double *g0;          // [dim]: sum_s kcoef_s (q_s - mu), the K = 1 part of dE/dq
+};
+
+// Per-launch site addressing: site i reads CSR row site_row[i] of the pair
+// arrays and its results belong to atom site_atom[i].
+struct SiteArgs {
+    int n_sites;
+    const int *site_row;
+    const int *site_atom;
+    const int64_t *pstart;
+    const int *nbr;          // 0-based supercell index per pair
+    const double *xyz;       // (3, P) MIC vectors r_j - r_i
+    const int *species;      // global species id per unit-cell atom
+};
+
+struct DescOut {
+    __nv_bfloat16 *qsplit;   // [n_sites][K1]: bf16 split of delta = q - mu
+    float *q;                // [n_sites][dim]: delta = q - mu (fp32)
+    double *qoff;            // [n_sites]: delta . mu (FP64)
+    double *pnorm;           // [n_sites]
+    float *c;                // [n_sites][ntot][nlm]
+};
+
+struct ForceIn {
+    const float *g;          // sum_s (kd_s - kcoef_s)(Q_s - mu), [n_sites][dim] (GEMM 2)
+    const float *q;          // delta = q - mu
+    const double *pnorm;
+    const float *c;
+    const double *epart;     // [n_sites][n_etiles]: sum_s alpha_s K^zeta per tile
+    const double *kdsum;     // [n_sites][n_etiles]: sum_s kd_s per tile
+    int n_etiles;
+    double delta2;
+};
+
+struct ForceOut {
+    double *forces;          // (3, n_atoms), accumulated
+    double *energies;        // (n_atoms), accumulated
+    double *vpart;           // [gridDim][9]
+    unsigned *err;
+};
+
+// Host-side construction of the FP64 tables on the device.
+struct SoapHostHypers {
+    int ns, lmax, radial_enhancement, central_species;
+    int alpha_max[kMaxSpecies], species_z[kMaxSpecies];
+    double rcut_hard[kMaxSpecies], rcut_soft[kMaxSpecies], nf[kMaxSpecies],
+        global_scaling[kMaxSpecies], sigma_r[kMaxSpecies], sigma_r_scaling[kMaxSpecies],
+        sigma_t[kMaxSpecies], sigma_t_scaling[kMaxSpecies], amplitude_scaling[kMaxSpecies],
+        central_weight[kMaxSpecies];
+};
+
+// Builds table and self_R (device buffers owned by the caller) in FP64 on the GPU.
+int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st);
+
+// Launchers; return TG_ERR_ARG for unsupported (ns, amax, lmax).
+bool soap_shape_supported(int ns, int amax, int lmax);
+int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st);
+int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
+                      int *n_vpart_blocks, cudaStream_t st);
+int launch_virial_reduce(const double *vpart, int nblk, double *virial_out, cudaStream_t st);
+
+}  // namespace tgb
