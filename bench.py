@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""SOAP-GAP E+F atom-steps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ch32k] [--precision bf16x3|bf16]
+
+One step is one NVE velocity-Verlet MD step of the workload through the
+device-resident engine: neighbour list rebuild, every soap_turbo block
+(descriptor, tcgen05 GAP GEMMs, adjoint forces/virial), wrap_pbc,
+remove_cm_vel and velocity_verlet, replayed from a CUDA graph. ``value`` is
+atoms x steps / device time (CUDA events on the engine's stream, max over
+ranks). ``e2e`` is the same metric through the public C-ABI with host buffers:
+each step uploads the positions from pinned host memory and reads energies,
+forces and virial back. N > 1 runs one independent replica per GPU (weak
+scaling; no data-path collective). ``--impl reference`` times the FP64 CPU port
+of the reference path on the host cores (the Fortran reference cannot be built
+here).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from turbogap_b200 import synth  # noqa: E402
+from turbogap_b200.workloads import WORKLOADS, build_blocks  # noqa: E402
+
+METRIC = "SOAP-GAP E+F atom-steps/s on 1 B200 (plain bf16x3 form)"
+UNIT = "atom-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ch32k", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "bf16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local, dist
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gemm_flops_per_step(blocks, structure):
+    """Algorithmic FLOPs of the two GAP GEMMs per step: 4 D M per central atom."""
+    tot = 0
+    for b in blocks:
+        h = b.hypers
+        zs = set(h.species_z) if h.central_species == 0 else {h.species_z[h.central_species - 1]}
+        nb = int(np.isin(structure.species, list(zs)).sum())
+        tot += 4 * h.dim * b.n_sparse * nb
+    return tot
+
+
+# ------------------------------------------------------------------ CPU (oracle)
+def oracle_blocks(w):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _util import oracle_descriptors
+    return build_blocks(w, lambda h, st: oracle_descriptors(st, h)[0])
+
+
+def time_oracle_sample(O, st, blocks, n_sites):
+    t0 = time.perf_counter()
+    O.evaluate(st.positions, st.species, st.box, blocks, site_range=(0, n_sites))
+    return time.perf_counter() - t0
+
+
+def calibrate_sample(O, st, blocks, target_s):
+    t = time_oracle_sample(O, st, blocks, 128)
+    per_site = t / 128.0
+    return int(max(64, min(st.n, round(target_s / per_site)))), per_site
+
+
+def cpu_baseline_leg(w, st, target_s=15.0):
+    import oracle as O
+    blocks = oracle_blocks(w)
+    n, per = calibrate_sample(O, st, blocks, target_s)
+    t = time_oracle_sample(O, st, blocks, n)
+    cores = os.cpu_count()
+    return {"value": n / t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"E+F of sites 0..{n - 1} of the {w.name} structure (the share of one "
+                      f"MPI rank, all blocks), FP64 oracle port, {cores} OpenMP threads, {t:.1f} s"}
+
+
+def run_reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle as O
+    w = WORKLOADS[a.workload]
+    st = w.structure()
+    blocks = oracle_blocks(w)
+    n, _ = calibrate_sample(O, st, blocks, 2.0)
+    for _ in range(a.warmup):
+        time_oracle_sample(O, st, blocks, n)
+    t = 0.0
+    for _ in range(a.steps):
+        t += time_oracle_sample(O, st, blocks, n)
+    value = n * a.steps / t
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{w.name}: {w.description}", "sample_sites": n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"each step: E+F of sites 0..{n - 1} of {w.name} (one MPI "
+                                   f"rank's share), FP64 port of the reference CPU path; the "
+                                   f"Fortran reference cannot be built here"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU
+def run_ours(a):
+    world, rank, local, dist = dist_setup(a.gpus)
+    import torch
+    from turbogap_b200 import backend as B
+    from turbogap_b200.workloads import descriptors_gpu
+
+    torch.cuda.set_device(local)
+    B.gpu_context_init(rank, local)
+    w = WORKLOADS[a.workload]
+    prec = B.TG_PREC_BF16X3 if a.precision == "bf16x3" else B.TG_PREC_BF16
+    blocks = build_blocks(w, lambda h, st: descriptors_gpu(B, h, st, key=900))
+    keys = []
+    for i, b in enumerate(blocks):
+        B.soap_backend_begin(b, key=i + 1, precision=prec)
+        keys.append(i + 1)
+    st = w.structure(replica=rank)
+    eng = B.Engine(st.positions, st.species, st.masses, st.box, keys)
+    eng.set_state(st.positions, synth.maxwell_velocities(st.masses, w.temperature, w.seed))
+    n_pairs = eng.n_pairs()
+    ext = torch.cuda.ExternalStream(eng.stream())
+
+    # warm-up: first step eager, then the step graph is captured and replayed
+    eng.md(max(a.warmup, 3), w.dt, energies=False)
+    kernels_per_step = eng.graph_kernels()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        eng.md(a.steps, w.dt, energies=False)
+        e1.record(ext)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    t_dev = e0.elapsed_time(e1) / 1e3
+    t_max = max_over_ranks(t_dev, dist)
+    value = st.n * a.steps * world / t_max
+    clocks = clk.summary()
+
+    # per-pass CUDA-event profile (eager steps on the same stream)
+    prof = eng.profile(a.profile_steps, w.dt)
+    peaks, peak_kind = measured_peaks()
+    flops = gemm_flops_per_step(blocks, st)
+    gemm_s = (prof["gemm1"] + prof["gemm2"]) / 1e3
+    achieved = flops / gemm_s / 1e12
+    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+    nsplit = 3 if a.precision == "bf16x3" else 1
+
+    # e2e through the C-ABI with pinned host buffers
+    n = st.n
+    pos_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    en_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    f_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    v_h = torch.empty(9, dtype=torch.float64, pin_memory=True)
+    p_now, _, _ = eng.get_state()
+    pos_h.copy_(torch.from_numpy(p_now))
+    lib = B.lib()
+    h = eng.handle
+    for _ in range(2):
+        B.check(lib.tg_engine_set_state(h, C.c_void_p(pos_h.data_ptr()), None))
+        B.check(lib.tg_engine_compute(h, C.c_void_p(en_h.data_ptr()), C.c_void_p(f_h.data_ptr()),
+                                      C.c_void_p(v_h.data_ptr())))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(ext)
+    for _ in range(a.e2e_steps):
+        B.check(lib.tg_engine_set_state(h, C.c_void_p(pos_h.data_ptr()), None))
+        B.check(lib.tg_engine_compute(h, C.c_void_p(en_h.data_ptr()), C.c_void_p(f_h.data_ptr()),
+                                      C.c_void_p(v_h.data_ptr())))
+    e3.record(ext)
+    e3.synchronize()
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, dist)
+    e2e = {"value": n * a.e2e_steps * world / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": int(pos_h.numel() * 8),
+           "d2h_bytes_per_step": int((en_h.numel() + f_h.numel() + v_h.numel()) * 8),
+           "api": "tg_engine_set_state + tg_engine_compute (host positions in, host energies/"
+                  "forces/virial out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_leg(w, w.structure())
+        except Exception as ex:  # keep the bench line even if the oracle cannot run
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic",
+        "config": {"workload": f"{w.name}: {w.description}", "atoms_per_gpu": st.n,
+                   "pairs": n_pairs, "dt_fs": w.dt, "md": "NVE velocity-Verlet, neighbour list "
+                   "rebuilt every step", "precision": a.precision,
+                   "l2": "inputs larger than L2 (GEMM operands and kd scratch > 126 MB)",
+                   "parallelism": f"{world} independent replica(s), one per GPU"},
+        "roofline": {"kernel": "tcgen05 GAP GEMMs (kernel K = q.Q_s^T and dE/dq)",
+                     "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"{peak_kind} bf16 dense (sustained)",
+                     "algorithmic_flops_per_step": flops,
+                     "issue_rate_tflops": achieved * nsplit,
+                     "ms_per_step_by_pass": prof},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": kernels_per_step * a.steps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -170,6 +170,14 @@ int tg_engine_stream(tg_engine *e, void **stream);
 /* Evaluate energies+forces on the device without copying results out; the
  * bench uses this for device-resident timing. */
 int tg_engine_compute_device(tg_engine *e);
+/* n_steps MD steps launched eagerly with CUDA events between the passes of each
+ * step on the engine's stream; ms_per_pass[6] receives the mean milliseconds per
+ * step of: neighbour list, descriptor, GEMM 1, GEMM 2, forces+virial, integrate
+ * (every block summed into its pass). *n_passes = 6. */
+int tg_engine_profile(tg_engine *e, int32_t n_steps, double dt, double *ms_per_pass,
+                      int32_t *n_passes);
+/* Kernel launches in one graph-captured MD step (0 before the first graph exists). */
+int tg_engine_graph_kernels(tg_engine *e, int32_t *n_kernels);
 
 #ifdef __cplusplus
 }

@@ -88,6 +88,10 @@ def lib():
         L.orc_evaluate.argtypes = [C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int, C.POINTER(_Block),
                                    C.c_void_p, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp,
                                    C.POINTER(C.c_int64)]
+        L.orc_evaluate_range.argtypes = [C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int,
+                                         C.POINTER(_Block), C.c_void_p, C.c_int, C.c_double,
+                                         C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
+                                         C.POINTER(C.c_int64)]
     return _lib
 
 
@@ -290,11 +294,13 @@ def wrap_pbc(positions, a, b, c):
     lib().orc_wrap_pbc(positions.shape[0], positions, _f64(a), _f64(b), _f64(c))
 
 
-def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max_gbytes=1.0):
+def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max_gbytes=1.0,
+             site_range=None):
     """Energies (n), forces (n,3), virial (3,3) of one periodic structure.
 
     ``blocks``: sequence of objects with ``hypers`` (attributes as HypersC),
-    ``Qs`` (M, D), ``alphas`` (M), ``delta``, ``zeta``."""
+    ``Qs`` (M, D), ``alphas`` (M), ``delta``, ``zeta``. ``site_range`` = (beg, end)
+    restricts the work to those sites (one MPI rank's share)."""
     n = positions.shape[0]
     box = _f64(box)
     keep = []
@@ -315,11 +321,13 @@ def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max
     f = np.zeros((n, 3))
     vir = np.zeros(9)
     npairs = C.c_int64(0)
-    rc = lib().orc_evaluate(n, _f64(positions), _i32(species), _f64(box[0]), _f64(box[1]),
-                            _f64(box[2]), len(blocks), arr,
-                            e0a.ctypes.data if e0a is not None else None,
-                            len(e0a) if e0a is not None else 0, float(neighbors_buffer),
-                            float(max_gbytes), en, f, vir, C.byref(npairs))
+    beg, end = site_range if site_range is not None else (0, n)
+    rc = lib().orc_evaluate_range(n, _f64(positions), _i32(species), _f64(box[0]), _f64(box[1]),
+                                  _f64(box[2]), len(blocks), arr,
+                                  e0a.ctypes.data if e0a is not None else None,
+                                  len(e0a) if e0a is not None else 0, float(neighbors_buffer),
+                                  float(max_gbytes), int(beg), int(end), en, f, vir,
+                                  C.byref(npairs))
     if rc != 0:
         raise RuntimeError(f"oracle evaluate failed: {rc}")
     return en, f, vir.reshape(3, 3).T, int(npairs.value)

@@ -50,6 +50,53 @@ inline void cross3(const double *a, const double *b, double *c) {
     c[2] = a[0] * b[1] - a[1] * b[0];
 }
 
+// Cache-blocked FP64 GEMMs standing in for BLAS dgemm (the reference links a
+// system BLAS). AVX2/FMA clones are selected at run time; OpenMP over rows.
+// C[n x m] = A[n x k] . B[m x k]^T (all row-major)
+__attribute__((target_clones("avx2,fma", "default"), optimize("fp-contract=fast")))
+void gemm_nt_blocked(int n, int m, int k, const double *A, const double *B, double *C) {
+    const int BI = 16, BS = 96;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i0 = 0; i0 < n; i0 += BI) {
+        const int i1 = std::min(n, i0 + BI);
+        for (int s0 = 0; s0 < m; s0 += BS) {
+            const int s1 = std::min(m, s0 + BS);
+            for (int i = i0; i < i1; ++i) {
+                const double *a = A + (size_t)i * k;
+                for (int s = s0; s < s1; ++s) {
+                    const double *b = B + (size_t)s * k;
+                    double acc = 0.0;
+#pragma omp simd reduction(+ : acc)
+                    for (int d = 0; d < k; ++d) acc += a[d] * b[d];
+                    C[(size_t)i * m + s] = acc;
+                }
+            }
+        }
+    }
+}
+
+// C[n x m] = A[n x k] . B[k x m] (all row-major), C zeroed by the caller.
+__attribute__((target_clones("avx2,fma", "default"), optimize("fp-contract=fast")))
+void gemm_nn_blocked(int n, int m, int k, const double *A, const double *B, double *C) {
+    const int BI = 16, BS = 64;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i0 = 0; i0 < n; i0 += BI) {
+        const int i1 = std::min(n, i0 + BI);
+        for (int s0 = 0; s0 < k; s0 += BS) {
+            const int s1 = std::min(k, s0 + BS);
+            for (int i = i0; i < i1; ++i) {
+                double *c = C + (size_t)i * m;
+                for (int s = s0; s < s1; ++s) {
+                    const double f = A[(size_t)i * k + s];
+                    const double *b = B + (size_t)s * m;
+#pragma omp simd
+                    for (int d = 0; d < m; ++d) c[d] += f * b[d];
+                }
+            }
+        }
+    }
+}
+
 inline bool box_is_orthorhombic(const double *a, const double *b, const double *c) {
     const double tol = 1.e-6;
     return std::fabs(a[1]) < tol && std::fabs(a[2]) < tol && std::fabs(b[0]) < tol &&
@@ -695,16 +742,7 @@ void orc_soap_energy_and_forces(int n_soap, int n_sites, const double *soap,
     };
     // kernels(n_sites, n_sparse) = soap^T Qs  (dgemm 't','n'), kept row-major per site here
     std::vector<double> K((size_t)n_sites * n_sparse);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < n_sites; ++i) {
-        const double *qi = soap + (size_t)i * n_soap;
-        for (int s = 0; s < n_sparse; ++s) {
-            const double *qs = Qs + (size_t)s * n_soap;
-            double acc = 0.0;
-            for (int d = 0; d < n_soap; ++d) acc += qi[d] * qs[d];
-            K[(size_t)i * n_sparse + s] = acc;
-        }
-    }
+    gemm_nt_blocked(n_sites, n_sparse, n_soap, soap, Qs, K.data());
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n_sites; ++i) {
         double e = 0.0;
@@ -719,23 +757,16 @@ void orc_soap_energy_and_forces(int n_soap, int n_sites, const double *soap,
     // kernels_der = K^(zeta-1) (alphas folded in); Qss = -zeta delta^2 kernels_der Qs^T
     std::vector<double> Qss((size_t)n_sites * n_soap, 0.0);
     const double pref = -zeta * delta * delta;
-#pragma omp parallel
-    {
-        std::vector<double> kd(n_sparse);
-#pragma omp for schedule(static)
-        for (int i = 0; i < n_sites; ++i) {
-            for (int s = 0; s < n_sparse; ++s) {
-                const double k = K[(size_t)i * n_sparse + s];
-                kd[s] = (is_zeta_int ? ipow(k, zeta_int - 1) : std::pow(k, zeta - 1.0)) * alphas[s];
-            }
-            double *out = &Qss[(size_t)i * n_soap];
-            for (int s = 0; s < n_sparse; ++s) {
-                const double f = pref * kd[s];
-                const double *qs = Qs + (size_t)s * n_soap;
-                for (int d = 0; d < n_soap; ++d) out[d] += f * qs[d];
-            }
+    // kernels_der (alphas folded in, times -zeta delta^2), then Qss = kd Qs (dgemm 'n','t')
+    std::vector<double> KD((size_t)n_sites * n_sparse);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_sites; ++i)
+        for (int s = 0; s < n_sparse; ++s) {
+            const double k = K[(size_t)i * n_sparse + s];
+            KD[(size_t)i * n_sparse + s] =
+                pref * (is_zeta_int ? ipow(k, zeta_int - 1) : std::pow(k, zeta - 1.0)) * alphas[s];
         }
-    }
+    gemm_nn_blocked(n_sites, n_soap, n_sparse, KD.data(), Qs, Qss.data());
     // pair loop (gap.f90:206-224); each pair's force computed in parallel, then
     // accumulated in the reference's serial order.
     std::vector<int64_t> start(n_sites + 1, 0);
@@ -967,11 +998,33 @@ void orc_wrap_pbc(int n, double *positions, const double *a, const double *b, co
 
 // turbogap.f90:896-997 + 1253-1378 + 1941/2009: one structure, every block,
 // memory-budget batches, summed into totals; e0 by species.
+int orc_evaluate_range(int n_sites, const double *positions, const int *species,
+                       const double *a, const double *b, const double *c, int n_blocks,
+                       const orc_gap_block *blocks, const double *e0_by_species,
+                       int n_species_total, double neighbors_buffer, double max_gbytes,
+                       int site_beg, int site_end, double *energies, double *forces,
+                       double *virial, int64_t *n_pairs_out);
+
 int orc_evaluate(int n_sites, const double *positions, const int *species, const double *a,
                  const double *b, const double *c, int n_blocks, const orc_gap_block *blocks,
                  const double *e0_by_species, int n_species_total, double neighbors_buffer,
                  double max_gbytes, double *energies, double *forces, double *virial,
                  int64_t *n_pairs_out) {
+    return orc_evaluate_range(n_sites, positions, species, a, b, c, n_blocks, blocks,
+                              e0_by_species, n_species_total, neighbors_buffer, max_gbytes, 0,
+                              n_sites, energies, forces, virial, n_pairs_out);
+}
+
+// The share of one MPI rank (turbogap.f90:930-942): neighbour lists and SOAP work
+// for sites site_beg..site_end-1 only (do_list), forces from those sites' energies.
+int orc_evaluate_range(int n_sites, const double *positions, const int *species,
+                       const double *a, const double *b, const double *c, int n_blocks,
+                       const orc_gap_block *blocks, const double *e0_by_species,
+                       int n_species_total, double neighbors_buffer, double max_gbytes,
+                       int site_beg, int site_end, double *energies, double *forces,
+                       double *virial, int64_t *n_pairs_out) {
+    if (site_beg < 0) site_beg = 0;
+    if (site_end > n_sites || site_end < 0) site_end = n_sites;
     double rcut_max = 0.0;
     for (int b = 0; b < n_blocks; ++b)
         for (int s = 0; s < blocks[b].hypers.n_species; ++s)
@@ -990,7 +1043,8 @@ int orc_evaluate(int n_sites, const double *positions, const int *species, const
         B[q] = b[q] * indices[1];
         C[q] = c[q] * indices[2];
     }
-    std::vector<int> do_list(n_sites, 1), n_neigh(n_sites);
+    std::vector<int> do_list(n_sites, 0), n_neigh(n_sites);
+    for (int i = site_beg; i < site_end; ++i) do_list[i] = 1;
     int64_t cap = (int64_t)n_sites * 64;
     std::vector<int> nl, nspec;
     std::vector<double> rjs, th, ph, xyz;
@@ -1023,12 +1077,14 @@ int orc_evaluate(int n_sites, const double *positions, const int *species, const
         double brc = 0.0;
         for (int s = 0; s < h->n_species; ++s) brc = std::max(brc, h->rcut_hard[s]);
         const int nmax = orc_soap_n_tot(h), dim = orc_soap_dim(h);
-        const int nch = orc_atom_pair_batches(n_sites, n_neigh.data(), rjs.data(), brc, h->l_max,
-                                              nmax, dim, h->n_species, max_gbytes, ib.data(),
-                                              ie.data(), jb.data(), je.data());
+        const int nr = site_end - site_beg;
+        const int64_t p_off = pstart[site_beg];
+        const int nch = orc_atom_pair_batches(nr, n_neigh.data() + site_beg, rjs.data() + p_off, brc,
+                                              h->l_max, nmax, dim, h->n_species, max_gbytes,
+                                              ib.data(), ie.data(), jb.data(), je.data());
         for (int ch = 0; ch < nch; ++ch) {
-            const int i0 = ib[ch] - 1, i1 = ie[ch];
-            const int64_t j0 = jb[ch] - 1;
+            const int i0 = site_beg + ib[ch] - 1, i1 = site_beg + ie[ch];
+            const int64_t j0 = p_off + jb[ch] - 1;
             std::fill(te.begin(), te.end(), 0.0);
             std::fill(tf.begin(), tf.end(), 0.0);
             double tv[9];

@@ -160,6 +160,15 @@ int orc_evaluate(int n_sites, const double *positions, const int *species,
                  double *energies, double *forces, double *virial,
                  int64_t *n_pairs_out);
 
+/* As orc_evaluate for the sites site_beg..site_end-1 only (0-based): the work one
+ * MPI rank owns in the reference (turbogap.f90:930-942). */
+int orc_evaluate_range(int n_sites, const double *positions, const int *species,
+                       const double *a, const double *b, const double *c, int n_blocks,
+                       const orc_gap_block *blocks, const double *e0_by_species,
+                       int n_species_total, double neighbors_buffer, double max_gbytes,
+                       int site_beg, int site_end, double *energies, double *forces,
+                       double *virial, int64_t *n_pairs_out);
+
 int orc_set_threads(int n);
 
 #ifdef __cplusplus

@@ -75,6 +75,8 @@ SIGNATURES = [
     ("tg_engine_n_pairs", C.c_int, [_vp, C.POINTER(C.c_int64)]),
     ("tg_engine_stream", C.c_int, [_vp, C.POINTER(_vp)]),
     ("tg_engine_compute_device", C.c_int, [_vp]),
+    ("tg_engine_profile", C.c_int, [_vp, C.c_int32, C.c_double, dp, C.POINTER(C.c_int32)]),
+    ("tg_engine_graph_kernels", C.c_int, [_vp, C.POINTER(C.c_int32)]),
     ("tgx_gemm_bf16_tn", C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16p, u16p, f32p]),
 ]
 

@@ -230,12 +230,34 @@ class Engine:
     def compute_device(self):
         check(lib().tg_engine_compute_device(self._h))
 
-    def md(self, n_steps: int, dt: float):
-        """n_steps NVE velocity-Verlet steps; returns (E_pot, E_kin) after them."""
+    def md(self, n_steps: int, dt: float, energies: bool = True):
+        """n_steps NVE velocity-Verlet steps; returns (E_pot, E_kin) after them
+        (None when ``energies`` is False: nothing is read back)."""
+        if not energies:
+            check(lib().tg_engine_md(self._h, int(n_steps), float(dt), None, None))
+            return None
         ep = C.c_double(0.0)
         ek = C.c_double(0.0)
         check(lib().tg_engine_md(self._h, int(n_steps), float(dt), C.byref(ep), C.byref(ek)))
         return float(ep.value), float(ek.value)
+
+    def graph_kernels(self) -> int:
+        n = C.c_int32(0)
+        check(lib().tg_engine_graph_kernels(self._h, C.byref(n)))
+        return int(n.value)
+
+    @property
+    def handle(self):
+        return self._h
+
+    PASSES = ("neighbors", "descriptor", "gemm1", "gemm2", "forces", "integrate")
+
+    def profile(self, n_steps: int, dt: float) -> dict:
+        """Mean ms per step of each pass over n_steps eager MD steps (CUDA events)."""
+        ms = np.zeros(8)
+        npass = C.c_int32(0)
+        check(lib().tg_engine_profile(self._h, int(n_steps), float(dt), ms, C.byref(npass)))
+        return {k: float(ms[i]) for i, k in enumerate(self.PASSES)}
 
     def get_state(self):
         p = np.zeros((self.n, 3))

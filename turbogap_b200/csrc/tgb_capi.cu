@@ -170,14 +170,56 @@ __global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad, dou
 
 }  // namespace
 
+// Optional CUDA-event log of the passes of a step: mark(pass) records an event
+// on the stream; the time since the previous mark is booked to that pass.
+enum Pass { PASS_NEIGH = 0, PASS_DESC, PASS_GEMM1, PASS_GEMM2, PASS_FORCE, PASS_INTEGRATE, N_PASS };
+
+struct EventLog {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> pass;
+    size_t used = 0;
+    int mark(int p, cudaStream_t st) {
+        if (used == ev.size()) {
+            cudaEvent_t e;
+            TGB_CUDA(cudaEventCreate(&e));
+            ev.push_back(e);
+            pass.push_back(p);
+        }
+        pass[used] = p;
+        TGB_CUDA(cudaEventRecord(ev[used], st));
+        ++used;
+        return TG_OK;
+    }
+    // accumulate ms per pass over the recorded marks (stream must be synchronised)
+    int collect(double *ms) {
+        for (size_t i = 1; i < used; ++i) {
+            float t = 0.f;
+            TGB_CUDA(cudaEventElapsedTime(&t, ev[i - 1], ev[i]));
+            if (pass[i] >= 0) ms[pass[i]] += t;
+        }
+        used = 0;
+        return TG_OK;
+    }
+    ~EventLog() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+#define TGB_MARK(log, p, st)                     \
+    do {                                         \
+        if (log) TGB_TRY((log)->mark((p), (st))); \
+    } while (0)
+
 // Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces.
 int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
-                   double *energies, double *virial, unsigned *err, cudaStream_t st) {
+                   double *energies, double *virial, unsigned *err, cudaStream_t st,
+                   EventLog *log = nullptr) {
     if (S.n_sites <= 0) return TG_OK;
     TGB_TRY(w.ensure(b, S.n_sites));
     const SoapParams P = b.params(n_atoms);
     DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
     TGB_TRY(launch_soap_expand(P, S, O, st));
+    TGB_MARK(log, PASS_DESC, st);
     GemmEpi e1{};
     e1.mode = EPI_GAP_KERNEL;
     e1.rows = S.n_sites;
@@ -195,6 +237,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
     TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st));
+    TGB_MARK(log, PASS_GEMM1, st);
     GemmEpi e2{};
     e2.mode = EPI_STORE_F32;
     e2.rows = S.n_sites;
@@ -202,11 +245,13 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.out = w.g.p;
     e2.ldo = b.dim;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
+    TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_tiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
     int nblk = 0;
     TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
+    TGB_MARK(log, PASS_FORCE, st);
     return TG_OK;
 }
 
@@ -377,7 +422,7 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     b->K1 = round_up(b->nsplit * b->dim, kGemmBK);
     b->K2 = b->nsplit * b->Mpad;
     b->n_tiles = gemm_n_tiles(b->Mpad);
-    b->tw = ((3 * b->amax + 3 * (b->lmax + 1)) + 3) / 4 * 4;
+    b->tw = table_width(b->amax, b->lmax);
     b->delta = delta;
     b->rcut_max = 0.0;
     for (int s = 0; s < hh.ns; ++s) b->rcut_max = std::max(b->rcut_max, hh.rcut_hard[s]);
@@ -831,29 +876,34 @@ struct Engine {
         if (st) cudaStreamDestroy(st);
     }
 
-    int compute_ef() {
+    EventLog prof;
+
+    int compute_ef(EventLog *log = nullptr) {
+        TGB_MARK(log, -1, st);
         const double *p = pos.p;
         if (nsc > n) {
             TGB_TRY(launch_supercell(n, pos.p, abc.p, indices, pos_sc.p, st));
             p = pos_sc.p;
         }
         TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        TGB_MARK(log, PASS_NEIGH, st);
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
-            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
+            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log));
         }
         return TG_OK;
     }
 
-    int md_step(double dt, bool first) {
-        TGB_TRY(compute_ef());
+    int md_step(double dt, bool first, EventLog *log = nullptr) {
+        TGB_TRY(compute_ef(log));
         TGB_TRY(launch_wrap(n, pos.p, box_prim, st));
         TGB_TRY(launch_remove_cm(n, vel.p, mass.p, acc4.p, st));
         TGB_TRY(launch_velocity_verlet(n, pos.p, pos_prev.p, vel.p, f.p, f_prev.p, mass.p, dt,
                                        first ? dt : dt_prev, first ? 1 : 0, st));
+        TGB_MARK(log, PASS_INTEGRATE, st);
         return TG_OK;
     }
 };
@@ -1080,6 +1130,50 @@ int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {
     Engine &E = eh->e;
     TGB_CUDA(cudaMemcpyAsync(n_pairs, E.nl.pstart + E.n, sizeof(int64_t), cudaMemcpyDeviceToHost, E.st));
     TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+int tg_engine_profile(tg_engine *eh, int32_t n_steps, double dt, double *ms_per_pass,
+                      int32_t *n_passes) {
+    TGB_CHECK(eh && ms_per_pass && n_steps >= 1, TG_ERR_ARG, "bad profile arguments");
+    Engine &E = eh->e;
+    double acc[N_PASS] = {0};
+    for (int s = 0; s < n_steps; ++s) {
+        const bool first = E.first_step;
+        TGB_TRY(E.md_step(dt, first, &E.prof));
+        E.first_step = false;
+        E.dt_prev = dt;
+        TGB_CUDA(cudaStreamSynchronize(E.st));
+        TGB_TRY(E.prof.collect(acc));
+    }
+    for (int p = 0; p < N_PASS; ++p) ms_per_pass[p] = acc[p] / n_steps;
+    if (n_passes) *n_passes = N_PASS;
+    return engine_errors(E);
+}
+
+int tg_engine_graph_kernels(tg_engine *eh, int32_t *n_kernels) {
+    TGB_CHECK(eh && n_kernels, TG_ERR_ARG, "null argument");
+    Engine &E = eh->e;
+    *n_kernels = 0;
+    if (!E.graph) return TG_OK;
+    cudaGraph_t g;
+    TGB_CUDA(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+    int r = E.md_step(E.graph_dt, false);
+    cudaError_t ce = cudaStreamEndCapture(E.st, &g);
+    TGB_TRY(r);
+    TGB_CUDA(ce);
+    size_t n = 0;
+    ce = cudaGraphGetNodes(g, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (ce == cudaSuccess && n) ce = cudaGraphGetNodes(g, nodes.data(), &n);
+    int k = 0;
+    for (size_t i = 0; ce == cudaSuccess && i < n; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    cudaGraphDestroy(g);
+    TGB_CUDA(ce);
+    *n_kernels = k;
     return TG_OK;
 }
 

@@ -141,36 +141,49 @@ __device__ __forceinline__ float ipow_f(float x, int e) {
 constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK, STAGES = kGemmStages;
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
 constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256;
+constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent: CTA b processes tiles b, b + gridDim.x, ... (column tile fastest,
+// so concurrently resident CTAs share A rows in L2). Stage counters of the
+// shared-memory ring run across tiles; accumulator it % 2 is reused every
+// second tile once the epilogue has released it.
 __global__ void __launch_bounds__(192, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-              int num_kb, int n_tiles_n, GemmEpi ep, unsigned *err) {
+              int num_kb, int n_tiles_m, int n_tiles_n, GemmEpi ep, unsigned *err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
     const uint32_t sA = base, sB = base + STAGES * A_BYTES;
-    const uint32_t bars = sB + STAGES * B_BYTES;   // full[STAGES], empty[STAGES], acc
-    const uint32_t full0 = bars, empty0 = bars + 8 * STAGES, accb = bars + 16 * STAGES;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + (bars - base) + 16 * STAGES + 8);
-    const uint32_t slot_addr = bars + 16 * STAGES + 8;
+    // barriers: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], then the TMEM slot
+    const uint32_t bars = sB + STAGES * B_BYTES;
+    const uint32_t full0 = bars, empty0 = bars + 8 * STAGES;
+    const uint32_t accf0 = bars + 16 * STAGES, acce0 = accf0 + 16;
+    const uint32_t slot_addr = acce0 + 16;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + (slot_addr - base));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile_m = blockIdx.x / n_tiles_n, tile_n = blockIdx.x % n_tiles_n;
-    const int m0 = tile_m * BM, n0 = tile_n * BN;
+    const int n_tiles = n_tiles_m * n_tiles_n;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
-        mbar_init(accb, 1);
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(accf0 + 8 * a, 1);   // tcgen05.commit of the last k-block
+            mbar_init(acce0 + 8 * a, 4);   // one arrive per epilogue warp
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot_addr),
-                     "r"((uint32_t)BN)
+                     "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -181,99 +194,140 @@ __global__ void __launch_bounds__(192, 1)
 
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
-        int issued = 0;
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) {
-                atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_TMA);
-                break;
+        int g = 0;   // k-blocks issued so far (all tiles)
+        bool ok = true;
+        for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+            const int m0 = (t / n_tiles_n) * BM, n0 = (t % n_tiles_n) * BN;
+            for (int kb = 0; kb < num_kb; ++kb, ++g) {
+                const int s = g % STAGES;
+                const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) {
+                    atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_TMA);
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
+                tma_load_2d(sA + s * A_BYTES, &tmA, kb * BK, m0, full0 + 8 * s);
+                tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
             }
-            mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
-            tma_load_2d(sA + s * A_BYTES, &tmA, kb * BK, m0, full0 + 8 * s);
-            tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
-            issued = kb + 1;
         }
         // Drain: the last load of every stage has landed before the CTA may exit
         // (already true on the normal path, where the MMA consumed them).
-        for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
-            (void)mbar_wait(full0 + 8 * (kb % STAGES), (uint32_t)(kb / STAGES) & 1u, err);
+        for (int k = g > STAGES ? g - STAGES : 0; k < g; ++k)
+            (void)mbar_wait(full0 + 8 * (k % STAGES), (uint32_t)(k / STAGES) & 1u, err);
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer
         constexpr uint32_t idesc = make_idesc(BM, BN);
+        int g = 0, it = 0;
         bool ok = true;
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (!mbar_wait(full0 + 8 * s, ph, err)) {
+        for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++it) {
+            const int a = it & 1;
+            const uint32_t use = (uint32_t)(it >> 1);
+            if (!mbar_wait(acce0 + 8 * a, (use & 1u) ^ 1u, err)) {
                 atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_MMA);
-                ok = false;
                 break;
             }
             tc_fence_after();
-            const uint32_t a0 = sA + s * A_BYTES, b0 = sB + s * B_BYTES;
+            const uint32_t dacc = tmem + (uint32_t)(a * BN);
+            for (int kb = 0; kb < num_kb; ++kb, ++g) {
+                const int s = g % STAGES;
+                const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                if (!mbar_wait(full0 + 8 * s, ph, err)) {
+                    atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_MMA);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a0 = sA + s * A_BYTES, b0 = sB + s * B_BYTES;
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk)
-                tc_mma(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), idesc,
-                       (kb > 0 || kk > 0) ? 1u : 0u);
-            tc_commit(empty0 + 8 * s);
+                for (int kk = 0; kk < BK / 16; ++kk)
+                    tc_mma(dacc, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), idesc,
+                           (kb > 0 || kk > 0) ? 1u : 0u);
+                tc_commit(empty0 + 8 * s);
+            }
+            tc_commit(accf0 + 8 * a);
         }
-        (void)ok;
-        tc_commit(accb);
     } else if (warp >= 2) {
-        // ---- epilogue
-        const bool ready = mbar_wait(accb, 0, err);
-        if (!ready && lane == 0) atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_EPI);
+      // ---- epilogue, one tile at a time
+      int it = 0;
+      for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+        const int a = it & 1;
+        const uint32_t use = (uint32_t)(it >> 1);
+        const int tile_n = t % n_tiles_n;
+        const int m0 = (t / n_tiles_n) * BM, n0 = tile_n * BN;
+        const bool ready = mbar_wait(accf0 + 8 * a, use & 1u, err);
+        if (!ready) {
+            if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_EPI);
+            break;
+        }
         tc_fence_after();
         const int q = warp & 3;
         const int row = m0 + q * 32 + lane;
-        const bool row_ok = ready && row < ep.rows;
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
+        const bool row_ok = row < ep.rows;
+        const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
         if (ep.mode == EPI_GAP_KERNEL) {
-            double e = 0.0, ks = 0.0;
+            double e[4] = {0, 0, 0, 0}, ks[4] = {0, 0, 0, 0};
             const double qo = row_ok ? ep.qoff[row] : 0.0;
-            for (int c = 0; c < BN / 16; ++c) {
-                float v[16];
-                __syncwarp();
-                tmem_ld16(taddr + c * 16, v);
-                const int col0 = n0 + c * 16;
-                if (!row_ok || col0 >= ep.Mpad) continue;
-                __align__(16) __nv_bfloat16 hi[16], lo[16];
+            for (int c = 0; c < BN / 32; ++c) {
+                // column parameters of this 32-column block: lane l loads column l,
+                // the j loop broadcasts them by shuffle
+                const int cl = n0 + c * 32 + lane;
+                const bool cin = cl < ep.Mpad;
+                const double p_al = cin ? ep.alpha[cl] : 0.0;
+                const double p_kc = cin ? ep.kcoef[cl] : 0.0;
+                const double p_ao = cin ? ep.aoff[cl] : 0.0;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int s = col0 + j;
-                    const double K = (double)v[j] + ep.aoff[s] + qo;
-                    double kz, km1;
-                    if (ep.zeta_int > 0) {
-                        km1 = ipow_d(K, ep.zeta_int - 1);
-                        kz = km1 * K;
-                    } else {
-                        km1 = pow(K, ep.zeta_f - 1.0);
-                        kz = pow(K, ep.zeta_f);
+                for (int h = 0; h < 2; ++h) {
+                    float v[16];
+                    __syncwarp();
+                    tmem_ld16(taddr + c * 32 + h * 16, v);
+                    const int col0 = n0 + c * 32 + h * 16;
+                    __align__(16) __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int src = h * 16 + j;
+                        const double al = __shfl_sync(0xffffffffu, p_al, src);
+                        const double kc = __shfl_sync(0xffffffffu, p_kc, src);
+                        const double ao = __shfl_sync(0xffffffffu, p_ao, src);
+                        const double K = (double)v[j] + ao + qo;
+                        double kz, km1;
+                        if (ep.zeta_int == 4) {
+                            const double K2 = K * K;
+                            km1 = K2 * K;
+                            kz = K2 * K2;
+                        } else if (ep.zeta_int > 0) {
+                            km1 = ipow_d(K, ep.zeta_int - 1);
+                            kz = km1 * K;
+                        } else {
+                            km1 = pow(K, ep.zeta_f - 1.0);
+                            kz = pow(K, ep.zeta_f);
+                        }
+                        e[j & 3] += al * kz;
+                        const double kd = kc * km1;
+                        ks[j & 3] += kd;
+                        bf16_split((float)(kd - kc), hi[j], lo[j]);
                     }
-                    e += ep.alpha[s] * kz;
-                    const double kd = ep.kcoef[s] * km1;
-                    ks += kd;
-                    bf16_split((float)(kd - ep.kcoef[s]), hi[j], lo[j]);
-                }
-                __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + col0;
-                const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
-                const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
-                uint4 *d0 = reinterpret_cast<uint4 *>(kr);
-                d0[0] = h4[0];
-                d0[1] = h4[1];
-                if (ep.nsplit == 3) {
-                    uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
-                    uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
-                    d1[0] = h4[0];
-                    d1[1] = h4[1];
-                    d2[0] = l4[0];
-                    d2[1] = l4[1];
+                    if (row_ok && col0 < ep.Mpad) {
+                        __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + col0;
+                        const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
+                        const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
+                        uint4 *d0 = reinterpret_cast<uint4 *>(kr);
+                        d0[0] = h4[0];
+                        d0[1] = h4[1];
+                        if (ep.nsplit == 3) {
+                            uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
+                            uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
+                            d1[0] = h4[0];
+                            d1[1] = h4[1];
+                            d2[0] = l4[0];
+                            d2[1] = l4[1];
+                        }
+                    }
                 }
             }
             if (row_ok) {
-                ep.epart[(size_t)row * n_tiles_n + tile_n] = e;
-                ep.kdsum[(size_t)row * n_tiles_n + tile_n] = ks;
+                ep.epart[(size_t)row * n_tiles_n + tile_n] = (e[0] + e[1]) + (e[2] + e[3]);
+                ep.kdsum[(size_t)row * n_tiles_n + tile_n] = (ks[0] + ks[1]) + (ks[2] + ks[3]);
             }
         } else {
             for (int c = 0; c < BN / 16; ++c) {
@@ -293,6 +347,11 @@ __global__ void __launch_bounds__(192, 1)
                 }
             }
         }
+        // release accumulator a to the MMA issuer
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * a);
+      }
     }
     __syncwarp();
     tc_fence_before();
@@ -300,7 +359,7 @@ __global__ void __launch_bounds__(192, 1)
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"((uint32_t)BN)
+                     "r"(TMEM_COLS)
                      : "memory");
     }
 }
@@ -357,8 +416,15 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
                                       (int)SMEM_BYTES));
         attr = true;
     }
+    static int n_sm = 0;
+    if (!n_sm) {
+        int dev = 0;
+        TGB_CUDA(cudaGetDevice(&dev));
+        TGB_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    }
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
-    k_gemm_tn<<<tm * tn, 192, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tn, ep, err);
+    const int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
+    k_gemm_tn<<<grid, 192, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tm, tn, ep, err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -168,52 +168,105 @@ struct PairSink {
     }
 };
 
-// Cell-list search (neighbors.f90:409-472): self first, then cells k3 (z)
-// outer, j3, i3 inner with the reference's skips for 1- and 2-cell axes.
-__global__ void k_nl_cells(int n_sites, const double *__restrict__ pos, Box bx, CellGrid g,
-                           double rcut, const int *__restrict__ do_list,
-                           const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
-                           const int *__restrict__ cell_count, const int *__restrict__ cell_atoms,
-                           int *__restrict__ n_neigh, const int64_t *__restrict__ pstart,
-                           int64_t cap, int *__restrict__ nbr, double *__restrict__ rjs,
-                           double *__restrict__ xyz, unsigned *err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Cell-list search (neighbors.f90:409-472), one warp per atom: self first, then
+// the cells k3 (z) outer, j3, i3 inner with the reference's skips for 1- and
+// 2-cell axes, each cell in descending atom index. The candidates of the (up to)
+// 27 cells form one flattened sequence in that order; lanes test 32 consecutive
+// candidates at a time and emit the accepted ones in sequence order (ballot +
+// prefix popcount), so the pairs come out exactly in the reference's order.
+__global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box bx, CellGrid g,
+                                double rcut, const int *__restrict__ do_list,
+                                const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
+                                const int *__restrict__ cell_count,
+                                const int *__restrict__ cell_atoms, int *__restrict__ n_neigh,
+                                const int64_t *__restrict__ pstart, int64_t cap,
+                                int *__restrict__ nbr, double *__restrict__ rjs,
+                                double *__restrict__ xyz, unsigned *err) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n_sites) return;
     if (do_list && !do_list[i]) {
-        if (!pstart) n_neigh[i] = 0;
+        if (!pstart && lane == 0) n_neigh[i] = 0;
         return;
     }
-    PairSink sink{pstart ? pstart[i] : 0, cap, pstart ? nbr : nullptr, rjs, xyz, err, 0};
-    const double zero3[3] = {0.0, 0.0, 0.0};
-    sink.emit(i, 0.0, zero3);
-    const double *pi = pos + 3 * (size_t)i;
     const int i2 = 1 + cell_xyz[3 * i], j2 = 1 + cell_xyz[3 * i + 1], k2 = 1 + cell_xyz[3 * i + 2];
     const int mx = g.mx, my = g.my, mz = g.mz;
-    for (int k3 = k2 - 1; k3 <= k2 + 1; ++k3) {
-        if (mz == 1 && k3 != 1) continue;
-        if (mz == 2 && k2 == 1 && k3 == 0) continue;
-        if (mz == 2 && k2 == 2 && k3 == 3) continue;
-        for (int j3 = j2 - 1; j3 <= j2 + 1; ++j3) {
-            if (my == 1 && j3 != 1) continue;
-            if (my == 2 && j2 == 1 && j3 == 0) continue;
-            if (my == 2 && j2 == 2 && j3 == 3) continue;
-            for (int i3 = i2 - 1; i3 <= i2 + 1; ++i3) {
-                if (mx == 1 && i3 != 1) continue;
-                if (mx == 2 && i2 == 1 && i3 == 0) continue;
-                if (mx == 2 && i2 == 2 && i3 == 3) continue;
-                const int c = imod(i3 - 1, mx) + imod(j3 - 1, my) * mx + imod(k3 - 1, mz) * mx * my;
-                const int s = cell_start[c], e = s + cell_count[c];
-                for (int q = s; q < e; ++q) {
-                    const int k = cell_atoms[q];
-                    if (k == i) continue;
-                    double dist[3], d;
-                    get_distance(pi, pos + 3 * (size_t)k, bx, dist, &d);
-                    if (d < rcut) sink.emit(k, d, dist);
-                }
-            }
+    // lane c < 27: cell (k3, j3, i3) = (k2-1 + c/9, j2-1 + (c/3)%3, i2-1 + c%3)
+    int cstart = 0, ccount = 0;
+    if (lane < 27) {
+        const int k3 = k2 - 1 + lane / 9, j3 = j2 - 1 + (lane / 3) % 3, i3 = i2 - 1 + lane % 3;
+        bool skip = false;
+        skip |= (mz == 1 && k3 != 1) || (mz == 2 && k2 == 1 && k3 == 0) || (mz == 2 && k2 == 2 && k3 == 3);
+        skip |= (my == 1 && j3 != 1) || (my == 2 && j2 == 1 && j3 == 0) || (my == 2 && j2 == 2 && j3 == 3);
+        skip |= (mx == 1 && i3 != 1) || (mx == 2 && i2 == 1 && i3 == 0) || (mx == 2 && i2 == 2 && i3 == 3);
+        if (!skip) {
+            const int c = imod(i3 - 1, mx) + imod(j3 - 1, my) * mx + imod(k3 - 1, mz) * mx * my;
+            cstart = cell_start[c];
+            ccount = cell_count[c];
         }
     }
-    if (!pstart) n_neigh[i] = sink.count;
+    // inclusive scan of the cell counts over lanes
+    int incl = ccount;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    const int64_t base = pstart ? pstart[i] : 0;
+    if (pstart && lane == 0) {   // self pair first
+        if (base < cap) {
+            nbr[base] = i;
+            rjs[base] = 0.0;
+            xyz[3 * base] = 0.0;
+            xyz[3 * base + 1] = 0.0;
+            xyz[3 * base + 2] = 0.0;
+        } else {
+            atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+        }
+    }
+    int count = 1;
+    for (int f0 = 0; f0 < total; f0 += 32) {   // warp-uniform trip count
+        const int f = f0 + lane;
+        const int fc = f < total ? f : total - 1;
+        // cell of candidate fc: c = #{cells with incl <= fc}, by fixed-step binary
+        // lifting so that every lane executes every shuffle
+        int c = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            const int probe = c + step - 1;
+            const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
+            if (probe < 27 && v <= fc) c += step;
+        }
+        const int cs = __shfl_sync(0xffffffffu, cstart, c);
+        const int before = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, ccount, c);
+        bool take = false;
+        int k = -1;
+        double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
+        if (f < total) {
+            k = cell_atoms[cs + (fc - before)];
+            if (k != i) {
+                get_distance(pi, pos + 3 * (size_t)k, bx, dist, &d);
+                take = d < rcut;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, take);
+        if (pstart && take) {
+            const int64_t p = base + count + __popc(m & ((1u << lane) - 1u));
+            if (p < cap) {
+                nbr[p] = k;
+                rjs[p] = d;
+                xyz[3 * p] = dist[0];
+                xyz[3 * p + 1] = dist[1];
+                xyz[3 * p + 2] = dist[2];
+            } else {
+                atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+            }
+        }
+        count += __popc(m);
+    }
+    if (!pstart && lane == 0) n_neigh[i] = count;
 }
 
 // O(N * N_supercell) search (neighbors.f90:474-514): ascending supercell index.
@@ -492,6 +545,7 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
              cudaStream_t st) {
     const int TB = 128;
     const int gb = (n_sites + TB - 1) / TB;
+    const int gw = (int)(((int64_t)n_sites * 32 + TB - 1) / TB);   // one warp per site
     if (use_cells) {
         const int ncells = g.mx * g.my * g.mz;
         TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
@@ -504,9 +558,10 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
                                        nl.cell_atoms);
         k_cell_sort<<<(ncells + TB - 1) / TB, TB, 0, st>>>(ncells, nl.cell_start, nl.cell_count,
                                                            nl.cell_atoms);
-        k_nl_cells<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                      nl.cell_start, nl.cell_count, nl.cell_atoms, nl.n_neigh,
-                                      nullptr, nl.cap, nullptr, nullptr, nullptr, nl.err);
+        k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
+                                           nl.cell_start, nl.cell_count, nl.cell_atoms,
+                                           nl.n_neigh, nullptr, nl.cap, nullptr, nullptr, nullptr,
+                                           nl.err);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nullptr,
                                       nl.cap, nullptr, nullptr, nullptr, nl.err);
@@ -516,9 +571,10 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n_sites,
                                            st));
     if (use_cells) {
-        k_nl_cells<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                      nl.cell_start, nl.cell_count, nl.cell_atoms, nl.n_neigh,
-                                      nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);
+        k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
+                                           nl.cell_start, nl.cell_count, nl.cell_atoms,
+                                           nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
+                                           nl.err);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nl.pstart,
                                       nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);

@@ -8,9 +8,9 @@
 //   q           = p / |p|
 // R_n (poly3, orthonormalised by the FP64 Jacobi matrix) and a_l (smeared
 // angular factor 4 pi e^{-k} i_l(k)) are tabulated per species in FP64 on the
-// GPU and interpolated in FP32 (cubic Hermite, derivative of the interpolant).
-// Forces contract dE/dq through the normalisation and the power spectrum back
-// to dE/dc on chip; the per-pair Cartesian derivative of q is never formed.
+// GPU and interpolated in FP32 (cubic Hermite). Forces contract dE/dq through
+// the normalisation and the power spectrum back to dE/dc on chip; the per-pair
+// Cartesian derivative of q is never formed.
 
 #include "tgb_soap.cuh"
 
@@ -164,12 +164,13 @@ __device__ void d_functions(const TableHyper &h, const double *W, double r, doub
     }
 }
 
-// One node per thread. Per node: [R~ | R~' | R~'' | a | a' | a''] (fp32). Values
-// and first derivatives are analytic (FP64); second derivatives are the central
-// difference of the analytic first derivative (FP64, step 1e-5 A), used only to
-// interpolate the first derivative as a cubic Hermite function of its own.
-__global__ void k_build_table(TableHyper h, const double *__restrict__ W, int tw,
-                              float *__restrict__ out) {
+// One node per thread. Per node and function (R~_0..R~_{A-1}, a_0..a_lmax) one
+// float4 (f, f', f'', 0). Values and first derivatives are analytic (FP64);
+// second derivatives are the central difference of the analytic first
+// derivative (FP64, step 1e-5 A), used only to interpolate the first derivative
+// as a cubic Hermite function of its own (O(h^4) instead of the O(h^3) of the
+// differentiated value interpolant).
+__global__ void k_build_table(TableHyper h, const double *__restrict__ W, float4 *__restrict__ out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k > kTableIntervals) return;
     const double r = h.rh * (double)k / (double)kTableIntervals;
@@ -181,18 +182,12 @@ __global__ void k_build_table(TableHyper h, const double *__restrict__ W, int tw
     d_functions(h, W, r + eps, Rp, dRp, ap, dap);
     d_functions(h, W, r - eps, Rm, dRm, am, dam);
     const int A = h.amax, nl = h.lmax + 1;
-    float *o = out + (size_t)k * tw;
-    for (int n = 0; n < A; ++n) {
-        o[n] = (float)R[n];
-        o[A + n] = (float)dR[n];
-        o[2 * A + n] = (float)((dRp[n] - dRm[n]) / (2.0 * eps));
-    }
-    for (int l = 0; l < nl; ++l) {
-        o[3 * A + l] = (float)a[l];
-        o[3 * A + nl + l] = (float)da[l];
-        o[3 * A + 2 * nl + l] = (float)((dap[l] - dam[l]) / (2.0 * eps));
-    }
-    for (int q = 3 * A + 3 * nl; q < tw; ++q) o[q] = 0.0f;
+    float4 *o = out + (size_t)k * (A + nl);
+    for (int n = 0; n < A; ++n)
+        o[n] = make_float4((float)R[n], (float)dR[n], (float)((dRp[n] - dRm[n]) / (2.0 * eps)), 0.f);
+    for (int l = 0; l < nl; ++l)
+        o[A + l] = make_float4((float)a[l], (float)da[l],
+                               (float)((dap[l] - dam[l]) / (2.0 * eps)), 0.f);
 }
 
 // Central atom: weight global_scaling * central_weight, Gaussian at r = 0,
@@ -228,10 +223,11 @@ static void poly3_jacobi_W(int amax, double *W) {
     }
 }
 
+int table_width(int amax, int lmax) { return 4 * (amax + lmax + 1); }
+
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st) {
     const int amax = h.alpha_max[0];
-    const int nl = h.lmax + 1;
-    const int tw = ((3 * amax + 3 * nl) + 3) / 4 * 4;
+    const int tw = table_width(amax, h.lmax);
     std::vector<double> W(amax * amax);
     poly3_jacobi_W(amax, W.data());
     double *dW = nullptr;
@@ -243,7 +239,7 @@ int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cuda
                       h.amplitude_scaling[s], h.central_weight[s], amax, h.lmax,
                       h.radial_enhancement};
         k_build_table<<<(kTableIntervals + 1 + 127) / 128, 128, 0, st>>>(
-            th, dW, tw, table + (size_t)s * (kTableIntervals + 1) * tw);
+            th, dW, reinterpret_cast<float4 *>(table + (size_t)s * (kTableIntervals + 1) * tw));
         k_build_self<<<1, 32, 0, st>>>(th, dW, self_R + s * amax);
     }
     cudaError_t e = cudaGetLastError();
@@ -258,79 +254,34 @@ int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cuda
 
 namespace {
 
-template <int AMAX, int NL>
-struct RadAng {
-    float R[AMAX], dR[AMAX], a[NL], da[NL];
+// Cubic Hermite weights at fractional position t in a node interval of width h;
+// the derivative-carrying weights h10, h11 include the factor h.
+struct Hermite {
+    int k;
+    float h00, h10, h01, h11;
+    __device__ __forceinline__ Hermite(float r, float h, float inv_h) {
+        const float x = r * inv_h;
+        int kk = (int)x;
+        kk = kk > kTableIntervals - 1 ? kTableIntervals - 1 : (kk < 0 ? 0 : kk);
+        k = kk;
+        const float t = x - (float)kk, t2 = t * t, t3 = t2 * t;
+        h00 = 2.f * t3 - 3.f * t2 + 1.f;
+        h10 = (t3 - 2.f * t2 + t) * h;
+        h01 = -2.f * t3 + 3.f * t2;
+        h11 = (t3 - t2) * h;
+    }
+    // value from (f, f') and, when wanted, first derivative from (f', f'') of function j
+    __device__ __forceinline__ float value(const float4 *T, int nf, int j) const {
+        const float4 a = __ldg(T + (size_t)k * nf + j), b = __ldg(T + (size_t)(k + 1) * nf + j);
+        return h00 * a.x + h10 * a.y + h01 * b.x + h11 * b.y;
+    }
+    __device__ __forceinline__ void value_deriv(const float4 *T, int nf, int j, float &v,
+                                                float &d) const {
+        const float4 a = __ldg(T + (size_t)k * nf + j), b = __ldg(T + (size_t)(k + 1) * nf + j);
+        v = h00 * a.x + h10 * a.y + h01 * b.x + h11 * b.y;
+        d = h00 * a.y + h10 * a.z + h01 * b.y + h11 * b.z;
+    }
 };
-
-// Cubic Hermite interpolation of the species table at r. Values use the node
-// values and first derivatives; first derivatives use the node first and
-// second derivatives (an O(h^4) derivative, where differentiating the value
-// interpolant would only be O(h^3)). WITH_D = false skips the derivatives.
-template <int AMAX, int NL, int TW, bool WITH_D>
-__device__ __forceinline__ void table_eval(const float *__restrict__ T, float r, float h,
-                                           float inv_h, RadAng<AMAX, NL> &o) {
-    float x = r * inv_h;
-    int k = (int)x;
-    if (k > kTableIntervals - 1) k = kTableIntervals - 1;
-    if (k < 0) k = 0;
-    const float t = x - (float)k;
-    const float t2 = t * t, t3 = t2 * t;
-    const float h00 = 2.f * t3 - 3.f * t2 + 1.f, h10 = (t3 - 2.f * t2 + t) * h;
-    const float h01 = -2.f * t3 + 3.f * t2, h11 = (t3 - t2) * h;
-    const float *n0 = T + (size_t)k * TW;
-    const float *n1 = n0 + TW;
-    float b0[TW], b1[TW];
-#pragma unroll
-    for (int q = 0; q < TW; q += 4) {
-        const float4 v0 = __ldg(reinterpret_cast<const float4 *>(n0 + q));
-        const float4 v1 = __ldg(reinterpret_cast<const float4 *>(n1 + q));
-        b0[q] = v0.x; b0[q + 1] = v0.y; b0[q + 2] = v0.z; b0[q + 3] = v0.w;
-        b1[q] = v1.x; b1[q + 1] = v1.y; b1[q + 2] = v1.z; b1[q + 3] = v1.w;
-    }
-    constexpr int cA = 3 * AMAX;
-#pragma unroll
-    for (int n = 0; n < AMAX; ++n) {
-        o.R[n] = h00 * b0[n] + h10 * b0[AMAX + n] + h01 * b1[n] + h11 * b1[AMAX + n];
-        if (WITH_D)
-            o.dR[n] = h00 * b0[AMAX + n] + h10 * b0[2 * AMAX + n] + h01 * b1[AMAX + n] +
-                      h11 * b1[2 * AMAX + n];
-    }
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        o.a[l] = h00 * b0[cA + l] + h10 * b0[cA + NL + l] + h01 * b1[cA + l] + h11 * b1[cA + NL + l];
-        if (WITH_D)
-            o.da[l] = h00 * b0[cA + NL + l] + h10 * b0[cA + 2 * NL + l] + h01 * b1[cA + NL + l] +
-                      h11 * b1[cA + 2 * NL + l];
-    }
-}
-
-// Associated Legendre derivative polynomials Q[l][m] = d^m P_l/dz^m for m <= l,
-// and Q[l][l+1] = 0, by the standard upward recurrence in l.
-template <int LMAX>
-__device__ __forceinline__ void legendre_q(float z, float (&Q)[LMAX + 1][LMAX + 2]) {
-#pragma unroll
-    for (int m = 0; m <= LMAX; ++m) {
-        Q[m][m] = cDf[m];
-        if (m + 1 <= LMAX) Q[m + 1][m] = (float)(2 * m + 1) * z * Q[m][m];
-#pragma unroll
-        for (int l = m + 2; l <= LMAX; ++l)
-            Q[l][m] = cRa[l][m] * z * Q[l - 1][m] - cRb[l][m] * Q[l - 2][m];
-    }
-#pragma unroll
-    for (int l = 0; l <= LMAX; ++l) Q[l][l + 1] = 0.f;
-}
-
-template <int LMAX>
-__device__ __forceinline__ void cos_sin_m(float x, float y, float (&C)[LMAX + 1], float (&S)[LMAX + 1]) {
-    C[0] = 1.f;
-    S[0] = 0.f;
-#pragma unroll
-    for (int m = 1; m <= LMAX; ++m) {
-        C[m] = x * C[m - 1] - y * S[m - 1];
-        S[m] = x * S[m - 1] + y * C[m - 1];
-    }
-}
 
 __device__ __forceinline__ int fold_index(int j, int n) {
     return j < n ? j : j % n;
@@ -339,6 +290,37 @@ __device__ __forceinline__ int fold_index(int j, int n) {
 // Descriptor species of a global species id, -1 when the block does not see it.
 __device__ __forceinline__ int zlookup(const SoapParams &P, int z) {
     return (z >= 0 && z < kMaxZ) ? (int)P.zmap[z] : -1;
+}
+
+// Real spherical harmonics of unit u into Y[l*l + l + m] (m = -l..l), by the
+// running Legendre recurrence in l for each m (Q_l^m = d^m P_l/dz^m) and the
+// running (x + iy)^m: a handful of live registers.
+template <int LMAX>
+__device__ __forceinline__ void real_ylm(float x, float y, float z, float *Y) {
+    float cm = 1.f, sm = 0.f;
+#pragma unroll
+    for (int m = 0; m <= LMAX; ++m) {
+        float q2 = 0.f, q1 = 0.f;
+#pragma unroll
+        for (int l = m; l <= LMAX; ++l) {
+            float q;
+            if (l == m) q = cDf[m];
+            else if (l == m + 1) q = (float)(2 * m + 1) * z * q1;
+            else q = cRa[l][m] * z * q1 - cRb[l][m] * q2;
+            const float f = cYn[l][m] * q;
+            if (m == 0) {
+                Y[l * l + l] = f;
+            } else {
+                Y[l * l + l + m] = f * cm;
+                Y[l * l + l - m] = f * sm;
+            }
+            q2 = q1;
+            q1 = q;
+        }
+        const float c2 = x * cm - y * sm;
+        sm = x * sm + y * cm;
+        cm = c2;
+    }
 }
 
 }  // namespace
@@ -350,30 +332,40 @@ struct DescShape {
     static constexpr int NL = LMAX + 1;
     static constexpr int NLM = NL * NL;
     static constexpr int NT = NS * AMAX;
+    static constexpr int NF = AMAX + NL;          // tabulated functions per node
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
-    static constexpr int DSLOTS = (DIM + 31) / 32;
-    static constexpr int TW = ((3 * AMAX + 3 * NL) + 3) / 4 * 4;
-    static constexpr int RHO = AMAX * NL;          // per-pair radial*angular products
     static constexpr int CHUNK = 32;
     static constexpr int WARPS = 4;
-    // shared memory per warp (floats): Y rows + rho rows (+ reused for c)
+    // per-warp shared memory (floats): Y rows (odd stride NLM), R rows (stride
+    // AMAX, read as broadcast float4), a rows (odd stride NL), pair species.
+    // The FP64 coefficients of the power-spectrum phase reuse the same area.
     static constexpr int YS = CHUNK * NLM;
-    static constexpr int RS = CHUNK * RHO;
-    static constexpr int WARP_FLOATS = YS + RS + CHUNK;
-    static_assert(2 * NT * NLM <= YS + RS, "FP64 c must fit in the per-warp staging area");
-    static_assert(AMAX % 4 == 0, "float4 reads of rho rows need alpha_max % 4 == 0");
+    static constexpr int RS = CHUNK * AMAX;
+    static constexpr int AS = CHUNK * NL;
+    static constexpr int STAGE = YS + RS + AS + CHUNK;
+    static constexpr int CWORDS = 2 * NT * NLM;
+    static constexpr int WARP_FLOATS = ((STAGE > CWORDS ? STAGE : CWORDS) + 3) / 4 * 4;
+    static_assert(AMAX % 4 == 0, "float4 reads of R rows need alpha_max % 4 == 0");
+    static_assert(YS % 4 == 0 && RS % 4 == 0, "R rows must stay 16-byte aligned");
 };
 
+// One warp per central atom. Lanes evaluate 32 pairs at a time (table
+// interpolation, Y_lm) into shared memory; then each lane owns (l, m) slots and
+// accumulates c_{n,lm} over the chunk's pairs in FP32. The central atom's
+// constant contribution to c_{n,00} is added in FP64 afterwards (it dominates
+// c_{n,00}, and FP32 sums on top of it were the main descriptor error).
+// Power spectrum and |p| in FP64.
 template <int NS, int AMAX, int LMAX>
-__global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
+__global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
     using Sh = DescShape<NS, AMAX, LMAX>;
-    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, DIM = Sh::DIM;
+    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, NF = Sh::NF, DIM = Sh::DIM;
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *Ys = smem + warp * Sh::WARP_FLOATS;
-    float *rho = Ys + Sh::YS;
-    int *pspec = reinterpret_cast<int *>(rho + Sh::RS);
+    float *Rs = Ys + Sh::YS;
+    float *As = Rs + Sh::RS;
+    int *pspec = reinterpret_cast<int *>(As + Sh::AS);
     __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
     for (int t = threadIdx.x; t < NT * (NT + 1) / 2; t += blockDim.x) {
         int n = 0, rem = t;
@@ -388,6 +380,7 @@ __global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, D
     const int catom = S.site_atom[site];
     const int64_t p0 = S.pstart[row];
     const int np = (int)(S.pstart[row + 1] - p0);
+    const int scen = zlookup(P, S.species[catom]);   // central atom's descriptor species
 
     int lmk[Sh::SLOTS], lk[Sh::SLOTS];
 #pragma unroll
@@ -397,62 +390,35 @@ __global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, D
         while ((l + 1) * (l + 1) <= lmk[k]) ++l;
         lk[k] = l;
     }
-    // c accumulates in FP64: FP32 sums of ~30 pair terms onto the large central
-    // contribution were the dominant descriptor error.
-    double acc[NT][Sh::SLOTS];
+    float acc[NT][Sh::SLOTS];
 #pragma unroll
     for (int n = 0; n < NT; ++n)
 #pragma unroll
-        for (int k = 0; k < Sh::SLOTS; ++k) acc[n][k] = 0.0;
+        for (int k = 0; k < Sh::SLOTS; ++k) acc[n][k] = 0.f;
 
-    for (int base = 0; base < np; base += Sh::CHUNK) {
+    // the self pair (first of the list) is not part of the chunks
+    for (int base = 1; base < np; base += Sh::CHUNK) {
         const int t = lane;
         int s = -1;
         if (base + t < np) {
-            float *Yr = Ys + t * NLM;
-            float *rr = rho + t * Sh::RHO;   // layout [l][n]
-            if (base + t == 0) {
-                s = zlookup(P, S.species[catom]);
-                if (s >= 0) {
-                    for (int lm = 0; lm < NLM; ++lm) Yr[lm] = (lm == 0) ? 1.f : 0.f;
-                    for (int l = 0; l < NL; ++l)
-                        for (int n = 0; n < AMAX; ++n)
-                            rr[l * AMAX + n] = (l == 0) ? P.self_R[s * AMAX + n] : 0.f;
-                }
+            const int64_t p = p0 + base + t;
+            const int ja = fold_index(S.nbr[p], P.n_atoms);
+            s = zlookup(P, S.species[ja]);
+            const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
+                        z = (float)S.xyz[3 * p + 2];
+            const float r = sqrtf(x * x + y * y + z * z);
+            if (s >= 0 && r < P.rcut[s] && r > 0.f) {
+                const float4 *T = reinterpret_cast<const float4 *>(
+                    P.table + (size_t)s * (kTableIntervals + 1) * (4 * NF));
+                const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
+#pragma unroll
+                for (int n = 0; n < AMAX; ++n) Rs[t * AMAX + n] = hm.value(T, NF, n);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) As[t * NL + l] = hm.value(T, NF, AMAX + l);
+                const float ir = 1.f / r;
+                real_ylm<LMAX>(x * ir, y * ir, z * ir, Ys + t * NLM);
             } else {
-                const int64_t p = p0 + base + t;
-                const int ja = fold_index(S.nbr[p], P.n_atoms);
-                s = zlookup(P, S.species[ja]);
-                const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
-                            z = (float)S.xyz[3 * p + 2];
-                const float r = sqrtf(x * x + y * y + z * z);
-                if (s >= 0 && r < P.rcut[s] && r > 0.f) {
-                    RadAng<AMAX, NL> ra;
-                    table_eval<AMAX, NL, Sh::TW, false>(P.table + (size_t)s * (kTableIntervals + 1) * Sh::TW,
-                                                        r, P.tab_h[s], P.tab_inv_h[s], ra);
-                    const float ir = 1.f / r;
-                    const float ux = x * ir, uy = y * ir, uz = z * ir;
-                    float C[LMAX + 1], Sn[LMAX + 1];
-                    cos_sin_m<LMAX>(ux, uy, C, Sn);
-                    float Q[LMAX + 1][LMAX + 2];
-                    legendre_q<LMAX>(uz, Q);
-#pragma unroll
-                    for (int l = 0; l <= LMAX; ++l) {
-                        Yr[l * l + l] = cYn[l][0] * Q[l][0];
-#pragma unroll
-                        for (int m = 1; m <= l; ++m) {
-                            const float f = cYn[l][m] * Q[l][m];
-                            Yr[l * l + l + m] = f * C[m];
-                            Yr[l * l + l - m] = f * Sn[m];
-                        }
-                    }
-#pragma unroll
-                    for (int l = 0; l < NL; ++l)
-#pragma unroll
-                        for (int n = 0; n < AMAX; ++n) rr[l * AMAX + n] = ra.R[n] * ra.a[l];
-                } else {
-                    s = -1;
-                }
+                s = -1;
             }
         }
         pspec[t] = s;
@@ -461,25 +427,24 @@ __global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, D
         for (int tt = 0; tt < cnt; ++tt) {
             const int ss = pspec[tt];
             if (ss < 0) continue;
+            float rv[AMAX];
+            const float4 *r4 = reinterpret_cast<const float4 *>(Rs + tt * AMAX);
+#pragma unroll
+            for (int q = 0; q < AMAX / 4; ++q) {
+                const float4 v = r4[q];
+                rv[4 * q] = v.x; rv[4 * q + 1] = v.y; rv[4 * q + 2] = v.z; rv[4 * q + 3] = v.w;
+            }
             const float *Yr = Ys + tt * NLM;
-            const float *rr = rho + tt * Sh::RHO;
+            const float *Ar = As + tt * NL;
 #pragma unroll
             for (int k = 0; k < Sh::SLOTS; ++k) {
                 if (lmk[k] < NLM) {
-                    const float yv = Yr[lmk[k]];
-                    const float4 *r4 = reinterpret_cast<const float4 *>(rr + lk[k] * AMAX);
-                    float rv[AMAX];
-#pragma unroll
-                    for (int q = 0; q < AMAX / 4; ++q) {
-                        const float4 v = r4[q];
-                        rv[4 * q] = v.x; rv[4 * q + 1] = v.y; rv[4 * q + 2] = v.z; rv[4 * q + 3] = v.w;
-                    }
+                    const float ya = Yr[lmk[k]] * Ar[lk[k]];
 #pragma unroll
                     for (int sp = 0; sp < NS; ++sp) {
                         if (ss == sp) {
 #pragma unroll
-                            for (int n = 0; n < AMAX; ++n)
-                                acc[sp * AMAX + n][k] += (double)(rv[n] * yv);
+                            for (int n = 0; n < AMAX; ++n) acc[sp * AMAX + n][k] += rv[n] * ya;
                         }
                     }
                 }
@@ -487,15 +452,18 @@ __global__ void __launch_bounds__(128) k_soap_expand(SoapParams P, SiteArgs S, D
         }
         __syncwarp();
     }
-    // c to shared (FP64, layout [n][lm]) and to global (fp32) for the force pass
+    // c to shared (FP64, layout [n][lm]) with the central term, and to global (fp32)
     double *cs = reinterpret_cast<double *>(Ys);
 #pragma unroll
     for (int n = 0; n < NT; ++n)
 #pragma unroll
         for (int k = 0; k < Sh::SLOTS; ++k)
             if (lmk[k] < NLM) {
-                cs[n * NLM + lmk[k]] = acc[n][k];
-                O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)acc[n][k];
+                double v = (double)acc[n][k];
+                if (lmk[k] == 0 && scen >= 0 && n / AMAX == scen)
+                    v += (double)P.self_R[scen * AMAX + n % AMAX];
+                cs[n * NLM + lmk[k]] = v;
+                O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)v;
             }
     __syncwarp();
     auto power = [&](int d) -> double {
@@ -548,9 +516,9 @@ struct ForceShape {
     static constexpr int NL = LMAX + 1;
     static constexpr int NLM = NL * NL;
     static constexpr int NT = NS * AMAX;
+    static constexpr int NF = AMAX + NL;
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
-    static constexpr int TW = ((3 * AMAX + 3 * NL) + 3) / 4 * 4;
     static constexpr int WARPS = 4;
     static constexpr int BSTRIDE = NT * NT + 1;    // per-l stride of the B matrices (bank spread)
     static constexpr int BAREA = (NL * BSTRIDE + 3) / 4 * 4;   // keeps gam 16-byte aligned
@@ -558,10 +526,13 @@ struct ForceShape {
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
 };
 
+// One warp per central atom: dE/dq -> dE/dp (normalisation, FP64) -> B_l -> Gamma =
+// dE/dc (shared memory), then one lane per pair contracts Gamma with d(c)/d(r_j)
+// on the fly: F_j -= dE_i/dr_j, F_i += dE_i/dr_j, virial += 1/2 (f x + x f).
 template <int NS, int AMAX, int LMAX>
 __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
     using Sh = ForceShape<NS, AMAX, LMAX>;
-    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, DIM = Sh::DIM;
+    constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, NF = Sh::NF, DIM = Sh::DIM;
     extern __shared__ __align__(16) float smem[];
     __shared__ double vred[Sh::WARPS][6];
     __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
@@ -640,77 +611,96 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             }
         }
         __syncwarp();
-        // pairs: lane per pair
+        // pairs: lane per pair (the self pair, first in the list, is the -sum)
         double fs[3] = {0, 0, 0};
         for (int pp = 1 + lane; pp < np; pp += 32) {
             const int64_t p = p0 + pp;
-            const int j = S.nbr[p];
-            const int ja = fold_index(j, P.n_atoms);
+            const int ja = fold_index(S.nbr[p], P.n_atoms);
             const int s = zlookup(P, S.species[ja]);
             const double X = S.xyz[3 * p], Yy = S.xyz[3 * p + 1], Z = S.xyz[3 * p + 2];
             const float x = (float)X, y = (float)Yy, z = (float)Z;
             const float r = sqrtf(x * x + y * y + z * z);
             if (s < 0 || !(r < P.rcut[s]) || !(r > 0.f)) continue;
-            RadAng<AMAX, NL> ra;
-            table_eval<AMAX, NL, Sh::TW, true>(P.table + (size_t)s * (kTableIntervals + 1) * Sh::TW,
-                                               r, P.tab_h[s], P.tab_inv_h[s], ra);
+            const float4 *T = reinterpret_cast<const float4 *>(
+                P.table + (size_t)s * (kTableIntervals + 1) * (4 * NF));
+            const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
+            float R[AMAX], dR[AMAX], al[NL], dal[NL];
+#pragma unroll
+            for (int n = 0; n < AMAX; ++n) hm.value_deriv(T, NF, n, R[n], dR[n]);
+#pragma unroll
+            for (int l = 0; l < NL; ++l) hm.value_deriv(T, NF, AMAX + l, al[l], dal[l]);
             const float ir = 1.f / r;
-            const float u[3] = {x * ir, y * ir, z * ir};
-            float C[LMAX + 1], Sn[LMAX + 1];
-            cos_sin_m<LMAX>(u[0], u[1], C, Sn);
-            float Q[LMAX + 1][LMAX + 2];
-            legendre_q<LMAX>(u[2], Q);
+            const float u0 = x * ir, u1 = y * ir, u2 = z * ir;
             float T1 = 0.f, T2x = 0.f, T2y = 0.f, T2z = 0.f;
             const int ch = s * AMAX;
+            // m outer, l inner: Q_l^m and Q_l^{m+1} by running recurrences in l;
+            // (C_m, S_m) = (x + iy)^m and (C_{m-1}, S_{m-1}) running in m.
+            float cm = 1.f, sm = 0.f, cm1 = 0.f, sm1 = 0.f;
 #pragma unroll
-            for (int l = 0; l <= LMAX; ++l) {
-                const float al = ra.a[l], dal = ra.da[l];
+            for (int m = 0; m <= LMAX; ++m) {
+                float qa2 = 0.f, qa1 = 0.f, qb2 = 0.f, qb1 = 0.f;
 #pragma unroll
-                for (int m = 0; m <= l; ++m) {
-                    // G = sum_n Gamma R_n, G' = sum_n Gamma dR_n for +m (C) and -m (S)
-                    const int lmp = l * l + l + m, lmn = l * l + l - m;
-                    float Gp = 0.f, dGp = 0.f, Gn = 0.f, dGn = 0.f;
+                for (int l = m; l <= LMAX; ++l) {
+                    float qa, qb;
+                    if (l == m) qa = cDf[m];
+                    else if (l == m + 1) qa = (float)(2 * m + 1) * u2 * qa1;
+                    else qa = cRa[l][m] * u2 * qa1 - cRb[l][m] * qa2;
+                    if (l == m) qb = 0.f;
+                    else if (l == m + 1) qb = cDf[m + 1];
+                    else if (l == m + 2) qb = (float)(2 * m + 3) * u2 * qb1;
+                    else qb = cRa[l][m + 1] * u2 * qb1 - cRb[l][m + 1] * qb2;
+                    qa2 = qa1; qa1 = qa;
+                    qb2 = qb1; qb1 = qb;
+                    // G = sum_n Gamma R_n, G' = sum_n Gamma R_n' for +m (C) and -m (S)
+                    const int lmp = l * l + l + m;
+                    float Gp = 0.f, dGp = 0.f;
                     const float4 *gp = reinterpret_cast<const float4 *>(gam + lmp * NT + ch);
 #pragma unroll
                     for (int qd = 0; qd < AMAX / 4; ++qd) {
                         const float4 v = gp[qd];
-                        Gp += v.x * ra.R[4 * qd] + v.y * ra.R[4 * qd + 1] + v.z * ra.R[4 * qd + 2] +
-                              v.w * ra.R[4 * qd + 3];
-                        dGp += v.x * ra.dR[4 * qd] + v.y * ra.dR[4 * qd + 1] +
-                               v.z * ra.dR[4 * qd + 2] + v.w * ra.dR[4 * qd + 3];
+                        Gp += v.x * R[4 * qd] + v.y * R[4 * qd + 1] + v.z * R[4 * qd + 2] +
+                              v.w * R[4 * qd + 3];
+                        dGp += v.x * dR[4 * qd] + v.y * dR[4 * qd + 1] + v.z * dR[4 * qd + 2] +
+                               v.w * dR[4 * qd + 3];
                     }
                     const float f = cYn[l][m];
-                    const float Qlm = Q[l][m], Qlm1 = Q[l][m + 1];
+                    const float a = al[l], da = dal[l];
                     if (m == 0) {
-                        const float yv = f * Qlm;
-                        T1 += yv * (al * dGp + dal * Gp);
-                        T2z += al * Gp * f * Qlm1;
+                        T1 += f * qa * (a * dGp + da * Gp);
+                        T2z += a * Gp * f * qb;
                     } else {
+                        const int lmn = l * l + l - m;
+                        float Gn = 0.f, dGn = 0.f;
                         const float4 *gn = reinterpret_cast<const float4 *>(gam + lmn * NT + ch);
 #pragma unroll
                         for (int qd = 0; qd < AMAX / 4; ++qd) {
                             const float4 v = gn[qd];
-                            Gn += v.x * ra.R[4 * qd] + v.y * ra.R[4 * qd + 1] +
-                                  v.z * ra.R[4 * qd + 2] + v.w * ra.R[4 * qd + 3];
-                            dGn += v.x * ra.dR[4 * qd] + v.y * ra.dR[4 * qd + 1] +
-                                   v.z * ra.dR[4 * qd + 2] + v.w * ra.dR[4 * qd + 3];
+                            Gn += v.x * R[4 * qd] + v.y * R[4 * qd + 1] + v.z * R[4 * qd + 2] +
+                                  v.w * R[4 * qd + 3];
+                            dGn += v.x * dR[4 * qd] + v.y * dR[4 * qd + 1] +
+                                   v.z * dR[4 * qd + 2] + v.w * dR[4 * qd + 3];
                         }
-                        const float yc = f * Qlm * C[m], ys = f * Qlm * Sn[m];
-                        T1 += yc * (al * dGp + dal * Gp) + ys * (al * dGn + dal * Gn);
-                        const float wc = al * Gp, wsn = al * Gn;
-                        const float fm = f * Qlm * (float)m;
-                        // grad of sqrt2 N Q C_m: (m C_{m-1}, -m S_{m-1}, Q' C_m)
-                        T2x += wc * fm * C[m - 1] + wsn * fm * Sn[m - 1];
-                        T2y += -wc * fm * Sn[m - 1] + wsn * fm * C[m - 1];
-                        T2z += (wc * C[m] + wsn * Sn[m]) * f * Qlm1;
+                        const float yc = f * qa * cm, ys = f * qa * sm;
+                        T1 += yc * (a * dGp + da * Gp) + ys * (a * dGn + da * Gn);
+                        const float wc = a * Gp, wsn = a * Gn;
+                        const float fm = f * qa * (float)m;
+                        // grad of sqrt2 N Q C_m: (m C_{m-1}, -m S_{m-1}, Q' C_m); S_m likewise
+                        T2x += wc * fm * cm1 + wsn * fm * sm1;
+                        T2y += -wc * fm * sm1 + wsn * fm * cm1;
+                        T2z += (wc * cm + wsn * sm) * f * qb;
                     }
                 }
+                cm1 = cm;
+                sm1 = sm;
+                const float c2 = u0 * cm - u1 * sm;
+                sm = u0 * sm + u1 * cm;
+                cm = c2;
             }
-            const float ut2 = u[0] * T2x + u[1] * T2y + u[2] * T2z;
+            const float ut2 = u0 * T2x + u1 * T2y + u2 * T2z;
             // f_pair = -dE_i/dr_j = -(T1 u + (T2 - (u.T2) u)/r)
-            const float fx = -(T1 * u[0] + (T2x - ut2 * u[0]) * ir);
-            const float fy = -(T1 * u[1] + (T2y - ut2 * u[1]) * ir);
-            const float fz = -(T1 * u[2] + (T2z - ut2 * u[2]) * ir);
+            const float fx = -(T1 * u0 + (T2x - ut2 * u0) * ir);
+            const float fy = -(T1 * u1 + (T2y - ut2 * u1) * ir);
+            const float fz = -(T1 * u2 + (T2z - ut2 * u2) * ir);
             atomicAdd(&O.forces[3 * (size_t)ja], (double)fx);
             atomicAdd(&O.forces[3 * (size_t)ja + 1], (double)fy);
             atomicAdd(&O.forces[3 * (size_t)ja + 2], (double)fz);

@@ -72,6 +72,10 @@ struct SoapHostHypers {
         central_weight[kMaxSpecies];
 };
 
+// Floats per table node: one float4 (f, f', f'', 0) per tabulated function
+// (alpha_max radial functions, then l_max + 1 angular factors).
+int table_width(int amax, int lmax);
+
 // Builds table and self_R (device buffers owned by the caller) in FP64 on the GPU.
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st);
 

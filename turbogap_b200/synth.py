@@ -75,6 +75,9 @@ def random_structure(n: int, L: float, d_min: float, seed: int, h_fraction: floa
     return Structure(positions=pos, species=species, box=np.eye(3) * L)
 
 
+WORKLOAD_NAMES = ("carbon216", "ch32k", "carbon131k", "ch1m", "cells512")
+
+
 def workload_structure(name: str, sub: int | None = None) -> Structure:
     """The seeded structure of a named workload (sub-structure index for cells512)."""
     if name == "carbon216":
