@@ -69,7 +69,8 @@ typedef struct {
 } tg_soap_hypers;
 
 /* ---- device context: gpu_context_init / gpu_context_finalize
- *      (src/gpu_context.f90:41-58). n_omp is set to 1 as on the CPU path. */
+ *      (src/gpu_context.f90:41-58). n_omp is set to 1 as on the CPU path.
+ *      device < 0 selects rank mod (visible devices): one MPI rank per GPU. */
 int tg_context_init(int32_t rank, int32_t device, int32_t *n_omp);
 int tg_context_finalize(void);
 

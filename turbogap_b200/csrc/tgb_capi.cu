@@ -306,11 +306,11 @@ extern "C" {
 const char *tg_last_error(void) { return tgb::last_error(); }
 
 int tg_context_init(int32_t rank, int32_t device, int32_t *n_omp) {
-    (void)rank;
     if (n_omp) *n_omp = 1;
     if (g_ctx) return TG_OK;
     int ndev = 0;
     TGB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 && ndev > 0) device = (rank < 0 ? 0 : rank) % ndev;   // one rank per GPU
     TGB_CHECK(device >= 0 && device < ndev, TG_ERR_ARG, "device %d not present (%d devices)", device,
               ndev);
     TGB_CUDA(cudaSetDevice(device));
