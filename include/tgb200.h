@@ -136,6 +136,30 @@ int tg_build_neighbors_list(int32_t n_sites_supercell, const double *positions,
                             double *rjs, double *thetas, double *phis, double *xyz,
                             int32_t *neighbor_species, int64_t *n_pairs);
 
+/* ---- Neighbour list that allocates nothing. No reference counterpart: the
+ *   reference has no device-memory discipline to honour. It serves callers
+ *   that own every device byte (an arena-managed or offload host) or may not
+ *   allocate inside their time step. Same cell-list kernels as
+ *   tg_build_neighbors_list, for ONE orthorhombic box of at least 2 rcut_max
+ *   (no supercell, no do_list); scratch lives in a fixed file-scope device
+ *   array of about 4.2 MB per GPU, so n_sites <= 131072 and at most 131072
+ *   cells, else TG_ERR_CAPACITY. All pointers except the box vectors are
+ *   DEVICE pointers on the current device: positions (3, n_sites);
+ *   n_neigh (n_sites); pstart (n_sites + 1), pair k of site i at
+ *   pstart[i] + k; neighbors_list (cap) 1-based; rjs (cap); xyz (3, cap).
+ *   stream: a cudaStream_t (NULL = legacy default stream); the call
+ *   synchronises it before returning. *n_pairs = pairs needed; more than cap
+ *   gives TG_ERR_CAPACITY. Make the first call on a device outside stream
+ *   capture (it resolves the scratch address). Calls that overlap on one
+ *   device share the scratch and race: serialise them. Needs no
+ *   tg_context_init. */
+int tg_build_neighbors_list_noalloc(int32_t n_sites, const double *positions,
+                                    const double *a_box, const double *b_box,
+                                    const double *c_box, double rcut_max, int64_t cap,
+                                    int32_t *n_neigh, int64_t *pstart,
+                                    int32_t *neighbors_list, double *rjs, double *xyz,
+                                    int64_t *n_pairs, void *stream);
+
 /* ---- velocity_verlet (src/md.f90:226-283), no fixed atoms, arrays (3, n). */
 int tg_velocity_verlet(int32_t n, double *positions, double *positions_prev,
                        double *velocities, const double *forces, double *forces_prev,

@@ -62,6 +62,9 @@ SIGNATURES = [
     ("tg_build_neighbors_list", C.c_int, [C.c_int32, dp, C.c_int32, dp, dp, dp, C.c_double, ip,
                                           ip, _vp, C.c_int64, ip, ip, dp, dp, dp, dp, ip,
                                           C.POINTER(C.c_int64)]),
+    ("tg_build_neighbors_list_noalloc", C.c_int, [C.c_int32, _vp, dp, dp, dp, C.c_double,
+                                                  C.c_int64, _vp, _vp, _vp, _vp, _vp,
+                                                  C.POINTER(C.c_int64), _vp]),
     ("tg_velocity_verlet", C.c_int, [C.c_int32, dp, dp, dp, dp, dp, dp, C.c_double,
                                      C.POINTER(C.c_double), C.c_int32]),
     ("tg_engine_create", C.c_int, [C.c_int32, dp, ip, dp, dp, dp, dp, C.c_int32, ip, _vp,

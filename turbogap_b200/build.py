@@ -28,6 +28,7 @@ SOURCES = {
     "tgb_gemm.cu": [],
     "tgb_mlp.cu": [],
     "tgb_capi.cu": [],
+    "tgb_noalloc.cu": ["--fmad=false"],
 }
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
