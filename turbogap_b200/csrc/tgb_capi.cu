@@ -57,13 +57,13 @@ struct Block {
     int key = 0, precision = TG_PREC_BF16X3;
     SoapHostHypers hh{};
     int ns = 0, amax = 0, lmax = 0, ntot = 0, nlm = 0, dim = 0;
-    int M = 0, Mpad = 0, K1 = 0, K2 = 0, nsplit = 3, n_tiles = 0, tw = 0;
+    int M = 0, Mpad = 0, K1 = 0, K2 = 0, nsplit = 3, n_etiles = 0, tw = 0;
     double delta = 1.0, zeta = 1.0, rcut_max = 0.0;
     int zeta_int = 0;
     signed char zmap[kMaxZ];
     DBuf<float> table, selfR;
     DBuf<__nv_bfloat16> QsA, QsT;
-    DBuf<double> alpha, kcoef, mu, aoff, g0;
+    DBuf<double> alpha, mu, aoff, g0;
     TmaMap tmB1{}, tmB2{};
 
     SoapParams params(int n_atoms) const {
@@ -98,7 +98,7 @@ struct Workspace {
         const int n = n_sites > 0 ? n_sites : 1;
         if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.K2 ||
             qsplit.n < (size_t)n * b.K1 || c.n < (size_t)n * b.ntot * b.nlm ||
-            epart.n < (size_t)n * b.n_tiles || kdsum.n < (size_t)n * b.n_tiles) {
+            epart.n < (size_t)n * b.n_etiles || kdsum.n < (size_t)n * b.n_etiles) {
             const int nc = n > cap ? n : cap;
             TGB_TRY(qsplit.ensure((size_t)nc * b.K1));
             TGB_TRY(kd.ensure((size_t)nc * b.K2));
@@ -106,8 +106,8 @@ struct Workspace {
             TGB_TRY(g.ensure((size_t)nc * b.dim));
             TGB_TRY(c.ensure((size_t)nc * b.ntot * b.nlm));
             TGB_TRY(pnorm.ensure(nc));
-            TGB_TRY(epart.ensure((size_t)nc * b.n_tiles));
-            TGB_TRY(kdsum.ensure((size_t)nc * b.n_tiles));
+            TGB_TRY(epart.ensure((size_t)nc * b.n_etiles));
+            TGB_TRY(kdsum.ensure((size_t)nc * b.n_etiles));
             TGB_TRY(qoff.ensure(nc));
             TGB_TRY(vpart.ensure((size_t)9 * ((nc + 3) / 4 + 1)));
             cap = nc;
@@ -159,13 +159,11 @@ __global__ void k_prep_sparse(const double *__restrict__ Qs, const double *__res
     }
 }
 
-__global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad, double coef,
-                             double *__restrict__ alpha, double *__restrict__ kcoef) {
+__global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad,
+                             double *__restrict__ alpha) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= Mpad) return;
-    const double a = s < M ? al[s] : 0.0;
-    alpha[s] = a;
-    kcoef[s] = coef * a;
+    alpha[s] = s < M ? al[s] : 0.0;
 }
 
 }  // namespace
@@ -225,7 +223,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e1.rows = S.n_sites;
     e1.cols = b.Mpad;
     e1.alpha = b.alpha.p;
-    e1.kcoef = b.kcoef.p;
+    e1.c0 = b.zeta * b.delta * b.delta;
     e1.zeta_int = b.zeta_int;
     e1.zeta_f = b.zeta;
     e1.epart = w.epart.p;
@@ -246,7 +244,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.ldo = b.dim;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
     TGB_MARK(log, PASS_GEMM2, st);
-    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_tiles, b.delta * b.delta};
+    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
     int nblk = 0;
     TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
@@ -421,7 +419,7 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     b->Mpad = round_up(n_sparse, 64);
     b->K1 = round_up(b->nsplit * b->dim, kGemmBK);
     b->K2 = b->nsplit * b->Mpad;
-    b->n_tiles = gemm_n_tiles(b->Mpad);
+    b->n_etiles = gemm_n_etiles(b->Mpad);
     b->tw = table_width(b->amax, b->lmax);
     b->delta = delta;
     b->rcut_max = 0.0;
@@ -441,7 +439,6 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     TGB_TRY(b->QsA.ensure((size_t)b->Mpad * b->K1));
     TGB_TRY(b->QsT.ensure((size_t)b->dim * b->K2));
     TGB_TRY(b->alpha.ensure(b->Mpad));
-    TGB_TRY(b->kcoef.ensure(b->Mpad));
     TGB_TRY(b->mu.ensure(b->dim));
     TGB_TRY(b->aoff.ensure(b->Mpad));
     TGB_TRY(b->g0.ensure(b->dim));
@@ -478,9 +475,7 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     k_prep_sparse<<<(unsigned)((tot + 255) / 256), 256, 0, C.st>>>(tq.p, b->mu.p, b->M, b->Mpad,
                                                                    b->dim, b->K1, b->K2, b->nsplit,
                                                                    b->QsA.p, b->QsT.p);
-    k_prep_alpha<<<(b->Mpad + 255) / 256, 256, 0, C.st>>>(ta.p, b->M, b->Mpad,
-                                                          b->zeta * delta * delta, b->alpha.p,
-                                                          b->kcoef.p);
+    k_prep_alpha<<<(b->Mpad + 255) / 256, 256, 0, C.st>>>(ta.p, b->M, b->Mpad, b->alpha.p);
     TGB_CUDA(cudaGetLastError());
     TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st));
     TGB_TRY(make_tma_bf16(&b->tmB1, b->QsA.p, b->Mpad, b->K1, b->K1, kGemmBN));

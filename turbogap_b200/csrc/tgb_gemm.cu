@@ -113,18 +113,17 @@ __host__ __device__ constexpr uint32_t make_idesc(int M, int N) {
            ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32"
-        " {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// 32 consecutive accumulator columns of this warp's 32 TMEM lanes (one row per
+// lane). The wait names the destination registers as operands, so no use of
+// them can be scheduled before the load has completed.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31]) : : "memory");
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
 __device__ __forceinline__ double ipow_d(double x, int e) {
@@ -132,16 +131,25 @@ __device__ __forceinline__ double ipow_d(double x, int e) {
     for (int k = 0; k < e; ++k) r *= x;
     return r;
 }
-__device__ __forceinline__ float ipow_f(float x, int e) {
-    float r = 1.f;
-    for (int k = 0; k < e; ++k) r *= x;
-    return r;
-}
 
 constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK, STAGES = kGemmStages;
+constexpr int EPI_WARPS = 4 * kGemmEpiGroups;        // kGemmEpiGroups warps per TMEM lane quarter
+constexpr int THREADS = 64 + 32 * EPI_WARPS;
+constexpr int COLS_PER_WARP = BN / kGemmEpiGroups;   // accumulator columns one epilogue warp reads
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
-constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256;
+constexpr size_t PRM_BYTES = (size_t)EPI_WARPS * 32 * sizeof(double2);
+constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256 + PRM_BYTES;
 constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
+
+// Epilogue variants (compile-time, so the element loop has no mode branches).
+enum { MODE_GAP_Z4 = 0, MODE_GAP_ZINT = 1, MODE_GAP_ZREAL = 2, MODE_STORE = 3 };
+
+template <int MODE>
+__device__ __forceinline__ double kpow_m1(double K, const GemmEpi &ep) {
+    if (MODE == MODE_GAP_Z4) return (K * K) * K;
+    if (MODE == MODE_GAP_ZINT) return ipow_d(K, ep.zeta_int - 1);
+    return pow(K, ep.zeta_f - 1.0);
+}
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
@@ -150,8 +158,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 // Persistent: CTA b processes tiles b, b + gridDim.x, ... (column tile fastest,
 // so concurrently resident CTAs share A rows in L2). Stage counters of the
 // shared-memory ring run across tiles; accumulator it % 2 is reused every
-// second tile once the epilogue has released it.
-__global__ void __launch_bounds__(192, 1)
+// second tile once all epilogue warps have released it.
+template <int MODE>
+__global__ void __launch_bounds__(THREADS, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               int num_kb, int n_tiles_m, int n_tiles_n, GemmEpi ep, unsigned *err) {
     extern __shared__ uint8_t smem_raw[];
@@ -159,12 +168,14 @@ __global__ void __launch_bounds__(192, 1)
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
     const uint32_t sA = base, sB = base + STAGES * A_BYTES;
-    // barriers: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], then the TMEM slot
+    // barriers: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], then the
+    // TMEM slot; the per-warp column-parameter slots follow the 256-byte block
     const uint32_t bars = sB + STAGES * B_BYTES;
     const uint32_t full0 = bars, empty0 = bars + 8 * STAGES;
     const uint32_t accf0 = bars + 16 * STAGES, acce0 = accf0 + 16;
     const uint32_t slot_addr = acce0 + 16;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + (slot_addr - base));
+    double2 *prm_all = reinterpret_cast<double2 *>(gbase + (bars + 256 - base));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_tiles = n_tiles_m * n_tiles_n;
@@ -175,8 +186,8 @@ __global__ void __launch_bounds__(192, 1)
             mbar_init(empty0 + 8 * s, 1);
         }
         for (int a = 0; a < 2; ++a) {
-            mbar_init(accf0 + 8 * a, 1);   // tcgen05.commit of the last k-block
-            mbar_init(acce0 + 8 * a, 4);   // one arrive per epilogue warp
+            mbar_init(accf0 + 8 * a, 1);           // tcgen05.commit of the last k-block
+            mbar_init(acce0 + 8 * a, EPI_WARPS);   // one arrive per epilogue warp
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -248,7 +259,11 @@ __global__ void __launch_bounds__(192, 1)
             tc_commit(accf0 + 8 * a);
         }
     } else if (warp >= 2) {
-      // ---- epilogue, one tile at a time
+      // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (the lane quarter
+      // the hardware lets it access) and column group (w - 2) / 4 of the tile
+      const int q = warp & 3;
+      const int grp = (warp - 2) >> 2;
+      double2 *prm = prm_all + (warp - 2) * 32;
       int it = 0;
       for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
         const int a = it & 1;
@@ -261,89 +276,76 @@ __global__ void __launch_bounds__(192, 1)
             break;
         }
         tc_fence_after();
-        const int q = warp & 3;
         const int row = m0 + q * 32 + lane;
         const bool row_ok = row < ep.rows;
         const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
-        if (ep.mode == EPI_GAP_KERNEL) {
-            double e[4] = {0, 0, 0, 0}, ks[4] = {0, 0, 0, 0};
+        if constexpr (MODE != MODE_STORE) {
+            double e4[4] = {0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};
             const double qo = row_ok ? ep.qoff[row] : 0.0;
-            for (int c = 0; c < BN / 32; ++c) {
-                // column parameters of this 32-column block: lane l loads column l,
-                // the j loop broadcasts them by shuffle
-                const int cl = n0 + c * 32 + lane;
-                const bool cin = cl < ep.Mpad;
-                const double p_al = cin ? ep.alpha[cl] : 0.0;
-                const double p_kc = cin ? ep.kcoef[cl] : 0.0;
-                const double p_ao = cin ? ep.aoff[cl] : 0.0;
+            const float c0f = (float)ep.c0;
+            for (int c = 0; c < COLS_PER_WARP / 32; ++c) {
+                const int col = grp * COLS_PER_WARP + c * 32;
+                const int gcol = n0 + col;
+                if (gcol >= ep.Mpad) break;   // warp-uniform; Mpad is a multiple of 32
+                // column parameters (alpha_s, mu . q_s): lane l loads column gcol + l,
+                // the element loop reads them back as shared-memory broadcasts
+                __syncwarp();
+                prm[lane] = make_double2(ep.alpha[gcol + lane], ep.aoff[gcol + lane]);
+                __syncwarp();
+                float v[32];
+                tmem_ld32(taddr + (uint32_t)col, v);
+                __align__(16) __nv_bfloat16 hi[32], lo[32];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float v[16];
-                    __syncwarp();
-                    tmem_ld16(taddr + c * 32 + h * 16, v);
-                    const int col0 = n0 + c * 32 + h * 16;
-                    __align__(16) __nv_bfloat16 hi[16], lo[16];
+                for (int j = 0; j < 32; ++j) {
+                    const double2 p = prm[j];
+                    const double K = ((double)v[j] + p.y) + qo;
+                    const double t1 = p.x * kpow_m1<MODE>(K, ep);   // alpha_s K^(zeta-1)
+                    k4[j & 3] += t1;
+                    e4[j & 3] = fma(t1, K, e4[j & 3]);
+                    // kd_s - kcoef_s = zeta delta^2 (alpha_s K^(zeta-1) - alpha_s)
+                    bf16_split((float)(t1 - p.x) * c0f, hi[j], lo[j]);
+                }
+                if (row_ok) {
+                    __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + gcol;
+                    const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
+                    const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
+                    uint4 *d0 = reinterpret_cast<uint4 *>(kr);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int src = h * 16 + j;
-                        const double al = __shfl_sync(0xffffffffu, p_al, src);
-                        const double kc = __shfl_sync(0xffffffffu, p_kc, src);
-                        const double ao = __shfl_sync(0xffffffffu, p_ao, src);
-                        const double K = (double)v[j] + ao + qo;
-                        double kz, km1;
-                        if (ep.zeta_int == 4) {
-                            const double K2 = K * K;
-                            km1 = K2 * K;
-                            kz = K2 * K2;
-                        } else if (ep.zeta_int > 0) {
-                            km1 = ipow_d(K, ep.zeta_int - 1);
-                            kz = km1 * K;
-                        } else {
-                            km1 = pow(K, ep.zeta_f - 1.0);
-                            kz = pow(K, ep.zeta_f);
-                        }
-                        e[j & 3] += al * kz;
-                        const double kd = kc * km1;
-                        ks[j & 3] += kd;
-                        bf16_split((float)(kd - kc), hi[j], lo[j]);
-                    }
-                    if (row_ok && col0 < ep.Mpad) {
-                        __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + col0;
-                        const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
-                        const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
-                        uint4 *d0 = reinterpret_cast<uint4 *>(kr);
-                        d0[0] = h4[0];
-                        d0[1] = h4[1];
-                        if (ep.nsplit == 3) {
-                            uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
-                            uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
-                            d1[0] = h4[0];
-                            d1[1] = h4[1];
-                            d2[0] = l4[0];
-                            d2[1] = l4[1];
+                    for (int u = 0; u < 4; ++u) d0[u] = h4[u];
+                    if (ep.nsplit == 3) {
+                        uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
+                        uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            d1[u] = h4[u];
+                            d2[u] = l4[u];
                         }
                     }
                 }
             }
             if (row_ok) {
-                ep.epart[(size_t)row * n_tiles_n + tile_n] = (e[0] + e[1]) + (e[2] + e[3]);
-                ep.kdsum[(size_t)row * n_tiles_n + tile_n] = (ks[0] + ks[1]) + (ks[2] + ks[3]);
+                const size_t o = ((size_t)row * n_tiles_n + tile_n) * kGemmEpiGroups + grp;
+                ep.epart[o] = (e4[0] + e4[1]) + (e4[2] + e4[3]);
+                ep.kdsum[o] = ep.c0 * ((k4[0] + k4[1]) + (k4[2] + k4[3]));
             }
         } else {
-            for (int c = 0; c < BN / 16; ++c) {
-                float v[16];
-                __syncwarp();
-                tmem_ld16(taddr + c * 16, v);
-                const int col0 = n0 + c * 16;
-                if (!row_ok || col0 >= ep.cols) continue;
-                float *o = ep.out + (size_t)row * ep.ldo + col0;
-                if (col0 + 16 <= ep.cols) {
+            for (int c = 0; c < COLS_PER_WARP / 32; ++c) {
+                const int col = grp * COLS_PER_WARP + c * 32;
+                const int gcol = n0 + col;
+                if (gcol >= ep.cols) break;   // warp-uniform
+                float v[32];
+                tmem_ld32(taddr + (uint32_t)col, v);
+                if (!row_ok) continue;
+                float *o = ep.out + (size_t)row * ep.ldo + gcol;
+                if (gcol + 32 <= ep.cols) {
                     float4 *o4 = reinterpret_cast<float4 *>(o);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j)
+                    for (int j = 0; j < 8; ++j)
                         o4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
                 } else {
-                    for (int j = 0; j < 16 && col0 + j < ep.cols; ++j) o[j] = v[j];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (gcol + j < ep.cols) o[j] = v[j];
                 }
             }
         }
@@ -406,15 +408,21 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
     // 16-byte vector stores in the epilogues
     TGB_CHECK(ep.mode != EPI_STORE_F32 || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
               TG_ERR_ARG, "fp32 output rows must be 16-byte aligned (ldo %% 4 == 0)");
-    TGB_CHECK(ep.mode != EPI_GAP_KERNEL || (ep.K2 % 8 == 0 && ep.Mpad % 16 == 0 &&
+    TGB_CHECK(ep.mode != EPI_GAP_KERNEL || (ep.K2 % 8 == 0 && ep.Mpad % 32 == 0 &&
                                             ((uintptr_t)ep.kd & 15) == 0),
-              TG_ERR_ARG, "bf16 kernel-derivative rows must be 16-byte aligned");
+              TG_ERR_ARG, "bf16 kernel-derivative rows must be 16-byte aligned, Mpad %% 32 == 0");
     if (M <= 0 || N <= 0) return TG_OK;
-    static bool attr = false;
-    if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    int mode = MODE_STORE;
+    if (ep.mode == EPI_GAP_KERNEL)
+        mode = ep.zeta_int == 4 ? MODE_GAP_Z4 : ep.zeta_int > 0 ? MODE_GAP_ZINT : MODE_GAP_ZREAL;
+    using Kern = void (*)(CUtensorMap, CUtensorMap, int, int, int, GemmEpi, unsigned *);
+    static const Kern kerns[4] = {k_gemm_tn<MODE_GAP_Z4>, k_gemm_tn<MODE_GAP_ZINT>,
+                                  k_gemm_tn<MODE_GAP_ZREAL>, k_gemm_tn<MODE_STORE>};
+    static bool attr[4] = {false, false, false, false};
+    if (!attr[mode]) {
+        TGB_CUDA(cudaFuncSetAttribute(kerns[mode], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)SMEM_BYTES));
-        attr = true;
+        attr[mode] = true;
     }
     static int n_sm = 0;
     if (!n_sm) {
@@ -424,7 +432,7 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
     }
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     const int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
-    k_gemm_tn<<<grid, 192, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tm, tn, ep, err);
+    kerns[mode]<<<grid, THREADS, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tm, tn, ep, err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -11,11 +11,13 @@ namespace tgb {
 // contiguous), fp32 accumulation in tensor memory, fused epilogue:
 //   EPI_GAP_KERNEL  (GEMM 1 on centred operands, C = (q - mu).(q_s - mu)):
 //       K = C + aoff[s] + qoff[row]                          (FP64; the exact rank-1 terms)
-//       epart[row][tile] = sum_s alpha_s K^zeta              (FP64)
-//       kdsum[row][tile] = sum_s kd_s                        (FP64)
+//       epart[row][e] = sum_s alpha_s K^zeta                 (FP64)
+//       kdsum[row][e] = sum_s kd_s                           (FP64)
 //       kd[row][s + t*Mpad] = split(kd_s - kcoef_s), kd_s = kcoef_s K^(zeta-1),
-//                             kcoef_s = zeta delta^2 alpha_s (the K = 1 value is
-//                             carried exactly by the caller)
+//                             kcoef_s = c0 alpha_s, c0 = zeta delta^2 (the K = 1
+//                             value is carried exactly by the caller)
+//     The partial sums e run over the gemm_n_etiles(Mpad) column slices of
+//     kGemmBN / kGemmEpiGroups sparse points; the consumer adds them up.
 //   EPI_STORE_F32   (GEMM 2, sum_s (kd_s - kcoef_s)(q_s - mu)): out[row][col] = C
 enum EpiMode { EPI_GAP_KERNEL = 0, EPI_STORE_F32 = 1 };
 
@@ -25,11 +27,11 @@ struct GemmEpi {
     int cols;             // valid columns of C
     // EPI_GAP_KERNEL
     const double *alpha;  // [Mpad]
-    const double *kcoef;  // [Mpad] = zeta delta^2 alpha_s
+    double c0;            // zeta delta^2
     int zeta_int;         // > 0: integer power; 0: use zeta_f
     double zeta_f;
-    double *epart;        // [rows][n_tiles_n]
-    double *kdsum;        // [rows][n_tiles_n]
+    double *epart;        // [rows][gemm_n_etiles(Mpad)]
+    double *kdsum;        // [rows][gemm_n_etiles(Mpad)]
     const double *aoff;   // [Mpad]: mu . q_s
     const double *qoff;   // [rows]: (q - mu) . mu
     __nv_bfloat16 *kd;    // [rows][K2]
@@ -43,6 +45,7 @@ constexpr int kGemmBM = 128;
 constexpr int kGemmBN = 256;
 constexpr int kGemmBK = 64;
 constexpr int kGemmStages = 4;
+constexpr int kGemmEpiGroups = 2;   // epilogue warps per TMEM lane quarter (column groups)
 
 struct TmaMap {
     alignas(64) CUtensorMap map;
@@ -56,7 +59,8 @@ int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
                    unsigned *err, cudaStream_t st);
 
-// Number of N tiles the energy partials are split into.
 inline int gemm_n_tiles(int N) { return (N + kGemmBN - 1) / kGemmBN; }
+// Number of column slices the energy partials are split into.
+inline int gemm_n_etiles(int N) { return gemm_n_tiles(N) * kGemmEpiGroups; }
 
 }  // namespace tgb
