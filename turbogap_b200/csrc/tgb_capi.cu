@@ -64,6 +64,7 @@ struct Block {
     DBuf<float> table, selfR;
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
+    DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d
     TmaMap tmB1{}, tmB2{};
 
     SoapParams params(int n_atoms) const {
@@ -442,6 +443,17 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     TGB_TRY(b->mu.ensure(b->dim));
     TGB_TRY(b->aoff.ensure(b->Mpad));
     TGB_TRY(b->g0.ensure(b->dim));
+    TGB_TRY(b->ref_index.ensure(b->dim));
+    // The device keeps descriptor entries in its internal order (l-major); the
+    // sparse set is permuted into that order once here.
+    std::vector<int> ref(b->dim);
+    for (int d = 0; d < b->dim; ++d) ref[d] = descriptor_ref_index(d, b->ntot, b->lmax + 1);
+    std::vector<double> Qi((size_t)n_sparse * b->dim);
+    for (int s = 0; s < n_sparse; ++s)
+        for (int d = 0; d < b->dim; ++d)
+            Qi[(size_t)s * b->dim + d] = Qs[(size_t)s * b->dim + ref[d]];
+    Qs = Qi.data();
+    TGB_CUDA(cudaMemcpy(b->ref_index.p, ref.data(), sizeof(int) * b->dim, cudaMemcpyHostToDevice));
     // Centre of the sparse set (FP64): the GEMMs run on q - mu and q_s - mu, the
     // exact rank-1 terms mu.q_s and (q - mu).mu are added in the epilogue.
     {
@@ -537,10 +549,14 @@ __global__ void k_seen(int n_sites, const int *__restrict__ site_row, const int6
 }
 
 // q = mu + delta (rows of dim)
+// q = mu + delta, written back in the reference order of the descriptor entries.
 __global__ void k_d2f(int64_t n, int dim, const float *__restrict__ a, const double *__restrict__ mu,
-                      double *__restrict__ b) {
+                      const int *__restrict__ ref_index, double *__restrict__ b) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) b[i] = mu[i % dim] + (double)a[i];
+    if (i >= n) return;
+    const int64_t site = i / dim;
+    const int d = (int)(i - site * dim);
+    b[site * dim + ref_index[d]] = mu[d] + (double)a[i];
 }
 
 __global__ void k_gather_species(int64_t P, const int *__restrict__ nbr, const int *__restrict__ sp,
@@ -720,7 +736,7 @@ int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0
     DBuf<double> out;
     TGB_TRY(out.ensure((size_t)nc * b.dim));
     k_d2f<<<grid_for((int64_t)nc * b.dim), 256, 0, C.st>>>((int64_t)nc * b.dim, b.dim, wp->q.p,
-                                                            b.mu.p, out.p);
+                                                            b.mu.p, b.ref_index.p, out.p);
     TGB_CUDA(cudaGetLastError());
     TGB_CUDA(cudaMemcpyAsync(soap, out.p, sizeof(double) * nc * b.dim, cudaMemcpyDeviceToHost, C.st));
     TGB_CUDA(cudaStreamSynchronize(C.st));

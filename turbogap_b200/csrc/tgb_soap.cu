@@ -225,6 +225,12 @@ static void poly3_jacobi_W(int amax, double *W) {
 
 int table_width(int amax, int lmax) { return 4 * (amax + lmax + 1); }
 
+int descriptor_ref_index(int d_internal, int nt, int nl) {
+    const int np = nt * (nt + 1) / 2;
+    const int l = d_internal / np, pi = d_internal - l * np;
+    return pi * nl + l;
+}
+
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st) {
     const int amax = h.alpha_max[0];
     const int tw = table_width(amax, h.lmax);
@@ -411,8 +417,13 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                 const float4 *T = reinterpret_cast<const float4 *>(
                     P.table + (size_t)s * (kTableIntervals + 1) * (4 * NF));
                 const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
+                float rv[AMAX];
 #pragma unroll
-                for (int n = 0; n < AMAX; ++n) Rs[t * AMAX + n] = hm.value(T, NF, n);
+                for (int n = 0; n < AMAX; ++n) rv[n] = hm.value(T, NF, n);
+                float4 *r4 = reinterpret_cast<float4 *>(Rs + t * AMAX);
+#pragma unroll
+                for (int q = 0; q < AMAX / 4; ++q)
+                    r4[q] = make_float4(rv[4 * q], rv[4 * q + 1], rv[4 * q + 2], rv[4 * q + 3]);
 #pragma unroll
                 for (int l = 0; l < NL; ++l) As[t * NL + l] = hm.value(T, NF, AMAX + l);
                 const float ir = 1.f / r;
@@ -466,41 +477,52 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                 O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)v;
             }
     __syncwarp();
-    auto power = [&](int d) -> double {
-        const int pi = d / NL, l = d - pi * NL;
+    // Power spectrum in the internal order u = l * NP + pi. For each l the NP
+    // channel pairs (n <= n2) run across lanes, so one warp-wide load reads
+    // c_{n,lm} of at most NT distinct n: distinct bank pairs (the row stride NLM
+    // is odd), one shared-memory wavefront per load and no divergence in m.
+    constexpr int NP = NT * (NT + 1) / 2;
+    auto power = [&](int l, int pi) -> double {
         const int n = pair_n[pi], n2 = pair_n2[pi];
         const double *c1 = cs + n * NLM + l * l, *c2 = cs + n2 * NLM + l * l;
         double v = 0.0;
+#pragma unroll
         for (int m = 0; m < 2 * l + 1; ++m) v += c1[m] * c2[m];
         return n != n2 ? v * 1.4142135623730951 : v;
     };
     // pass 1: |p| (FP64)
     double nrm2 = 0.0;
-    for (int d = lane; d < DIM; d += 32) {
-        const double v = power(d);
-        nrm2 += v * v;
-    }
+#pragma unroll
+    for (int l = 0; l < NL; ++l)
+        for (int pi = lane; pi < NP; pi += 32) {
+            const double v = power(l, pi);
+            nrm2 += v * v;
+        }
     nrm2 = warp_sum(nrm2);
     const double nrm = sqrt(nrm2);
     const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
     // pass 2: q = p/|p|, delta = q - mu, delta . mu; operand rows hold split(delta)
     const int K1 = P.K1;
     __nv_bfloat16 *qs = O.qsplit + (size_t)site * K1;
+    float *qrow = O.q + (size_t)site * DIM;
     double off = 0.0;
-    for (int d = lane; d < DIM; d += 32) {
-        const double mu = P.mu[d];
-        const double dl = power(d) * inv - mu;
-        off += dl * mu;
-        const float df = (float)dl;
-        O.q[(size_t)site * DIM + d] = df;
-        __nv_bfloat16 hi, lo;
-        bf16_split(df, hi, lo);
-        qs[d] = hi;
-        if (P.nsplit == 3) {
-            qs[DIM + d] = hi;
-            qs[2 * DIM + d] = lo;
+#pragma unroll
+    for (int l = 0; l < NL; ++l)
+        for (int pi = lane; pi < NP; pi += 32) {
+            const int u = l * NP + pi;
+            const double mu = P.mu[u];
+            const double dl = power(l, pi) * inv - mu;
+            off += dl * mu;
+            const float df = (float)dl;
+            qrow[u] = df;
+            __nv_bfloat16 hi, lo;
+            bf16_split(df, hi, lo);
+            qs[u] = hi;
+            if (P.nsplit == 3) {
+                qs[DIM + u] = hi;
+                qs[2 * DIM + u] = lo;
+            }
         }
-    }
     off = warp_sum(off);
     for (int d = P.nsplit * DIM + lane; d < K1; d += 32) qs[d] = __float2bfloat16_rn(0.f);
     if (lane == 0) {
@@ -569,19 +591,24 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
         dot = warp_sum(dot);
         const double nrm = I.pnorm[site];
         const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-        for (int d = lane; d < DIM; d += 32) {
-            const double mu = P.mu[d];
-            const double gd = ksum * mu + P.g0[d] + (double)g[d], qd = mu + (double)q[d];
-            const float h = (float)((gd - dot * qd) * inv);
-            const int pi = d / NL, l = d - pi * NL;
-            const int n = pair_n[pi], n2 = pair_n2[pi];
+        // descriptor entries in the internal order d = l * NP + pi
+        constexpr int NP = NT * (NT + 1) / 2;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
             float *Bl = Bm + l * Sh::BSTRIDE;
-            if (n == n2) {
-                Bl[n * NT + n] = 2.f * h;
-            } else {
-                const float v = 1.41421356237309515f * h;
-                Bl[n * NT + n2] = v;
-                Bl[n2 * NT + n] = v;
+            for (int pi = lane; pi < NP; pi += 32) {
+                const int d = l * NP + pi;
+                const double mu = P.mu[d];
+                const double gd = ksum * mu + P.g0[d] + (double)g[d], qd = mu + (double)q[d];
+                const float h = (float)((gd - dot * qd) * inv);
+                const int n = pair_n[pi], n2 = pair_n2[pi];
+                if (n == n2) {
+                    Bl[n * NT + n] = 2.f * h;
+                } else {
+                    const float v = 1.41421356237309515f * h;
+                    Bl[n * NT + n2] = v;
+                    Bl[n2 * NT + n] = v;
+                }
             }
         }
         __syncwarp();

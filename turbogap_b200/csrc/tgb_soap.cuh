@@ -36,6 +36,12 @@ struct SiteArgs {
     const int *species;      // global species id per unit-cell atom
 };
 
+// Descriptor entries on the device run in the internal order d = l * NP + pi
+// (NP = NT (NT + 1) / 2 channel pairs n <= n2, pi in row-major upper-triangle
+// order); the reference order is pi * (l_max + 1) + l. The sparse set, mu and g0
+// are stored in the internal order, so the GEMMs see a consistent permutation.
+int descriptor_ref_index(int d_internal, int nt, int nl);
+
 struct DescOut {
     __nv_bfloat16 *qsplit;   // [n_sites][K1]: bf16 split of delta = q - mu
     float *q;                // [n_sites][dim]: delta = q - mu (fp32)
