@@ -196,13 +196,58 @@ int tg_engine_stream(tg_engine *e, void **stream);
  * bench uses this for device-resident timing. */
 int tg_engine_compute_device(tg_engine *e);
 /* n_steps MD steps launched eagerly with CUDA events between the passes of each
- * step on the engine's stream; ms_per_pass[6] receives the mean milliseconds per
- * step of: neighbour list, descriptor, GEMM 1, GEMM 2, forces+virial, integrate
- * (every block summed into its pass). *n_passes = 6. */
+ * step on the engine's stream; ms_per_pass[7] receives the mean milliseconds per
+ * step of: neighbour list, descriptor, GEMM 1, GEMM 2, forces+virial, integrate,
+ * MLP ensemble + gate (every block summed into its pass). *n_passes = 7. */
 int tg_engine_profile(tg_engine *e, int32_t n_steps, double dt, double *ms_per_pass,
                       int32_t *n_passes);
 /* Kernel launches in one graph-captured MD step (0 before the first graph exists). */
 int tg_engine_graph_kernels(tg_engine *e, int32_t *n_kernels);
+
+/* ---- learned surrogate (mixed form). No reference counterpart: TurboGAP has
+ *   no learned model. Per block, an ensemble of n_members MLPs
+ *   dim -> hidden -> hidden -> 1 (SiLU) maps delta = q - mu of a central site
+ *   (the block's internal descriptor order, as the engine holds it) to its GAP
+ *   energy; dE/dq comes from the network's input gradient and goes through the
+ *   same fused force contraction as the GAP path. Training runs on the GPU
+ *   (bf16 GEMMs, fp32 accumulation and master weights, Adam) on (delta, E,
+ *   dE/dq) samples, with the loss 1/B sum (E - y)^2 + lam/(B D) sum |dE/dx - G|^2
+ *   in units normalised by sigma_x (delta scale) and sigma_e (energy scale).
+ *   W1 is hidden x dim, W2 hidden x hidden, row-major FP64 on the host. */
+typedef struct tg_mlp tg_mlp;
+
+int tg_mlp_create(int32_t dim, int32_t hidden, int32_t n_members, uint64_t seed, tg_mlp **out);
+int tg_mlp_destroy(tg_mlp *m);
+int tg_mlp_set_member(tg_mlp *m, int32_t member, const double *W1, const double *b1,
+                      const double *W2, const double *b2, const double *w3, double b3);
+int tg_mlp_get_member(tg_mlp *m, int32_t member, double *W1, double *b1, double *W2, double *b2,
+                      double *w3, double *b3);
+/* Scales of the normalised units; unset (0) they are taken from the data set at
+ * the first tg_mlp_train. */
+int tg_mlp_set_normalisation(tg_mlp *m, double sigma_x, double mean_e, double sigma_e);
+int tg_mlp_get_normalisation(tg_mlp *m, double *sigma_x, double *mean_e, double *sigma_e);
+/* Append samples: delta (n, dim) fp32, energies (n) eV, dE/dq (n, dim) fp32. */
+int tg_mlp_add_samples(tg_mlp *m, int32_t n, const float *delta, const double *energy,
+                       const float *dedq);
+/* Append the central sites of engine block `block` (0-based) from its last exact
+ * evaluation (tg_engine_compute or an MD step), device to device. */
+int tg_mlp_add_engine_samples(tg_mlp *m, tg_engine *e, int32_t block);
+int tg_mlp_n_samples(tg_mlp *m, int64_t *n);
+/* epochs over the shuffled data set in batches of `batch` (a multiple of 32);
+ * loss_per_epoch[epochs] receives the mean normalised loss of each epoch. */
+int tg_mlp_train(tg_mlp *m, int32_t epochs, int32_t batch, double lr, double force_weight,
+                 uint64_t seed, double *loss_per_epoch);
+/* Ensemble mean energy (eV), its spread (population standard deviation over
+ * members, eV; may be NULL) and mean dE/d(delta) (n, dim; may be NULL). */
+int tg_mlp_predict(tg_mlp *m, int32_t n, const float *delta, double *energy_mean,
+                   double *energy_std, double *dedq_mean);
+/* Mixed form for engine block `block`: every step the ensemble evaluates all
+ * central sites; sites whose spread exceeds gate_ev are evaluated by the exact
+ * GAP kernel instead (compacted on the device, same CUDA graph). m = NULL
+ * returns the block to the exact form. The MLP must outlive its use here. */
+int tg_engine_set_mlp(tg_engine *e, int32_t block, tg_mlp *m, double gate_ev);
+/* Sites of the block and how many the last step sent to the exact kernel. */
+int tg_engine_mlp_stats(tg_engine *e, int32_t block, int32_t *n_gated, int32_t *n_sites);
 
 #ifdef __cplusplus
 }

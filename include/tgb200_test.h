@@ -20,6 +20,17 @@ extern "C" {
 int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t *A, const uint16_t *B,
                      float *C);
 
+struct tg_mlp;
+/* Loss and parameter gradients of one member on one batch of B normalised
+ * samples (x (B, dim), y (B), gref (B, dim) fp32), without updating it. grads
+ * uses the flat parameter layout of tgx_mlp_layout; E (B) and G (B, Dp) receive
+ * the forward energies and input gradients. */
+int tgx_mlp_batch_grads(struct tg_mlp *m, int32_t member, int32_t B, const float *x,
+                        const float *y, const float *gref, double lam, double *grads,
+                        double *loss, float *E, float *G);
+/* offsets[9] = {D, Dp, H, offset of W1, b1, W2, b2, w3, b3} in the flat layout. */
+int tgx_mlp_layout(struct tg_mlp *m, int64_t *offsets);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,7 +80,25 @@ SIGNATURES = [
     ("tg_engine_compute_device", C.c_int, [_vp]),
     ("tg_engine_profile", C.c_int, [_vp, C.c_int32, C.c_double, dp, C.POINTER(C.c_int32)]),
     ("tg_engine_graph_kernels", C.c_int, [_vp, C.POINTER(C.c_int32)]),
+    ("tg_mlp_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_vp)]),
+    ("tg_mlp_destroy", C.c_int, [_vp]),
+    ("tg_mlp_set_member", C.c_int, [_vp, C.c_int32, dp, dp, dp, dp, dp, C.c_double]),
+    ("tg_mlp_get_member", C.c_int, [_vp, C.c_int32, dp, dp, dp, dp, dp, C.POINTER(C.c_double)]),
+    ("tg_mlp_set_normalisation", C.c_int, [_vp, C.c_double, C.c_double, C.c_double]),
+    ("tg_mlp_get_normalisation", C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]),
+    ("tg_mlp_add_samples", C.c_int, [_vp, C.c_int32, f32p, dp, f32p]),
+    ("tg_mlp_add_engine_samples", C.c_int, [_vp, _vp, C.c_int32]),
+    ("tg_mlp_n_samples", C.c_int, [_vp, C.POINTER(C.c_int64)]),
+    ("tg_mlp_train", C.c_int, [_vp, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_uint64,
+                               dp]),
+    ("tg_mlp_predict", C.c_int, [_vp, C.c_int32, f32p, dp, dp, dp]),
+    ("tg_engine_set_mlp", C.c_int, [_vp, C.c_int32, _vp, C.c_double]),
+    ("tg_engine_mlp_stats", C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("tgx_gemm_bf16_tn", C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16p, u16p, f32p]),
+    ("tgx_mlp_batch_grads", C.c_int, [_vp, C.c_int32, C.c_int32, f32p, f32p, f32p, C.c_double, dp,
+                                      C.POINTER(C.c_double), f32p, f32p]),
+    ("tgx_mlp_layout", C.c_int, [_vp, i64p]),
 ]
 
 _lib = None

@@ -250,7 +250,7 @@ class Engine:
     def handle(self):
         return self._h
 
-    PASSES = ("neighbors", "descriptor", "gemm1", "gemm2", "forces", "integrate")
+    PASSES = ("neighbors", "descriptor", "gemm1", "gemm2", "forces", "integrate", "mlp")
 
     def profile(self, n_steps: int, dt: float) -> dict:
         """Mean ms per step of each pass over n_steps eager MD steps (CUDA events)."""
@@ -285,3 +285,112 @@ def gemm_bf16_tn(A_bf16: np.ndarray, B_bf16: np.ndarray) -> np.ndarray:
     check(lib().tgx_gemm_bf16_tn(M, N, K, np.ascontiguousarray(A_bf16, np.uint16),
                                  np.ascontiguousarray(B_bf16, np.uint16), out))
     return out
+
+
+class Mlp:
+    """Ensemble of per-atom energy MLPs for one SOAP block (the learned surrogate).
+
+    Inputs are delta = q - mu rows of the block (the device's descriptor order);
+    outputs are per-atom energies (eV) and dE/d(delta). Training, inference and
+    the engine's mixed form run on the GPU through libtgb200.so."""
+
+    def __init__(self, dim: int, hidden: int = 256, n_members: int = 4, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().tg_mlp_create(int(dim), int(hidden), int(n_members), int(seed), C.byref(h)))
+        self._h = h
+        self.dim, self.hidden, self.n_members = int(dim), int(hidden), int(n_members)
+
+    def close(self):
+        if self._h:
+            lib().tg_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_member(self, k, W1, b1, W2, b2, w3, b3):
+        check(lib().tg_mlp_set_member(self._h, int(k), _f64(W1), _f64(b1), _f64(W2), _f64(b2),
+                                      _f64(w3), float(b3)))
+
+    def get_member(self, k):
+        H, D = self.hidden, self.dim
+        W1, b1, W2 = np.zeros((H, D)), np.zeros(H), np.zeros((H, H))
+        b2, w3, b3 = np.zeros(H), np.zeros(H), C.c_double(0.0)
+        check(lib().tg_mlp_get_member(self._h, int(k), W1, b1, W2, b2, w3, C.byref(b3)))
+        return W1, b1, W2, b2, w3, float(b3.value)
+
+    def set_normalisation(self, sigma_x, mean_e, sigma_e):
+        check(lib().tg_mlp_set_normalisation(self._h, float(sigma_x), float(mean_e), float(sigma_e)))
+
+    def normalisation(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(lib().tg_mlp_get_normalisation(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def add_samples(self, delta, energy, dedq):
+        delta = np.ascontiguousarray(delta, np.float32)
+        check(lib().tg_mlp_add_samples(self._h, delta.shape[0], delta, _f64(energy),
+                                       np.ascontiguousarray(dedq, np.float32)))
+
+    def add_engine_samples(self, engine: "Engine", block: int):
+        check(lib().tg_mlp_add_engine_samples(self._h, engine.handle, int(block)))
+
+    def n_samples(self) -> int:
+        n = C.c_int64(0)
+        check(lib().tg_mlp_n_samples(self._h, C.byref(n)))
+        return int(n.value)
+
+    def train(self, epochs: int, batch: int = 512, lr: float = 1e-3, force_weight: float = 1.0,
+              seed: int = 0) -> np.ndarray:
+        loss = np.zeros(max(int(epochs), 1))
+        check(lib().tg_mlp_train(self._h, int(epochs), int(batch), float(lr), float(force_weight),
+                                 int(seed), loss))
+        return loss[:int(epochs)]
+
+    def predict(self, delta):
+        delta = np.ascontiguousarray(delta, np.float32)
+        n = delta.shape[0]
+        em, es, g = np.zeros(n), np.zeros(n), np.zeros((n, self.dim))
+        check(lib().tg_mlp_predict(self._h, n, delta, em, es, g))
+        return em, es, g
+
+    def layout(self):
+        o = np.zeros(9, np.int64)
+        check(lib().tgx_mlp_layout(self._h, o))
+        return dict(zip(("D", "Dp", "H", "W1", "b1", "W2", "b2", "w3", "b3"), map(int, o)))
+
+    def batch_grads(self, member, x, y, gref, lam):
+        """Test hook: loss, flat gradients, E and G of one normalised batch."""
+        L = self.layout()
+        B = x.shape[0]
+        n = L["b3"] + 1
+        n = (n + 63) // 64 * 64
+        grads = np.zeros(n)
+        loss = C.c_double(0.0)
+        E = np.zeros(B, np.float32)
+        G = np.zeros((B, L["Dp"]), np.float32)
+        check(lib().tgx_mlp_batch_grads(self._h, int(member), B, np.ascontiguousarray(x, np.float32),
+                                        np.ascontiguousarray(y, np.float32),
+                                        np.ascontiguousarray(gref, np.float32), float(lam), grads,
+                                        C.byref(loss), E, G))
+        return float(loss.value), grads, E, G
+
+
+def engine_set_mlp(engine: "Engine", block: int, mlp: Optional[Mlp], gate_ev: float = 0.005):
+    """Run engine block `block` in the mixed form (MLP ensemble, exact GAP where
+    the ensemble spread exceeds gate_ev); mlp=None restores the exact form."""
+    check(lib().tg_engine_set_mlp(engine.handle, int(block), mlp.handle if mlp else None,
+                                  float(gate_ev)))
+
+
+def engine_mlp_stats(engine: "Engine", block: int):
+    g, n = C.c_int32(0), C.c_int32(0)
+    check(lib().tg_engine_mlp_stats(engine.handle, int(block), C.byref(g), C.byref(n)))
+    return int(g.value), int(n.value)

@@ -3,6 +3,7 @@
 
 #include "tgb_common.cuh"
 #include "tgb_gemm.cuh"
+#include "tgb_mlp.cuh"
 #include "tgb_neighbors.cuh"
 #include "tgb_soap.cuh"
 
@@ -171,7 +172,9 @@ __global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad,
 
 // Optional CUDA-event log of the passes of a step: mark(pass) records an event
 // on the stream; the time since the previous mark is booked to that pass.
-enum Pass { PASS_NEIGH = 0, PASS_DESC, PASS_GEMM1, PASS_GEMM2, PASS_FORCE, PASS_INTEGRATE, N_PASS };
+enum Pass {
+    PASS_NEIGH = 0, PASS_DESC, PASS_GEMM1, PASS_GEMM2, PASS_FORCE, PASS_INTEGRATE, PASS_MLP, N_PASS
+};
 
 struct EventLog {
     std::vector<cudaEvent_t> ev;
@@ -244,6 +247,175 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.out = w.g.p;
     e2.ldo = b.dim;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
+    TGB_MARK(log, PASS_GEMM2, st);
+    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
+    ForceOut FO{forces, energies, w.vpart.p, err};
+    int nblk = 0;
+    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
+    TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
+    TGB_MARK(log, PASS_FORCE, st);
+    return TG_OK;
+}
+
+static unsigned grid_for(int64_t n, int tb = 256) { return (unsigned)((n + tb - 1) / tb); }
+
+// ---------------------------------------------------------------- mixed form
+// Sites whose ensemble spread exceeds the gate go back to the exact GAP kernel:
+// they are compacted on the device and the two GEMMs run over the compacted
+// rows, their count read on the device (the step stays one CUDA graph).
+
+// one warp per site: MLP sites get epart = E / delta^2, kdsum = 0 and
+// g = dE/dq - g0 (so that the force pass's g0 + g is the MLP's dE/dq); gated
+// sites are appended to gidx
+__global__ void k_mlp_mix(int n, int D, int n_et, const double *__restrict__ emean,
+                          const double *__restrict__ estd, double gate, double inv_delta2,
+                          const double *__restrict__ g0, float *__restrict__ g,
+                          double *__restrict__ epart, double *__restrict__ kdsum,
+                          int *__restrict__ gidx, int *__restrict__ gcount) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const bool gated = !(estd[row] <= gate);   // a NaN spread is gated too
+    if (lane == 0) {
+        if (gated) gidx[atomicAdd(gcount, 1)] = row;
+        for (int t = 0; t < n_et; ++t) {
+            epart[(size_t)row * n_et + t] = (!gated && t == 0) ? emean[row] * inv_delta2 : 0.0;
+            kdsum[(size_t)row * n_et + t] = 0.0;
+        }
+    }
+    if (!gated)
+        for (int d = lane; d < D; d += 32) g[(size_t)row * D + d] -= (float)g0[d];
+}
+
+// compacted GEMM-1 operand rows and delta.mu of the gated sites
+__global__ void k_gather_gated(const int *__restrict__ gcount, const int *__restrict__ gidx, int K1,
+                               const __nv_bfloat16 *__restrict__ qsplit,
+                               const double *__restrict__ qoff, __nv_bfloat16 *__restrict__ Qg,
+                               double *__restrict__ qoff_g) {
+    const int r = blockIdx.x;
+    if (r >= *gcount) return;
+    const int site = gidx[r];
+    const uint4 *src = reinterpret_cast<const uint4 *>(qsplit + (size_t)site * K1);
+    uint4 *dst = reinterpret_cast<uint4 *>(Qg + (size_t)r * K1);
+    for (int k = threadIdx.x; k < K1 / 8; k += blockDim.x) dst[k] = src[k];
+    if (threadIdx.x == 0) qoff_g[r] = qoff[site];
+}
+
+__global__ void k_scatter_gated(const int *__restrict__ gcount, const int *__restrict__ gidx, int D,
+                                int n_et, const double *__restrict__ epart_g,
+                                const double *__restrict__ kdsum_g, const float *__restrict__ g_g,
+                                double *__restrict__ epart, double *__restrict__ kdsum,
+                                float *__restrict__ g) {
+    const int r = blockIdx.x;
+    if (r >= *gcount) return;
+    const int site = gidx[r];
+    for (int d = threadIdx.x; d < D; d += blockDim.x) g[(size_t)site * D + d] = g_g[(size_t)r * D + d];
+    for (int t = threadIdx.x; t < n_et; t += blockDim.x) {
+        epart[(size_t)site * n_et + t] = epart_g[(size_t)r * n_et + t];
+        kdsum[(size_t)site * n_et + t] = kdsum_g[(size_t)r * n_et + t];
+    }
+}
+
+// training triples of a block after an exact evaluation: E = delta^2 sum epart,
+// dE/dq = (sum kdsum) mu + g0 + g (one warp per site)
+__global__ void k_collect(int n, int D, int n_et, double delta2, const double *__restrict__ epart,
+                          const double *__restrict__ kdsum, const double *__restrict__ mu,
+                          const double *__restrict__ g0, const float *__restrict__ g,
+                          double *__restrict__ E, float *__restrict__ G) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double ks = 0.0, e = 0.0;
+    for (int t = 0; t < n_et; ++t) {
+        ks += kdsum[(size_t)row * n_et + t];
+        e += epart[(size_t)row * n_et + t];
+    }
+    for (int d = lane; d < D; d += 32)
+        G[(size_t)row * D + d] = (float)(ks * mu[d] + g0[d] + (double)g[(size_t)row * D + d]);
+    if (lane == 0) E[row] = delta2 * e;
+}
+
+struct MixedRun {
+    Mlp *mlp = nullptr;
+    MlpInferWork *iw = nullptr;   // this block's inference buffers
+    double gate = 0.0;
+    int cap = 0;
+    DBuf<__nv_bfloat16> Qg;
+    DBuf<double> qoff_g, epart_g, kdsum_g, emean, estd;
+    DBuf<float> g_g;
+    DBuf<int> gidx, gcount;
+    TmaMap tmQg{};
+
+    int ensure(const Block &b, int n_sites) {
+        const int n = n_sites > 0 ? n_sites : 1;
+        if (n <= cap) return TG_OK;
+        TGB_TRY(Qg.ensure((size_t)n * b.K1));
+        TGB_TRY(qoff_g.ensure(n));
+        TGB_TRY(epart_g.ensure((size_t)n * b.n_etiles));
+        TGB_TRY(kdsum_g.ensure((size_t)n * b.n_etiles));
+        TGB_TRY(emean.ensure(n));
+        TGB_TRY(estd.ensure(n));
+        TGB_TRY(g_g.ensure((size_t)n * b.dim));
+        TGB_TRY(gidx.ensure(n));
+        TGB_TRY(gcount.ensure(1));
+        TGB_TRY(make_tma_bf16(&tmQg, Qg.p, n, b.K1, b.K1, kGemmBM));
+        cap = n;
+        return TG_OK;
+    }
+    ~MixedRun() { mlp_infer_work_delete(iw); }
+};
+
+// Descriptor, MLP ensemble, gate; exact GAP for the gated sites; forces.
+int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S, int n_atoms,
+                         double *forces, double *energies, double *virial, unsigned *err,
+                         cudaStream_t st, EventLog *log = nullptr) {
+    const int n = S.n_sites;
+    if (n <= 0) return TG_OK;
+    TGB_TRY(w.ensure(b, n));
+    TGB_TRY(x.ensure(b, n));
+    TGB_CHECK(x.mlp->L.D == b.dim, TG_ERR_ARG, "MLP input size %d does not match block dim %d",
+              x.mlp->L.D, b.dim);
+    const SoapParams P = b.params(n_atoms);
+    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
+    TGB_TRY(launch_soap_expand(P, S, O, st));
+    TGB_MARK(log, PASS_DESC, st);
+    TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim, st));
+    TGB_CUDA(cudaMemsetAsync(x.gcount.p, 0, sizeof(int), st));
+    k_mlp_mix<<<grid_for((int64_t)n * 32), 256, 0, st>>>(
+        n, b.dim, b.n_etiles, x.emean.p, x.estd.p, x.gate, 1.0 / (b.delta * b.delta), b.g0.p, w.g.p,
+        w.epart.p, w.kdsum.p, x.gidx.p, x.gcount.p);
+    k_gather_gated<<<n, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.K1, w.qsplit.p, w.qoff.p, x.Qg.p,
+                                      x.qoff_g.p);
+    TGB_CUDA(cudaGetLastError());
+    TGB_MARK(log, PASS_MLP, st);
+    GemmEpi e1{};
+    e1.mode = EPI_GAP_KERNEL;
+    e1.rows = n;
+    e1.rows_dev = x.gcount.p;
+    e1.cols = b.Mpad;
+    e1.alpha = b.alpha.p;
+    e1.c0 = b.zeta * b.delta * b.delta;
+    e1.zeta_int = b.zeta_int;
+    e1.zeta_f = b.zeta;
+    e1.epart = x.epart_g.p;
+    e1.kdsum = x.kdsum_g.p;
+    e1.aoff = b.aoff.p;
+    e1.qoff = x.qoff_g.p;
+    e1.kd = w.kd.p;
+    e1.K2 = b.K2;
+    e1.Mpad = b.Mpad;
+    e1.nsplit = b.nsplit;
+    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st));
+    TGB_MARK(log, PASS_GEMM1, st);
+    GemmEpi e2{};
+    e2.mode = EPI_STORE_F32;
+    e2.rows = n;
+    e2.rows_dev = x.gcount.p;
+    e2.cols = b.dim;
+    e2.out = x.g_g.p;
+    e2.ldo = b.dim;
+    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st));
+    k_scatter_gated<<<n, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
+                                       x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
+    TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
@@ -586,7 +758,6 @@ __global__ void k_energy_e0(int n, const int *__restrict__ sp, const double *__r
 
 }  // namespace
 
-static unsigned grid_for(int64_t n, int tb = 256) { return (unsigned)((n + tb - 1) / tb); }
 
 // Shared front half of tg_get_gap_soap / tg_get_soap: uploads the batch and
 // builds the central-site list (gap_interface.f90:178-309 semantics).
@@ -859,6 +1030,7 @@ namespace tgb {
 struct BlockRun {
     Block *b = nullptr;
     std::unique_ptr<Workspace> w;
+    std::unique_ptr<MixedRun> mix;   // set: the block runs in the mixed (MLP + gate) form
     DBuf<int> sites;
     int n_sites = 0;
 };
@@ -903,7 +1075,11 @@ struct Engine {
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
-            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log));
+            if (r->mix)
+                TGB_TRY(evaluate_block_mixed(*r->b, *r->w, *r->mix, S, n, f.p, en.p, vir.p, err.p,
+                                             st, log));
+            else
+                TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log));
         }
         return TG_OK;
     }
@@ -1194,6 +1370,216 @@ int tg_engine_stream(tg_engine *eh, void **stream) {
     return TG_OK;
 }
 
+// ---------------------------------------------------------------- learned surrogate
+struct tg_mlp {
+    tgb::Mlp *m = nullptr;
+};
+
+int tg_mlp_create(int32_t dim, int32_t hidden, int32_t n_members, uint64_t seed, tg_mlp **out) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(out, TG_ERR_ARG, "null output");
+    Mlp *m = nullptr;
+    TGB_TRY(mlp_create(dim, hidden, n_members, (unsigned long long)seed, &m));
+    *out = new tg_mlp{m};
+    return TG_OK;
+}
+
+int tg_mlp_destroy(tg_mlp *h) {
+    if (!h) return TG_OK;
+    mlp_destroy(h->m);
+    delete h;
+    return TG_OK;
+}
+
+int tg_mlp_set_member(tg_mlp *h, int32_t member, const double *W1, const double *b1,
+                      const double *W2, const double *b2, const double *w3, double b3) {
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    return mlp_set_member(*h->m, member, W1, b1, W2, b2, w3, b3);
+}
+
+int tg_mlp_get_member(tg_mlp *h, int32_t member, double *W1, double *b1, double *W2, double *b2,
+                      double *w3, double *b3) {
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    return mlp_get_member(*h->m, member, W1, b1, W2, b2, w3, b3);
+}
+
+int tg_mlp_set_normalisation(tg_mlp *h, double sigma_x, double mean_e, double sigma_e) {
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    TGB_CHECK(sigma_x > 0.0 && sigma_e > 0.0, TG_ERR_ARG, "scales must be positive");
+    Mlp &m = *h->m;
+    m.sx = sigma_x;
+    m.muE = mean_e;
+    m.sE = sigma_e;
+    for (int k = 0; k < m.n_members; ++k) {   // rebuild the inference copies
+        std::vector<double> W1((size_t)m.L.H * m.L.D), b1(m.L.H), W2((size_t)m.L.H * m.L.H),
+            b2(m.L.H), w3(m.L.H);
+        double b3 = 0.0;
+        TGB_TRY(mlp_get_member(m, k, W1.data(), b1.data(), W2.data(), b2.data(), w3.data(), &b3));
+        const long long t = m.adam_t[k];
+        TGB_TRY(mlp_set_member(m, k, W1.data(), b1.data(), W2.data(), b2.data(), w3.data(), b3));
+        m.adam_t[k] = t;
+    }
+    return TG_OK;
+}
+
+int tg_mlp_get_normalisation(tg_mlp *h, double *sigma_x, double *mean_e, double *sigma_e) {
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    if (sigma_x) *sigma_x = h->m->sx;
+    if (mean_e) *mean_e = h->m->muE;
+    if (sigma_e) *sigma_e = h->m->sE;
+    return TG_OK;
+}
+
+int tg_mlp_add_samples(tg_mlp *h, int32_t n, const float *delta, const double *energy,
+                       const float *dedq) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(h && n >= 0 && (n == 0 || (delta && energy && dedq)), TG_ERR_ARG, "bad samples");
+    if (n == 0) return TG_OK;
+    Context &C = *g_ctx;
+    Mlp &m = *h->m;
+    const int D = m.L.D;
+    DBuf<float> x, g;
+    DBuf<double> e;
+    TGB_TRY(x.ensure((size_t)n * D));
+    TGB_TRY(g.ensure((size_t)n * D));
+    TGB_TRY(e.ensure(n));
+    TGB_CUDA(cudaMemcpyAsync(x.p, delta, sizeof(float) * n * D, cudaMemcpyHostToDevice, C.st));
+    TGB_CUDA(cudaMemcpyAsync(g.p, dedq, sizeof(float) * n * D, cudaMemcpyHostToDevice, C.st));
+    TGB_CUDA(cudaMemcpyAsync(e.p, energy, sizeof(double) * n, cudaMemcpyHostToDevice, C.st));
+    TGB_TRY(mlp_append_device(m, n, x.p, D, e.p, g.p, D, C.st));
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    return TG_OK;
+}
+
+int tg_mlp_add_engine_samples(tg_mlp *h, tg_engine *eh, int32_t block) {
+    TGB_CHECK(h && eh, TG_ERR_ARG, "null argument");
+    Engine &E = eh->e;
+    TGB_CHECK(block >= 0 && block < (int)E.runs.size(), TG_ERR_ARG, "block %d out of range", block);
+    BlockRun &r = *E.runs[block];
+    TGB_CHECK(!r.mix, TG_ERR_STATE, "block %d runs the mixed form; samples come from exact steps",
+              block);
+    Block &b = *r.b;
+    Mlp &m = *h->m;
+    TGB_CHECK(m.L.D == b.dim, TG_ERR_ARG, "MLP input size %d does not match block dim %d", m.L.D,
+              b.dim);
+    const int n = r.n_sites;
+    if (n == 0) return TG_OK;
+    Workspace &w = *r.w;
+    DBuf<float> G;
+    DBuf<double> e;
+    TGB_TRY(G.ensure((size_t)n * b.dim));
+    TGB_TRY(e.ensure(n));
+    k_collect<<<grid_for((int64_t)n * 32), 256, 0, E.st>>>(n, b.dim, b.n_etiles, b.delta * b.delta,
+                                                           w.epart.p, w.kdsum.p, b.mu.p, b.g0.p,
+                                                           w.g.p, e.p, G.p);
+    TGB_CUDA(cudaGetLastError());
+    TGB_TRY(mlp_append_device(m, n, w.q.p, b.dim, e.p, G.p, b.dim, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+int tg_mlp_n_samples(tg_mlp *h, int64_t *n) {
+    TGB_CHECK(h && n, TG_ERR_ARG, "null argument");
+    *n = h->m->n_data;
+    return TG_OK;
+}
+
+int tg_mlp_train(tg_mlp *h, int32_t epochs, int32_t batch, double lr, double force_weight,
+                 uint64_t seed, double *loss_per_epoch) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    return mlp_train(*h->m, epochs, batch, lr, force_weight, (unsigned long long)seed,
+                     loss_per_epoch, g_ctx->st);
+}
+
+__global__ void k_rows_to_bf16(int n, int D, int Dp, const float *__restrict__ x,
+                               __nv_bfloat16 *__restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * Dp) return;
+    const int64_t r = i / Dp;
+    const int d = (int)(i - r * Dp);
+    out[i] = __float2bfloat16_rn(d < D ? x[r * D + d] : 0.f);
+}
+
+int tg_mlp_predict(tg_mlp *h, int32_t n, const float *delta, double *energy_mean,
+                   double *energy_std, double *dedq_mean) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(h && n >= 0 && (n == 0 || (delta && energy_mean)), TG_ERR_ARG, "bad arguments");
+    if (n == 0) return TG_OK;
+    Context &C = *g_ctx;
+    Mlp &m = *h->m;
+    const int D = m.L.D, Dp = m.L.Dp;
+    DBuf<float> x, g;
+    DBuf<__nv_bfloat16> xb;
+    DBuf<double> em, es;
+    TGB_TRY(x.ensure((size_t)n * D));
+    TGB_TRY(g.ensure((size_t)n * D));
+    TGB_TRY(xb.ensure((size_t)n * Dp));
+    TGB_TRY(em.ensure(n));
+    TGB_TRY(es.ensure(n));
+    TGB_CUDA(cudaMemcpyAsync(x.p, delta, sizeof(float) * n * D, cudaMemcpyHostToDevice, C.st));
+    k_rows_to_bf16<<<grid_for((int64_t)n * Dp), 256, 0, C.st>>>(n, D, Dp, x.p, xb.p);
+    TGB_CUDA(cudaGetLastError());
+    std::unique_ptr<MlpInferWork, void (*)(MlpInferWork *)> iw(mlp_infer_work_new(),
+                                                                mlp_infer_work_delete);
+    TGB_TRY(mlp_infer(m, *iw, n, xb.p, Dp, em.p, es.p, g.p, D, C.st));
+    TGB_TRY(mlp_check_err(m, C.st));
+    TGB_CUDA(cudaMemcpyAsync(energy_mean, em.p, sizeof(double) * n, cudaMemcpyDeviceToHost, C.st));
+    if (energy_std)
+        TGB_CUDA(cudaMemcpyAsync(energy_std, es.p, sizeof(double) * n, cudaMemcpyDeviceToHost, C.st));
+    std::vector<float> gh;
+    if (dedq_mean) {
+        gh.resize((size_t)n * D);
+        TGB_CUDA(cudaMemcpyAsync(gh.data(), g.p, sizeof(float) * n * D, cudaMemcpyDeviceToHost, C.st));
+    }
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    if (dedq_mean)
+        for (size_t i = 0; i < gh.size(); ++i) dedq_mean[i] = gh[i];
+    return TG_OK;
+}
+
+int tg_engine_set_mlp(tg_engine *eh, int32_t block, tg_mlp *h, double gate_ev) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    TGB_CHECK(block >= 0 && block < (int)E.runs.size(), TG_ERR_ARG, "block %d out of range", block);
+    BlockRun &r = *E.runs[block];
+    TGB_TRY(engine_errors(E));
+    if (E.graph) {   // the captured step no longer matches
+        cudaGraphExecDestroy(E.graph);
+        E.graph = nullptr;
+    }
+    if (!h) {
+        r.mix.reset();
+        return TG_OK;
+    }
+    TGB_CHECK(h->m->L.D == r.b->dim, TG_ERR_ARG, "MLP input size %d does not match block dim %d",
+              h->m->L.D, r.b->dim);
+    TGB_CHECK(h->m->infer_ready, TG_ERR_STATE, "MLP has no inference weights");
+    TGB_CHECK(gate_ev >= 0.0, TG_ERR_ARG, "negative gate");
+    r.mix = std::make_unique<MixedRun>();
+    r.mix->mlp = h->m;
+    r.mix->iw = mlp_infer_work_new();
+    r.mix->gate = gate_ev;
+    TGB_TRY(r.mix->ensure(*r.b, r.n_sites));
+    return TG_OK;
+}
+
+int tg_engine_mlp_stats(tg_engine *eh, int32_t block, int32_t *n_gated, int32_t *n_sites) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    TGB_CHECK(block >= 0 && block < (int)E.runs.size(), TG_ERR_ARG, "block %d out of range", block);
+    BlockRun &r = *E.runs[block];
+    if (n_sites) *n_sites = r.n_sites;
+    if (n_gated) {
+        *n_gated = r.n_sites;
+        if (r.mix) {
+            TGB_CUDA(cudaMemcpyAsync(n_gated, r.mix->gcount.p, sizeof(int), cudaMemcpyDeviceToHost, E.st));
+            TGB_CUDA(cudaStreamSynchronize(E.st));
+        }
+    }
+    return TG_OK;
+}
+
 }  // extern "C"
 
 // ============================================================== test-only
@@ -1225,5 +1611,22 @@ extern "C" int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t 
     TGB_TRY(check_err_word(C, C.err.p));
     TGB_CUDA(cudaMemcpyAsync(Cout, c.p, sizeof(float) * M * N, cudaMemcpyDeviceToHost, C.st));
     TGB_CUDA(cudaStreamSynchronize(C.st));
+    return TG_OK;
+}
+
+extern "C" int tgx_mlp_batch_grads(tg_mlp *h, int32_t member, int32_t B, const float *x,
+                                   const float *y, const float *gref, double lam, double *grads,
+                                   double *loss, float *E, float *G) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(h, TG_ERR_ARG, "null MLP");
+    return mlp_batch_grads(*h->m, member, B, x, y, gref, lam, grads, loss, E, G, g_ctx->st);
+}
+
+extern "C" int tgx_mlp_layout(tg_mlp *h, int64_t *offsets) {
+    TGB_CHECK(h && offsets, TG_ERR_ARG, "null argument");
+    const MlpLayout &L = h->m->L;
+    const int64_t v[9] = {L.D, L.Dp, L.H, (int64_t)L.oW1, (int64_t)L.ob1, (int64_t)L.oW2,
+                          (int64_t)L.ob2, (int64_t)L.ow3, (int64_t)L.ob3};
+    for (int i = 0; i < 9; ++i) offsets[i] = v[i];
     return TG_OK;
 }

@@ -178,7 +178,11 @@ __global__ void __launch_bounds__(THREADS, 1)
     double2 *prm_all = reinterpret_cast<double2 *>(gbase + (bars + 256 - base));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n_tiles = n_tiles_m * n_tiles_n;
+    // rows known only on the device (a compacted row list): tiles past them are
+    // skipped by every role alike
+    int rows = ep.rows;
+    if (ep.rows_dev) rows = min(rows, max(*ep.rows_dev, 0));
+    const int n_tiles = min(n_tiles_m, (rows + BM - 1) / BM) * n_tiles_n;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         tc_fence_after();
         const int row = m0 + q * 32 + lane;
-        const bool row_ok = row < ep.rows;
+        const bool row_ok = row < rows;
         const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
         if constexpr (MODE != MODE_STORE) {
             double e4[4] = {0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};

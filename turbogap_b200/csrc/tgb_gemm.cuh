@@ -23,7 +23,8 @@ enum EpiMode { EPI_GAP_KERNEL = 0, EPI_STORE_F32 = 1 };
 
 struct GemmEpi {
     int mode;
-    int rows;             // valid rows of C
+    int rows;             // valid rows of C (and the rows the launch is sized for)
+    const int *rows_dev;  // optional: the valid rows are min(rows, *rows_dev), read on the device
     int cols;             // valid columns of C
     // EPI_GAP_KERNEL
     const double *alpha;  // [Mpad]
