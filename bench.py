@@ -35,7 +35,9 @@ sys.path.insert(0, ROOT)
 from turbogap_b200 import synth  # noqa: E402
 from turbogap_b200.workloads import WORKLOADS, build_blocks  # noqa: E402
 
-METRIC = "SOAP-GAP E+F atom-steps/s on 1 B200 (plain bf16x3 form)"
+# value: the plain (bf16x3, FP64-faithful) form; the line's "mixed" object holds
+# the mixed+MLP form on the same workload with its error against the plain path
+METRIC = "SOAP-GAP E+F atom-steps/s on 1 B200: plain vs mixed+MLP at \u22641 meV/atom"
 UNIT = "atom-steps/s"
 
 
@@ -50,6 +52,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed (MLP + gate) leg")
+    ap.add_argument("--mixed-steps", type=int, default=200)
+    ap.add_argument("--mlp-data-steps", type=int, default=16,
+                    help="exact MD snapshots (every 2 steps) the MLPs are trained on")
+    ap.add_argument("--mlp-epochs", type=int, default=10)
+    ap.add_argument("--gate-ev", type=float, default=0.005)
     return ap.parse_args()
 
 
@@ -161,6 +169,76 @@ def gemm_flops_per_step(blocks, structure, sites_only=False):
 # divided by its sites); traffic grows with the sites at fixed D and M.
 GEMM1_DRAM_BYTES_PER_SITE = (155.823104e6 + 257.426432e6) / 12288
 GEMM2_DRAM_BYTES_PER_SITE = (416.886016e6 + 43.268864e6) / 12288
+
+
+# ------------------------------------------------------------------ mixed form
+def mixed_leg(B, eng, blocks, w, a, ext, dist, plain_ms):
+    """The mixed form: per block a 4-member MLP ensemble, trained on the GPU from
+    exact MD snapshots of this workload, replaces the GAP GEMMs; sites whose
+    ensemble spread exceeds the gate go back to the exact kernel. Accuracy is
+    measured against the exact bf16x3 path at the same configurations (that path
+    matches the FP64 oracle to 1e-6 eV/atom)."""
+    import torch
+    t0 = time.time()
+    mlps = [B.Mlp(b.hypers.dim, 256, 4, seed=100 + i) for i, b in enumerate(blocks)]
+    for _ in range(a.mlp_data_steps):
+        eng.md(2, w.dt, energies=False)
+        for i, m in enumerate(mlps):
+            m.add_engine_samples(eng, i)
+    t_data = time.time() - t0
+    losses = [m.train(a.mlp_epochs, batch=512, lr=1e-3, force_weight=1.0, seed=7 + i)
+              for i, m in enumerate(mlps)]
+    t_train = time.time() - t0 - t_data
+
+    def errors():
+        for i in range(len(mlps)):
+            B.engine_set_mlp(eng, i, None)
+        e_ref, f_ref, _ = eng.compute()
+        for i, m in enumerate(mlps):
+            B.engine_set_mlp(eng, i, m, gate_ev=a.gate_ev)
+        e_mix, f_mix, _ = eng.compute()
+        gated = sum(B.engine_mlp_stats(eng, i)[0] for i in range(len(mlps)))
+        return (float(np.sqrt(np.mean((e_mix - e_ref) ** 2))),
+                float(np.sqrt(np.mean((f_mix - f_ref) ** 2))), gated)
+
+    eng.md(20, w.dt, energies=False)        # a configuration the networks were not trained on
+    err_fresh = errors()
+    eng.md(max(a.warmup, 3), w.dt, energies=False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    eng.md(a.mixed_steps, w.dt, energies=False)
+    e1.record(ext)
+    e1.synchronize()
+    t_max = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    prof = eng.profile(3, w.dt)
+    err_after = errors()                    # at the end of the mixed-form trajectory
+    for i in range(len(mlps)):
+        B.engine_set_mlp(eng, i, None)
+    n = eng.n
+    ms = 1e3 * t_max / a.mixed_steps
+    out = {
+        "value": n * a.mixed_steps * (dist.get_world_size() if dist else 1) / t_max,
+        "unit": UNIT, "ms_per_step": ms, "steps": a.mixed_steps,
+        "speedup_vs_plain": plain_ms / ms,
+        "gate_ev": a.gate_ev,
+        "rmse_e_mev_per_atom": 1e3 * err_fresh[0], "rmse_f_mev_per_A": 1e3 * err_fresh[1],
+        "gated_sites": err_fresh[2], "sites": n,
+        "after_mixed_md": {"rmse_e_mev_per_atom": 1e3 * err_after[0],
+                           "rmse_f_mev_per_A": 1e3 * err_after[1], "gated_sites": err_after[2]},
+        "reference": "exact bf16x3 GPU path at the same configurations",
+        "mlp": "4 members x (D -> 256 -> 256 -> 1, SiLU) per block, bf16 GEMMs, fp32 accumulation",
+        "training": {"samples": [m.n_samples() for m in mlps], "epochs": a.mlp_epochs,
+                     "batch": 512, "data_seconds": t_data, "train_seconds": t_train,
+                     "final_loss": [float(l_[-1]) for l_ in losses]},
+        "ms_per_step_by_pass": prof,
+    }
+    for m in mlps:
+        m.close()
+    return out
 
 
 # ------------------------------------------------------------------ CPU (oracle)
@@ -311,6 +389,10 @@ def run_ours(a):
            "api": "tg_engine_set_state + tg_engine_compute (host positions in, host energies/"
                   "forces/virial out)"}
 
+    mixed = None
+    if not a.no_mixed:
+        mixed = mixed_leg(B, eng, blocks, w, a, ext, dist, 1e3 * t_max / a.steps)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -344,6 +426,7 @@ def run_ours(a):
                                "issue_rate_tflops": achieved2 * nsplit},
                      "ms_per_step_by_pass": prof},
         "cpu_baseline": cpu,
+        "mixed": mixed,
         "e2e": e2e,
         "gpu_launches": kernels_per_step * a.steps,
         "clocks": clocks,
