@@ -74,15 +74,19 @@ def _mm(a, b, bf16):
     return a @ b
 
 
-def forward(p: Params, X, bf16=False):
-    """Energies E (B) and input gradients G (B, Dp) of a batch X (B, Dp)."""
+def forward(p: Params, X, bf16=False, s1_bf16=False):
+    """Energies E (B) and input gradients G (B, Dp) of a batch X (B, Dp).
+
+    s1_bf16 rounds silu'(z1) to bf16 before it scales v1, as the GPU inference
+    path does (it stores silu'(z1) in bf16 from the layer-1 GEMM epilogue)."""
     z1 = _mm(X, p.W1.T, bf16) + p.b1
     h1 = silu(z1)
     z2 = _mm(h1, p.W2.T, bf16) + p.b2
     E = silu(z2) @ p.w3 + p.b3
     u2 = dsilu(z2) * p.w3
     v1 = _mm(u2, p.W2, bf16)
-    u1 = v1 * dsilu(z1)
+    s1 = round_bf16(dsilu(z1)) if s1_bf16 else dsilu(z1)
+    u1 = v1 * s1
     G = _mm(u1, p.W1, bf16)
     return E, G
 

@@ -97,7 +97,7 @@ def test_predict_matches_oracle_ensemble(gpu):
     X[:, :D] = delta / sx
     Es, Gs = [], []
     for p in members:
-        E, G = M.forward(p, X, bf16=True)
+        E, G = M.forward(p, X, bf16=True, s1_bf16=True)
         Es.append(se * E + mu_e)
         Gs.append(se / sx * G[:, :D])
     Es, Gs = np.array(Es), np.array(Gs)

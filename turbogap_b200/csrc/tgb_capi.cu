@@ -65,6 +65,7 @@ struct Block {
     DBuf<float> table, selfR;
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
+    DBuf<float> g0f;       // g0 in fp32: subtracted from the MLP's dE/dq rows
     DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d
     TmaMap tmB1{}, tmB2{};
 
@@ -264,26 +265,21 @@ static unsigned grid_for(int64_t n, int tb = 256) { return (unsigned)((n + tb - 
 // they are compacted on the device and the two GEMMs run over the compacted
 // rows, their count read on the device (the step stays one CUDA graph).
 
-// one warp per site: MLP sites get epart = E / delta^2, kdsum = 0 and
-// g = dE/dq - g0 (so that the force pass's g0 + g is the MLP's dE/dq); gated
-// sites are appended to gidx
-__global__ void k_mlp_mix(int n, int D, int n_et, const double *__restrict__ emean,
+// one thread per site: MLP sites get epart = E / delta^2 and kdsum = 0 (their g
+// rows already hold dE/dq - g0, so that the force pass's g0 + g is the MLP's
+// dE/dq); gated sites are appended to gidx
+__global__ void k_mlp_mix(int n, int n_et, const double *__restrict__ emean,
                           const double *__restrict__ estd, double gate, double inv_delta2,
-                          const double *__restrict__ g0, float *__restrict__ g,
                           double *__restrict__ epart, double *__restrict__ kdsum,
                           int *__restrict__ gidx, int *__restrict__ gcount) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= n) return;
     const bool gated = !(estd[row] <= gate);   // a NaN spread is gated too
-    if (lane == 0) {
-        if (gated) gidx[atomicAdd(gcount, 1)] = row;
-        for (int t = 0; t < n_et; ++t) {
-            epart[(size_t)row * n_et + t] = (!gated && t == 0) ? emean[row] * inv_delta2 : 0.0;
-            kdsum[(size_t)row * n_et + t] = 0.0;
-        }
+    if (gated) gidx[atomicAdd(gcount, 1)] = row;
+    for (int t = 0; t < n_et; ++t) {
+        epart[(size_t)row * n_et + t] = (!gated && t == 0) ? emean[row] * inv_delta2 : 0.0;
+        kdsum[(size_t)row * n_et + t] = 0.0;
     }
-    if (!gated)
-        for (int d = lane; d < D; d += 32) g[(size_t)row * D + d] -= (float)g0[d];
 }
 
 // compacted GEMM-1 operand rows and delta.mu of the gated sites
@@ -377,11 +373,12 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
     TGB_TRY(launch_soap_expand(P, S, O, st));
     TGB_MARK(log, PASS_DESC, st);
-    TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim, st));
+    TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim,
+                      b.g0f.p, st));
     TGB_CUDA(cudaMemsetAsync(x.gcount.p, 0, sizeof(int), st));
-    k_mlp_mix<<<grid_for((int64_t)n * 32), 256, 0, st>>>(
-        n, b.dim, b.n_etiles, x.emean.p, x.estd.p, x.gate, 1.0 / (b.delta * b.delta), b.g0.p, w.g.p,
-        w.epart.p, w.kdsum.p, x.gidx.p, x.gcount.p);
+    k_mlp_mix<<<grid_for(n), 256, 0, st>>>(n, b.n_etiles, x.emean.p, x.estd.p, x.gate,
+                                           1.0 / (b.delta * b.delta), w.epart.p, w.kdsum.p,
+                                           x.gidx.p, x.gcount.p);
     k_gather_gated<<<n, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.K1, w.qsplit.p, w.qoff.p, x.Qg.p,
                                       x.qoff_g.p);
     TGB_CUDA(cudaGetLastError());
@@ -647,6 +644,9 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
             for (int d = 0; d < b->dim; ++d) g0[d] += c * (Qs[(size_t)s * b->dim + d] - mu[d]);
         }
         TGB_CUDA(cudaMemcpy(b->g0.p, g0.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
+        std::vector<float> g0f(g0.begin(), g0.end());
+        TGB_TRY(b->g0f.ensure(b->dim));
+        TGB_CUDA(cudaMemcpy(b->g0f.p, g0f.data(), sizeof(float) * b->dim, cudaMemcpyHostToDevice));
         TGB_CUDA(cudaMemcpy(b->mu.p, mu.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
         TGB_CUDA(cudaMemcpy(b->aoff.p, aoff.data(), sizeof(double) * b->Mpad, cudaMemcpyHostToDevice));
     }
@@ -1509,11 +1509,12 @@ int tg_mlp_predict(tg_mlp *h, int32_t n, const float *delta, double *energy_mean
     Context &C = *g_ctx;
     Mlp &m = *h->m;
     const int D = m.L.D, Dp = m.L.Dp;
+    const int ldg = (D + 3) / 4 * 4;
     DBuf<float> x, g;
     DBuf<__nv_bfloat16> xb;
     DBuf<double> em, es;
     TGB_TRY(x.ensure((size_t)n * D));
-    TGB_TRY(g.ensure((size_t)n * D));
+    TGB_TRY(g.ensure((size_t)n * ldg));
     TGB_TRY(xb.ensure((size_t)n * Dp));
     TGB_TRY(em.ensure(n));
     TGB_TRY(es.ensure(n));
@@ -1522,19 +1523,20 @@ int tg_mlp_predict(tg_mlp *h, int32_t n, const float *delta, double *energy_mean
     TGB_CUDA(cudaGetLastError());
     std::unique_ptr<MlpInferWork, void (*)(MlpInferWork *)> iw(mlp_infer_work_new(),
                                                                 mlp_infer_work_delete);
-    TGB_TRY(mlp_infer(m, *iw, n, xb.p, Dp, em.p, es.p, g.p, D, C.st));
+    TGB_TRY(mlp_infer(m, *iw, n, xb.p, Dp, em.p, es.p, g.p, ldg, nullptr, C.st));
     TGB_TRY(mlp_check_err(m, C.st));
     TGB_CUDA(cudaMemcpyAsync(energy_mean, em.p, sizeof(double) * n, cudaMemcpyDeviceToHost, C.st));
     if (energy_std)
         TGB_CUDA(cudaMemcpyAsync(energy_std, es.p, sizeof(double) * n, cudaMemcpyDeviceToHost, C.st));
     std::vector<float> gh;
     if (dedq_mean) {
-        gh.resize((size_t)n * D);
-        TGB_CUDA(cudaMemcpyAsync(gh.data(), g.p, sizeof(float) * n * D, cudaMemcpyDeviceToHost, C.st));
+        gh.resize((size_t)n * ldg);
+        TGB_CUDA(cudaMemcpyAsync(gh.data(), g.p, sizeof(float) * n * ldg, cudaMemcpyDeviceToHost, C.st));
     }
     TGB_CUDA(cudaStreamSynchronize(C.st));
     if (dedq_mean)
-        for (size_t i = 0; i < gh.size(); ++i) dedq_mean[i] = gh[i];
+        for (int r = 0; r < n; ++r)
+            for (int d = 0; d < D; ++d) dedq_mean[(size_t)r * D + d] = gh[(size_t)r * ldg + d];
     return TG_OK;
 }
 

@@ -142,7 +142,19 @@ constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256 
 constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
 
 // Epilogue variants (compile-time, so the element loop has no mode branches).
-enum { MODE_GAP_Z4 = 0, MODE_GAP_ZINT = 1, MODE_GAP_ZREAL = 2, MODE_STORE = 3 };
+enum {
+    MODE_GAP_Z4 = 0, MODE_GAP_ZINT = 1, MODE_GAP_ZREAL = 2, MODE_STORE = 3, MODE_MLP_L1 = 4,
+    MODE_MLP_L2 = 5, MODE_MLP_L2B = 6, MODE_MLP_L1B = 7, N_MODES = 8
+};
+
+__device__ __forceinline__ float sigmoid_f(float z) { return 1.f / (1.f + expf(-z)); }
+
+__device__ __forceinline__ void store_bf16x32(__nv_bfloat16 *dst, const __nv_bfloat16 (&v)[32]) {
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(v);
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) d4[u] = s4[u];
+}
 
 template <int MODE>
 __device__ __forceinline__ double kpow_m1(double K, const GemmEpi &ep) {
@@ -283,7 +295,85 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int row = m0 + q * 32 + lane;
         const bool row_ok = row < rows;
         const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
-        if constexpr (MODE != MODE_STORE) {
+        if constexpr (MODE >= MODE_MLP_L1) {
+            // the MLP epilogues: float column parameters staged per warp like the GAP ones
+            float2 *pf = reinterpret_cast<float2 *>(prm);
+            float racc = 0.f;
+            for (int c = 0; c < COLS_PER_WARP / 32; ++c) {
+                const int col = grp * COLS_PER_WARP + c * 32;
+                const int gcol = n0 + col;
+                if (gcol >= ep.cols) break;   // warp-uniform
+                if constexpr (MODE != MODE_MLP_L2B) {
+                    __syncwarp();
+                    const int cl = gcol + lane;
+                    float a0 = 0.f, a1 = 0.f;
+                    if (cl < ep.cols) {
+                        if (ep.p0) a0 = ep.p0[cl];
+                        if constexpr (MODE == MODE_MLP_L2) a1 = ep.p1[cl];
+                    }
+                    pf[lane] = make_float2(a0, a1);
+                    __syncwarp();
+                }
+                float v[32];
+                tmem_ld32(taddr + (uint32_t)col, v);
+                if constexpr (MODE == MODE_MLP_L1) {
+                    __align__(16) __nv_bfloat16 hb[32], sb[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const float z = v[j] + pf[j].x, sg = sigmoid_f(z);
+                        hb[j] = __float2bfloat16_rn(z * sg);
+                        sb[j] = __float2bfloat16_rn(sg * (1.f + z * (1.f - sg)));
+                    }
+                    if (row_ok) {
+                        store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, hb);
+                        store_bf16x32(ep.out_b1 + (size_t)row * ep.ldb + gcol, sb);
+                    }
+                } else if constexpr (MODE == MODE_MLP_L2) {
+                    __align__(16) __nv_bfloat16 ub[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const float2 q2 = pf[j];
+                        const float z = v[j] + q2.x, sg = sigmoid_f(z);
+                        racc += q2.y * z * sg;
+                        ub[j] = __float2bfloat16_rn(q2.y * sg * (1.f + z * (1.f - sg)));
+                    }
+                    if (row_ok) store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, ub);
+                } else if constexpr (MODE == MODE_MLP_L2B) {
+                    if (row_ok) {
+                        __align__(16) __nv_bfloat16 sf[32], ub[32];
+                        const uint4 *s4 = reinterpret_cast<const uint4 *>(ep.in_b + (size_t)row * ep.ldi + gcol);
+                        uint4 *t4 = reinterpret_cast<uint4 *>(sf);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) t4[u] = s4[u];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            ub[j] = __float2bfloat16_rn(v[j] * __bfloat162float(sf[j]));
+                        store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, ub);
+                    }
+                } else {   // MODE_MLP_L1B
+                    if (row_ok) {
+                        float *o = ep.out + (size_t)row * ep.ldo + gcol;
+                        if (gcol + 32 <= ep.cols) {
+                            float4 *o4 = reinterpret_cast<float4 *>(o);
+#pragma unroll
+                            for (int j = 0; j < 8; ++j)
+                                o4[j] = make_float4(ep.scale * v[4 * j] - pf[4 * j].x,
+                                                    ep.scale * v[4 * j + 1] - pf[4 * j + 1].x,
+                                                    ep.scale * v[4 * j + 2] - pf[4 * j + 2].x,
+                                                    ep.scale * v[4 * j + 3] - pf[4 * j + 3].x);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                if (gcol + j < ep.cols) o[j] = ep.scale * v[j] - pf[j].x;
+                        }
+                    }
+                }
+            }
+            if constexpr (MODE == MODE_MLP_L2) {
+                if (row_ok)
+                    ep.rowpart[(size_t)row * ep.rowpart_ld + tile_n * kGemmEpiGroups + grp] = racc;
+            }
+        } else if constexpr (MODE != MODE_STORE) {
             double e4[4] = {0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};
             const double qo = row_ok ? ep.qoff[row] : 0.0;
             const float c0f = (float)ep.c0;
@@ -416,13 +506,30 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
                                             ((uintptr_t)ep.kd & 15) == 0),
               TG_ERR_ARG, "bf16 kernel-derivative rows must be 16-byte aligned, Mpad %% 32 == 0");
     if (M <= 0 || N <= 0) return TG_OK;
+    TGB_CHECK(ep.mode < EPI_MLP_L1 || ep.mode == EPI_MLP_L1B ||
+                  (ep.ldb % 8 == 0 && ((uintptr_t)ep.out_b0 & 15) == 0 && N % 32 == 0),
+              TG_ERR_ARG, "bf16 MLP outputs need 16-byte rows and N %% 32 == 0");
+    TGB_CHECK(ep.mode != EPI_MLP_L2B || (ep.ldi % 8 == 0 && ((uintptr_t)ep.in_b & 15) == 0),
+              TG_ERR_ARG, "bf16 MLP factor rows must be 16-byte aligned");
+    TGB_CHECK(ep.mode != EPI_MLP_L1B || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
+              TG_ERR_ARG, "fp32 output rows must be 16-byte aligned (ldo %% 4 == 0)");
     int mode = MODE_STORE;
-    if (ep.mode == EPI_GAP_KERNEL)
-        mode = ep.zeta_int == 4 ? MODE_GAP_Z4 : ep.zeta_int > 0 ? MODE_GAP_ZINT : MODE_GAP_ZREAL;
+    switch (ep.mode) {
+        case EPI_GAP_KERNEL:
+            mode = ep.zeta_int == 4 ? MODE_GAP_Z4 : ep.zeta_int > 0 ? MODE_GAP_ZINT : MODE_GAP_ZREAL;
+            break;
+        case EPI_MLP_L1: mode = MODE_MLP_L1; break;
+        case EPI_MLP_L2: mode = MODE_MLP_L2; break;
+        case EPI_MLP_L2B: mode = MODE_MLP_L2B; break;
+        case EPI_MLP_L1B: mode = MODE_MLP_L1B; break;
+        default: mode = MODE_STORE;
+    }
     using Kern = void (*)(CUtensorMap, CUtensorMap, int, int, int, GemmEpi, unsigned *);
-    static const Kern kerns[4] = {k_gemm_tn<MODE_GAP_Z4>, k_gemm_tn<MODE_GAP_ZINT>,
-                                  k_gemm_tn<MODE_GAP_ZREAL>, k_gemm_tn<MODE_STORE>};
-    static bool attr[4] = {false, false, false, false};
+    static const Kern kerns[N_MODES] = {
+        k_gemm_tn<MODE_GAP_Z4>, k_gemm_tn<MODE_GAP_ZINT>, k_gemm_tn<MODE_GAP_ZREAL>,
+        k_gemm_tn<MODE_STORE>, k_gemm_tn<MODE_MLP_L1>, k_gemm_tn<MODE_MLP_L2>,
+        k_gemm_tn<MODE_MLP_L2B>, k_gemm_tn<MODE_MLP_L1B>};
+    static bool attr[N_MODES] = {};
     if (!attr[mode]) {
         TGB_CUDA(cudaFuncSetAttribute(kerns[mode], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)SMEM_BYTES));

@@ -265,62 +265,25 @@ __global__ void k_refresh_infer(const float *__restrict__ P, MlpLayout L, int k,
 }
 
 // ---------------------------------------------------------------- inference stages
-__global__ void k_i1(int64_t n, int HH, const float *__restrict__ Z1, const float *__restrict__ b1,
-                     bf16 *__restrict__ H1) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float z = Z1[i] + b1[i % HH];
-    H1[i] = __float2bfloat16_rn(silu_f(z, sigm(z)));
-}
-
-// one warp per row, all members: E_m = w3.h2 + b3 and u2 = w3 silu'(z2) (bf16)
-__global__ void k_i2(int n, int H, int nm, const float *__restrict__ Z2, const float *__restrict__ b2,
-                     const float *__restrict__ w3, const float *__restrict__ b3,
-                     bf16 *__restrict__ U2, float *__restrict__ Em) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+// One thread per row: member energies from the layer-2 epilogue's row partials
+// (E_k = sum_t part[row][k][t] + b3_k), their mean and spread (FP64).
+__global__ void k_i_energy(int n, int nm, int npart, const float *__restrict__ part,
+                           const float *__restrict__ b3, double *__restrict__ e_mean,
+                           double *__restrict__ e_std) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= n) return;
-    const int HH = nm * H;
+    double Ek[8], s = 0.0;
     for (int k = 0; k < nm; ++k) {
-        float acc = 0.f;
-        for (int j = lane; j < H; j += 32) {
-            const int c = k * H + j;
-            const float z = Z2[(size_t)row * HH + c] + b2[c], s = sigm(z);
-            acc += w3[c] * silu_f(z, s);
-            U2[(size_t)row * HH + c] = __float2bfloat16_rn(w3[c] * dsilu_f(z, s));
-        }
-        acc = warp_sum(acc);
-        if (lane == 0) Em[(size_t)row * nm + k] = acc + b3[k];
+        double e = b3[k];
+        for (int t = 0; t < npart; ++t) e += part[((size_t)row * nm + k) * npart + t];
+        Ek[k] = e;
+        s += e;
     }
-}
-
-__global__ void k_i3(int64_t n, int HH, const float *__restrict__ V1, const float *__restrict__ Z1,
-                     const float *__restrict__ b1, bf16 *__restrict__ U1) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float z = Z1[i] + b1[i % HH];
-    U1[i] = __float2bfloat16_rn(V1[i] * dsilu_f(z, sigm(z)));
-}
-
-// one warp per row: member mean and spread of E (FP64), mean dE/d(delta) rows
-__global__ void k_i4(int n, int D, int Dp, int nm, const float *__restrict__ Em,
-                     const float *__restrict__ Gs, double *__restrict__ e_mean,
-                     double *__restrict__ e_std, float *__restrict__ g, int ldg) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float inv = 1.f / (float)nm;
-    if (g)
-        for (int d = lane; d < D; d += 32) g[(size_t)row * ldg + d] = Gs[(size_t)row * Dp + d] * inv;
-    if (lane == 0) {
-        double s = 0.0, s2 = 0.0;
-        for (int k = 0; k < nm; ++k) s += Em[(size_t)row * nm + k];
-        const double mean = s / nm;
-        for (int k = 0; k < nm; ++k) {
-            const double d = Em[(size_t)row * nm + k] - mean;
-            s2 += d * d;
-        }
-        e_mean[row] = mean;
-        if (e_std) e_std[row] = sqrt(s2 / nm);
-    }
+    const double mean = s / nm;
+    double s2 = 0.0;
+    for (int k = 0; k < nm; ++k) s2 += (Ek[k] - mean) * (Ek[k] - mean);
+    e_mean[row] = mean;
+    if (e_std) e_std[row] = sqrt(s2 / nm);
 }
 
 // moments of the data set for the normalisation: sum x^2 (all entries), sum E, sum E^2
@@ -355,10 +318,12 @@ __global__ void k_copy_rows(int n, int D, const float *__restrict__ x, int ldx, 
 // ---------------------------------------------------------------- GEMM plans
 struct Plan {
     TmaMap a{}, b{};
-    int M = 0, N = 0, K = 0, ldo = 0;
-    float *out = nullptr;
+    int M = 0, N = 0, K = 0;
+    GemmEpi ep{};
 };
 
+// C[M x N] = A . B^T (K-major bf16, row strides lda / ldb); fp32 store epilogue
+// into out (row stride ldo) unless the caller replaces p.ep afterwards.
 int plan(Plan &p, const bf16 *A, int M, int lda, const bf16 *Bm, int N, int ldb, int K, float *out,
          int ldo) {
     TGB_TRY(make_tma_bf16(&p.a, A, M, K, lda, kGemmBM));
@@ -366,19 +331,17 @@ int plan(Plan &p, const bf16 *A, int M, int lda, const bf16 *Bm, int N, int ldb,
     p.M = M;
     p.N = N;
     p.K = K;
-    p.out = out;
-    p.ldo = ldo;
+    p.ep = GemmEpi{};
+    p.ep.mode = EPI_STORE_F32;
+    p.ep.rows = M;
+    p.ep.cols = N;
+    p.ep.out = out;
+    p.ep.ldo = ldo;
     return TG_OK;
 }
 
 int run(const Plan &p, unsigned *err, cudaStream_t st) {
-    GemmEpi ep{};
-    ep.mode = EPI_STORE_F32;
-    ep.rows = p.M;
-    ep.cols = p.N;
-    ep.out = p.out;
-    ep.ldo = p.ldo;
-    return launch_gemm_tn(p.a, p.b, p.M, p.N, p.K, ep, err, st);
+    return launch_gemm_tn(p.a, p.b, p.M, p.N, p.K, p.ep, err, st);
 }
 
 int transpose(int R, int C, const bf16 *in, int ldi, bf16 *out, int ldo, cudaStream_t st) {
@@ -437,40 +400,67 @@ struct MlpTrainWork {
 
 struct MlpInferWork {
     int cap = 0;
+    // binding of the current plans
     const bf16 *X = nullptr;
-    int n = 0, ldx = 0;
-    Buf<float> Z1, Z2, V1, Gs, Em;
-    Buf<bf16> H1, U2, U1;
+    int n = 0, ldx = 0, ldg = 0;
+    float *g = nullptr;
+    const float *sub = nullptr;
+    Buf<bf16> H1, S1, U2, U1;
+    Buf<float> part;
     Plan p1, p4;
     std::vector<Plan> p2, p3;
+
+    int npart(const Mlp &m) const { return gemm_n_tiles(m.L.H) * kGemmEpiGroups; }
 
     int ensure(Mlp &m, int rows) {
         if (rows > cap) {
             const size_t hh = (size_t)m.n_members * m.L.H;
-            TGB_TRY(Z1.ensure(rows * hh)); TGB_TRY(Z2.ensure(rows * hh));
-            TGB_TRY(V1.ensure(rows * hh)); TGB_TRY(Gs.ensure((size_t)rows * m.L.Dp));
-            TGB_TRY(Em.ensure((size_t)rows * m.n_members));
-            TGB_TRY(H1.ensure(rows * hh)); TGB_TRY(U2.ensure(rows * hh)); TGB_TRY(U1.ensure(rows * hh));
+            TGB_TRY(H1.ensure(rows * hh)); TGB_TRY(S1.ensure(rows * hh));
+            TGB_TRY(U2.ensure(rows * hh)); TGB_TRY(U1.ensure(rows * hh));
+            TGB_TRY(part.ensure((size_t)rows * m.n_members * npart(m)));
             cap = rows;
             X = nullptr;
         }
         return TG_OK;
     }
-    // GEMM plans for input rows X (re-encoded when the input or its size changes)
-    int bind(Mlp &m, const bf16 *x, int rows, int ld) {
-        if (x == X && rows == n && ld == ldx) return TG_OK;
-        const int H = m.L.H, Dp = m.L.Dp, nm = m.n_members, HH = nm * H;
-        TGB_TRY(plan(p1, x, rows, ld, m.W1cat, HH, Dp, Dp, Z1.p, HH));
+    // GEMM plans with their fused epilogues for input rows X and output rows g
+    int bind(Mlp &m, const bf16 *x, int rows, int ld, float *gout, int ldgo, const float *s) {
+        if (x == X && rows == n && ld == ldx && gout == g && ldgo == ldg && s == sub) return TG_OK;
+        const int H = m.L.H, Dp = m.L.Dp, nm = m.n_members, HH = nm * H, np = npart(m);
+        TGB_TRY(plan(p1, x, rows, ld, m.W1cat, HH, Dp, Dp, nullptr, 0));
+        p1.ep.mode = EPI_MLP_L1;
+        p1.ep.p0 = m.b1cat;
+        p1.ep.out_b0 = H1.p;
+        p1.ep.out_b1 = S1.p;
+        p1.ep.ldb = HH;
         p2.assign(nm, Plan{});
         p3.assign(nm, Plan{});
         for (int k = 0; k < nm; ++k) {
-            TGB_TRY(plan(p2[k], H1.p + k * H, rows, HH, m.W2b[k], H, H, H, Z2.p + k * H, HH));
-            TGB_TRY(plan(p3[k], U2.p + k * H, rows, HH, m.W2Tb[k], H, H, H, V1.p + k * H, HH));
+            TGB_TRY(plan(p2[k], H1.p + k * H, rows, HH, m.W2b[k], H, H, H, nullptr, 0));
+            p2[k].ep.mode = EPI_MLP_L2;
+            p2[k].ep.p0 = m.b2cat + k * H;
+            p2[k].ep.p1 = m.w3cat + k * H;
+            p2[k].ep.out_b0 = U2.p + k * H;
+            p2[k].ep.ldb = HH;
+            p2[k].ep.rowpart = part.p + (size_t)k * np;
+            p2[k].ep.rowpart_ld = nm * np;
+            TGB_TRY(plan(p3[k], U2.p + k * H, rows, HH, m.W2Tb[k], H, H, H, nullptr, 0));
+            p3[k].ep.mode = EPI_MLP_L2B;
+            p3[k].ep.in_b = S1.p + k * H;
+            p3[k].ep.ldi = HH;
+            p3[k].ep.out_b0 = U1.p + k * H;
+            p3[k].ep.ldb = HH;
         }
-        TGB_TRY(plan(p4, U1.p, rows, HH, m.W1Tcat, Dp, HH, HH, Gs.p, Dp));
+        TGB_TRY(plan(p4, U1.p, rows, HH, m.W1Tcat, m.L.D, HH, HH, gout, ldgo));
+        p4.ep.mode = EPI_MLP_L1B;
+        p4.ep.scale = 1.f / (float)nm;
+        p4.ep.p0 = s;
         X = x;
         n = rows;
         ldx = ld;
+        g = gout;
+        ldg = ldgo;
+        sub = s;
         return TG_OK;
     }
 };
@@ -825,24 +815,22 @@ MlpInferWork *mlp_infer_work_new() { return new MlpInferWork(); }
 void mlp_infer_work_delete(MlpInferWork *w) { delete w; }
 
 int mlp_infer(Mlp &m, MlpInferWork &w, int n, const bf16 *X, int ldx, double *e_mean,
-              double *e_std, float *g_mean, int ldg, cudaStream_t st) {
+              double *e_std, float *g_mean, int ldg, const float *g_sub, cudaStream_t st) {
     if (n <= 0) return TG_OK;
     TGB_CHECK(m.infer_ready, TG_ERR_STATE, "MLP has no inference weights");
     TGB_CHECK(ldx >= m.L.Dp && ldx % 8 == 0, TG_ERR_ARG, "input row stride %d < %d or not a multiple of 8",
               ldx, m.L.Dp);
+    TGB_CHECK(g_mean && ldg >= m.L.D && ldg % 4 == 0, TG_ERR_ARG,
+              "dE/d(delta) rows need a stride >= %d and a multiple of 4", m.L.D);
     TGB_TRY(w.ensure(m, n));
-    TGB_TRY(w.bind(m, X, n, ldx));
-    const int H = m.L.H, nm = m.n_members, HH = nm * H;
-    const int64_t nh = (int64_t)n * HH;
+    TGB_TRY(w.bind(m, X, n, ldx, g_mean, ldg, g_sub));
+    const int nm = m.n_members;
     TGB_TRY(run(w.p1, m.err, st));
-    k_i1<<<blocks_for(nh), 256, 0, st>>>(nh, HH, w.Z1.p, m.b1cat, w.H1.p);
     for (int k = 0; k < nm; ++k) TGB_TRY(run(w.p2[k], m.err, st));
-    const unsigned wb = blocks_for((size_t)n * 32);
-    k_i2<<<wb, 256, 0, st>>>(n, H, nm, w.Z2.p, m.b2cat, m.w3cat, m.b3cat, w.U2.p, w.Em.p);
     for (int k = 0; k < nm; ++k) TGB_TRY(run(w.p3[k], m.err, st));
-    k_i3<<<blocks_for(nh), 256, 0, st>>>(nh, HH, w.V1.p, w.Z1.p, m.b1cat, w.U1.p);
     TGB_TRY(run(w.p4, m.err, st));
-    k_i4<<<wb, 256, 0, st>>>(n, m.L.D, m.L.Dp, nm, w.Em.p, w.Gs.p, e_mean, e_std, g_mean, ldg);
+    k_i_energy<<<blocks_for((size_t)n), 256, 0, st>>>(n, nm, w.npart(m), w.part.p, m.b3cat, e_mean,
+                                                       e_std);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -79,9 +79,10 @@ MlpInferWork *mlp_infer_work_new();
 void mlp_infer_work_delete(MlpInferWork *w);
 // Inference on bf16 rows X (row stride ldx >= Dp; entries D..Dp-1 are ignored)
 // for all members: energy mean and spread (eV) per row, and the member-mean
-// dE/d(delta) as fp32 rows of length D (row stride ldg).
+// dE/d(delta) minus g_sub (per column, may be null) as fp32 rows of length D
+// (row stride ldg, a multiple of 4). Every stage is a fused GEMM epilogue.
 int mlp_infer(Mlp &m, MlpInferWork &w, int n, const __nv_bfloat16 *X, int ldx, double *e_mean,
-              double *e_std, float *g_mean, int ldg, cudaStream_t st);
+              double *e_std, float *g_mean, int ldg, const float *g_sub, cudaStream_t st);
 int mlp_check_err(Mlp &m, cudaStream_t st);
 
 }  // namespace tgb
