@@ -287,13 +287,14 @@ __global__ void k_gather_gated(const int *__restrict__ gcount, const int *__rest
                                const __nv_bfloat16 *__restrict__ qsplit,
                                const double *__restrict__ qoff, __nv_bfloat16 *__restrict__ Qg,
                                double *__restrict__ qoff_g) {
-    const int r = blockIdx.x;
-    if (r >= *gcount) return;
-    const int site = gidx[r];
-    const uint4 *src = reinterpret_cast<const uint4 *>(qsplit + (size_t)site * K1);
-    uint4 *dst = reinterpret_cast<uint4 *>(Qg + (size_t)r * K1);
-    for (int k = threadIdx.x; k < K1 / 8; k += blockDim.x) dst[k] = src[k];
-    if (threadIdx.x == 0) qoff_g[r] = qoff[site];
+    const int cnt = *gcount;
+    for (int r = blockIdx.x; r < cnt; r += gridDim.x) {
+        const int site = gidx[r];
+        const uint4 *src = reinterpret_cast<const uint4 *>(qsplit + (size_t)site * K1);
+        uint4 *dst = reinterpret_cast<uint4 *>(Qg + (size_t)r * K1);
+        for (int k = threadIdx.x; k < K1 / 8; k += blockDim.x) dst[k] = src[k];
+        if (threadIdx.x == 0) qoff_g[r] = qoff[site];
+    }
 }
 
 __global__ void k_scatter_gated(const int *__restrict__ gcount, const int *__restrict__ gidx, int D,
@@ -301,13 +302,15 @@ __global__ void k_scatter_gated(const int *__restrict__ gcount, const int *__res
                                 const double *__restrict__ kdsum_g, const float *__restrict__ g_g,
                                 double *__restrict__ epart, double *__restrict__ kdsum,
                                 float *__restrict__ g) {
-    const int r = blockIdx.x;
-    if (r >= *gcount) return;
-    const int site = gidx[r];
-    for (int d = threadIdx.x; d < D; d += blockDim.x) g[(size_t)site * D + d] = g_g[(size_t)r * D + d];
-    for (int t = threadIdx.x; t < n_et; t += blockDim.x) {
-        epart[(size_t)site * n_et + t] = epart_g[(size_t)r * n_et + t];
-        kdsum[(size_t)site * n_et + t] = kdsum_g[(size_t)r * n_et + t];
+    const int cnt = *gcount;
+    for (int r = blockIdx.x; r < cnt; r += gridDim.x) {
+        const int site = gidx[r];
+        for (int d = threadIdx.x; d < D; d += blockDim.x)
+            g[(size_t)site * D + d] = g_g[(size_t)r * D + d];
+        for (int t = threadIdx.x; t < n_et; t += blockDim.x) {
+            epart[(size_t)site * n_et + t] = epart_g[(size_t)r * n_et + t];
+            kdsum[(size_t)site * n_et + t] = kdsum_g[(size_t)r * n_et + t];
+        }
     }
 }
 
@@ -379,7 +382,8 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     k_mlp_mix<<<grid_for(n), 256, 0, st>>>(n, b.n_etiles, x.emean.p, x.estd.p, x.gate,
                                            1.0 / (b.delta * b.delta), w.epart.p, w.kdsum.p,
                                            x.gidx.p, x.gcount.p);
-    k_gather_gated<<<n, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.K1, w.qsplit.p, w.qoff.p, x.Qg.p,
+    const unsigned gg = (unsigned)std::min(n, 1184);   // grid-stride over the gated rows
+    k_gather_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.K1, w.qsplit.p, w.qoff.p, x.Qg.p,
                                       x.qoff_g.p);
     TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_MLP, st);
@@ -410,7 +414,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e2.out = x.g_g.p;
     e2.ldo = b.dim;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st));
-    k_scatter_gated<<<n, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
+    k_scatter_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
                                        x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
     TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_GEMM2, st);

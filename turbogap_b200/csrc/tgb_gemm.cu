@@ -137,7 +137,8 @@ constexpr int EPI_WARPS = 4 * kGemmEpiGroups;        // kGemmEpiGroups warps per
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
 constexpr int COLS_PER_WARP = BN / kGemmEpiGroups;   // accumulator columns one epilogue warp reads
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
-constexpr size_t PRM_BYTES = (size_t)EPI_WARPS * 32 * sizeof(double2);
+constexpr int CHUNKS = COLS_PER_WARP / 32;          // 32-column chunks per epilogue warp
+constexpr size_t PRM_BYTES = (size_t)EPI_WARPS * CHUNKS * 32 * sizeof(double2);
 constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256 + PRM_BYTES;
 constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
 
@@ -225,6 +226,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bool ok = true;
         for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
             const int m0 = (t / n_tiles_n) * BM, n0 = (t % n_tiles_n) * BN;
+            const int ak = ep.bd_block > 0 ? (n0 / ep.bd_block) * ep.bd_block : 0;
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
                 const int s = g % STAGES;
                 const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     break;
                 }
                 mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
-                tma_load_2d(sA + s * A_BYTES, &tmA, kb * BK, m0, full0 + 8 * s);
+                tma_load_2d(sA + s * A_BYTES, &tmA, ak + kb * BK, m0, full0 + 8 * s);
                 tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
             }
         }
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       // the hardware lets it access) and column group (w - 2) / 4 of the tile
       const int q = warp & 3;
       const int grp = (warp - 2) >> 2;
-      double2 *prm = prm_all + (warp - 2) * 32;
+      double2 *prm = prm_all + (warp - 2) * CHUNKS * 32;
       int it = 0;
       for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
         const int a = it & 1;
@@ -297,23 +299,31 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
         if constexpr (MODE >= MODE_MLP_L1) {
             // the MLP epilogues: float column parameters staged per warp like the GAP ones
-            float2 *pf = reinterpret_cast<float2 *>(prm);
+            // column parameters of all this warp's chunks, loaded together at tile start
+            float2 *pfall = reinterpret_cast<float2 *>(prm);
+            if constexpr (MODE != MODE_MLP_L2B) {
+                float a0[CHUNKS], a1[CHUNKS];
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c) {
+                    const int cl = n0 + grp * COLS_PER_WARP + c * 32 + lane;
+                    a0[c] = 0.f;
+                    a1[c] = 0.f;
+                    if (cl < ep.cols) {
+                        if (ep.p0) a0[c] = ep.p0[cl];
+                        if constexpr (MODE == MODE_MLP_L2) a1[c] = ep.p1[cl];
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c) pfall[c * 32 + lane] = make_float2(a0[c], a1[c]);
+                __syncwarp();
+            }
             float racc = 0.f;
-            for (int c = 0; c < COLS_PER_WARP / 32; ++c) {
+            for (int c = 0; c < CHUNKS; ++c) {
                 const int col = grp * COLS_PER_WARP + c * 32;
                 const int gcol = n0 + col;
                 if (gcol >= ep.cols) break;   // warp-uniform
-                if constexpr (MODE != MODE_MLP_L2B) {
-                    __syncwarp();
-                    const int cl = gcol + lane;
-                    float a0 = 0.f, a1 = 0.f;
-                    if (cl < ep.cols) {
-                        if (ep.p0) a0 = ep.p0[cl];
-                        if constexpr (MODE == MODE_MLP_L2) a1 = ep.p1[cl];
-                    }
-                    pf[lane] = make_float2(a0, a1);
-                    __syncwarp();
-                }
+                const float2 *pf = pfall + c * 32;
                 float v[32];
                 tmem_ld32(taddr + (uint32_t)col, v);
                 if constexpr (MODE == MODE_MLP_L1) {
@@ -377,21 +387,33 @@ __global__ void __launch_bounds__(THREADS, 1)
             double e4[4] = {0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};
             const double qo = row_ok ? ep.qoff[row] : 0.0;
             const float c0f = (float)ep.c0;
-            for (int c = 0; c < COLS_PER_WARP / 32; ++c) {
+            // column parameters (alpha_s, mu . q_s) of all this warp's chunks: lane l
+            // loads column l of each chunk (all loads in flight together), the element
+            // loop reads them back as shared-memory broadcasts
+            {
+                double a0[CHUNKS], a1[CHUNKS];
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c) {
+                    const int cl = n0 + grp * COLS_PER_WARP + c * 32 + lane;
+                    a0[c] = cl < ep.Mpad ? ep.alpha[cl] : 0.0;
+                    a1[c] = cl < ep.Mpad ? ep.aoff[cl] : 0.0;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c) prm[c * 32 + lane] = make_double2(a0[c], a1[c]);
+                __syncwarp();
+            }
+            for (int c = 0; c < CHUNKS; ++c) {
                 const int col = grp * COLS_PER_WARP + c * 32;
                 const int gcol = n0 + col;
                 if (gcol >= ep.Mpad) break;   // warp-uniform; Mpad is a multiple of 32
-                // column parameters (alpha_s, mu . q_s): lane l loads column gcol + l,
-                // the element loop reads them back as shared-memory broadcasts
-                __syncwarp();
-                prm[lane] = make_double2(ep.alpha[gcol + lane], ep.aoff[gcol + lane]);
-                __syncwarp();
+                const double2 *pc = prm + c * 32;
                 float v[32];
                 tmem_ld32(taddr + (uint32_t)col, v);
                 __align__(16) __nv_bfloat16 hi[32], lo[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const double2 p = prm[j];
+                    const double2 p = pc[j];
                     const double K = ((double)v[j] + p.y) + qo;
                     const double t1 = p.x * kpow_m1<MODE>(K, ep);   // alpha_s K^(zeta-1)
                     k4[j & 3] += t1;

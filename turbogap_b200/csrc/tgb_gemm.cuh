@@ -33,6 +33,8 @@ struct GemmEpi {
     int mode;
     int rows;             // valid rows of C (and the rows the launch is sized for)
     const int *rows_dev;  // optional: the valid rows are min(rows, *rows_dev), read on the device
+    int bd_block;         // > 0: block-diagonal product; output columns [j b, (j+1) b) use A's
+                          // K range [j b, j b + K) (b a multiple of kGemmBN)
     int cols;             // valid columns of C
     // EPI_GAP_KERNEL
     const double *alpha;  // [Mpad]

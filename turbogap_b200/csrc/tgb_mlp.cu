@@ -241,16 +241,23 @@ __global__ void k_refresh(const float *__restrict__ P, MlpLayout L, bf16 *__rest
 }
 
 // inference copy of member k: W1 / sx into rows k H .. of W1cat and columns of
-// W1Tcat; biases; w3 sE; b3 sE + muE
+// W1Tcat; W2 and W2^T into rows k H .. of W2cat, W2Tcat; biases; w3 sE; b3 sE + muE
 __global__ void k_refresh_infer(const float *__restrict__ P, MlpLayout L, int k, int nm, float inv_sx,
                                 float sE, float muE, bf16 *__restrict__ W1cat,
-                                bf16 *__restrict__ W1Tcat, float *__restrict__ b1cat,
+                                bf16 *__restrict__ W1Tcat, bf16 *__restrict__ W2cat,
+                                bf16 *__restrict__ W2Tcat, float *__restrict__ b1cat,
                                 float *__restrict__ b2cat, float *__restrict__ w3cat,
                                 float *__restrict__ b3cat) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t n1 = (int64_t)L.H * L.Dp;
+    const int64_t n1 = (int64_t)L.H * L.Dp, n2 = (int64_t)L.H * L.H;
     const int HH = nm * L.H;
-    if (i < n1) {
+    if (i >= n1 + L.H && i < n1 + L.H + n2) {
+        const int64_t q = i - n1 - L.H;
+        const int r = (int)(q / L.H), c = (int)(q % L.H);
+        const bf16 v = __float2bfloat16_rn(P[L.oW2 + q]);
+        W2cat[((size_t)k * L.H + r) * L.H + c] = v;
+        W2Tcat[((size_t)k * L.H + c) * L.H + r] = v;
+    } else if (i < n1) {
         const int r = (int)(i / L.Dp), c = (int)(i % L.Dp);
         const bf16 v = __float2bfloat16_rn(c < L.D ? P[L.oW1 + i] * inv_sx : 0.f);
         W1cat[(size_t)(k * L.H + r) * L.Dp + c] = v;
@@ -433,9 +440,34 @@ struct MlpInferWork {
         p1.ep.out_b0 = H1.p;
         p1.ep.out_b1 = S1.p;
         p1.ep.ldb = HH;
-        p2.assign(nm, Plan{});
-        p3.assign(nm, Plan{});
-        for (int k = 0; k < nm; ++k) {
+        // layer 2 and its adjoint: one block-diagonal launch over all members when a
+        // member's columns are whole tiles, else one launch per member
+        const bool bd = H % kGemmBN == 0;
+        const int nl = bd ? 1 : nm;
+        p2.assign(nl, Plan{});
+        p3.assign(nl, Plan{});
+        if (bd) {
+            // the A maps span every member's columns: tile column j reads K range [j H, j H + H)
+            TGB_TRY(plan(p2[0], H1.p, rows, HH, m.W2cat, HH, H, H, nullptr, 0));
+            TGB_TRY(make_tma_bf16(&p2[0].a, H1.p, rows, HH, HH, kGemmBM));
+            p2[0].ep.mode = EPI_MLP_L2;
+            p2[0].ep.bd_block = H;
+            p2[0].ep.p0 = m.b2cat;
+            p2[0].ep.p1 = m.w3cat;
+            p2[0].ep.out_b0 = U2.p;
+            p2[0].ep.ldb = HH;
+            p2[0].ep.rowpart = part.p;
+            p2[0].ep.rowpart_ld = nm * np;
+            TGB_TRY(plan(p3[0], U2.p, rows, HH, m.W2Tcat, HH, H, H, nullptr, 0));
+            TGB_TRY(make_tma_bf16(&p3[0].a, U2.p, rows, HH, HH, kGemmBM));
+            p3[0].ep.mode = EPI_MLP_L2B;
+            p3[0].ep.bd_block = H;
+            p3[0].ep.in_b = S1.p;
+            p3[0].ep.ldi = HH;
+            p3[0].ep.out_b0 = U1.p;
+            p3[0].ep.ldb = HH;
+        }
+        for (int k = 0; k < nm && !bd; ++k) {
             TGB_TRY(plan(p2[k], H1.p + k * H, rows, HH, m.W2b[k], H, H, H, nullptr, 0));
             p2[k].ep.mode = EPI_MLP_L2;
             p2[k].ep.p0 = m.b2cat + k * H;
@@ -497,6 +529,8 @@ int mlp_create(int dim, int hidden, int n_members, unsigned long long seed, Mlp 
     const size_t HH = (size_t)n_members * L.H;
     if (rc == TG_OK) rc = dev_alloc(&m->W1cat, HH * L.Dp);
     if (rc == TG_OK) rc = dev_alloc(&m->W1Tcat, HH * L.Dp);
+    if (rc == TG_OK) rc = dev_alloc(&m->W2cat, HH * L.H);
+    if (rc == TG_OK) rc = dev_alloc(&m->W2Tcat, HH * L.H);
     if (rc == TG_OK) rc = dev_alloc(&m->b1cat, HH);
     if (rc == TG_OK) rc = dev_alloc(&m->b2cat, HH);
     if (rc == TG_OK) rc = dev_alloc(&m->w3cat, HH);
@@ -533,7 +567,8 @@ void mlp_destroy(Mlp *m) {
         for (auto &p : *v) dev_free(p);
     for (auto *v : {&m->W1b, &m->W1Tb, &m->W2b, &m->W2Tb})
         for (auto &p : *v) dev_free(p);
-    dev_free(m->W1cat); dev_free(m->W1Tcat); dev_free(m->b1cat); dev_free(m->b2cat);
+    dev_free(m->W1cat); dev_free(m->W1Tcat); dev_free(m->W2cat); dev_free(m->W2Tcat);
+    dev_free(m->b1cat); dev_free(m->b2cat);
     dev_free(m->w3cat); dev_free(m->b3cat); dev_free(m->dx); dev_free(m->dg); dev_free(m->de);
     dev_free(m->err);
     delete m->tw;
@@ -552,11 +587,12 @@ static int refresh_member(Mlp &m, int k, cudaStream_t st) {
 static int refresh_infer(Mlp &m, cudaStream_t st) {
     const MlpLayout &L = m.L;
     const double sx = m.sx > 0 ? m.sx : 1.0, sE = m.sE > 0 ? m.sE : 1.0;
-    const int64_t n = (int64_t)L.H * L.Dp + L.H;
+    const int64_t n = (int64_t)L.H * L.Dp + L.H + (int64_t)L.H * L.H;
     for (int k = 0; k < m.n_members; ++k) {
         k_refresh_infer<<<blocks_for(n), 256, 0, st>>>(m.P[k], L, k, m.n_members, (float)(1.0 / sx),
                                                        (float)sE, (float)m.muE, m.W1cat, m.W1Tcat,
-                                                       m.b1cat, m.b2cat, m.w3cat, m.b3cat);
+                                                       m.W2cat, m.W2Tcat, m.b1cat, m.b2cat,
+                                                       m.w3cat, m.b3cat);
         TGB_CUDA(cudaGetLastError());
     }
     m.infer_ready = true;
@@ -826,8 +862,8 @@ int mlp_infer(Mlp &m, MlpInferWork &w, int n, const bf16 *X, int ldx, double *e_
     TGB_TRY(w.bind(m, X, n, ldx, g_mean, ldg, g_sub));
     const int nm = m.n_members;
     TGB_TRY(run(w.p1, m.err, st));
-    for (int k = 0; k < nm; ++k) TGB_TRY(run(w.p2[k], m.err, st));
-    for (int k = 0; k < nm; ++k) TGB_TRY(run(w.p3[k], m.err, st));
+    for (const Plan &q : w.p2) TGB_TRY(run(q, m.err, st));
+    for (const Plan &q : w.p3) TGB_TRY(run(q, m.err, st));
     TGB_TRY(run(w.p4, m.err, st));
     k_i_energy<<<blocks_for((size_t)n), 256, 0, st>>>(n, nm, w.npart(m), w.part.p, m.b3cat, e_mean,
                                                        e_std);

@@ -52,6 +52,7 @@ struct Mlp {
     long long n_data = 0, cap_data = 0;
     // inference weights of all members (refreshed after training / set)
     __nv_bfloat16 *W1cat = nullptr, *W1Tcat = nullptr;   // [nm H][Dp], [Dp][nm H]
+    __nv_bfloat16 *W2cat = nullptr, *W2Tcat = nullptr;   // [nm H][H]: W2, W2^T of member k at row k H
     float *b1cat = nullptr, *b2cat = nullptr, *w3cat = nullptr, *b3cat = nullptr;
     bool infer_ready = false;
     MlpTrainWork *tw = nullptr;

@@ -542,7 +542,9 @@ struct ForceShape {
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
     static constexpr int WARPS = 4;
-    static constexpr int BSTRIDE = NT * NT + 1;    // per-l stride of the B matrices (bank spread)
+    static constexpr int BROW = NT + 1;            // row stride of B_l: the transposed writes
+                                                   // (lanes 16 apart) stay on distinct banks
+    static constexpr int BSTRIDE = NT * BROW + 1;  // per-l stride of the B matrices (odd)
     static constexpr int BAREA = (NL * BSTRIDE + 3) / 4 * 4;   // keeps gam 16-byte aligned
     static constexpr int WARP_FLOATS = BAREA + NLM * NT;
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
@@ -581,8 +583,14 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
         // q = mu + delta. dE/dp = (dE/dq - (dE/dq . q) q) / |p|, all in FP64.
         const float *g = I.g + (size_t)site * DIM;
         const float *q = I.q + (size_t)site * DIM;
-        double ksum = 0.0;
-        for (int t = 0; t < I.n_etiles; ++t) ksum += I.kdsum[(size_t)site * I.n_etiles + t];
+        // per-slice partial sums: lanes load in parallel, a butterfly adds them
+        double ksum = 0.0, esum = 0.0;
+        for (int t = lane; t < I.n_etiles; t += 32) {
+            ksum += I.kdsum[(size_t)site * I.n_etiles + t];
+            esum += I.epart[(size_t)site * I.n_etiles + t];
+        }
+        ksum = warp_sum(ksum);
+        esum = warp_sum(esum);
         double dot = 0.0;
         for (int d = lane; d < DIM; d += 32) {
             const double mu = P.mu[d];
@@ -603,11 +611,11 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
                 const float h = (float)((gd - dot * qd) * inv);
                 const int n = pair_n[pi], n2 = pair_n2[pi];
                 if (n == n2) {
-                    Bl[n * NT + n] = 2.f * h;
+                    Bl[n * Sh::BROW + n] = 2.f * h;
                 } else {
                     const float v = 1.41421356237309515f * h;
-                    Bl[n * NT + n2] = v;
-                    Bl[n2 * NT + n] = v;
+                    Bl[n * Sh::BROW + n2] = v;
+                    Bl[n2 * Sh::BROW + n] = v;
                 }
             }
         }
@@ -633,7 +641,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             for (int n = 0; n < NT; ++n) {
                 float v = 0.f;
 #pragma unroll
-                for (int n2 = 0; n2 < NT; ++n2) v += Bl[n * NT + n2] * cr[n2];
+                for (int n2 = 0; n2 < NT; ++n2) v += Bl[n * Sh::BROW + n2] * cr[n2];
                 gam[lmk[k] * NT + n] = v;
             }
         }
@@ -746,9 +754,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             atomicAdd(&O.forces[3 * (size_t)catom], fs[0]);
             atomicAdd(&O.forces[3 * (size_t)catom + 1], fs[1]);
             atomicAdd(&O.forces[3 * (size_t)catom + 2], fs[2]);
-            double e = 0.0;
-            for (int t = 0; t < I.n_etiles; ++t) e += I.epart[(size_t)site * I.n_etiles + t];
-            O.energies[catom] += I.delta2 * e;
+            O.energies[catom] += I.delta2 * esum;
         }
     }
 #pragma unroll
