@@ -93,7 +93,7 @@ struct Workspace {
     DBuf<__nv_bfloat16> qsplit, kd;
     DBuf<float> q, c, g;
     DBuf<double> pnorm, epart, kdsum, qoff, vpart;
-    TmaMap tmA1{}, tmA2{};
+    TmaMap tmA1{}, tmA2{}, tmKd{};   // tmKd: the GAP epilogue's TMA stores into kd
     int tm_rows = -1;
     const void *tm_p1 = nullptr, *tm_p2 = nullptr;
 
@@ -118,6 +118,7 @@ struct Workspace {
         if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p) {
             TGB_TRY(make_tma_bf16(&tmA1, qsplit.p, n, b.K1, b.K1, kGemmBM));
             TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.K2, b.K2, kGemmBM));
+            TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, n, b.K2, b.K2));
             tm_rows = n;
             tm_p1 = qsplit.p;
             tm_p2 = kd.p;
@@ -239,7 +240,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e1.K2 = b.K2;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st));
+    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st, &w.tmKd));
     TGB_MARK(log, PASS_GEMM1, st);
     GemmEpi e2{};
     e2.mode = EPI_STORE_F32;
@@ -404,7 +405,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e1.K2 = b.K2;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st));
+    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st, &w.tmKd));
     TGB_MARK(log, PASS_GEMM1, st);
     GemmEpi e2{};
     e2.mode = EPI_STORE_F32;

@@ -139,7 +139,11 @@ constexpr int COLS_PER_WARP = BN / kGemmEpiGroups;   // accumulator columns one 
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
 constexpr int CHUNKS = COLS_PER_WARP / 32;          // 32-column chunks per epilogue warp
 constexpr size_t PRM_BYTES = (size_t)EPI_WARPS * CHUNKS * 32 * sizeof(double2);
-constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256 + PRM_BYTES;
+// kd staging of the GAP epilogue: per warp two buffers of a 32 x 32 hi and lo block
+// (64-byte rows, 64-byte swizzle), written out by TMA tensor stores
+constexpr uint32_t STG_HALF = 32 * 32 * 2;           // one 32 x 32 bf16 block
+constexpr uint32_t STG_BUF = 2 * STG_HALF;           // hi + lo
+constexpr uint32_t STG_WARP = 2 * STG_BUF;           // double buffered
 constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
 
 // Epilogue variants (compile-time, so the element loop has no mode branches).
@@ -168,6 +172,33 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// Shared-memory plan of a mode: the GAP epilogue stages its kd blocks for TMA
+// stores and therefore runs a 3-stage operand ring; the others run 4 stages.
+__host__ __device__ constexpr bool gap_mode(int mode) { return mode <= MODE_GAP_ZREAL; }
+__host__ __device__ constexpr int stages_for(int mode) { return gap_mode(mode) ? 3 : STAGES; }
+__host__ __device__ constexpr size_t stg_offset(int mode) {   // from the 1024-aligned base
+    return ((size_t)stages_for(mode) * (A_BYTES + B_BYTES) + 256 + PRM_BYTES + 1023) / 1024 * 1024;
+}
+__host__ __device__ constexpr size_t smem_bytes_for(int mode) {
+    return 1024 + stg_offset(mode) + (gap_mode(mode) ? (size_t)EPI_WARPS * STG_WARP : 0);
+}
+static_assert(smem_bytes_for(MODE_GAP_Z4) <= 232448 && smem_bytes_for(MODE_STORE) <= 232448,
+              "shared memory plan exceeds 227 KB");
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
+                 "r"(v.w)
+                 : "memory");
+}
+
+// TMA tensor store of a staged block (shared -> global), tracked by a bulk group
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(src)
+                 : "memory");
+}
+
 // Persistent: CTA b processes tiles b, b + gridDim.x, ... (column tile fastest,
 // so concurrently resident CTAs share A rows in L2). Stage counters of the
 // shared-memory ring run across tiles; accumulator it % 2 is reused every
@@ -175,17 +206,21 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 template <int MODE>
 __global__ void __launch_bounds__(THREADS, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-              int num_kb, int n_tiles_m, int n_tiles_n, GemmEpi ep, unsigned *err) {
+              const __grid_constant__ CUtensorMap tmC, int num_kb, int n_tiles_m, int n_tiles_n,
+              GemmEpi ep, unsigned *err) {
+    constexpr int NST = stages_for(MODE);
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
-    const uint32_t sA = base, sB = base + STAGES * A_BYTES;
-    // barriers: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], then the
-    // TMEM slot; the per-warp column-parameter slots follow the 256-byte block
-    const uint32_t bars = sB + STAGES * B_BYTES;
-    const uint32_t full0 = bars, empty0 = bars + 8 * STAGES;
-    const uint32_t accf0 = bars + 16 * STAGES, acce0 = accf0 + 16;
+    const uint32_t sA = base, sB = base + NST * A_BYTES;
+    // barriers: full[NST], empty[NST], acc_full[2], acc_empty[2], then the TMEM
+    // slot; the per-warp column-parameter slots follow the 256-byte block, the kd
+    // staging buffers (GAP modes) the next 1024-byte boundary
+    const uint32_t bars = sB + NST * B_BYTES;
+    const uint32_t full0 = bars, empty0 = bars + 8 * NST;
+    const uint32_t accf0 = bars + 16 * NST, acce0 = accf0 + 16;
+    const uint32_t stg0 = base + (uint32_t)stg_offset(MODE);
     const uint32_t slot_addr = acce0 + 16;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + (slot_addr - base));
     double2 *prm_all = reinterpret_cast<double2 *>(gbase + (bars + 256 - base));
@@ -198,7 +233,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int n_tiles = min(n_tiles_m, (rows + BM - 1) / BM) * n_tiles_n;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < NST; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
@@ -228,8 +263,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int m0 = (t / n_tiles_n) * BM, n0 = (t % n_tiles_n) * BN;
             const int ak = ep.bd_block > 0 ? (n0 / ep.bd_block) * ep.bd_block : 0;
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
-                const int s = g % STAGES;
-                const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                const int s = g % NST;
+                const uint32_t ph = (uint32_t)(g / NST) & 1u;
                 if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) {
                     atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_TMA);
                     ok = false;
@@ -242,8 +277,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         // Drain: the last load of every stage has landed before the CTA may exit
         // (already true on the normal path, where the MMA consumed them).
-        for (int k = g > STAGES ? g - STAGES : 0; k < g; ++k)
-            (void)mbar_wait(full0 + 8 * (k % STAGES), (uint32_t)(k / STAGES) & 1u, err);
+        for (int k = g > NST ? g - NST : 0; k < g; ++k)
+            (void)mbar_wait(full0 + 8 * (k % NST), (uint32_t)(k / NST) & 1u, err);
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer
         constexpr uint32_t idesc = make_idesc(BM, BN);
@@ -259,8 +294,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             tc_fence_after();
             const uint32_t dacc = tmem + (uint32_t)(a * BN);
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
-                const int s = g % STAGES;
-                const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                const int s = g % NST;
+                const uint32_t ph = (uint32_t)(g / NST) & 1u;
                 if (!mbar_wait(full0 + 8 * s, ph, err)) {
                     atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_MMA);
                     ok = false;
@@ -282,6 +317,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int q = warp & 3;
       const int grp = (warp - 2) >> 2;
       double2 *prm = prm_all + (warp - 2) * CHUNKS * 32;
+      const uint32_t stg_warp = stg0 + (uint32_t)(warp - 2) * STG_WARP;
+      int nbuf = 0;   // kd staging buffers used so far (alternating)
       int it = 0;
       for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
         const int a = it & 1;
@@ -421,23 +458,35 @@ __global__ void __launch_bounds__(THREADS, 1)
                     // kd_s - kcoef_s = zeta delta^2 (alpha_s K^(zeta-1) - alpha_s)
                     bf16_split((float)(t1 - p.x) * c0f, hi[j], lo[j]);
                 }
-                if (row_ok) {
-                    __nv_bfloat16 *kr = ep.kd + (size_t)row * ep.K2 + gcol;
+                // Stage the 32 x 32 hi / lo blocks (64-byte rows, 64-byte swizzle: the
+                // 16-byte chunk u of row r sits at chunk u ^ ((r >> 1) & 3)) and let TMA
+                // write them out as whole lines. Rows past the tensor are clipped by TMA.
+                const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
+                if (lane == 0)   // the group that last used this buffer has read it
+                    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                __syncwarp();
+                {
                     const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
                     const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
-                    uint4 *d0 = reinterpret_cast<uint4 *>(kr);
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) d0[u] = h4[u];
-                    if (ep.nsplit == 3) {
-                        uint4 *d1 = reinterpret_cast<uint4 *>(kr + ep.Mpad);
-                        uint4 *d2 = reinterpret_cast<uint4 *>(kr + 2 * ep.Mpad);
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            d1[u] = h4[u];
-                            d2[u] = l4[u];
-                        }
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t off = (uint32_t)lane * 64u + (uint32_t)((u ^ ((lane >> 1) & 3)) * 16);
+                        st_shared_v4(sbuf + off, h4[u]);
+                        if (ep.nsplit == 3) st_shared_v4(sbuf + STG_HALF + off, l4[u]);
                     }
                 }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                const int y = m0 + q * 32;   // warp-uniform
+                if (lane == 0 && y < rows) {   // partial blocks are clipped by TMA
+                    tma_store_2d(&tmC, sbuf, gcol, y);
+                    if (ep.nsplit == 3) {
+                        tma_store_2d(&tmC, sbuf, ep.Mpad + gcol, y);
+                        tma_store_2d(&tmC, sbuf + STG_HALF, 2 * ep.Mpad + gcol, y);
+                    }
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+                ++nbuf;
             }
             if (row_ok) {
                 const size_t o = ((size_t)row * n_tiles_n + tile_n) * kGemmEpiGroups + grp;
@@ -469,6 +518,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(acce0 + 8 * a);
+      }
+      if constexpr (gap_mode(MODE)) {   // the kd stores have landed before the CTA exits
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+          __syncwarp();
       }
     }
     __syncwarp();
@@ -518,15 +571,33 @@ int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64
     return TG_OK;
 }
 
+int make_tma_store_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld) {
+    TGB_TRY(get_encoder());
+    TGB_CHECK(((uintptr_t)base & 15) == 0, TG_ERR_ARG, "TMA base address not 16-byte aligned");
+    TGB_CHECK((ld * 2) % 16 == 0, TG_ERR_ARG, "TMA row stride %lld B not a multiple of 16",
+              (long long)(ld * 2));
+    TGB_CHECK(rows >= 1 && cols >= 1, TG_ERR_ARG, "empty TMA extent");
+    cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(&m->map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base),
+                          gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TGB_CHECK(r == CUDA_SUCCESS, TG_ERR_CUDA, "cuTensorMapEncodeTiled (store) failed (%d)", (int)r);
+    return TG_OK;
+}
+
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
-                   unsigned *err, cudaStream_t st) {
+                   unsigned *err, cudaStream_t st, const TmaMap *C) {
     TGB_CHECK(K % kGemmBK == 0, TG_ERR_ARG, "GEMM K=%d must be a multiple of %d", K, kGemmBK);
     // 16-byte vector stores in the epilogues
     TGB_CHECK(ep.mode != EPI_STORE_F32 || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
               TG_ERR_ARG, "fp32 output rows must be 16-byte aligned (ldo %% 4 == 0)");
     TGB_CHECK(ep.mode != EPI_GAP_KERNEL || (ep.K2 % 8 == 0 && ep.Mpad % 32 == 0 &&
-                                            ((uintptr_t)ep.kd & 15) == 0),
-              TG_ERR_ARG, "bf16 kernel-derivative rows must be 16-byte aligned, Mpad %% 32 == 0");
+                                            ((uintptr_t)ep.kd & 15) == 0 && C != nullptr),
+              TG_ERR_ARG, "GAP epilogue: 16-byte kd rows, Mpad %% 32 == 0 and a kd store map");
     if (M <= 0 || N <= 0) return TG_OK;
     TGB_CHECK(ep.mode < EPI_MLP_L1 || ep.mode == EPI_MLP_L1B ||
                   (ep.ldb % 8 == 0 && ((uintptr_t)ep.out_b0 & 15) == 0 && N % 32 == 0),
@@ -546,7 +617,7 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
         case EPI_MLP_L1B: mode = MODE_MLP_L1B; break;
         default: mode = MODE_STORE;
     }
-    using Kern = void (*)(CUtensorMap, CUtensorMap, int, int, int, GemmEpi, unsigned *);
+    using Kern = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, int, int, int, GemmEpi, unsigned *);
     static const Kern kerns[N_MODES] = {
         k_gemm_tn<MODE_GAP_Z4>, k_gemm_tn<MODE_GAP_ZINT>, k_gemm_tn<MODE_GAP_ZREAL>,
         k_gemm_tn<MODE_STORE>, k_gemm_tn<MODE_MLP_L1>, k_gemm_tn<MODE_MLP_L2>,
@@ -554,7 +625,7 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
     static bool attr[N_MODES] = {};
     if (!attr[mode]) {
         TGB_CUDA(cudaFuncSetAttribute(kerns[mode], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)SMEM_BYTES));
+                                      (int)smem_bytes_for(mode)));
         attr[mode] = true;
     }
     static int n_sm = 0;
@@ -565,7 +636,8 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
     }
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     const int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
-    kerns[mode]<<<grid, THREADS, SMEM_BYTES, st>>>(A.map, B.map, K / kGemmBK, tm, tn, ep, err);
+    kerns[mode]<<<grid, THREADS, smem_bytes_for(mode), st>>>(A.map, B.map, C ? C->map : A.map,
+                                                             K / kGemmBK, tm, tn, ep, err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -76,8 +76,13 @@ struct TmaMap {
 int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld,
                   int box_rows);
 
+// 2-D bf16 tensor map for TMA stores of 32 x 32 blocks (64-byte swizzle): the
+// GAP epilogue's kd scratch.
+int make_tma_store_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld);
+
+// C (map for the GAP epilogue's kd stores) is required in EPI_GAP_KERNEL mode.
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
-                   unsigned *err, cudaStream_t st);
+                   unsigned *err, cudaStream_t st, const TmaMap *C = nullptr);
 
 inline int gemm_n_tiles(int N) { return (N + kGemmBN - 1) / kGemmBN; }
 // Number of column slices the energy partials are split into.
