@@ -154,12 +154,6 @@ enum {
 
 __device__ __forceinline__ float sigmoid_f(float z) { return 1.f / (1.f + expf(-z)); }
 
-__device__ __forceinline__ void store_bf16x32(__nv_bfloat16 *dst, const __nv_bfloat16 (&v)[32]) {
-    const uint4 *s4 = reinterpret_cast<const uint4 *>(v);
-    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) d4[u] = s4[u];
-}
 
 template <int MODE>
 __device__ __forceinline__ double kpow_m1(double K, const GemmEpi &ep) {
@@ -172,15 +166,19 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Shared-memory plan of a mode: the GAP epilogue stages its kd blocks for TMA
-// stores and therefore runs a 3-stage operand ring; the others run 4 stages.
+// Shared-memory plan of a mode: epilogues with bf16 outputs (the GAP kd scratch,
+// the MLP activations) stage 32 x 32 blocks for TMA stores and therefore run a
+// 3-stage operand ring; the fp32-store modes run 4 stages.
 __host__ __device__ constexpr bool gap_mode(int mode) { return mode <= MODE_GAP_ZREAL; }
-__host__ __device__ constexpr int stages_for(int mode) { return gap_mode(mode) ? 3 : STAGES; }
+__host__ __device__ constexpr bool staged_mode(int mode) {
+    return gap_mode(mode) || mode == MODE_MLP_L1 || mode == MODE_MLP_L2 || mode == MODE_MLP_L2B;
+}
+__host__ __device__ constexpr int stages_for(int mode) { return staged_mode(mode) ? 3 : STAGES; }
 __host__ __device__ constexpr size_t stg_offset(int mode) {   // from the 1024-aligned base
     return ((size_t)stages_for(mode) * (A_BYTES + B_BYTES) + 256 + PRM_BYTES + 1023) / 1024 * 1024;
 }
 __host__ __device__ constexpr size_t smem_bytes_for(int mode) {
-    return 1024 + stg_offset(mode) + (gap_mode(mode) ? (size_t)EPI_WARPS * STG_WARP : 0);
+    return 1024 + stg_offset(mode) + (staged_mode(mode) ? (size_t)EPI_WARPS * STG_WARP : 0);
 }
 static_assert(smem_bytes_for(MODE_GAP_Z4) <= 232448 && smem_bytes_for(MODE_STORE) <= 232448,
               "shared memory plan exceeds 227 KB");
@@ -189,6 +187,27 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
                  "r"(v.w)
                  : "memory");
+}
+
+// Lane r's 32 bf16 values as row r of a 32 x 32 staging block: 64-byte rows with
+// the 64-byte swizzle of the store map (16-byte chunk u sits at u ^ ((r >> 1) & 3)).
+__device__ __forceinline__ void stage_row(uint32_t buf, int lane, const __nv_bfloat16 (&v)[32]) {
+    const uint4 *v4 = reinterpret_cast<const uint4 *>(v);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        st_shared_v4(buf + (uint32_t)lane * 64u + (uint32_t)((u ^ ((lane >> 1) & 3)) * 16), v4[u]);
+}
+
+// Before a warp refills staging buffer nbuf & 1: the bulk group that last read it
+// (two chunks ago) has finished reading.
+__device__ __forceinline__ void stage_acquire(int lane) {
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+    __syncwarp();
+}
+// After the warp's shared stores: make them visible to the async proxy.
+__device__ __forceinline__ void stage_release() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
 }
 
 // TMA tensor store of a staged block (shared -> global), tracked by a bulk group
@@ -371,10 +390,19 @@ __global__ void __launch_bounds__(THREADS, 1)
                         hb[j] = __float2bfloat16_rn(z * sg);
                         sb[j] = __float2bfloat16_rn(sg * (1.f + z * (1.f - sg)));
                     }
-                    if (row_ok) {
-                        store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, hb);
-                        store_bf16x32(ep.out_b1 + (size_t)row * ep.ldb + gcol, sb);
+                    // h1 and silu'(z1) blocks of one [rows x 2 HH] matrix (s at x2 + col)
+                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
+                    stage_acquire(lane);
+                    stage_row(sbuf, lane, hb);
+                    stage_row(sbuf + STG_HALF, lane, sb);
+                    stage_release();
+                    const int y = m0 + q * 32;
+                    if (lane == 0 && y < rows) {
+                        tma_store_2d(&tmC, sbuf, gcol, y);
+                        tma_store_2d(&tmC, sbuf + STG_HALF, ep.x2 + gcol, y);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
+                    ++nbuf;
                 } else if constexpr (MODE == MODE_MLP_L2) {
                     __align__(16) __nv_bfloat16 ub[32];
 #pragma unroll
@@ -384,19 +412,40 @@ __global__ void __launch_bounds__(THREADS, 1)
                         racc += q2.y * z * sg;
                         ub[j] = __float2bfloat16_rn(q2.y * sg * (1.f + z * (1.f - sg)));
                     }
-                    if (row_ok) store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, ub);
+                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
+                    stage_acquire(lane);
+                    stage_row(sbuf, lane, ub);
+                    stage_release();
+                    const int y = m0 + q * 32;
+                    if (lane == 0 && y < rows) {
+                        tma_store_2d(&tmC, sbuf, gcol, y);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                    }
+                    ++nbuf;
                 } else if constexpr (MODE == MODE_MLP_L2B) {
+                    __align__(16) __nv_bfloat16 sf[32], ub[32];
+                    uint4 *t4 = reinterpret_cast<uint4 *>(sf);
                     if (row_ok) {
-                        __align__(16) __nv_bfloat16 sf[32], ub[32];
                         const uint4 *s4 = reinterpret_cast<const uint4 *>(ep.in_b + (size_t)row * ep.ldi + gcol);
-                        uint4 *t4 = reinterpret_cast<uint4 *>(sf);
 #pragma unroll
                         for (int u = 0; u < 4; ++u) t4[u] = s4[u];
+                    } else {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            ub[j] = __float2bfloat16_rn(v[j] * __bfloat162float(sf[j]));
-                        store_bf16x32(ep.out_b0 + (size_t)row * ep.ldb + gcol, ub);
+                        for (int u = 0; u < 4; ++u) t4[u] = make_uint4(0, 0, 0, 0);
                     }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        ub[j] = __float2bfloat16_rn(v[j] * __bfloat162float(sf[j]));
+                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
+                    stage_acquire(lane);
+                    stage_row(sbuf, lane, ub);
+                    stage_release();
+                    const int y = m0 + q * 32;
+                    if (lane == 0 && y < rows) {
+                        tma_store_2d(&tmC, sbuf, gcol, y);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                    }
+                    ++nbuf;
                 } else {   // MODE_MLP_L1B
                     if (row_ok) {
                         float *o = ep.out + (size_t)row * ep.ldo + gcol;
@@ -462,21 +511,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 // 16-byte chunk u of row r sits at chunk u ^ ((r >> 1) & 3)) and let TMA
                 // write them out as whole lines. Rows past the tensor are clipped by TMA.
                 const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
-                if (lane == 0)   // the group that last used this buffer has read it
-                    asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-                __syncwarp();
-                {
-                    const uint4 *h4 = reinterpret_cast<const uint4 *>(hi);
-                    const uint4 *l4 = reinterpret_cast<const uint4 *>(lo);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const uint32_t off = (uint32_t)lane * 64u + (uint32_t)((u ^ ((lane >> 1) & 3)) * 16);
-                        st_shared_v4(sbuf + off, h4[u]);
-                        if (ep.nsplit == 3) st_shared_v4(sbuf + STG_HALF + off, l4[u]);
-                    }
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
+                stage_acquire(lane);
+                stage_row(sbuf, lane, hi);
+                if (ep.nsplit == 3) stage_row(sbuf + STG_HALF, lane, lo);
+                stage_release();
                 const int y = m0 + q * 32;   // warp-uniform
                 if (lane == 0 && y < rows) {   // partial blocks are clipped by TMA
                     tma_store_2d(&tmC, sbuf, gcol, y);
@@ -519,7 +557,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(acce0 + 8 * a);
       }
-      if constexpr (gap_mode(MODE)) {   // the kd stores have landed before the CTA exits
+      if constexpr (staged_mode(MODE)) {   // the staged stores have landed before the CTA exits
           if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
           __syncwarp();
       }
@@ -599,9 +637,9 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
                                             ((uintptr_t)ep.kd & 15) == 0 && C != nullptr),
               TG_ERR_ARG, "GAP epilogue: 16-byte kd rows, Mpad %% 32 == 0 and a kd store map");
     if (M <= 0 || N <= 0) return TG_OK;
-    TGB_CHECK(ep.mode < EPI_MLP_L1 || ep.mode == EPI_MLP_L1B ||
-                  (ep.ldb % 8 == 0 && ((uintptr_t)ep.out_b0 & 15) == 0 && N % 32 == 0),
-              TG_ERR_ARG, "bf16 MLP outputs need 16-byte rows and N %% 32 == 0");
+    TGB_CHECK(ep.mode < EPI_MLP_L1 || ep.mode == EPI_MLP_L1B || (C != nullptr && N % 32 == 0 &&
+                                                                   ep.x2 % 32 == 0),
+              TG_ERR_ARG, "bf16 MLP outputs need a store map, N %% 32 == 0 and x2 %% 32 == 0");
     TGB_CHECK(ep.mode != EPI_MLP_L2B || (ep.ldi % 8 == 0 && ((uintptr_t)ep.in_b & 15) == 0),
               TG_ERR_ARG, "bf16 MLP factor rows must be 16-byte aligned");
     TGB_CHECK(ep.mode != EPI_MLP_L1B || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),

@@ -19,10 +19,11 @@ namespace tgb {
 //     The partial sums e run over the gemm_n_etiles(Mpad) column slices of
 //     kGemmBN / kGemmEpiGroups sparse points; the consumer adds them up.
 //   EPI_STORE_F32   (GEMM 2, sum_s (kd_s - kcoef_s)(q_s - mu)): out[row][col] = C
-//   EPI_MLP_L1   z = C + p0[col]: out_b0 = bf16(silu z), out_b1 = bf16(silu' z)
-//   EPI_MLP_L2   z = C + p0[col]: out_b0 = bf16(p1[col] silu' z) and the row sums
-//                of p1[col] silu z into rowpart[row * rowpart_ld + tile * groups + group]
-//   EPI_MLP_L2B  out_b0 = bf16(C * in_b[row][col])
+//   EPI_MLP_L1   z = C + p0[col]: bf16(silu z) at column col and bf16(silu' z) at
+//                column x2 + col of the store map
+//   EPI_MLP_L2   z = C + p0[col]: bf16(p1[col] silu' z) through the store map and the
+//                row sums of p1[col] silu z into rowpart[row * rowpart_ld + tile * groups + group]
+//   EPI_MLP_L2B  bf16(C * in_b[row][col]) through the store map
 //   EPI_MLP_L1B  out[row][col] = scale C - p0[col] (p0 may be null), fp32, cols < cols
 enum EpiMode {
     EPI_GAP_KERNEL = 0, EPI_STORE_F32 = 1, EPI_MLP_L1 = 2, EPI_MLP_L2 = 3, EPI_MLP_L2B = 4,
@@ -52,8 +53,9 @@ struct GemmEpi {
     int ldo;
     // EPI_MLP_*
     const float *p0, *p1;           // per-column parameters
-    __nv_bfloat16 *out_b0, *out_b1; // bf16 outputs, row stride ldb
+    __nv_bfloat16 *out_b0, *out_b1; // bf16 outputs, row stride ldb (unused with a store map)
     int ldb;
+    int x2;                         // EPI_MLP_L1: column offset of silu'(z) in the store map
     const __nv_bfloat16 *in_b;      // bf16 elementwise factor, row stride ldi
     int ldi;
     float scale;

@@ -324,7 +324,8 @@ __global__ void k_copy_rows(int n, int D, const float *__restrict__ x, int ldx, 
 
 // ---------------------------------------------------------------- GEMM plans
 struct Plan {
-    TmaMap a{}, b{};
+    TmaMap a{}, b{}, c{};   // c: store map of the staged bf16 epilogues
+    bool has_c = false;
     int M = 0, N = 0, K = 0;
     GemmEpi ep{};
 };
@@ -348,7 +349,14 @@ int plan(Plan &p, const bf16 *A, int M, int lda, const bf16 *Bm, int N, int ldb,
 }
 
 int run(const Plan &p, unsigned *err, cudaStream_t st) {
-    return launch_gemm_tn(p.a, p.b, p.M, p.N, p.K, p.ep, err, st);
+    return launch_gemm_tn(p.a, p.b, p.M, p.N, p.K, p.ep, err, st, p.has_c ? &p.c : nullptr);
+}
+
+// bf16 output of a staged epilogue: rows x cols at base, row stride ld
+int plan_store(Plan &p, const bf16 *base, int rows, int cols, int ld) {
+    TGB_TRY(make_tma_store_bf16(&p.c, base, rows, cols, ld));
+    p.has_c = true;
+    return TG_OK;
 }
 
 int transpose(int R, int C, const bf16 *in, int ldi, bf16 *out, int ldo, cudaStream_t st) {
@@ -412,7 +420,7 @@ struct MlpInferWork {
     int n = 0, ldx = 0, ldg = 0;
     float *g = nullptr;
     const float *sub = nullptr;
-    Buf<bf16> H1, S1, U2, U1;
+    Buf<bf16> HS, U2, U1;   // HS: [rows][2 HH] = h1 | silu'(z1)
     Buf<float> part;
     Plan p1, p4;
     std::vector<Plan> p2, p3;
@@ -422,7 +430,7 @@ struct MlpInferWork {
     int ensure(Mlp &m, int rows) {
         if (rows > cap) {
             const size_t hh = (size_t)m.n_members * m.L.H;
-            TGB_TRY(H1.ensure(rows * hh)); TGB_TRY(S1.ensure(rows * hh));
+            TGB_TRY(HS.ensure(rows * 2 * hh));
             TGB_TRY(U2.ensure(rows * hh)); TGB_TRY(U1.ensure(rows * hh));
             TGB_TRY(part.ensure((size_t)rows * m.n_members * npart(m)));
             cap = rows;
@@ -437,9 +445,8 @@ struct MlpInferWork {
         TGB_TRY(plan(p1, x, rows, ld, m.W1cat, HH, Dp, Dp, nullptr, 0));
         p1.ep.mode = EPI_MLP_L1;
         p1.ep.p0 = m.b1cat;
-        p1.ep.out_b0 = H1.p;
-        p1.ep.out_b1 = S1.p;
-        p1.ep.ldb = HH;
+        p1.ep.x2 = HH;
+        TGB_TRY(plan_store(p1, HS.p, rows, 2 * HH, 2 * HH));
         // layer 2 and its adjoint: one block-diagonal launch over all members when a
         // member's columns are whole tiles, else one launch per member
         const bool bd = H % kGemmBN == 0;
@@ -448,40 +455,36 @@ struct MlpInferWork {
         p3.assign(nl, Plan{});
         if (bd) {
             // the A maps span every member's columns: tile column j reads K range [j H, j H + H)
-            TGB_TRY(plan(p2[0], H1.p, rows, HH, m.W2cat, HH, H, H, nullptr, 0));
-            TGB_TRY(make_tma_bf16(&p2[0].a, H1.p, rows, HH, HH, kGemmBM));
+            TGB_TRY(plan(p2[0], HS.p, rows, 2 * HH, m.W2cat, HH, H, H, nullptr, 0));
+            TGB_TRY(make_tma_bf16(&p2[0].a, HS.p, rows, HH, 2 * HH, kGemmBM));
             p2[0].ep.mode = EPI_MLP_L2;
             p2[0].ep.bd_block = H;
             p2[0].ep.p0 = m.b2cat;
             p2[0].ep.p1 = m.w3cat;
-            p2[0].ep.out_b0 = U2.p;
-            p2[0].ep.ldb = HH;
             p2[0].ep.rowpart = part.p;
             p2[0].ep.rowpart_ld = nm * np;
+            TGB_TRY(plan_store(p2[0], U2.p, rows, HH, HH));
             TGB_TRY(plan(p3[0], U2.p, rows, HH, m.W2Tcat, HH, H, H, nullptr, 0));
             TGB_TRY(make_tma_bf16(&p3[0].a, U2.p, rows, HH, HH, kGemmBM));
             p3[0].ep.mode = EPI_MLP_L2B;
             p3[0].ep.bd_block = H;
-            p3[0].ep.in_b = S1.p;
-            p3[0].ep.ldi = HH;
-            p3[0].ep.out_b0 = U1.p;
-            p3[0].ep.ldb = HH;
+            p3[0].ep.in_b = HS.p + HH;
+            p3[0].ep.ldi = 2 * HH;
+            TGB_TRY(plan_store(p3[0], U1.p, rows, HH, HH));
         }
         for (int k = 0; k < nm && !bd; ++k) {
-            TGB_TRY(plan(p2[k], H1.p + k * H, rows, HH, m.W2b[k], H, H, H, nullptr, 0));
+            TGB_TRY(plan(p2[k], HS.p + k * H, rows, 2 * HH, m.W2b[k], H, H, H, nullptr, 0));
             p2[k].ep.mode = EPI_MLP_L2;
             p2[k].ep.p0 = m.b2cat + k * H;
             p2[k].ep.p1 = m.w3cat + k * H;
-            p2[k].ep.out_b0 = U2.p + k * H;
-            p2[k].ep.ldb = HH;
             p2[k].ep.rowpart = part.p + (size_t)k * np;
             p2[k].ep.rowpart_ld = nm * np;
+            TGB_TRY(plan_store(p2[k], U2.p + k * H, rows, H, HH));
             TGB_TRY(plan(p3[k], U2.p + k * H, rows, HH, m.W2Tb[k], H, H, H, nullptr, 0));
             p3[k].ep.mode = EPI_MLP_L2B;
-            p3[k].ep.in_b = S1.p + k * H;
-            p3[k].ep.ldi = HH;
-            p3[k].ep.out_b0 = U1.p + k * H;
-            p3[k].ep.ldb = HH;
+            p3[k].ep.in_b = HS.p + HH + k * H;
+            p3[k].ep.ldi = 2 * HH;
+            TGB_TRY(plan_store(p3[k], U1.p + k * H, rows, H, HH));
         }
         TGB_TRY(plan(p4, U1.p, rows, HH, m.W1Tcat, m.L.D, HH, HH, gout, ldgo));
         p4.ep.mode = EPI_MLP_L1B;
