@@ -350,7 +350,10 @@ struct DescShape {
     static constexpr int RS = CHUNK * AMAX;
     static constexpr int AS = CHUNK * NL;
     static constexpr int STAGE = YS + RS + AS + CHUNK;
-    static constexpr int CWORDS = 2 * NT * NLM;
+    // FP64 c rows for the power spectrum: stride CS = 4 mod 16 doubles, so an
+    // 8 x 4 DMMA fragment load (rows lane/4, columns lane%4) is two wavefronts
+    static constexpr int CS = (NLM + 11) / 16 * 16 + 4;
+    static constexpr int CWORDS = 2 * NT * CS;
     static constexpr int WARP_FLOATS = ((STAGE > CWORDS ? STAGE : CWORDS) + 3) / 4 * 4;
     static_assert(AMAX % 4 == 0, "float4 reads of R rows need alpha_max % 4 == 0");
     static_assert(YS % 4 == 0 && RS % 4 == 0, "R rows must stay 16-byte aligned");
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                 double v = (double)acc[n][k];
                 if (lmk[k] == 0 && scen >= 0 && n / AMAX == scen)
                     v += (double)P.self_R[scen * AMAX + n % AMAX];
-                cs[n * NLM + lmk[k]] = v;
+                cs[n * Sh::CS + lmk[k]] = v;
                 O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)v;
             }
     __syncwarp();
@@ -484,45 +487,105 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
     constexpr int NP = NT * (NT + 1) / 2;
     auto power = [&](int l, int pi) -> double {
         const int n = pair_n[pi], n2 = pair_n2[pi];
-        const double *c1 = cs + n * NLM + l * l, *c2 = cs + n2 * NLM + l * l;
+        const double *c1 = cs + n * Sh::CS + l * l, *c2 = cs + n2 * Sh::CS + l * l;
         double v = 0.0;
 #pragma unroll
         for (int m = 0; m < 2 * l + 1; ++m) v += c1[m] * c2[m];
         return n != n2 ? v * 1.4142135623730951 : v;
     };
-    // pass 1: |p| (FP64)
-    double nrm2 = 0.0;
-#pragma unroll
-    for (int l = 0; l < NL; ++l)
-        for (int pi = lane; pi < NP; pi += 32) {
-            const double v = power(l, pi);
-            nrm2 += v * v;
-        }
-    nrm2 = warp_sum(nrm2);
-    const double nrm = sqrt(nrm2);
-    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-    // pass 2: q = p/|p|, delta = q - mu, delta . mu; operand rows hold split(delta)
     const int K1 = P.K1;
     __nv_bfloat16 *qs = O.qsplit + (size_t)site * K1;
     float *qrow = O.q + (size_t)site * DIM;
-    double off = 0.0;
-#pragma unroll
-    for (int l = 0; l < NL; ++l)
-        for (int pi = lane; pi < NP; pi += 32) {
-            const int u = l * NP + pi;
-            const double mu = P.mu[u];
-            const double dl = power(l, pi) * inv - mu;
-            off += dl * mu;
-            const float df = (float)dl;
-            qrow[u] = df;
-            __nv_bfloat16 hi, lo;
-            bf16_split(df, hi, lo);
-            qs[u] = hi;
-            if (P.nsplit == 3) {
-                qs[DIM + u] = hi;
-                qs[2 * DIM + u] = lo;
-            }
+    auto emit = [&](int u, double v, double invv, double &offv) {
+        const double mu = P.mu[u];
+        const double dl = v * invv - mu;
+        offv += dl * mu;
+        const float df = (float)dl;
+        qrow[u] = df;
+        __nv_bfloat16 hi, lo;
+        bf16_split(df, hi, lo);
+        qs[u] = hi;
+        if (P.nsplit == 3) {
+            qs[DIM + u] = hi;
+            qs[2 * DIM + u] = lo;
         }
+    };
+    double nrm2 = 0.0, off = 0.0, inv = 0.0;
+    if constexpr (NT % 8 == 0) {
+        // FP64 tensor cores: per l, the Gram blocks G_ab = C_a C_b^T of the 8-channel
+        // blocks a <= b (C_a = c[8a .. 8a+7][l^2 .. l^2+2l]), k-steps of 4 m values
+        // (zero-padded). Lane (g = lane/4, t = lane%4) holds G_ab[g][2t], G_ab[g][2t+1].
+        constexpr int NB = NT / 8;
+        const int g8 = lane >> 2, t4 = lane & 3;
+        auto gram = [&](int l, int a, int b, double &d0, double &d1) {
+            d0 = 0.0;
+            d1 = 0.0;
+            const double *ra = cs + (8 * a + g8) * Sh::CS + l * l;
+            const double *rb = cs + (8 * b + g8) * Sh::CS + l * l;
+            const int M = 2 * l + 1;
+#pragma unroll
+            for (int kb = 0; kb < M; kb += 4) {
+                const int m = kb + t4;
+                const double va = m < M ? ra[m] : 0.0;
+                const double vb = a == b ? va : (m < M ? rb[m] : 0.0);
+                asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                    : "+d"(d0), "+d"(d1)
+                    : "d"(va), "d"(vb));
+            }
+        };
+        // pass 1: |p|
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = a; b < NB; ++b) {
+                    double d[2];
+                    gram(l, a, b, d[0], d[1]);
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int n = 8 * a + g8, n2 = 8 * b + 2 * t4 + e;
+                        if (n > n2) continue;
+                        const double v = n != n2 ? d[e] * 1.4142135623730951 : d[e];
+                        nrm2 += v * v;
+                    }
+                }
+        nrm2 = warp_sum(nrm2);
+        inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+        // pass 2: q = p/|p|, delta = q - mu, delta . mu at u = l NP + pi(n, n2)
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = a; b < NB; ++b) {
+                    double d[2];
+                    gram(l, a, b, d[0], d[1]);
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int n = 8 * a + g8, n2 = 8 * b + 2 * t4 + e;
+                        if (n > n2) continue;
+                        const double v = n != n2 ? d[e] * 1.4142135623730951 : d[e];
+                        const int pi = n * NT - (n * (n - 1)) / 2 + (n2 - n);
+                        emit(l * NP + pi, v, inv, off);
+                    }
+                }
+    } else {
+        // pass 1: |p| (FP64)
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+            for (int pi = lane; pi < NP; pi += 32) {
+                const double v = power(l, pi);
+                nrm2 += v * v;
+            }
+        nrm2 = warp_sum(nrm2);
+        inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+        // pass 2: q = p/|p|, delta = q - mu, delta . mu; operand rows hold split(delta)
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+            for (int pi = lane; pi < NP; pi += 32) emit(l * NP + pi, power(l, pi), inv, off);
+    }
+    const double nrm = sqrt(nrm2);
     off = warp_sum(off);
     for (int d = P.nsplit * DIM + lane; d < K1; d += 32) qs[d] = __float2bfloat16_rn(0.f);
     if (lane == 0) {
@@ -542,9 +605,9 @@ struct ForceShape {
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
     static constexpr int WARPS = 4;
-    static constexpr int BROW = NT + 1;            // row stride of B_l: the transposed writes
-                                                   // (lanes 16 apart) stay on distinct banks
-    static constexpr int BSTRIDE = NT * BROW + 1;  // per-l stride of the B matrices (odd)
+    static constexpr int BROW = NT + 4;            // row stride of B_l: rows read as float4, the
+                                                   // transposed writes spread over the banks
+    static constexpr int BSTRIDE = NT * BROW + 4;  // per-l stride (multiple of 4, 4 mod 32)
     static constexpr int BAREA = (NL * BSTRIDE + 3) / 4 * 4;   // keeps gam 16-byte aligned
     static constexpr int WARP_FLOATS = BAREA + NLM * NT;
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
@@ -591,32 +654,64 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
         }
         ksum = warp_sum(ksum);
         esum = warp_sum(esum);
+        // descriptor entries in the internal order d = l * NP + pi
+        constexpr int NP = NT * (NT + 1) / 2;
+        // Four consecutive entries per lane and 16-byte loads; a group of four never
+        // crosses an l boundary because NP % 4 == 0.
+        constexpr bool VEC = (DIM % 4 == 0) && (NP % 4 == 0);
+        auto put_b = [&](int d, double gd, double qd, double dotv, double invv) {
+            const int l = d / NP, pi = d - l * NP;
+            float *Bl = Bm + l * Sh::BSTRIDE;
+            const float h = (float)((gd - dotv * qd) * invv);
+            const int n = pair_n[pi], n2 = pair_n2[pi];
+            if (n == n2) {
+                Bl[n * Sh::BROW + n] = 2.f * h;
+            } else {
+                const float v = 1.41421356237309515f * h;
+                Bl[n * Sh::BROW + n2] = v;
+                Bl[n2 * Sh::BROW + n] = v;
+            }
+        };
         double dot = 0.0;
-        for (int d = lane; d < DIM; d += 32) {
-            const double mu = P.mu[d];
-            dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
+        if constexpr (VEC) {
+            for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
+                const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
+                const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
+                const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
+                const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
+                const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                dot += (ksum * m0.x + z0.x + (double)gv.x) * (m0.x + (double)qv.x);
+                dot += (ksum * m0.y + z0.y + (double)gv.y) * (m0.y + (double)qv.y);
+                dot += (ksum * m1.x + z1.x + (double)gv.z) * (m1.x + (double)qv.z);
+                dot += (ksum * m1.y + z1.y + (double)gv.w) * (m1.y + (double)qv.w);
+            }
+        } else {
+            for (int d = lane; d < DIM; d += 32) {
+                const double mu = P.mu[d];
+                dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
+            }
         }
         dot = warp_sum(dot);
         const double nrm = I.pnorm[site];
         const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-        // descriptor entries in the internal order d = l * NP + pi
-        constexpr int NP = NT * (NT + 1) / 2;
-#pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            float *Bl = Bm + l * Sh::BSTRIDE;
-            for (int pi = lane; pi < NP; pi += 32) {
-                const int d = l * NP + pi;
+        if constexpr (VEC) {
+            for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
+                const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
+                const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
+                const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
+                const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
+                const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                put_b(d0, ksum * m0.x + z0.x + (double)gv.x, m0.x + (double)qv.x, dot, inv);
+                put_b(d0 + 1, ksum * m0.y + z0.y + (double)gv.y, m0.y + (double)qv.y, dot, inv);
+                put_b(d0 + 2, ksum * m1.x + z1.x + (double)gv.z, m1.x + (double)qv.z, dot, inv);
+                put_b(d0 + 3, ksum * m1.y + z1.y + (double)gv.w, m1.y + (double)qv.w, dot, inv);
+            }
+        } else {
+            for (int d = lane; d < DIM; d += 32) {
                 const double mu = P.mu[d];
-                const double gd = ksum * mu + P.g0[d] + (double)g[d], qd = mu + (double)q[d];
-                const float h = (float)((gd - dot * qd) * inv);
-                const int n = pair_n[pi], n2 = pair_n2[pi];
-                if (n == n2) {
-                    Bl[n * Sh::BROW + n] = 2.f * h;
-                } else {
-                    const float v = 1.41421356237309515f * h;
-                    Bl[n * Sh::BROW + n2] = v;
-                    Bl[n2 * Sh::BROW + n] = v;
-                }
+                put_b(d, ksum * mu + P.g0[d] + (double)g[d], mu + (double)q[d], dot, inv);
             }
         }
         __syncwarp();
@@ -639,9 +734,14 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             const float *Bl = Bm + lk[k] * Sh::BSTRIDE;
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
+                const float4 *Bn = reinterpret_cast<const float4 *>(Bl + n * Sh::BROW);
                 float v = 0.f;
 #pragma unroll
-                for (int n2 = 0; n2 < NT; ++n2) v += Bl[n * Sh::BROW + n2] * cr[n2];
+                for (int j = 0; j < NT / 4; ++j) {
+                    const float4 b = Bn[j];
+                    v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
+                         b.w * cr[4 * j + 3];
+                }
                 gam[lmk[k] * NT + n] = v;
             }
         }
