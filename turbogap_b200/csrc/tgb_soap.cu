@@ -228,7 +228,10 @@ int table_width(int amax, int lmax) { return 4 * (amax + lmax + 1); }
 int descriptor_ref_index(int d_internal, int nt, int nl) {
     const int np = nt * (nt + 1) / 2;
     const int l = d_internal / np, pi = d_internal - l * np;
-    return pi * nl + l;
+    int n = 0, n2 = 0;
+    internal_pair(pi, nt, n, n2);
+    const int pi_ref = n * nt - n * (n - 1) / 2 + (n2 - n);   // row-major n <= n2
+    return pi_ref * nl + l;
 }
 
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st) {
@@ -377,10 +380,10 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
     int *pspec = reinterpret_cast<int *>(As + Sh::AS);
     __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
     for (int t = threadIdx.x; t < NT * (NT + 1) / 2; t += blockDim.x) {
-        int n = 0, rem = t;
-        while (rem >= NT - n) { rem -= NT - n; ++n; }
+        int n = 0, n2 = 0;
+        internal_pair(t, NT, n, n2);
         pair_n[t] = (unsigned char)n;
-        pair_n2[t] = (unsigned char)(n + rem);
+        pair_n2[t] = (unsigned char)n2;
     }
     __syncthreads();
     const int site = blockIdx.x * Sh::WARPS + warp;
@@ -552,7 +555,10 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                 }
         nrm2 = warp_sum(nrm2);
         inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
-        // pass 2: q = p/|p|, delta = q - mu, delta . mu at u = l NP + pi(n, n2)
+        // pass 2: q = p/|p|, delta = q - mu, delta . mu. The internal order follows
+        // the Gram blocks (internal_pair): an off-diagonal block's entries sit in lane
+        // order (2 lane + e), so its rows are written as pairs; a diagonal block keeps
+        // its upper triangle row by row.
 #pragma unroll
         for (int l = 0; l < NL; ++l)
 #pragma unroll
@@ -561,13 +567,33 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                 for (int b = a; b < NB; ++b) {
                     double d[2];
                     gram(l, a, b, d[0], d[1]);
+                    const int base = l * NP + gram_block_start(a, b, NB);
+                    if (a != b) {
+                        const int u = base + 2 * lane;   // even: 16-byte mu pairs
+                        const double2 mu2 = __ldg(reinterpret_cast<const double2 *>(P.mu + u));
+                        const double dl0 = d[0] * 1.4142135623730951 * inv - mu2.x;
+                        const double dl1 = d[1] * 1.4142135623730951 * inv - mu2.y;
+                        off += dl0 * mu2.x + dl1 * mu2.y;
+                        const float f0 = (float)dl0, f1 = (float)dl1;
+                        *reinterpret_cast<float2 *>(qrow + u) = make_float2(f0, f1);
+                        __nv_bfloat16 h0, l0, h1, l1;
+                        bf16_split(f0, h0, l0);
+                        bf16_split(f1, h1, l1);
+                        const __nv_bfloat162 hh = __halves2bfloat162(h0, h1);
+                        *reinterpret_cast<__nv_bfloat162 *>(qs + u) = hh;
+                        if (P.nsplit == 3) {
+                            *reinterpret_cast<__nv_bfloat162 *>(qs + DIM + u) = hh;
+                            *reinterpret_cast<__nv_bfloat162 *>(qs + 2 * DIM + u) =
+                                __halves2bfloat162(l0, l1);
+                        }
+                    } else {
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int n = 8 * a + g8, n2 = 8 * b + 2 * t4 + e;
-                        if (n > n2) continue;
-                        const double v = n != n2 ? d[e] * 1.4142135623730951 : d[e];
-                        const int pi = n * NT - (n * (n - 1)) / 2 + (n2 - n);
-                        emit(l * NP + pi, v, inv, off);
+                        for (int e = 0; e < 2; ++e) {
+                            const int j = 2 * t4 + e;
+                            if (g8 > j) continue;
+                            const double v = g8 != j ? d[e] * 1.4142135623730951 : d[e];
+                            emit(base + g8 * 8 - (g8 * (g8 - 1)) / 2 + (j - g8), v, inv, off);
+                        }
                     }
                 }
     } else {
@@ -625,10 +651,10 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
     __shared__ unsigned char pair_n[NT * (NT + 1) / 2], pair_n2[NT * (NT + 1) / 2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int t = threadIdx.x; t < NT * (NT + 1) / 2; t += blockDim.x) {
-        int n = 0, rem = t;
-        while (rem >= NT - n) { rem -= NT - n; ++n; }
+        int n = 0, n2 = 0;
+        internal_pair(t, NT, n, n2);
         pair_n[t] = (unsigned char)n;
-        pair_n2[t] = (unsigned char)(n + rem);
+        pair_n2[t] = (unsigned char)n2;
     }
     if (lane < 6) vred[warp][lane] = 0.0;
     __syncthreads();

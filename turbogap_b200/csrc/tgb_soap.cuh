@@ -37,9 +37,46 @@ struct SiteArgs {
 };
 
 // Descriptor entries on the device run in the internal order d = l * NP + pi
-// (NP = NT (NT + 1) / 2 channel pairs n <= n2, pi in row-major upper-triangle
-// order); the reference order is pi * (l_max + 1) + l. The sparse set, mu and g0
-// are stored in the internal order, so the GEMMs see a consistent permutation.
+// (NP = NT (NT + 1) / 2 channel pairs n <= n2); the reference order is
+// pi_ref * (l_max + 1) + l with pi_ref the row-major upper-triangle index. The
+// sparse set, mu and g0 are stored in the internal order, so the GEMMs see a
+// consistent permutation. Within one l the pairs follow the 8 x 8 Gram blocks of
+// the power spectrum's tensor-core products when NT % 8 == 0: blocks (a, b),
+// a <= b in row-major order; a diagonal block holds its upper triangle row by
+// row (36 entries), an off-diagonal block all 64 entries in the order
+// 8 (n - 8a) + (n2 - 8b). Otherwise pi is the row-major upper-triangle index.
+__host__ __device__ inline int gram_block_start(int a, int b, int nb) {
+    int s = 0;
+    for (int i = 0; i < a; ++i) s += 36 + 64 * (nb - 1 - i);
+    return s + (b == a ? 0 : 36 + 64 * (b - a - 1));
+}
+
+__host__ __device__ inline void internal_pair(int pi, int nt, int &n, int &n2) {
+    if (nt % 8 == 0) {
+        const int nb = nt / 8;
+        for (int a = 0; a < nb; ++a)
+            for (int b = a; b < nb; ++b) {
+                const int size = a == b ? 36 : 64;
+                const int k = pi - gram_block_start(a, b, nb);
+                if (k < 0 || k >= size) continue;
+                if (a != b) {
+                    n = 8 * a + k / 8;
+                    n2 = 8 * b + k % 8;
+                } else {
+                    int g = 0, rem = k;
+                    while (rem >= 8 - g) { rem -= 8 - g; ++g; }
+                    n = 8 * a + g;
+                    n2 = 8 * a + g + rem;
+                }
+                return;
+            }
+    }
+    int g = 0, rem = pi;
+    while (rem >= nt - g) { rem -= nt - g; ++g; }
+    n = g;
+    n2 = g + rem;
+}
+
 int descriptor_ref_index(int d_internal, int nt, int nl);
 
 struct DescOut {
