@@ -1057,11 +1057,34 @@ struct Engine {
     bool first_step = true;
     double dt_prev = 0.0;
     cudaStream_t st = nullptr;
+    // blocks after the first run on their own streams (forked after the neighbour
+    // list, joined before integration), so one block's kernels fill the SMs the
+    // other block's tail waves leave idle
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev_side;
+    cudaEvent_t ev_fork = nullptr;
 
     ~Engine() {
         if (graph) cudaGraphExecDestroy(graph);
         nl.release();
+        for (auto e : ev_side) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (auto s2 : side) cudaStreamDestroy(s2);
         if (st) cudaStreamDestroy(st);
+    }
+
+    int ensure_streams() {
+        const size_t need = runs.size() > 1 ? runs.size() - 1 : 0;
+        if (!ev_fork) TGB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        while (side.size() < need) {
+            cudaStream_t s2;
+            cudaEvent_t e2;
+            TGB_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+            TGB_CUDA(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+            side.push_back(s2);
+            ev_side.push_back(e2);
+        }
+        return TG_OK;
     }
 
     EventLog prof;
@@ -1078,14 +1101,28 @@ struct Engine {
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
-        for (auto &r : runs) {
+        // with a pass log every block runs on the main stream, so the marks time passes
+        const bool fork = !log && runs.size() > 1;
+        if (fork) {
+            TGB_TRY(ensure_streams());
+            TGB_CUDA(cudaEventRecord(ev_fork, st));
+            for (size_t k = 1; k < runs.size(); ++k) TGB_CUDA(cudaStreamWaitEvent(side[k - 1], ev_fork, 0));
+        }
+        for (size_t k = 0; k < runs.size(); ++k) {
+            auto &r = runs[k];
+            cudaStream_t sk = (fork && k > 0) ? side[k - 1] : st;
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
             if (r->mix)
                 TGB_TRY(evaluate_block_mixed(*r->b, *r->w, *r->mix, S, n, f.p, en.p, vir.p, err.p,
-                                             st, log));
+                                             sk, log));
             else
-                TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log));
+                TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, sk, log));
         }
+        if (fork)
+            for (size_t k = 1; k < runs.size(); ++k) {
+                TGB_CUDA(cudaEventRecord(ev_side[k - 1], side[k - 1]));
+                TGB_CUDA(cudaStreamWaitEvent(st, ev_side[k - 1], 0));
+            }
         return TG_OK;
     }
 

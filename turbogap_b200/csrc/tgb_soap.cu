@@ -905,7 +905,7 @@ __global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, doub
     double s = 0.0;
     for (int b = threadIdx.x; b < nblk; b += 32) s += vpart[(size_t)b * 9 + q];
     s = warp_sum(s);
-    if (threadIdx.x == 0) out[q] += s;
+    if (threadIdx.x == 0) atomicAdd(out + q, s);   // blocks may reduce concurrently
 }
 
 // ===================== launchers ============================================
