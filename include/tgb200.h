@@ -204,6 +204,31 @@ int tg_engine_profile(tg_engine *e, int32_t n_steps, double dt, double *ms_per_p
 /* Kernel launches in one graph-captured MD step (0 before the first graph exists). */
 int tg_engine_graph_kernels(tg_engine *e, int32_t *n_kernels);
 
+/* ---- batches of independent structures (uneven sizes): energies, forces and a
+ *   virial per structure for many orthorhombic cells at once, through one batched
+ *   neighbour list and the same block kernels, replayed as one CUDA graph. No
+ *   reference counterpart: the reference evaluates one structure per run.
+ *   positions (3, N) and species (N) concatenate the structures in order;
+ *   boxes[9 s .. 9 s + 8] are structure s's a, b, c rows. Neighbour lists follow
+ *   the reference's pair set (every periodic image within the cutoff; boxes
+ *   smaller than 2 rcut see several images of a neighbour) in their own order. */
+typedef struct tg_batch tg_batch;
+
+int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *positions,
+                    const int32_t *species, const double *boxes, int32_t n_blocks,
+                    const int32_t *block_keys, const double *e0_by_species,
+                    int32_t n_species_total, tg_batch **out);
+int tg_batch_destroy(tg_batch *b);
+/* New positions (3, N); the pair arrays keep the capacity sized at creation
+ * (+25 %): TG_ERR_DEVICE reports an overflow. */
+int tg_batch_set_positions(tg_batch *b, const double *positions);
+/* energies (N), forces (3, N), virials [n_structs][3][3]; any may be NULL. */
+int tg_batch_compute(tg_batch *b, double *energies, double *forces, double *virials);
+/* Evaluation on the device only (graph replay after the first call). */
+int tg_batch_compute_device(tg_batch *b);
+int tg_batch_stream(tg_batch *b, void **stream);
+int tg_batch_n_pairs(tg_batch *b, int64_t *n_pairs);
+
 /* ---- learned surrogate (mixed form). No reference counterpart: TurboGAP has
  *   no learned model. Per block, an ensemble of n_members MLPs
  *   dim -> hidden -> hidden -> 1 (SiLU) maps delta = q - mu of a central site

@@ -95,6 +95,14 @@ SIGNATURES = [
     ("tg_mlp_predict", C.c_int, [_vp, C.c_int32, f32p, dp, dp, dp]),
     ("tg_engine_set_mlp", C.c_int, [_vp, C.c_int32, _vp, C.c_double]),
     ("tg_engine_mlp_stats", C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("tg_batch_create", C.c_int, [C.c_int32, ip, dp, ip, dp, C.c_int32, ip, _vp, C.c_int32,
+                                  C.POINTER(_vp)]),
+    ("tg_batch_destroy", C.c_int, [_vp]),
+    ("tg_batch_set_positions", C.c_int, [_vp, dp]),
+    ("tg_batch_compute", C.c_int, [_vp, _vp, _vp, _vp]),
+    ("tg_batch_compute_device", C.c_int, [_vp]),
+    ("tg_batch_stream", C.c_int, [_vp, C.POINTER(_vp)]),
+    ("tg_batch_n_pairs", C.c_int, [_vp, C.POINTER(C.c_int64)]),
     ("tgx_gemm_bf16_tn", C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16p, u16p, f32p]),
     ("tgx_mlp_batch_grads", C.c_int, [_vp, C.c_int32, C.c_int32, f32p, f32p, f32p, C.c_double, dp,
                                       C.POINTER(C.c_double), f32p, f32p]),

@@ -394,3 +394,63 @@ def engine_mlp_stats(engine: "Engine", block: int):
     g, n = C.c_int32(0), C.c_int32(0)
     check(lib().tg_engine_mlp_stats(engine.handle, int(block), C.byref(g), C.byref(n)))
     return int(g.value), int(n.value)
+
+
+class Batch:
+    """Many independent orthorhombic structures evaluated together (energies,
+    forces, per-structure virials), e.g. cells of uneven size."""
+
+    def __init__(self, structures, block_keys: Sequence[int], e0_by_species=None):
+        self.n_atoms = np.array([s.n for s in structures], np.int32)
+        self.n = int(self.n_atoms.sum())
+        self.ns = len(structures)
+        pos = np.ascontiguousarray(np.concatenate([s.positions for s in structures]), np.float64)
+        sp = np.ascontiguousarray(np.concatenate([s.species for s in structures]), np.int32)
+        boxes = np.ascontiguousarray(np.stack([np.asarray(s.box, np.float64).reshape(9)
+                                               for s in structures]))
+        keys = _i32(block_keys)
+        e0 = _f64(e0_by_species) if e0_by_species is not None else None
+        h = C.c_void_p()
+        check(lib().tg_batch_create(self.ns, self.n_atoms, pos, sp, boxes, len(keys), keys,
+                                    e0.ctypes.data if e0 is not None else None,
+                                    len(e0) if e0 is not None else 0, C.byref(h)))
+        self._h = h
+        self._keep = e0
+
+    def close(self):
+        if self._h:
+            lib().tg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_positions(self, positions):
+        check(lib().tg_batch_set_positions(self._h, _f64(positions)))
+
+    def compute(self):
+        e = np.zeros(self.n)
+        f = np.zeros((self.n, 3))
+        v = np.zeros((self.ns, 3, 3))
+        check(lib().tg_batch_compute(self._h, e.ctypes.data, f.ctypes.data, v.ctypes.data))
+        return e, f, v
+
+    def compute_device(self):
+        check(lib().tg_batch_compute_device(self._h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().tg_batch_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+    def n_pairs(self) -> int:
+        n = C.c_int64(0)
+        check(lib().tg_batch_n_pairs(self._h, C.byref(n)))
+        return int(n.value)

@@ -217,7 +217,8 @@ struct EventLog {
 // Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces.
 int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
                    double *energies, double *virial, unsigned *err, cudaStream_t st,
-                   EventLog *log = nullptr) {
+                   EventLog *log = nullptr, const int *atom_struct = nullptr,
+                   double *vir_struct = nullptr) {
     if (S.n_sites <= 0) return TG_OK;
     TGB_TRY(w.ensure(b, S.n_sites));
     const SoapParams P = b.params(n_atoms);
@@ -251,7 +252,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
     TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
-    ForceOut FO{forces, energies, w.vpart.p, err};
+    ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct};
     int nblk = 0;
     TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
@@ -1621,6 +1622,267 @@ int tg_engine_mlp_stats(tg_engine *eh, int32_t block, int32_t *n_gated, int32_t 
             TGB_CUDA(cudaStreamSynchronize(E.st));
         }
     }
+    return TG_OK;
+}
+
+}  // extern "C"
+
+// ============================================================== batches
+// Many independent orthorhombic structures evaluated together (energies, forces
+// and a virial per structure): one batched neighbour list over all of them, then
+// every block's kernels over the concatenated central sites, all in one CUDA
+// graph after the first evaluation.
+namespace tgb {
+
+struct BatchEngine {
+    int n = 0, ns = 0, nz = 1;
+    double rcut = 0.0;
+    DBuf<double> pos, f, en, vir, vir_s, e0, xyz;
+    DBuf<int> species, atom_struct, cell_id, cell_count, cell_start, cell_fill, cell_atoms, n_neigh,
+        nbr;
+    DBuf<int64_t> pstart;
+    DBuf<BatchStruct> sdev;
+    DBuf<char> scan_tmp;
+    DBuf<unsigned> err;
+    BatchNL nl;
+    std::vector<std::unique_ptr<BlockRun>> runs;
+    std::vector<int> n_atoms_h;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t graph = nullptr;
+
+    ~BatchEngine() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int compute_ef() {
+        TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
+        TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
+        TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
+        TGB_CUDA(cudaMemsetAsync(vir_s.p, 0, sizeof(double) * 9 * ns, st));
+        for (auto &r : runs) {
+            SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, nullptr,
+                                   atom_struct.p, vir_s.p));
+        }
+        return TG_OK;
+    }
+
+    int errors() {
+        unsigned e1 = 0, e2 = 0;
+        TGB_CUDA(cudaMemcpyAsync(&e1, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        TGB_CUDA(cudaMemcpyAsync(&e2, nl.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        TGB_CUDA(cudaStreamSynchronize(st));
+        if (!(e1 | e2)) return TG_OK;
+        TGB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), st));
+        TGB_CUDA(cudaMemsetAsync(nl.err, 0, sizeof(unsigned), st));
+        set_error("device error word 0x%x%s", e1 | e2,
+                  (e2 & DEV_ERR_NEIGH_CAPACITY) ? " (neighbour pair capacity exceeded)" : "");
+        return (e1 & (DEV_ERR_TIMEOUT_TMA | DEV_ERR_TIMEOUT_MMA | DEV_ERR_TIMEOUT_EPI)) ? TG_ERR_TIMEOUT
+                                                                                        : TG_ERR_DEVICE;
+    }
+
+    // pair arrays sized from a counting build (with 25 % headroom for moved atoms)
+    int size_pairs() {
+        nl.cap = 0;
+        TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        int64_t P = 0;
+        TGB_CUDA(cudaMemcpyAsync(&P, nl.pstart + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        TGB_CUDA(cudaStreamSynchronize(st));
+        const int64_t cap = P + P / 4 + 64;
+        TGB_TRY(nbr.ensure(cap));
+        TGB_TRY(xyz.ensure(3 * (size_t)cap));
+        nl.nbr = nbr.p;
+        nl.xyz = xyz.p;
+        nl.cap = cap;
+        TGB_CUDA(cudaMemsetAsync(nl.err, 0, sizeof(unsigned), st));
+        TGB_CUDA(cudaStreamSynchronize(st));
+        return TG_OK;
+    }
+};
+
+}  // namespace tgb
+
+struct tg_batch {
+    tgb::BatchEngine e;
+};
+
+extern "C" {
+
+int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *positions,
+                    const int32_t *species, const double *boxes, int32_t n_blocks,
+                    const int32_t *block_keys, const double *e0_by_species,
+                    int32_t n_species_total, tg_batch **out) {
+    TGB_TRY(need_ctx());
+    TGB_CHECK(out && n_structs >= 1 && n_atoms && positions && species && boxes && n_blocks >= 1 &&
+                  block_keys,
+              TG_ERR_ARG, "bad batch arguments");
+    Context &C = *g_ctx;
+    auto holder = std::make_unique<tg_batch>();
+    BatchEngine &E = holder->e;
+    TGB_CUDA(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    double rcut = 0.0;
+    for (int k = 0; k < n_blocks; ++k) {
+        auto it = C.blocks.find(block_keys[k]);
+        TGB_CHECK(it != C.blocks.end(), TG_ERR_STATE, "block key %d was never begun", block_keys[k]);
+        rcut = std::max(rcut, it->second->rcut_max);
+    }
+    E.rcut = rcut;
+    E.ns = n_structs;
+    std::vector<BatchStruct> sh(n_structs);
+    std::vector<int> as;
+    int off = 0, ncells = 0;
+    for (int s = 0; s < n_structs; ++s) {
+        const double *bx = boxes + 9 * (size_t)s;
+        TGB_CHECK(n_atoms[s] >= 1, TG_ERR_ARG, "structure %d has no atoms", s);
+        const Box b = make_box(bx, bx + 3, bx + 6);
+        TGB_CHECK(b.ortho, TG_ERR_ARG, "structure %d: batches take orthorhombic boxes", s);
+        BatchStruct &q = sh[s];
+        q.off = off;
+        q.n = n_atoms[s];
+        for (int k = 0; k < 3; ++k) q.L[k] = b.L[k];
+        q.coff = ncells;
+        ncells += batch_plan_struct(q, rcut);
+        for (int i = 0; i < q.n; ++i) as.push_back(s);
+        off += q.n;
+    }
+    E.n = off;
+    E.n_atoms_h.assign(n_atoms, n_atoms + n_structs);
+    const int n = E.n;
+    const size_t n3 = 3 * (size_t)n;
+    cudaStream_t st = E.st;
+    TGB_TRY(E.pos.ensure(n3)); TGB_TRY(E.f.ensure(n3)); TGB_TRY(E.en.ensure(n));
+    TGB_TRY(E.vir.ensure(9)); TGB_TRY(E.vir_s.ensure(9 * (size_t)n_structs));
+    TGB_TRY(E.species.ensure(n)); TGB_TRY(E.atom_struct.ensure(n)); TGB_TRY(E.err.ensure(1));
+    TGB_TRY(E.sdev.ensure(n_structs)); TGB_TRY(E.cell_id.ensure(n)); TGB_TRY(E.n_neigh.ensure(n));
+    TGB_TRY(E.pstart.ensure((size_t)n + 1));
+    const int nc = std::max(ncells, 1);
+    TGB_TRY(E.cell_count.ensure(nc)); TGB_TRY(E.cell_start.ensure(nc));
+    TGB_TRY(E.cell_fill.ensure(nc)); TGB_TRY(E.cell_atoms.ensure(n));
+    size_t need1 = 0, need2 = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, need1, E.n_neigh.p, E.pstart.p + 1, n);
+    cub::DeviceScan::ExclusiveSum(nullptr, need2, E.cell_count.p, E.cell_start.p, nc);
+    TGB_TRY(E.scan_tmp.ensure(std::max(need1, need2)));
+    E.nz = std::max(n_species_total, 1);
+    TGB_TRY(E.e0.ensure(E.nz));
+    std::vector<double> e0(E.nz, 0.0);
+    if (e0_by_species)
+        for (int z = 0; z < n_species_total; ++z) e0[z] = e0_by_species[z];
+    TGB_CUDA(cudaMemcpyAsync(E.pos.p, positions, sizeof(double) * n3, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.species.p, species, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.atom_struct.p, as.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.sdev.p, sh.data(), sizeof(BatchStruct) * n_structs,
+                             cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(E.e0.p, e0.data(), sizeof(double) * E.nz, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemsetAsync(E.err.p, 0, sizeof(unsigned), st));
+    BatchNL &nl = E.nl;
+    nl.n_atoms = n;
+    nl.n_structs = n_structs;
+    nl.n_cells = ncells;
+    nl.st = E.sdev.p;
+    nl.atom_struct = E.atom_struct.p;
+    nl.cell_id = E.cell_id.p;
+    nl.cell_count = E.cell_count.p;
+    nl.cell_start = E.cell_start.p;
+    nl.cell_fill = E.cell_fill.p;
+    nl.cell_atoms = E.cell_atoms.p;
+    nl.n_neigh = E.n_neigh.p;
+    nl.pstart = E.pstart.p;
+    nl.scan_tmp = E.scan_tmp.p;
+    nl.scan_bytes = E.scan_tmp.n;
+    nl.err = E.err.p;
+    for (int k = 0; k < n_blocks; ++k) {
+        Block *b = C.blocks[block_keys[k]].get();
+        auto run = std::make_unique<BlockRun>();
+        run->b = b;
+        run->w = std::make_unique<Workspace>();
+        std::vector<int> sites;
+        for (int i = 0; i < n; ++i) {
+            const int z = species[i];
+            int first = 0;
+            for (int q = 0; q < b->ns; ++q)
+                if (b->hh.species_z[q] == z) { first = q + 1; break; }
+            if (b->hh.central_species == 0 || first == b->hh.central_species) sites.push_back(i);
+        }
+        run->n_sites = (int)sites.size();
+        TGB_TRY(run->sites.ensure(sites.size()));
+        if (!sites.empty())
+            TGB_CUDA(cudaMemcpyAsync(run->sites.p, sites.data(), sizeof(int) * sites.size(),
+                                     cudaMemcpyHostToDevice, st));
+        TGB_TRY(run->w->ensure(*b, run->n_sites));
+        E.runs.push_back(std::move(run));
+    }
+    TGB_TRY(E.size_pairs());
+    *out = holder.release();
+    return TG_OK;
+}
+
+int tg_batch_destroy(tg_batch *b) {
+    if (!b) return TG_OK;
+    cudaStreamSynchronize(b->e.st);
+    delete b;
+    return TG_OK;
+}
+
+int tg_batch_set_positions(tg_batch *bh, const double *positions) {
+    TGB_CHECK(bh && positions, TG_ERR_ARG, "null argument");
+    BatchEngine &E = bh->e;
+    TGB_CUDA(cudaMemcpyAsync(E.pos.p, positions, sizeof(double) * 3 * E.n, cudaMemcpyHostToDevice,
+                             E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
+// Evaluation without copies out: the first call runs eagerly, later calls replay
+// one CUDA graph of the whole evaluation.
+int tg_batch_compute_device(tg_batch *bh) {
+    TGB_CHECK(bh, TG_ERR_ARG, "null batch");
+    BatchEngine &E = bh->e;
+    if (!E.graph) {
+        TGB_TRY(E.compute_ef());
+        TGB_TRY(E.errors());
+        cudaGraph_t gr;
+        TGB_CUDA(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+        int r = E.compute_ef();
+        cudaError_t ce = cudaStreamEndCapture(E.st, &gr);
+        TGB_TRY(r);
+        TGB_CUDA(ce);
+        ce = cudaGraphInstantiate(&E.graph, gr, 0);
+        cudaGraphDestroy(gr);
+        TGB_CUDA(ce);
+        return TG_OK;
+    }
+    TGB_CUDA(cudaGraphLaunch(E.graph, E.st));
+    return TG_OK;
+}
+
+int tg_batch_compute(tg_batch *bh, double *energies, double *forces, double *virials) {
+    TGB_CHECK(bh, TG_ERR_ARG, "null batch");
+    BatchEngine &E = bh->e;
+    TGB_TRY(tg_batch_compute_device(bh));
+    if (energies)
+        TGB_CUDA(cudaMemcpyAsync(energies, E.en.p, sizeof(double) * E.n, cudaMemcpyDeviceToHost, E.st));
+    if (forces)
+        TGB_CUDA(cudaMemcpyAsync(forces, E.f.p, sizeof(double) * 3 * E.n, cudaMemcpyDeviceToHost, E.st));
+    if (virials)
+        TGB_CUDA(cudaMemcpyAsync(virials, E.vir_s.p, sizeof(double) * 9 * E.ns, cudaMemcpyDeviceToHost,
+                                 E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return E.errors();
+}
+
+int tg_batch_stream(tg_batch *bh, void **stream) {
+    TGB_CHECK(bh && stream, TG_ERR_ARG, "null argument");
+    *stream = (void *)bh->e.st;
+    return TG_OK;
+}
+
+int tg_batch_n_pairs(tg_batch *bh, int64_t *n_pairs) {
+    TGB_CHECK(bh && n_pairs, TG_ERR_ARG, "null argument");
+    BatchEngine &E = bh->e;
+    TGB_CUDA(cudaMemcpyAsync(n_pairs, E.nl.pstart + E.n, sizeof(int64_t), cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
     return TG_OK;
 }
 

@@ -583,6 +583,214 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     return TG_OK;
 }
 
+// ---------------------------------------------------------------- batches
+int batch_plan_struct(BatchStruct &b, double rcut) {
+    bool cells = true;
+    for (int k = 0; k < 3; ++k) {
+        b.m[k] = (int)(b.L[k] / rcut);
+        if (b.m[k] < 3) cells = false;
+        // images reaching within rcut of a minimum-image vector (|v| <= L / 2)
+        b.img[k] = (int)((rcut + 0.5 * b.L[k]) / b.L[k]);
+    }
+    b.mode = cells ? 0 : 1;
+    if (!cells) b.m[0] = b.m[1] = b.m[2] = 0;
+    return cells ? b.m[0] * b.m[1] * b.m[2] : 0;
+}
+
+namespace {
+
+__device__ __forceinline__ void batch_cell(const BatchStruct &b, const double *p, int *c) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double x = p[k] - b.L[k] * floor(p[k] / b.L[k]);   // into [0, L)
+        int ck = (int)(x / b.L[k] * b.m[k]);
+        c[k] = ck < 0 ? 0 : (ck >= b.m[k] ? b.m[k] - 1 : ck);
+    }
+}
+
+__global__ void k_bcell_assign(int n, const double *__restrict__ pos,
+                               const BatchStruct *__restrict__ st, const int *__restrict__ atom_struct,
+                               int *__restrict__ cell_id, int *__restrict__ cell_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BatchStruct b = st[atom_struct[i]];
+    if (b.mode != 0) {
+        cell_id[i] = -1;
+        return;
+    }
+    int c[3];
+    batch_cell(b, pos + 3 * (size_t)i, c);
+    const int id = b.coff + (c[0] * b.m[1] + c[1]) * b.m[2] + c[2];
+    cell_id[i] = id;
+    atomicAdd(&cell_count[id], 1);
+}
+
+__global__ void k_bcell_fill(int n, const int *__restrict__ cell_id,
+                             const int *__restrict__ cell_start, int *__restrict__ cell_fill,
+                             int *__restrict__ cell_atoms) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int id = cell_id[i];
+    if (id < 0) return;
+    cell_atoms[cell_start[id] + atomicAdd(&cell_fill[id], 1)] = i;
+}
+
+// ascending atom order inside each cell (a deterministic pair order)
+__global__ void k_bcell_sort(int ncells, const int *__restrict__ cell_start,
+                             const int *__restrict__ cell_count, int *__restrict__ cell_atoms) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int *a = cell_atoms + cell_start[c];
+    const int n = cell_count[c];
+    for (int i = 1; i < n; ++i) {
+        const int v = a[i];
+        int j = i - 1;
+        while (j >= 0 && a[j] > v) {
+            a[j + 1] = a[j];
+            --j;
+        }
+        a[j + 1] = v;
+    }
+}
+
+// One warp per atom. Candidates form one flattened sequence (the 27 cells around
+// the atom's cell, or (image, atom) pairs of the structure); lanes test 32 at a
+// time and emit accepted pairs in sequence order (ballot + prefix popcount).
+// Count mode when pstart is null.
+__global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStruct *__restrict__ st,
+                           const int *__restrict__ atom_struct, const int *__restrict__ cell_id,
+                           const int *__restrict__ cell_start, const int *__restrict__ cell_count,
+                           const int *__restrict__ cell_atoms, double rcut, int *__restrict__ n_neigh,
+                           const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
+                           double *__restrict__ xyz, unsigned *err) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;
+    const BatchStruct b = st[atom_struct[i]];
+    const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    // candidate segments: lane c < 27 describes cell c (mode 0); mode 1 has one
+    // segment per image
+    const int nimg = (2 * b.img[0] + 1) * (2 * b.img[1] + 1) * (2 * b.img[2] + 1);
+    int cstart = 0, ccount = 0;
+    if (b.mode == 0) {
+        if (lane < 27) {
+            const int ci = cell_id[i] - b.coff;
+            const int cx = ci / (b.m[1] * b.m[2]), cy = (ci / b.m[2]) % b.m[1], cz = ci % b.m[2];
+            const int x = (cx + lane / 9 - 1 + b.m[0]) % b.m[0];
+            const int y = (cy + (lane / 3) % 3 - 1 + b.m[1]) % b.m[1];
+            const int z = (cz + lane % 3 - 1 + b.m[2]) % b.m[2];
+            const int c = b.coff + (x * b.m[1] + y) * b.m[2] + z;
+            cstart = cell_start[c];
+            ccount = cell_count[c];
+        }
+    }
+    int incl = ccount;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int total = b.mode == 0 ? __shfl_sync(0xffffffffu, incl, 31) : b.n * nimg;
+    const int64_t base = pstart ? pstart[i] : 0;
+    if (pstart && lane == 0) {   // self pair first
+        if (base < cap) {
+            nbr[base] = i;
+            xyz[3 * base] = 0.0;
+            xyz[3 * base + 1] = 0.0;
+            xyz[3 * base + 2] = 0.0;
+        } else {
+            atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+        }
+    }
+    int count = 1;
+    for (int f0 = 0; f0 < total; f0 += 32) {   // warp-uniform trip count
+        const int f = f0 + lane;
+        const int fc = f < total ? f : total - 1;
+        int k = -1;
+        int t[3] = {0, 0, 0};
+        if (b.mode == 0) {
+            int c = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int probe = c + step - 1;
+                const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
+                if (probe < 27 && v <= fc) c += step;
+            }
+            const int cs = __shfl_sync(0xffffffffu, cstart, c);
+            const int before = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, ccount, c);
+            if (f < total) k = cell_atoms[cs + (fc - before)];
+        } else if (f < total) {
+            const int im = fc / b.n;
+            k = b.off + (fc - im * b.n);
+            const int ny = 2 * b.img[1] + 1, nz = 2 * b.img[2] + 1;
+            t[0] = im / (ny * nz) - b.img[0];
+            t[1] = (im / nz) % ny - b.img[1];
+            t[2] = im % nz - b.img[2];
+        }
+        bool take = false;
+        double dist[3] = {0.0, 0.0, 0.0};
+        if (k >= 0) {
+            double d2 = 0.0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                double v = pos[3 * (size_t)k + q] - pi[q];
+                v -= b.L[q] * rint(v / b.L[q]);   // minimum image
+                v += t[q] * b.L[q];
+                dist[q] = v;
+                d2 += v * v;
+            }
+            const bool self = k == i && t[0] == 0 && t[1] == 0 && t[2] == 0;
+            take = !self && d2 < rcut * rcut;
+        }
+        const unsigned msk = __ballot_sync(0xffffffffu, take);
+        if (pstart && take) {
+            const int64_t p = base + count + __popc(msk & ((1u << lane) - 1u));
+            if (p < cap) {
+                nbr[p] = k;
+                xyz[3 * p] = dist[0];
+                xyz[3 * p + 1] = dist[1];
+                xyz[3 * p + 2] = dist[2];
+            } else {
+                atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+            }
+        }
+        count += __popc(msk);
+    }
+    if (!pstart && lane == 0) n_neigh[i] = count;
+}
+
+}  // namespace
+
+int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st) {
+    const int TB = 128, n = nl.n_atoms;
+    const int gb = (n + TB - 1) / TB;
+    const int gw = (int)(((int64_t)n * 32 + TB - 1) / TB);
+    if (nl.n_cells > 0) {
+        TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * nl.n_cells, st));
+        TGB_CUDA(cudaMemsetAsync(nl.cell_fill, 0, sizeof(int) * nl.n_cells, st));
+    }
+    k_bcell_assign<<<gb, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_count);
+    if (nl.n_cells > 0) {
+        size_t bytes = nl.scan_bytes;
+        TGB_CUDA(cub::DeviceScan::ExclusiveSum(nl.scan_tmp, bytes, nl.cell_count, nl.cell_start,
+                                               nl.n_cells, st));
+        k_bcell_fill<<<gb, TB, 0, st>>>(n, nl.cell_id, nl.cell_start, nl.cell_fill, nl.cell_atoms);
+        k_bcell_sort<<<(nl.n_cells + TB - 1) / TB, TB, 0, st>>>(nl.n_cells, nl.cell_start,
+                                                                 nl.cell_count, nl.cell_atoms);
+    }
+    k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
+                                  nl.cell_count, nl.cell_atoms, rcut, nl.n_neigh, nullptr, nl.cap,
+                                  nullptr, nullptr, nl.err);
+    k_pstart_zero<<<1, 1, 0, st>>>(nl.pstart);
+    size_t bytes = nl.scan_bytes;
+    TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n, st));
+    k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
+                                  nl.cell_count, nl.cell_atoms, rcut, nl.n_neigh, nl.pstart, nl.cap,
+                                  nl.nbr, nl.xyz, nl.err);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 int launch_angles(int64_t P, const double *rjs, const double *xyz, const int *is_self, double *th,
                   double *ph, cudaStream_t st) {
     if (P == 0) return TG_OK;

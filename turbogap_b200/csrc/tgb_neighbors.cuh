@@ -74,6 +74,44 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
              const CellGrid &g, bool use_cells, double rcut, const int *do_list,
              cudaStream_t st);
 
+// ---- many independent orthorhombic structures at once (batched evaluation).
+// Structure s owns atoms [off, off + n) of the concatenated arrays. Boxes of at
+// least 3 rcut on every axis use a cell grid of >= 3 cells per axis (minimum
+// image); smaller boxes enumerate all atoms of the structure over the periodic
+// images within reach (img[k] per axis). Pairs: self first, then the accepted
+// candidates; nbr holds global atom indices (no supercell).
+struct BatchStruct {
+    int off, n;
+    double L[3];
+    int mode;        // 0: cells, 1: images
+    int m[3];        // cells per axis (mode 0)
+    int coff;        // first global cell (mode 0)
+    int img[3];      // image range per axis (mode 1)
+};
+
+// Host-side plan of one structure (cells or images, counts); returns the cells used.
+int batch_plan_struct(BatchStruct &b, double rcut);
+
+struct BatchNL {
+    int n_atoms = 0, n_structs = 0, n_cells = 0;
+    int64_t cap = 0;
+    BatchStruct *st = nullptr;     // device [n_structs]
+    int *atom_struct = nullptr;    // device [n_atoms]
+    int *cell_id = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+    int *cell_atoms = nullptr;
+    int *n_neigh = nullptr;
+    int64_t *pstart = nullptr;
+    int *nbr = nullptr;
+    double *xyz = nullptr;
+    void *scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    unsigned *err = nullptr;
+};
+
+// Count, scan and fill (pairs beyond nl.cap are dropped and flag DEV_ERR_NEIGH_CAPACITY;
+// pstart[n_atoms] is the required capacity).
+int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st);
+
 int launch_angles(int64_t P, const double *rjs, const double *xyz, const int *is_self, double *th,
                   double *ph, cudaStream_t st);
 int launch_supercell(int n, const double *pos, const double *abc_dev, const int *indices,

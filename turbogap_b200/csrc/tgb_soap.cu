@@ -887,6 +887,18 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
     for (int qd = 0; qd < 6; ++qd) vir[qd] = warp_sum(vir[qd]);
     if (lane == 0)
         for (int qd = 0; qd < 6; ++qd) vred[warp][qd] = vir[qd];
+    if (O.vir_struct && lane == 0 && site < S.n_sites) {   // per-structure virial (batches)
+        double *o = O.vir_struct + 9 * (size_t)O.atom_struct[S.site_atom[site]];
+        atomicAdd(o + 0, vir[0]);
+        atomicAdd(o + 4, vir[1]);
+        atomicAdd(o + 8, vir[2]);
+        atomicAdd(o + 1, vir[3]);
+        atomicAdd(o + 3, vir[3]);
+        atomicAdd(o + 2, vir[4]);
+        atomicAdd(o + 6, vir[4]);
+        atomicAdd(o + 5, vir[5]);
+        atomicAdd(o + 7, vir[5]);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         double v[6] = {0, 0, 0, 0, 0, 0};

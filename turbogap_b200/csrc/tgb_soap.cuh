@@ -103,6 +103,9 @@ struct ForceOut {
     double *energies;        // (n_atoms), accumulated
     double *vpart;           // [gridDim][9]
     unsigned *err;
+    // optional (batches): each site's virial is also added to vir_struct[atom_struct[atom]]
+    const int *atom_struct = nullptr;
+    double *vir_struct = nullptr;   // [n_structs][9]
 };
 
 // Host-side construction of the FP64 tables on the device.
