@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from turbogap_b200 import synth  # noqa: E402
-from turbogap_b200.workloads import WORKLOADS, build_blocks  # noqa: E402
+from turbogap_b200.workloads import WORKLOADS, build_blocks, descriptors_gpu  # noqa: E402
 
 # value: the plain (bf16x3, FP64-faithful) form; the line's "mixed" object holds
 # the mixed+MLP form on the same workload with its error against the plain path
@@ -271,6 +271,31 @@ def cpu_baseline_leg(w, st, target_s=15.0):
                       f"MPI rank, all blocks), FP64 oracle port, {cores} OpenMP threads, {t:.1f} s"}
 
 
+def run_reference_batch(a, w, world):
+    cells = batch_cells(w)
+    for _ in range(a.warmup):
+        oracle_batch_sample(w, cells[:1], 0.0)
+    atoms, t, k = 0, 0.0, 0
+    for _ in range(a.steps):
+        na, tt, k = oracle_batch_sample(w, cells, 2.0)
+        atoms += na
+        t += tt
+    value = atoms / t
+    cores = os.cpu_count()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"{w.name}: {w.description}",
+                                        "sample_cells": k},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"each step: E+F of the first {k} cells, FP64 port of the "
+                                   f"reference CPU path; the Fortran reference cannot be built here"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
 def run_reference(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,6 +303,8 @@ def run_reference(a):
         return 0
     import oracle as O
     w = WORKLOADS[a.workload]
+    if w.name in BATCH_WORKLOADS:
+        return run_reference_batch(a, w, world)
     st = w.structure()
     blocks = oracle_blocks(w)
     n, _ = calibrate_sample(O, st, blocks, 2.0)
@@ -304,9 +331,127 @@ def run_reference(a):
     return 0
 
 
+# ------------------------------------------------------------------ batches
+BATCH_WORKLOADS = {"cells512": 512}
+
+
+def batch_cells(w, replica=0):
+    from turbogap_b200.workloads import uneven_cells
+    return uneven_cells(BATCH_WORKLOADS[w.name], w.seed + 7919 * replica)
+
+
+def oracle_batch_sample(w, cells, target_s):
+    """Oracle E+F of the first cells until about target_s of CPU time."""
+    import oracle as O
+    blocks = oracle_blocks(w)
+    t, atoms, k = 0.0, 0, 0
+    while k < len(cells) and t < target_s:
+        st = cells[k]
+        t0 = time.perf_counter()
+        O.evaluate(st.positions, st.species, st.box, blocks)
+        t += time.perf_counter() - t0
+        atoms += st.n
+        k += 1
+    return atoms, t, k
+
+
+def run_batch(a, w, world, rank, local, dist):
+    """Energies and forces of every cell of a batch per step (no MD)."""
+    import torch
+    from turbogap_b200 import backend as B
+    torch.cuda.set_device(local)
+    B.gpu_context_init(rank, local)
+    blocks = build_blocks(w, lambda h, st: descriptors_gpu(B, h, st, key=900))
+    keys = []
+    for i, b in enumerate(blocks):
+        B.soap_backend_begin(b, key=i + 1)
+        keys.append(i + 1)
+    cells = batch_cells(w, rank)
+    bat = B.Batch(cells, keys)
+    n = bat.n
+    ext = torch.cuda.ExternalStream(bat.stream())
+    for _ in range(max(a.warmup, 3)):
+        bat.compute_device()
+    kernels = bat.graph_kernels()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(a.steps):
+            bat.compute_device()
+        e1.record(ext)
+        e1.synchronize()
+    t_max = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
+    value = n * a.steps * world / t_max
+    prof = bat.profile(a.profile_steps)
+    peaks, peak_kind = measured_peaks()
+    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+    h = blocks[0].hypers
+    flops = 2 * h.dim * blocks[0].n_sparse * n
+    achieved = flops / (prof["gemm1"] / 1e3) / 1e12
+    # e2e: host positions in, host energies / forces / virials out, every step
+    pos = np.ascontiguousarray(np.concatenate([c.positions for c in cells]))
+    pos_h = torch.from_numpy(pos).pin_memory()
+    en_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    f_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    v_h = torch.empty((len(cells), 9), dtype=torch.float64, pin_memory=True)
+    lib = B.lib()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(ext)
+    for _ in range(a.e2e_steps):
+        B.check(lib.tg_batch_set_positions(bat.handle, pos_h.numpy()))
+        B.check(lib.tg_batch_compute(bat.handle, C.c_void_p(en_h.data_ptr()),
+                                     C.c_void_p(f_h.data_ptr()), C.c_void_p(v_h.data_ptr())))
+    e3.record(ext)
+    e3.synchronize()
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1e3, dist)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        atoms, t, k = oracle_batch_sample(w, cells, 15.0)
+        cpu = {"value": atoms / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"E+F of the first {k} cells ({atoms} atoms), FP64 oracle port, "
+                         f"{os.cpu_count()} OpenMP threads, {t:.1f} s"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+        "config": {"workload": f"{w.name}: {w.description}", "cells": len(cells),
+                   "atoms_per_gpu": n, "pairs": bat.n_pairs(),
+                   "step": "energies, forces and virials of every cell (batched, one CUDA graph)",
+                   "l2": "inputs larger than L2",
+                   "parallelism": f"{world} independent replica(s), one per GPU"},
+        "roofline": {"kernel": "k_gemm_tn<GAP>: tcgen05 GEMM 1 (all cells' sites)", "bound": "tensor",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"{peak_kind} bf16 dense (sustained), of measured",
+                     "ms_per_step_by_pass": prof},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n * a.e2e_steps * world / t_e2e, "unit": UNIT,
+                "h2d_bytes_per_step": int(pos.nbytes),
+                "d2h_bytes_per_step": int((en_h.numel() + f_h.numel() + v_h.numel()) * 8),
+                "api": "tg_batch_set_positions + tg_batch_compute (host buffers)"},
+        "gpu_launches": kernels * a.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bat.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ GPU
 def run_ours(a):
     world, rank, local, dist = dist_setup(a.gpus)
+    if a.workload in BATCH_WORKLOADS:
+        return run_batch(a, WORKLOADS[a.workload], world, rank, local, dist)
     import torch
     from turbogap_b200 import backend as B
     from turbogap_b200.workloads import descriptors_gpu

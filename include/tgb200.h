@@ -227,6 +227,11 @@ int tg_batch_compute(tg_batch *b, double *energies, double *forces, double *viri
 /* Evaluation on the device only (graph replay after the first call). */
 int tg_batch_compute_device(tg_batch *b);
 int tg_batch_stream(tg_batch *b, void **stream);
+/* n_evals eager evaluations with CUDA events between passes; ms_per_pass[7] as
+ * for tg_engine_profile (the integrate and MLP entries stay 0). */
+int tg_batch_profile(tg_batch *b, int32_t n_evals, double *ms_per_pass, int32_t *n_passes);
+/* Kernel launches in one evaluation's CUDA graph. */
+int tg_batch_graph_kernels(tg_batch *b, int32_t *n_kernels);
 int tg_batch_n_pairs(tg_batch *b, int64_t *n_pairs);
 
 /* ---- learned surrogate (mixed form). No reference counterpart: TurboGAP has

@@ -454,3 +454,15 @@ class Batch:
         n = C.c_int64(0)
         check(lib().tg_batch_n_pairs(self._h, C.byref(n)))
         return int(n.value)
+
+    def graph_kernels(self) -> int:
+        n = C.c_int32(0)
+        check(lib().tg_batch_graph_kernels(self._h, C.byref(n)))
+        return int(n.value)
+
+    def profile(self, n_evals: int) -> dict:
+        """Mean ms per evaluation of each pass (eager, CUDA events)."""
+        ms = np.zeros(8)
+        npass = C.c_int32(0)
+        check(lib().tg_batch_profile(self._h, int(n_evals), ms, C.byref(npass)))
+        return {k: float(ms[i]) for i, k in enumerate(Engine.PASSES)}

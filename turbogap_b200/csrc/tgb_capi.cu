@@ -1655,15 +1655,19 @@ struct BatchEngine {
         if (st) cudaStreamDestroy(st);
     }
 
-    int compute_ef() {
+    EventLog prof;
+
+    int compute_ef(EventLog *log = nullptr) {
+        TGB_MARK(log, -1, st);
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        TGB_MARK(log, PASS_NEIGH, st);
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         TGB_CUDA(cudaMemsetAsync(vir_s.p, 0, sizeof(double) * 9 * ns, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
-            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, nullptr,
+            TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log,
                                    atom_struct.p, vir_s.p));
         }
         return TG_OK;
@@ -1875,6 +1879,44 @@ int tg_batch_compute(tg_batch *bh, double *energies, double *forces, double *vir
 int tg_batch_stream(tg_batch *bh, void **stream) {
     TGB_CHECK(bh && stream, TG_ERR_ARG, "null argument");
     *stream = (void *)bh->e.st;
+    return TG_OK;
+}
+
+int tg_batch_profile(tg_batch *bh, int32_t n_evals, double *ms_per_pass, int32_t *n_passes) {
+    TGB_CHECK(bh && ms_per_pass && n_evals >= 1, TG_ERR_ARG, "bad profile arguments");
+    BatchEngine &E = bh->e;
+    double acc[N_PASS] = {0};
+    for (int s = 0; s < n_evals; ++s) {
+        TGB_TRY(E.compute_ef(&E.prof));
+        TGB_CUDA(cudaStreamSynchronize(E.st));
+        TGB_TRY(E.prof.collect(acc));
+    }
+    for (int p = 0; p < N_PASS; ++p) ms_per_pass[p] = acc[p] / n_evals;
+    if (n_passes) *n_passes = N_PASS;
+    return E.errors();
+}
+
+int tg_batch_graph_kernels(tg_batch *bh, int32_t *n_kernels) {
+    TGB_CHECK(bh && n_kernels, TG_ERR_ARG, "null argument");
+    BatchEngine &E = bh->e;
+    cudaGraph_t g;
+    TGB_CUDA(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+    int r = E.compute_ef();
+    cudaError_t ce = cudaStreamEndCapture(E.st, &g);
+    TGB_TRY(r);
+    TGB_CUDA(ce);
+    size_t n = 0;
+    ce = cudaGraphGetNodes(g, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (ce == cudaSuccess && n) ce = cudaGraphGetNodes(g, nodes.data(), &n);
+    int k = 0;
+    for (size_t i = 0; ce == cudaSuccess && i < n; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    cudaGraphDestroy(g);
+    TGB_CUDA(ce);
+    *n_kernels = k;
     return TG_OK;
 }
 

@@ -9,6 +9,8 @@ atoms of further seeded structures of the same kind, computed by this backend
   ch32k      2 blocks (C and H), D = 1224, M = 4000 each, dt 1.0 fs, 300 K
   carbon131k 1 block  (C),      D = 324,  M = 1000, dt 1.0 fs, 300 K
   ch1m       2 blocks (C and H), D = 1224, M = 4000 each, dt 0.5 fs, 300 K
+  cells512   512 independent C cells (64-2048 atoms, 1.5-3.5 g/cm3), 1 block D = 324,
+             M = 2000; one step = energies and forces of every cell (batched)
 """
 from __future__ import annotations
 
@@ -74,10 +76,32 @@ WORKLOADS = {
 }
 
 
+def uneven_cells(n_cells: int, seed: int):
+    """Independent C cells: atoms log-uniform in 64..2048, density uniform in
+    1.5..3.5 g/cm3, minimum distance 1.2 A (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_cells):
+        n = int(round(np.exp(rng.uniform(np.log(64), np.log(2048)))))
+        rho = rng.uniform(1.5, 3.5)
+        L = (n / synth.carbon_number_density(rho)) ** (1 / 3)
+        out.append(synth.random_structure(n, L, 1.2, seed=seed * 1000 + k))
+    return out
+
+
+WORKLOADS["cells512"] = Workload(
+    "cells512", 2, [carbon_hypers()], [2000], 1.0, 300.0,
+    "512 independent C cells, atoms log-uniform 64-2048, 1.5-3.5 g/cm3, D=324, M=2000; "
+    "energies and forces of all cells per step (batched)",
+    source=lambda s: _c(216, s))
+
+
 def _source_structures(w: Workload):
     """Further seeded structures of the workload's kind, for the sparse sets."""
     if w.name in ("carbon216",):
         return [w.source(w.seed * 100 + i) for i in range(5)]
+    if w.name == "cells512":
+        return [_c(1000, w.seed * 100 + i, rho=2.0 + 0.5 * i) for i in range(3)]
     if w.name == "carbon131k":
         return [_c(4096, w.seed * 100 + i) for i in range(1)]
     return [_ch(32768, w.seed * 100 + 0)]
