@@ -181,7 +181,9 @@ def mixed_leg(B, eng, blocks, w, a, ext, dist, plain_ms):
     import torch
     t0 = time.time()
     mlps = [B.Mlp(b.hypers.dim, 256, 4, seed=100 + i) for i, b in enumerate(blocks)]
-    for _ in range(a.mlp_data_steps):
+    # at most about 400k samples per block (large systems take fewer snapshots)
+    data_steps = min(a.mlp_data_steps, max(1, -(-400000 // max(eng.n, 1))))
+    for _ in range(data_steps):
         eng.md(2, w.dt, energies=False)
         for i, m in enumerate(mlps):
             m.add_engine_samples(eng, i)
@@ -231,7 +233,8 @@ def mixed_leg(B, eng, blocks, w, a, ext, dist, plain_ms):
                            "rmse_f_mev_per_A": 1e3 * err_after[1], "gated_sites": err_after[2]},
         "reference": "exact bf16x3 GPU path at the same configurations",
         "mlp": "4 members x (D -> 256 -> 256 -> 1, SiLU) per block, bf16 GEMMs, fp32 accumulation",
-        "training": {"samples": [m.n_samples() for m in mlps], "epochs": a.mlp_epochs,
+        "training": {"samples": [m.n_samples() for m in mlps], "snapshots": data_steps,
+                     "epochs": a.mlp_epochs,
                      "batch": 512, "data_seconds": t_data, "train_seconds": t_train,
                      "final_loss": [float(l_[-1]) for l_ in losses]},
         "ms_per_step_by_pass": prof,

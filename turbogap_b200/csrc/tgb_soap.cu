@@ -635,7 +635,10 @@ struct ForceShape {
                                                    // transposed writes spread over the banks
     static constexpr int BSTRIDE = NT * BROW + 4;  // per-l stride (multiple of 4, 4 mod 32)
     static constexpr int BAREA = (NL * BSTRIDE + 3) / 4 * 4;   // keeps gam 16-byte aligned
-    static constexpr int WARP_FLOATS = BAREA + NLM * NT;
+    // Gamma rows [lm][n] with stride GS = NT + 4: a lane's four consecutive n go in
+    // one float4 store, and 8 lanes' stores hit 8 distinct 16-byte bank groups
+    static constexpr int GS = NT + 4;
+    static constexpr int WARP_FLOATS = BAREA + NLM * GS;
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
 };
 
@@ -759,16 +762,22 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             for (int n2 = 0; n2 < NT; ++n2) cr[n2] = cg[n2 * NLM + lmk[k]];
             const float *Bl = Bm + lk[k] * Sh::BSTRIDE;
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                const float4 *Bn = reinterpret_cast<const float4 *>(Bl + n * Sh::BROW);
-                float v = 0.f;
+            for (int n0 = 0; n0 < NT; n0 += 4) {
+                float v4[4];
 #pragma unroll
-                for (int j = 0; j < NT / 4; ++j) {
-                    const float4 b = Bn[j];
-                    v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
-                         b.w * cr[4 * j + 3];
+                for (int e = 0; e < 4; ++e) {
+                    const float4 *Bn = reinterpret_cast<const float4 *>(Bl + (n0 + e) * Sh::BROW);
+                    float v = 0.f;
+#pragma unroll
+                    for (int j = 0; j < NT / 4; ++j) {
+                        const float4 b = Bn[j];
+                        v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
+                             b.w * cr[4 * j + 3];
+                    }
+                    v4[e] = v;
                 }
-                gam[lmk[k] * NT + n] = v;
+                *reinterpret_cast<float4 *>(gam + lmk[k] * Sh::GS + n0) =
+                    make_float4(v4[0], v4[1], v4[2], v4[3]);
             }
         }
         __syncwarp();
@@ -815,7 +824,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
                     // G = sum_n Gamma R_n, G' = sum_n Gamma R_n' for +m (C) and -m (S)
                     const int lmp = l * l + l + m;
                     float Gp = 0.f, dGp = 0.f;
-                    const float4 *gp = reinterpret_cast<const float4 *>(gam + lmp * NT + ch);
+                    const float4 *gp = reinterpret_cast<const float4 *>(gam + lmp * Sh::GS + ch);
 #pragma unroll
                     for (int qd = 0; qd < AMAX / 4; ++qd) {
                         const float4 v = gp[qd];
@@ -832,7 +841,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
                     } else {
                         const int lmn = l * l + l - m;
                         float Gn = 0.f, dGn = 0.f;
-                        const float4 *gn = reinterpret_cast<const float4 *>(gam + lmn * NT + ch);
+                        const float4 *gn = reinterpret_cast<const float4 *>(gam + lmn * Sh::GS + ch);
 #pragma unroll
                         for (int qd = 0; qd < AMAX / 4; ++qd) {
                             const float4 v = gn[qd];
