@@ -167,8 +167,8 @@ def gemm_flops_per_step(blocks, structure, sites_only=False):
 # DRAM bytes per central site of one GEMM launch, from the ncu capture of the
 # 12288-site C block of ch16k (dram__bytes_read.sum + dram__bytes_write.sum
 # divided by its sites); traffic grows with the sites at fixed D and M.
-GEMM1_DRAM_BYTES_PER_SITE = (155.823104e6 + 257.426432e6) / 12288
-GEMM2_DRAM_BYTES_PER_SITE = (416.886016e6 + 43.268864e6) / 12288
+GEMM1_DRAM_BYTES_PER_SITE = (222.311424e6 + 264.274176e6) / 12288
+GEMM2_DRAM_BYTES_PER_SITE = (417.493760e6 + 42.420736e6) / 12288
 
 
 # ------------------------------------------------------------------ mixed form
