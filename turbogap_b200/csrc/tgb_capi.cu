@@ -63,6 +63,7 @@ struct Block {
     int zeta_int = 0;
     signed char zmap[kMaxZ];
     DBuf<float> table, selfR;
+    DBuf<float2> table_fd;   // the descriptor's (f, f') copy, function-major
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
     DBuf<float> g0f;       // g0 in fp32: subtracted from the MLP's dE/dq rows
@@ -80,6 +81,7 @@ struct Block {
             P.tab_inv_h[s] = (float)(kTableIntervals / hh.rcut_hard[s]);
         }
         P.table = table.p;
+        P.table_fd = table_fd.p;
         P.self_R = selfR.p;
         P.mu = mu.p;
         P.g0 = g0.p;
@@ -667,7 +669,8 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
                                                                    b->QsA.p, b->QsT.p);
     k_prep_alpha<<<(b->Mpad + 255) / 256, 256, 0, C.st>>>(ta.p, b->M, b->Mpad, b->alpha.p);
     TGB_CUDA(cudaGetLastError());
-    TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st));
+    TGB_TRY(b->table_fd.ensure((size_t)hh.ns * (b->amax + b->lmax + 1) * (kTableIntervals + 1)));
+    TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st, b->table_fd.p));
     TGB_TRY(make_tma_bf16(&b->tmB1, b->QsA.p, b->Mpad, b->K1, b->K1, kGemmBN));
     TGB_TRY(make_tma_bf16(&b->tmB2, b->QsT.p, b->dim, b->K2, b->K2, kGemmBN));
     TGB_CUDA(cudaStreamSynchronize(C.st));
@@ -1637,7 +1640,7 @@ namespace tgb {
 struct BatchEngine {
     int n = 0, ns = 0, nz = 1;
     double rcut = 0.0;
-    DBuf<double> pos, f, en, vir, vir_s, e0, xyz;
+    DBuf<double> pos, f, en, vir, vir_s, e0, xyz, cell_pos;
     DBuf<int> species, atom_struct, cell_id, cell_count, cell_start, cell_fill, cell_atoms, n_neigh,
         nbr;
     DBuf<int64_t> pstart;
@@ -1736,7 +1739,7 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
     E.ns = n_structs;
     std::vector<BatchStruct> sh(n_structs);
     std::vector<int> as;
-    int off = 0, ncells = 0;
+    int off = 0, ncells = 0, ncell_atoms = 0;
     for (int s = 0; s < n_structs; ++s) {
         const double *bx = boxes + 9 * (size_t)s;
         TGB_CHECK(n_atoms[s] >= 1, TG_ERR_ARG, "structure %d has no atoms", s);
@@ -1748,6 +1751,7 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
         for (int k = 0; k < 3; ++k) q.L[k] = b.L[k];
         q.coff = ncells;
         ncells += batch_plan_struct(q, rcut);
+        if (q.mode == 0) ncell_atoms += q.n;
         for (int i = 0; i < q.n; ++i) as.push_back(s);
         off += q.n;
     }
@@ -1764,6 +1768,7 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
     const int nc = std::max(ncells, 1);
     TGB_TRY(E.cell_count.ensure(nc)); TGB_TRY(E.cell_start.ensure(nc));
     TGB_TRY(E.cell_fill.ensure(nc)); TGB_TRY(E.cell_atoms.ensure(n));
+    TGB_TRY(E.cell_pos.ensure(3 * (size_t)n));
     size_t need1 = 0, need2 = 0;
     cub::DeviceScan::InclusiveSum(nullptr, need1, E.n_neigh.p, E.pstart.p + 1, n);
     cub::DeviceScan::ExclusiveSum(nullptr, need2, E.cell_count.p, E.cell_start.p, nc);
@@ -1791,6 +1796,8 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
     nl.cell_start = E.cell_start.p;
     nl.cell_fill = E.cell_fill.p;
     nl.cell_atoms = E.cell_atoms.p;
+    nl.cell_pos = E.cell_pos.p;
+    nl.n_cell_atoms = ncell_atoms;
     nl.n_neigh = E.n_neigh.p;
     nl.pstart = E.pstart.p;
     nl.scan_tmp = E.scan_tmp.p;

@@ -178,7 +178,8 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
                                 double rcut, const int *__restrict__ do_list,
                                 const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
                                 const int *__restrict__ cell_count,
-                                const int *__restrict__ cell_atoms, int *__restrict__ n_neigh,
+                                const int *__restrict__ cell_atoms,
+                                const double *__restrict__ cell_pos, int *__restrict__ n_neigh,
                                 const int64_t *__restrict__ pstart, int64_t cap,
                                 int *__restrict__ nbr, double *__restrict__ rjs,
                                 double *__restrict__ xyz, unsigned *err) {
@@ -214,6 +215,7 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
     }
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    const double rc2 = rcut * rcut, rc2_lo = rc2 * (1.0 - 1e-12), rc2_hi = rc2 * (1.0 + 1e-12);
     const int64_t base = pstart ? pstart[i] : 0;
     if (pstart && lane == 0) {   // self pair first
         if (base < cap) {
@@ -245,10 +247,29 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
         int k = -1;
         double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
         if (f < total) {
-            k = cell_atoms[cs + (fc - before)];
-            if (k != i) {
-                get_distance(pi, pos + 3 * (size_t)k, bx, dist, &d);
-                take = d < rcut;
+            const int slot = cs + (fc - before);
+            k = cell_atoms[slot];
+            if (k != i) {   // the same values from the cell-ordered copy when there is one
+                const double *pk = cell_pos ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
+                // minimum image as get_distance does it (orthorhombic: the cell path);
+                // the squared distance settles every candidate away from the cutoff,
+                // the correctly rounded sqrt decides the rest as the reference does
+                double d2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const double L = bx.L[q];
+                    double v = f_modulo(pk[q] - pi[q], L);
+                    if (v > L / 2.0) v = v - L;
+                    dist[q] = v;
+                    d2 = d2 + v * v;
+                }
+                if (d2 < rc2_lo) {
+                    take = true;
+                    if (pstart) d = sqrt(d2);
+                } else if (d2 <= rc2_hi) {
+                    d = sqrt(d2);
+                    take = d < rcut;
+                }
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, take);
@@ -294,6 +315,17 @@ __global__ void k_nl_brute(int n_sites, int n_sc, const double *__restrict__ pos
 }
 
 __global__ void k_pstart_zero(int64_t *pstart) { pstart[0] = 0; }
+
+// positions in cell order, so that a cell's candidates are read contiguously
+__global__ void k_cell_gather_pos(int n, const int *__restrict__ cell_atoms,
+                                  const double *__restrict__ pos, double *__restrict__ cell_pos) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int k = cell_atoms[s];
+    cell_pos[3 * (size_t)s] = pos[3 * (size_t)k];
+    cell_pos[3 * (size_t)s + 1] = pos[3 * (size_t)k + 1];
+    cell_pos[3 * (size_t)s + 2] = pos[3 * (size_t)k + 2];
+}
 
 __global__ void k_angles(int64_t P, const double *__restrict__ rjs, const double *__restrict__ xyz,
                          const int *__restrict__ is_self, double *__restrict__ th,
@@ -490,7 +522,9 @@ int NeighborList::reserve(int ns, int nsc, int64_t pair_cap, const CellGrid &g) 
     }
     if (nsc > n_alloc_sc) {
         dev_free(cell_atoms);
+        dev_free(cell_pos);
         TGB_TRY(dev_alloc(&cell_atoms, nsc));
+        TGB_TRY(dev_alloc(&cell_pos, 3 * (size_t)nsc));
         n_alloc_sc = nsc;
     }
     const int64_t ncells = (int64_t)g.mx * g.my * g.mz;
@@ -522,7 +556,7 @@ int NeighborList::reserve(int ns, int nsc, int64_t pair_cap, const CellGrid &g) 
 void NeighborList::release() {
     dev_free(n_neigh); dev_free(pstart); dev_free(cell_xyz); dev_free(cell_atoms);
     dev_free(cell_count); dev_free(cell_start); dev_free(cell_fill); dev_free(nbr);
-    dev_free(rjs); dev_free(xyz); dev_free(scan_tmp); dev_free(err);
+    dev_free(rjs); dev_free(xyz); dev_free(scan_tmp); dev_free(err); dev_free(cell_pos);
     *this = NeighborList{};
 }
 
@@ -558,8 +592,9 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
                                        nl.cell_atoms);
         k_cell_sort<<<(ncells + TB - 1) / TB, TB, 0, st>>>(ncells, nl.cell_start, nl.cell_count,
                                                            nl.cell_atoms);
+        if (nl.cell_pos) k_cell_gather_pos<<<gb, TB, 0, st>>>(n_sites, nl.cell_atoms, pos, nl.cell_pos);
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                           nl.cell_start, nl.cell_count, nl.cell_atoms,
+                                           nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
                                            nl.n_neigh, nullptr, nl.cap, nullptr, nullptr, nullptr,
                                            nl.err);
     } else {
@@ -572,7 +607,7 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
                                            st));
     if (use_cells) {
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                           nl.cell_start, nl.cell_count, nl.cell_atoms,
+                                           nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
                                            nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
                                            nl.err);
     } else {
@@ -660,7 +695,8 @@ __global__ void k_bcell_sort(int ncells, const int *__restrict__ cell_start,
 __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStruct *__restrict__ st,
                            const int *__restrict__ atom_struct, const int *__restrict__ cell_id,
                            const int *__restrict__ cell_start, const int *__restrict__ cell_count,
-                           const int *__restrict__ cell_atoms, double rcut, int *__restrict__ n_neigh,
+                           const int *__restrict__ cell_atoms, const double *__restrict__ cell_pos,
+                           double rcut, int *__restrict__ n_neigh,
                            const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
                            double *__restrict__ xyz, unsigned *err) {
     const int lane = threadIdx.x & 31;
@@ -706,7 +742,7 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
     for (int f0 = 0; f0 < total; f0 += 32) {   // warp-uniform trip count
         const int f = f0 + lane;
         const int fc = f < total ? f : total - 1;
-        int k = -1;
+        int k = -1, slot = -1;
         int t[3] = {0, 0, 0};
         if (b.mode == 0) {
             int c = 0;
@@ -718,7 +754,10 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
             }
             const int cs = __shfl_sync(0xffffffffu, cstart, c);
             const int before = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, ccount, c);
-            if (f < total) k = cell_atoms[cs + (fc - before)];
+            if (f < total) {
+                slot = cs + (fc - before);
+                k = cell_atoms[slot];
+            }
         } else if (f < total) {
             const int im = fc / b.n;
             k = b.off + (fc - im * b.n);
@@ -730,10 +769,11 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
         bool take = false;
         double dist[3] = {0.0, 0.0, 0.0};
         if (k >= 0) {
+            const double *pk = slot >= 0 ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
             double d2 = 0.0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                double v = pos[3 * (size_t)k + q] - pi[q];
+                double v = pk[q] - pi[q];
                 v -= b.L[q] * rint(v / b.L[q]);   // minimum image
                 v += t[q] * b.L[q];
                 dist[q] = v;
@@ -777,16 +817,17 @@ int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st)
         k_bcell_fill<<<gb, TB, 0, st>>>(n, nl.cell_id, nl.cell_start, nl.cell_fill, nl.cell_atoms);
         k_bcell_sort<<<(nl.n_cells + TB - 1) / TB, TB, 0, st>>>(nl.n_cells, nl.cell_start,
                                                                  nl.cell_count, nl.cell_atoms);
+        k_cell_gather_pos<<<gb, TB, 0, st>>>(nl.n_cell_atoms, nl.cell_atoms, pos, nl.cell_pos);
     }
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
-                                  nl.cell_count, nl.cell_atoms, rcut, nl.n_neigh, nullptr, nl.cap,
-                                  nullptr, nullptr, nl.err);
+                                  nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
+                                  nullptr, nl.cap, nullptr, nullptr, nl.err);
     k_pstart_zero<<<1, 1, 0, st>>>(nl.pstart);
     size_t bytes = nl.scan_bytes;
     TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n, st));
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
-                                  nl.cell_count, nl.cell_atoms, rcut, nl.n_neigh, nl.pstart, nl.cap,
-                                  nl.nbr, nl.xyz, nl.err);
+                                  nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
+                                  nl.pstart, nl.cap, nl.nbr, nl.xyz, nl.err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -54,6 +54,7 @@ struct NeighborList {
     int *nbr = nullptr;
     double *rjs = nullptr;
     double *xyz = nullptr;
+    double *cell_pos = nullptr;   // optional: positions in cell order (coalesced candidate reads)
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
     unsigned *err = nullptr;
@@ -94,11 +95,13 @@ int batch_plan_struct(BatchStruct &b, double rcut);
 
 struct BatchNL {
     int n_atoms = 0, n_structs = 0, n_cells = 0;
+    int n_cell_atoms = 0;          // atoms of the structures that use cells
     int64_t cap = 0;
     BatchStruct *st = nullptr;     // device [n_structs]
     int *atom_struct = nullptr;    // device [n_atoms]
     int *cell_id = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
     int *cell_atoms = nullptr;
+    double *cell_pos = nullptr;    // [n_atoms * 3] positions in cell order
     int *n_neigh = nullptr;
     int64_t *pstart = nullptr;
     int *nbr = nullptr;

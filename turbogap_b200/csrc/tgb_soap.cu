@@ -234,7 +234,17 @@ int descriptor_ref_index(int d_internal, int nt, int nl) {
     return pi_ref * nl + l;
 }
 
-int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st) {
+// (f, f') of every function and node (node-major, like the float4 table): the
+// descriptor's gathers touch half the bytes
+__global__ void k_table_fd(int nf, const float4 *__restrict__ T, float2 *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf * (kTableIntervals + 1)) return;
+    const float4 v = T[i];
+    out[i] = make_float2(v.x, v.y);
+}
+
+int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st,
+                      float2 *table_fd) {
     const int amax = h.alpha_max[0];
     const int tw = table_width(amax, h.lmax);
     std::vector<double> W(amax * amax);
@@ -250,6 +260,12 @@ int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cuda
         k_build_table<<<(kTableIntervals + 1 + 127) / 128, 128, 0, st>>>(
             th, dW, reinterpret_cast<float4 *>(table + (size_t)s * (kTableIntervals + 1) * tw));
         k_build_self<<<1, 32, 0, st>>>(th, dW, self_R + s * amax);
+        if (table_fd) {
+            const int nf = amax + h.lmax + 1, nodes = kTableIntervals + 1;
+            k_table_fd<<<(nf * nodes + 255) / 256, 256, 0, st>>>(
+                nf, reinterpret_cast<const float4 *>(table + (size_t)s * nodes * tw),
+                table_fd + (size_t)s * nf * nodes);
+        }
     }
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaStreamSynchronize(st);
@@ -278,6 +294,11 @@ struct Hermite {
         h10 = (t3 - 2.f * t2 + t) * h;
         h01 = -2.f * t3 + 3.f * t2;
         h11 = (t3 - t2) * h;
+    }
+    // value from the (f, f') table of function j
+    __device__ __forceinline__ float value_fd(const float2 *T, int nf, int j) const {
+        const float2 a = __ldg(T + (size_t)k * nf + j), b = __ldg(T + (size_t)(k + 1) * nf + j);
+        return h00 * a.x + h10 * a.y + h01 * b.x + h11 * b.y;
     }
     // value from (f, f') and, when wanted, first derivative from (f', f'') of function j
     __device__ __forceinline__ float value(const float4 *T, int nf, int j) const {
@@ -420,18 +441,18 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                         z = (float)S.xyz[3 * p + 2];
             const float r = sqrtf(x * x + y * y + z * z);
             if (s >= 0 && r < P.rcut[s] && r > 0.f) {
-                const float4 *T = reinterpret_cast<const float4 *>(
-                    P.table + (size_t)s * (kTableIntervals + 1) * (4 * NF));
+                const float2 *Tf = P.table_fd + (size_t)s * NF * (kTableIntervals + 1);
                 const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
                 float rv[AMAX];
 #pragma unroll
-                for (int n = 0; n < AMAX; ++n) rv[n] = hm.value(T, NF, n);
+                for (int n = 0; n < AMAX; ++n) rv[n] = hm.value_fd(Tf, NF, n);
                 float4 *r4 = reinterpret_cast<float4 *>(Rs + t * AMAX);
 #pragma unroll
                 for (int q = 0; q < AMAX / 4; ++q)
                     r4[q] = make_float4(rv[4 * q], rv[4 * q + 1], rv[4 * q + 2], rv[4 * q + 3]);
 #pragma unroll
-                for (int l = 0; l < NL; ++l) As[t * NL + l] = hm.value(T, NF, AMAX + l);
+                for (int l = 0; l < NL; ++l)
+                    As[t * NL + l] = hm.value_fd(Tf, NF, AMAX + l);
                 const float ir = 1.f / r;
                 real_ylm<LMAX>(x * ir, y * ir, z * ir, Ys + t * NLM);
             } else {
