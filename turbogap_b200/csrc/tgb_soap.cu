@@ -659,7 +659,10 @@ struct ForceShape {
     // Gamma rows [lm][n] with stride GS = NT + 4: a lane's four consecutive n go in
     // one float4 store, and 8 lanes' stores hit 8 distinct 16-byte bank groups
     static constexpr int GS = NT + 4;
-    static constexpr int WARP_FLOATS = BAREA + NLM * GS;
+    // Gamma is computed into registers and then written over the B area, which is
+    // dead by then: the warp's area is the larger of the two
+    static constexpr int GAREA = NLM * GS;
+    static constexpr int WARP_FLOATS = BAREA > GAREA ? BAREA : GAREA;
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
 };
 
@@ -667,7 +670,7 @@ struct ForceShape {
 // dE/dc (shared memory), then one lane per pair contracts Gamma with d(c)/d(r_j)
 // on the fly: F_j -= dE_i/dr_j, F_i += dE_i/dr_j, virial += 1/2 (f x + x f).
 template <int NS, int AMAX, int LMAX>
-__global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
+__global__ void __launch_bounds__(128, 4) k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
     using Sh = ForceShape<NS, AMAX, LMAX>;
     constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, NF = Sh::NF, DIM = Sh::DIM;
     extern __shared__ __align__(16) float smem[];
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
     if (lane < 6) vred[warp][lane] = 0.0;
     __syncthreads();
     float *Bm = smem + warp * Sh::WARP_FLOATS;   // [l][n][n2] (stride BSTRIDE per l)
-    float *gam = Bm + Sh::BAREA;                 // [lm][n]
+    float *gam = Bm;                             // [lm][n], over B once Gamma is computed
     const int site = blockIdx.x * Sh::WARPS + warp;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     if (site < S.n_sites) {
@@ -775,6 +778,7 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             lk[k] = l;
         }
         const float *cg = I.c + (size_t)site * NT * NLM;
+        float gv[Sh::SLOTS][NT];
 #pragma unroll
         for (int k = 0; k < Sh::SLOTS; ++k) {
             if (lmk[k] >= NLM) continue;
@@ -783,23 +787,26 @@ __global__ void __launch_bounds__(128) k_soap_force(SoapParams P, SiteArgs S, Fo
             for (int n2 = 0; n2 < NT; ++n2) cr[n2] = cg[n2 * NLM + lmk[k]];
             const float *Bl = Bm + lk[k] * Sh::BSTRIDE;
 #pragma unroll
-            for (int n0 = 0; n0 < NT; n0 += 4) {
-                float v4[4];
+            for (int n = 0; n < NT; ++n) {
+                const float4 *Bn = reinterpret_cast<const float4 *>(Bl + n * Sh::BROW);
+                float v = 0.f;
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const float4 *Bn = reinterpret_cast<const float4 *>(Bl + (n0 + e) * Sh::BROW);
-                    float v = 0.f;
-#pragma unroll
-                    for (int j = 0; j < NT / 4; ++j) {
-                        const float4 b = Bn[j];
-                        v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
-                             b.w * cr[4 * j + 3];
-                    }
-                    v4[e] = v;
+                for (int j = 0; j < NT / 4; ++j) {
+                    const float4 b = Bn[j];
+                    v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
+                         b.w * cr[4 * j + 3];
                 }
-                *reinterpret_cast<float4 *>(gam + lmk[k] * Sh::GS + n0) =
-                    make_float4(v4[0], v4[1], v4[2], v4[3]);
+                gv[k][n] = v;
             }
+        }
+        __syncwarp();   // every lane is done with B: Gamma goes over it
+#pragma unroll
+        for (int k = 0; k < Sh::SLOTS; ++k) {
+            if (lmk[k] >= NLM) continue;
+#pragma unroll
+            for (int n0 = 0; n0 < NT; n0 += 4)
+                *reinterpret_cast<float4 *>(gam + lmk[k] * Sh::GS + n0) =
+                    make_float4(gv[k][n0], gv[k][n0 + 1], gv[k][n0 + 2], gv[k][n0 + 3]);
         }
         __syncwarp();
         // pairs: lane per pair (the self pair, first in the list, is the -sum)
