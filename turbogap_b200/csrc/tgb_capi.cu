@@ -59,6 +59,7 @@ struct Block {
     SoapHostHypers hh{};
     int ns = 0, amax = 0, lmax = 0, ntot = 0, nlm = 0, dim = 0;
     int M = 0, Mpad = 0, K1 = 0, K2 = 0, nsplit = 3, n_etiles = 0, tw = 0;
+    int KD = 0;   // stored kd row: [hi | lo] (bf16x3) or [hi]; GEMM 2 reads hi twice
     double delta = 1.0, zeta = 1.0, rcut_max = 0.0;
     int zeta_int = 0;
     signed char zmap[kMaxZ];
@@ -101,12 +102,12 @@ struct Workspace {
 
     int ensure(const Block &b, int n_sites) {
         const int n = n_sites > 0 ? n_sites : 1;
-        if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.K2 ||
+        if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.KD ||
             qsplit.n < (size_t)n * b.K1 || c.n < (size_t)n * b.ntot * b.nlm ||
             epart.n < (size_t)n * b.n_etiles || kdsum.n < (size_t)n * b.n_etiles) {
             const int nc = n > cap ? n : cap;
             TGB_TRY(qsplit.ensure((size_t)nc * b.K1));
-            TGB_TRY(kd.ensure((size_t)nc * b.K2));
+            TGB_TRY(kd.ensure((size_t)nc * b.KD));
             TGB_TRY(q.ensure((size_t)nc * b.dim));
             TGB_TRY(g.ensure((size_t)nc * b.dim));
             TGB_TRY(c.ensure((size_t)nc * b.ntot * b.nlm));
@@ -119,8 +120,8 @@ struct Workspace {
         }
         if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p) {
             TGB_TRY(make_tma_bf16(&tmA1, qsplit.p, n, b.K1, b.K1, kGemmBM));
-            TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.K2, b.K2, kGemmBM));
-            TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, n, b.K2, b.K2));
+            TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.KD, b.KD, kGemmBM));
+            TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, n, b.KD, b.KD));
             tm_rows = n;
             tm_p1 = qsplit.p;
             tm_p2 = kd.p;
@@ -240,7 +241,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e1.aoff = b.aoff.p;
     e1.qoff = w.qoff.p;
     e1.kd = w.kd.p;
-    e1.K2 = b.K2;
+    e1.K2 = b.KD;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
     TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st, &w.tmKd));
@@ -251,6 +252,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.cols = b.dim;
     e2.out = w.g.p;
     e2.ldo = b.dim;
+    e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
     TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
@@ -405,7 +407,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e1.aoff = b.aoff.p;
     e1.qoff = x.qoff_g.p;
     e1.kd = w.kd.p;
-    e1.K2 = b.K2;
+    e1.K2 = b.KD;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
     TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st, &w.tmKd));
@@ -417,6 +419,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e2.cols = b.dim;
     e2.out = x.g_g.p;
     e2.ldo = b.dim;
+    e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st));
     k_scatter_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
                                        x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
@@ -597,6 +600,7 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     b->Mpad = round_up(n_sparse, 64);
     b->K1 = round_up(b->nsplit * b->dim, kGemmBK);
     b->K2 = b->nsplit * b->Mpad;
+    b->KD = (b->nsplit == 3 ? 2 : 1) * b->Mpad;
     b->n_etiles = gemm_n_etiles(b->Mpad);
     b->tw = table_width(b->amax, b->lmax);
     b->delta = delta;

@@ -290,7 +290,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                     break;
                 }
                 mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
-                tma_load_2d(sA + s * A_BYTES, &tmA, ak + kb * BK, m0, full0 + 8 * s);
+                int ax = ak + kb * BK;
+                if (ep.a_krep > 0 && ax >= ep.a_krep) ax -= ep.a_krep;
+                tma_load_2d(sA + s * A_BYTES, &tmA, ax, m0, full0 + 8 * s);
                 tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
             }
         }
@@ -518,10 +520,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int y = m0 + q * 32;   // warp-uniform
                 if (lane == 0 && y < rows) {   // partial blocks are clipped by TMA
                     tma_store_2d(&tmC, sbuf, gcol, y);
-                    if (ep.nsplit == 3) {
-                        tma_store_2d(&tmC, sbuf, ep.Mpad + gcol, y);
-                        tma_store_2d(&tmC, sbuf + STG_HALF, 2 * ep.Mpad + gcol, y);
-                    }
+                    if (ep.nsplit == 3) tma_store_2d(&tmC, sbuf + STG_HALF, ep.Mpad + gcol, y);
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }
                 ++nbuf;

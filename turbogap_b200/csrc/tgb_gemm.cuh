@@ -13,7 +13,7 @@ namespace tgb {
 //       K = C + aoff[s] + qoff[row]                          (FP64; the exact rank-1 terms)
 //       epart[row][e] = sum_s alpha_s K^zeta                 (FP64)
 //       kdsum[row][e] = sum_s kd_s                           (FP64)
-//       kd[row][s + t*Mpad] = split(kd_s - kcoef_s), kd_s = kcoef_s K^(zeta-1),
+//       kd[row][s + t*Mpad] = split(kd_s - kcoef_s) (t = 0: hi, t = 1: lo), kd_s = kcoef_s K^(zeta-1),
 //                             kcoef_s = c0 alpha_s, c0 = zeta delta^2 (the K = 1
 //                             value is carried exactly by the caller)
 //     The partial sums e run over the gemm_n_etiles(Mpad) column slices of
@@ -36,6 +36,8 @@ struct GemmEpi {
     const int *rows_dev;  // optional: the valid rows are min(rows, *rows_dev), read on the device
     int bd_block;         // > 0: block-diagonal product; output columns [j b, (j+1) b) use A's
                           // K range [j b, j b + K) (b a multiple of kGemmBN)
+    int a_krep;           // > 0: A's logical K column k >= a_krep is read from column k - a_krep
+                          // (GEMM 2's [hi | hi | lo] operand stored as [hi | lo])
     int cols;             // valid columns of C
     // EPI_GAP_KERNEL
     const double *alpha;  // [Mpad]
