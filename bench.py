@@ -181,8 +181,8 @@ def mixed_leg(B, eng, blocks, w, a, ext, dist, plain_ms):
     import torch
     t0 = time.time()
     mlps = [B.Mlp(b.hypers.dim, 256, 4, seed=100 + i) for i, b in enumerate(blocks)]
-    # at most about 400k samples per block (large systems take fewer snapshots)
-    data_steps = min(a.mlp_data_steps, max(1, -(-400000 // max(eng.n, 1))))
+    # at most about 2M samples (large systems take fewer snapshots)
+    data_steps = min(a.mlp_data_steps, max(1, -(-2000000 // max(eng.n, 1))))
     for _ in range(data_steps):
         eng.md(2, w.dt, energies=False)
         for i, m in enumerate(mlps):

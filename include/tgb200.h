@@ -263,7 +263,8 @@ int tg_mlp_add_samples(tg_mlp *m, int32_t n, const float *delta, const double *e
  * evaluation (tg_engine_compute or an MD step), device to device. */
 int tg_mlp_add_engine_samples(tg_mlp *m, tg_engine *e, int32_t block);
 int tg_mlp_n_samples(tg_mlp *m, int64_t *n);
-/* epochs over the shuffled data set in batches of `batch` (a multiple of 32);
+/* epochs over the shuffled data set in batches of `batch` (a multiple of 32),
+ * Adam with the step size decaying from lr to lr / 20 over the epochs (cosine);
  * loss_per_epoch[epochs] receives the mean normalised loss of each epoch. */
 int tg_mlp_train(tg_mlp *m, int32_t epochs, int32_t batch, double lr, double force_weight,
                  uint64_t seed, double *loss_per_epoch);

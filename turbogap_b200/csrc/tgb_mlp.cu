@@ -826,6 +826,10 @@ int mlp_train(Mlp &m, int epochs, int batch, double lr, double lam, unsigned lon
     const float inv_sx = (float)(1.0 / m.sx), gscale = (float)(m.sx / m.sE);
     const double inv_sE = 1.0 / m.sE;
     for (int ep = 0; ep < epochs; ++ep) {
+        // cosine decay of the step size from lr to lr / 20 over the epochs
+        const double lr_ep =
+            epochs > 1 ? lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(3.141592653589793 * ep / (epochs - 1))))
+                       : lr;
         std::shuffle(order.begin(), order.end(), gen);
         TGB_CUDA(cudaMemcpyAsync(ord.p, order.data(), sizeof(int64_t) * order.size(),
                                  cudaMemcpyHostToDevice, st));
@@ -837,7 +841,7 @@ int mlp_train(Mlp &m, int epochs, int batch, double lr, double lam, unsigned lon
             TGB_TRY(transpose(batch, Dp, w.Xb.p, Dp, w.BW1.p, 2 * batch, st));
             for (int k = 0; k < m.n_members; ++k) {
                 TGB_TRY(member_step(m, w, k, lam, st));
-                TGB_TRY(adam_member(m, k, lr, st));
+                TGB_TRY(adam_member(m, k, lr_ep, st));
             }
         }
         double l2[2];
