@@ -188,6 +188,13 @@ int tg_engine_compute(tg_engine *e, double *energies, double *forces, double *vi
  * potential energy and kinetic energy (eV). */
 int tg_engine_md(tg_engine *e, int32_t n_steps, double dt, double *e_pot, double *e_kin);
 int tg_engine_get_state(tg_engine *e, double *positions, double *velocities, double *forces);
+/* The frame of the last evaluation, as the reference writes it to its
+ * trajectory (turbogap_md.f90:357-380): after an MD step, the wrapped positions
+ * the forces were evaluated at (positions_prev) with the synchronous velocities;
+ * after tg_engine_compute, the current positions. Any output may be NULL:
+ * positions, velocities, forces (3, n), energies (n), virial (3, 3). */
+int tg_engine_get_frame(tg_engine *e, double *positions, double *velocities, double *forces,
+                        double *energies, double *virial);
 /* Pairs in the current neighbour list. */
 int tg_engine_n_pairs(tg_engine *e, int64_t *n_pairs);
 /* CUDA stream the engine launches on (cudaStream_t), for timing with events. */

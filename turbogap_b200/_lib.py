@@ -75,6 +75,7 @@ SIGNATURES = [
     ("tg_engine_md", C.c_int, [_vp, C.c_int32, C.c_double, C.POINTER(C.c_double),
                                C.POINTER(C.c_double)]),
     ("tg_engine_get_state", C.c_int, [_vp, _vp, _vp, _vp]),
+    ("tg_engine_get_frame", C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("tg_engine_n_pairs", C.c_int, [_vp, C.POINTER(C.c_int64)]),
     ("tg_engine_stream", C.c_int, [_vp, C.POINTER(_vp)]),
     ("tg_engine_compute_device", C.c_int, [_vp]),

@@ -266,6 +266,18 @@ class Engine:
         check(lib().tg_engine_get_state(self._h, p.ctypes.data, v.ctypes.data, f.ctypes.data))
         return p, v, f
 
+    def get_frame(self):
+        """(positions, velocities, forces, energies, virial) of the last evaluation:
+        after MD steps, the positions the forces were evaluated at."""
+        p = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        f = np.zeros((self.n, 3))
+        e = np.zeros(self.n)
+        w = np.zeros(9)
+        check(lib().tg_engine_get_frame(self._h, p.ctypes.data, v.ctypes.data, f.ctypes.data,
+                                        e.ctypes.data, w.ctypes.data))
+        return p, v, f, e, w.reshape(3, 3).T.copy()
+
     def n_pairs(self) -> int:
         n = C.c_int64(0)
         check(lib().tg_engine_n_pairs(self._h, C.byref(n)))

@@ -1063,6 +1063,7 @@ struct Engine {
     cudaGraphExec_t graph = nullptr;
     double graph_dt = 0.0;
     bool first_step = true;
+    bool frame_prev = false;    // the last evaluation saw pos_prev (an MD step ran)
     double dt_prev = 0.0;
     cudaStream_t st = nullptr;
     // blocks after the first run on their own streams (forked after the neighbour
@@ -1264,6 +1265,7 @@ int tg_engine_set_state(tg_engine *eh, const double *positions, const double *ve
     if (positions) TGB_CUDA(cudaMemcpyAsync(E.pos.p, positions, b3, cudaMemcpyHostToDevice, E.st));
     if (velocities) TGB_CUDA(cudaMemcpyAsync(E.vel.p, velocities, b3, cudaMemcpyHostToDevice, E.st));
     E.first_step = true;
+    E.frame_prev = false;
     TGB_CUDA(cudaStreamSynchronize(E.st));
     return TG_OK;
 }
@@ -1288,12 +1290,14 @@ static int engine_errors(Engine &E) {
 
 int tg_engine_compute_device(tg_engine *eh) {
     TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    eh->e.frame_prev = false;
     return eh->e.compute_ef();
 }
 
 int tg_engine_compute(tg_engine *eh, double *energies, double *forces, double *virial) {
     TGB_CHECK(eh, TG_ERR_ARG, "null engine");
     Engine &E = eh->e;
+    E.frame_prev = false;
     TGB_TRY(E.compute_ef());
     if (energies)
         TGB_CUDA(cudaMemcpyAsync(energies, E.en.p, sizeof(double) * E.n, cudaMemcpyDeviceToHost, E.st));
@@ -1334,6 +1338,7 @@ int tg_engine_md(tg_engine *eh, int32_t n_steps, double dt, double *e_pot, doubl
         TGB_CUDA(cudaGraphLaunch(E.graph, E.st));
         E.dt_prev = dt;
     }
+    if (n_steps > 0) E.frame_prev = true;
     TGB_TRY(engine_errors(E));
     if (e_kin) {
         TGB_TRY(launch_kinetic(E.n, E.vel.p, E.mass.p, E.ekin.p, E.st));
@@ -1362,6 +1367,24 @@ int tg_engine_get_state(tg_engine *eh, double *positions, double *velocities, do
     return TG_OK;
 }
 
+int tg_engine_get_frame(tg_engine *eh, double *positions, double *velocities, double *forces,
+                        double *energies, double *virial) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    const size_t b3 = sizeof(double) * 3 * E.n;
+    // after an MD step the evaluation saw pos_prev (turbogap_md.f90:357-358: the
+    // trajectory holds positions_prev, synchronous with the velocities)
+    const double *p = E.frame_prev ? E.pos_prev.p : E.pos.p;
+    if (positions) TGB_CUDA(cudaMemcpyAsync(positions, p, b3, cudaMemcpyDeviceToHost, E.st));
+    if (velocities) TGB_CUDA(cudaMemcpyAsync(velocities, E.vel.p, b3, cudaMemcpyDeviceToHost, E.st));
+    if (forces) TGB_CUDA(cudaMemcpyAsync(forces, E.f.p, b3, cudaMemcpyDeviceToHost, E.st));
+    if (energies)
+        TGB_CUDA(cudaMemcpyAsync(energies, E.en.p, sizeof(double) * E.n, cudaMemcpyDeviceToHost, E.st));
+    if (virial) TGB_CUDA(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    return TG_OK;
+}
+
 int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {
     TGB_CHECK(eh && n_pairs, TG_ERR_ARG, "null argument");
     Engine &E = eh->e;
@@ -1379,6 +1402,7 @@ int tg_engine_profile(tg_engine *eh, int32_t n_steps, double dt, double *ms_per_
         const bool first = E.first_step;
         TGB_TRY(E.md_step(dt, first, &E.prof));
         E.first_step = false;
+        E.frame_prev = true;
         E.dt_prev = dt;
         TGB_CUDA(cudaStreamSynchronize(E.st));
         TGB_TRY(E.prof.collect(acc));
