@@ -195,6 +195,25 @@ int tg_engine_get_state(tg_engine *e, double *positions, double *velocities, dou
  * positions, velocities, forces (3, n), energies (n), virial (3, 3). */
 int tg_engine_get_frame(tg_engine *e, double *positions, double *velocities, double *forces,
                         double *energies, double *virial);
+
+/* ---- a structure sharded over ranks (one process per GPU), as the reference
+ *      splits central atoms over MPI ranks (src/turbogap.f90:930-942) and sums
+ *      energies, forces and the virial (src/turbogap.f90:1876-1885).
+ * tg_engine_set_site_range: this engine evaluates the central sites in
+ *   [site_beg, site_end) (0-based) only; other sites' energies are zero (no e0),
+ *   forces and virial hold this range's share. Default: every site.
+ * tg_nccl_unique_id: 128 bytes for tg_engine_set_comm, made on one rank and
+ *   sent to the others by the host (e.g. a torch.distributed broadcast).
+ * tg_engine_set_comm: collective over n_ranks processes; afterwards every force
+ *   evaluation ends with one grouped NCCL all-reduce (sum) of forces, energies
+ *   and virial on the engine's stream (captured in the MD graph), so every rank
+ *   integrates the whole structure with the full forces. NCCL is loaded at run
+ *   time; initialisation and each all-reduce give up after TGB_NCCL_TIMEOUT_S
+ *   (default 120) seconds with TG_ERR_TIMEOUT. id128 NULL leaves the
+ *   communicator. */
+int tg_engine_set_site_range(tg_engine *e, int32_t site_beg, int32_t site_end);
+int tg_nccl_unique_id(void *id128);
+int tg_engine_set_comm(tg_engine *e, const void *id128, int32_t n_ranks, int32_t rank);
 /* Pairs in the current neighbour list. */
 int tg_engine_n_pairs(tg_engine *e, int64_t *n_pairs);
 /* CUDA stream the engine launches on (cudaStream_t), for timing with events. */

@@ -1061,9 +1061,12 @@ int orc_evaluate_range(int n_sites, const double *positions, const int *species,
         cap = -np;
     }
     if (n_pairs_out) *n_pairs_out = np;
+    // turbogap.f90:1253-1261: each rank assigns e0 to its own sites i_beg..i_end
     for (int i = 0; i < n_sites; ++i) {
         const int z = species[i];
-        energies[i] = (z >= 1 && z <= n_species_total && e0_by_species) ? e0_by_species[z - 1] : 0.0;
+        const bool mine = i >= site_beg && i < site_end;
+        energies[i] = (mine && z >= 1 && z <= n_species_total && e0_by_species) ? e0_by_species[z - 1]
+                                                                                 : 0.0;
     }
     std::vector<double> e_soap(n_sites, 0.0), f_soap(3 * (size_t)n_sites, 0.0);
     double v_soap[9] = {0};

@@ -69,3 +69,41 @@ def test_two_rank_decomposition_matches_single_process():
         assert p.exitcode == 0
     de, df, dv = res
     assert de < 1e-12 and df < 1e-12 and dv < 1e-11
+
+
+def _id_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        from turbogap_b200.parallel import share_id
+        made = []
+
+        def make():
+            made.append(rank)
+            return bytes(range(128))
+
+        got = share_id(make)
+        out.put((rank, got, made))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_communicator_id_reaches_every_rank():
+    """The NCCL id of a sharded engine is made on rank 0 only and every rank
+    receives the same 128 bytes (the host half of parallel.shard_engine)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_id_worker, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(3))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, got, made in res:
+        assert got == bytes(range(128))
+        assert made == ([0] if rank == 0 else [])

@@ -278,6 +278,19 @@ class Engine:
                                         e.ctypes.data, w.ctypes.data))
         return p, v, f, e, w.reshape(3, 3).T.copy()
 
+    def set_site_range(self, beg: int, end: int):
+        """Evaluate only the central sites in [beg, end) (one rank's share)."""
+        check(lib().tg_engine_set_site_range(self._h, int(beg), int(end)))
+
+    def set_comm(self, nccl_id: Optional[bytes], n_ranks: int = 1, rank: int = 0):
+        """Join (collectively) an NCCL communicator: each evaluation then sums
+        forces, energies and virial over the ranks. None leaves it."""
+        if nccl_id is None:
+            check(lib().tg_engine_set_comm(self._h, None, 0, 0))
+            return
+        buf = C.create_string_buffer(bytes(nccl_id), 128)
+        check(lib().tg_engine_set_comm(self._h, C.cast(buf, C.c_void_p), int(n_ranks), int(rank)))
+
     def n_pairs(self) -> int:
         n = C.c_int64(0)
         check(lib().tg_engine_n_pairs(self._h, C.byref(n)))
@@ -287,6 +300,13 @@ class Engine:
         s = C.c_void_p()
         check(lib().tg_engine_stream(self._h, C.byref(s)))
         return int(s.value or 0)
+
+
+def nccl_unique_id() -> bytes:
+    """128 bytes naming a new NCCL communicator (make on one rank, send to all)."""
+    buf = C.create_string_buffer(128)
+    check(lib().tg_nccl_unique_id(C.cast(buf, C.c_void_p)))
+    return buf.raw
 
 
 def gemm_bf16_tn(A_bf16: np.ndarray, B_bf16: np.ndarray) -> np.ndarray:

@@ -29,6 +29,7 @@ SOURCES = {
     "tgb_mlp.cu": [],
     "tgb_capi.cu": [],
     "tgb_noalloc.cu": ["--fmad=false"],
+    "tgb_comm.cu": [],
 }
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -84,7 +85,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
         objs = [f.result() for f in futs]
     objs = [o for o in objs if o]
     if force or _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -4,6 +4,7 @@
 #include "tgb_common.cuh"
 #include "tgb_gemm.cuh"
 #include "tgb_mlp.cuh"
+#include "tgb_comm.cuh"
 #include "tgb_neighbors.cuh"
 #include "tgb_soap.cuh"
 
@@ -761,12 +762,13 @@ __global__ void k_add1(int64_t P, int *__restrict__ v) {
 }
 
 // energies(i) = e0(species(i)) (turbogap.f90:1253-1261)
+// e0 of the sites in [beg, end) (the sites this rank owns), zero elsewhere
 __global__ void k_energy_e0(int n, const int *__restrict__ sp, const double *__restrict__ e0, int nz,
-                            double *__restrict__ en) {
+                            int beg, int end, double *__restrict__ en) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int z = sp[i];
-    en[i] = (z >= 1 && z <= nz) ? e0[z - 1] : 0.0;
+    en[i] = (i >= beg && i < end && z >= 1 && z <= nz) ? e0[z - 1] : 0.0;
 }
 
 }  // namespace
@@ -1063,6 +1065,9 @@ struct Engine {
     cudaGraphExec_t graph = nullptr;
     double graph_dt = 0.0;
     bool first_step = true;
+    std::vector<int> species_h;          // host copy, for the site lists
+    int site_beg = 0, site_end = 0;      // central sites of this rank
+    Comm *comm = nullptr;                // set: forces/energies/virial summed over ranks
     bool frame_prev = false;    // the last evaluation saw pos_prev (an MD step ran)
     double dt_prev = 0.0;
     cudaStream_t st = nullptr;
@@ -1074,7 +1079,9 @@ struct Engine {
     cudaEvent_t ev_fork = nullptr;
 
     ~Engine() {
-        if (graph) cudaGraphExecDestroy(graph);
+        if (graph) cudaGraphExecDestroy(graph);   // before the communicator its NCCL nodes use
+        if (st) cudaStreamSynchronize(st);
+        comm_destroy(comm);
         nl.release();
         for (auto e : ev_side) cudaEventDestroy(e);
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -1107,7 +1114,7 @@ struct Engine {
         }
         TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
         TGB_MARK(log, PASS_NEIGH, st);
-        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
+        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, site_beg, site_end, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         // with a pass log every block runs on the main stream, so the marks time passes
@@ -1132,6 +1139,34 @@ struct Engine {
                 TGB_CUDA(cudaEventRecord(ev_side[k - 1], side[k - 1]));
                 TGB_CUDA(cudaStreamWaitEvent(st, ev_side[k - 1], 0));
             }
+        // sharded structure: every rank holds its own sites' share; the sum over
+        // ranks is the whole (turbogap.f90:1876-1885)
+        if (comm) TGB_TRY(comm_allreduce3(comm, f.p, 3 * (size_t)n, en.p, n, vir.p, 9, st));
+        return TG_OK;
+    }
+
+    // central sites of each block within [site_beg, site_end); species never
+    // change during MD
+    int assign_sites() {
+        for (auto &run : runs) {
+            const Block *b = run->b;
+            std::vector<int> s;
+            for (int i = site_beg; i < site_end; ++i) {
+                const int z = species_h[i];
+                int first = 0;
+                for (int q = 0; q < b->ns; ++q)
+                    if (b->hh.species_z[q] == z) { first = q + 1; break; }
+                if (b->hh.central_species == 0 || first == b->hh.central_species) s.push_back(i);
+            }
+            run->n_sites = (int)s.size();
+            TGB_TRY(run->sites.ensure(std::max<size_t>(s.size(), 1)));
+            if (!s.empty())
+                TGB_CUDA(cudaMemcpyAsync(run->sites.p, s.data(), sizeof(int) * s.size(),
+                                         cudaMemcpyHostToDevice, st));
+            TGB_TRY(run->w->ensure(*b, run->n_sites));
+            if (run->mix) TGB_TRY(run->mix->ensure(*b, run->n_sites));
+        }
+        TGB_CUDA(cudaStreamSynchronize(st));
         return TG_OK;
     }
 
@@ -1210,28 +1245,16 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     TGB_CUDA(cudaMemcpyAsync(E.e0.p, e0.data(), sizeof(double) * E.nz, cudaMemcpyHostToDevice, st));
     TGB_CUDA(cudaMemcpyAsync(E.abc.p, abc_h, sizeof(abc_h), cudaMemcpyHostToDevice, st));
     TGB_CUDA(cudaMemsetAsync(E.err.p, 0, sizeof(unsigned), st));
-    // central sites of each block (species never change during MD)
+    E.species_h.assign(species, species + n_atoms);
+    E.site_beg = 0;
+    E.site_end = n_atoms;
     for (int k = 0; k < n_blocks; ++k) {
-        Block *b = C.blocks[block_keys[k]].get();
         auto run = std::make_unique<BlockRun>();
-        run->b = b;
+        run->b = C.blocks[block_keys[k]].get();
         run->w = std::make_unique<Workspace>();
-        std::vector<int> sites;
-        for (int i = 0; i < n_atoms; ++i) {
-            const int z = species[i];
-            int first = 0;
-            for (int s = 0; s < b->ns; ++s)
-                if (b->hh.species_z[s] == z) { first = s + 1; break; }
-            if (b->hh.central_species == 0 || first == b->hh.central_species) sites.push_back(i);
-        }
-        run->n_sites = (int)sites.size();
-        TGB_TRY(run->sites.ensure(sites.size()));
-        if (!sites.empty())
-            TGB_CUDA(cudaMemcpyAsync(run->sites.p, sites.data(), sizeof(int) * sites.size(),
-                                     cudaMemcpyHostToDevice, st));
-        TGB_TRY(run->w->ensure(*b, run->n_sites));
         E.runs.push_back(std::move(run));
     }
+    TGB_TRY(E.assign_sites());
     // size the pair arrays from a first build, with 40 % headroom for MD
     const double *p0 = E.pos.p;
     if (E.nsc > E.n) {
@@ -1383,6 +1406,37 @@ int tg_engine_get_frame(tg_engine *eh, double *positions, double *velocities, do
     if (virial) TGB_CUDA(cudaMemcpyAsync(virial, E.vir.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, E.st));
     TGB_CUDA(cudaStreamSynchronize(E.st));
     return TG_OK;
+}
+
+int tg_engine_set_site_range(tg_engine *eh, int32_t site_beg, int32_t site_end) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    TGB_CHECK(site_beg >= 0 && site_beg <= site_end && site_end <= E.n, TG_ERR_ARG,
+              "site range [%d, %d) outside [0, %d)", site_beg, site_end, E.n);
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    if (E.graph) {   // the captured step holds the old site lists
+        cudaGraphExecDestroy(E.graph);
+        E.graph = nullptr;
+    }
+    E.site_beg = site_beg;
+    E.site_end = site_end;
+    return E.assign_sites();
+}
+
+int tg_nccl_unique_id(void *id128) { return comm_unique_id(id128); }
+
+int tg_engine_set_comm(tg_engine *eh, const void *id128, int32_t n_ranks, int32_t rank) {
+    TGB_CHECK(eh, TG_ERR_ARG, "null engine");
+    Engine &E = eh->e;
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    if (E.graph) {
+        cudaGraphExecDestroy(E.graph);
+        E.graph = nullptr;
+    }
+    comm_destroy(E.comm);
+    E.comm = nullptr;
+    if (!id128) return TG_OK;
+    return comm_init(id128, n_ranks, rank, &E.comm);
 }
 
 int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {
@@ -1692,7 +1746,7 @@ struct BatchEngine {
         TGB_MARK(log, -1, st);
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
         TGB_MARK(log, PASS_NEIGH, st);
-        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, en.p);
+        k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, 0, n, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         TGB_CUDA(cudaMemsetAsync(vir_s.p, 0, sizeof(double) * 9 * ns, st));

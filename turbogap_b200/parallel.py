@@ -29,3 +29,28 @@ def reduce_efv(energies, forces, virial, group=None):
     for t in (energies, forces, virial):
         dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return energies, forces, virial
+
+
+def share_id(make_id, group=None) -> bytes:
+    """The bytes ``make_id()`` returns on rank 0, on every rank of the group
+    (a torch.distributed broadcast; any backend)."""
+    import torch.distributed as dist
+    box = [make_id() if dist.get_rank(group) == 0 else None]
+    dist.broadcast_object_list(box, src=0, group=group)
+    return bytes(box[0])
+
+
+def shard_engine(engine, group=None):
+    """Make ``engine`` (the same structure on every rank) one rank's shard: it
+    evaluates this rank's contiguous range of central sites and sums forces,
+    energies and the virial over the ranks with NCCL inside every step (the
+    reference's MPI split and reduction, turbogap.f90:930-942, 1876-1885).
+    Collective: every rank of ``group`` calls it. Returns (beg, end)."""
+    import torch.distributed as dist
+    from . import backend
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    beg, end = site_range(engine.n, world, rank)
+    engine.set_site_range(beg, end)
+    if world > 1:
+        engine.set_comm(share_id(backend.nccl_unique_id, group), world, rank)
+    return beg, end
