@@ -133,17 +133,14 @@ __device__ __forceinline__ double ipow_d(double x, int e) {
 }
 
 constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK, STAGES = kGemmStages;
-constexpr int EPI_WARPS = 4 * kGemmEpiGroups;        // kGemmEpiGroups warps per TMEM lane quarter
-constexpr int THREADS = 64 + 32 * EPI_WARPS;
-constexpr int COLS_PER_WARP = BN / kGemmEpiGroups;   // accumulator columns one epilogue warp reads
 constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
-constexpr int CHUNKS = COLS_PER_WARP / 32;          // 32-column chunks per epilogue warp
-constexpr size_t PRM_BYTES = (size_t)EPI_WARPS * CHUNKS * 32 * sizeof(double2);
-// kd staging of the GAP epilogue: per warp two buffers of a 32 x 32 hi and lo block
-// (64-byte rows, 64-byte swizzle), written out by TMA tensor stores
+// column parameters staged per epilogue warp: one double2 per accumulator column
+// of the tile and lane quarter, whatever the warp count
+constexpr size_t PRM_BYTES = (size_t)4 * BN * sizeof(double2);
+// Epilogue staging for TMA tensor stores: 32 x 32 blocks, a bf16 hi and lo (or h
+// and silu') pair of 64-byte-row blocks, or one fp32 block of 128-byte rows.
 constexpr uint32_t STG_HALF = 32 * 32 * 2;           // one 32 x 32 bf16 block
-constexpr uint32_t STG_BUF = 2 * STG_HALF;           // hi + lo
-constexpr uint32_t STG_WARP = 2 * STG_BUF;           // double buffered
+constexpr uint32_t STG_BUF = 2 * STG_HALF;           // hi + lo, or one 32 x 32 fp32 block
 constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulators: epilogue of tile i overlaps tile i+1
 
 // Epilogue variants (compile-time, so the element loop has no mode branches).
@@ -152,7 +149,10 @@ enum {
     MODE_MLP_L2 = 5, MODE_MLP_L2B = 6, MODE_MLP_L1B = 7, N_MODES = 8
 };
 
-__device__ __forceinline__ float sigmoid_f(float z) { return 1.f / (1.f + expf(-z)); }
+// The MLP epilogues round their outputs to bf16 (8-bit significand); the fast
+// exponential (a few ulp at the |z| of the hidden layers) and the correctly rounded
+// reciprocal are ample and keep the per-element work in the epilogue short.
+__device__ __forceinline__ float sigmoid_f(float z) { return __frcp_rn(1.f + __expf(-z)); }
 
 
 template <int MODE>
@@ -166,22 +166,37 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Shared-memory plan of a mode: epilogues with bf16 outputs (the GAP kd scratch,
-// the MLP activations) stage 32 x 32 blocks for TMA stores and therefore run a
-// 3-stage operand ring; the fp32-store modes run 4 stages.
+// Per-mode plan. The GAP epilogue (long K loop) has kGemmEpiGroups warps per TMEM
+// lane quarter, each with two staging buffers. The MLP epilogues follow short K
+// loops (256 .. 1232), so their element work is what bounds them: they run
+// kGemmMlpEpiGroups warps per quarter (twice the warps in flight) with one staging
+// buffer each. Staged modes (every output but the plain fp32 store) run a 3-stage
+// operand ring, the plain store 4.
 __host__ __device__ constexpr bool gap_mode(int mode) { return mode <= MODE_GAP_ZREAL; }
-__host__ __device__ constexpr bool staged_mode(int mode) {
-    return gap_mode(mode) || mode == MODE_MLP_L1 || mode == MODE_MLP_L2 || mode == MODE_MLP_L2B;
+__host__ __device__ constexpr bool mlp_mode(int mode) { return mode >= MODE_MLP_L1; }
+__host__ __device__ constexpr bool staged_mode(int mode) { return mode != MODE_STORE; }
+__host__ __device__ constexpr int epi_groups(int mode) {
+    return mlp_mode(mode) ? kGemmMlpEpiGroups : kGemmEpiGroups;
 }
+__host__ __device__ constexpr int epi_warps(int mode) { return 4 * epi_groups(mode); }
+__host__ __device__ constexpr int threads_for(int mode) { return 64 + 32 * epi_warps(mode); }
+__host__ __device__ constexpr int cols_per_warp(int mode) { return BN / epi_groups(mode); }
+__host__ __device__ constexpr int chunks_for(int mode) { return cols_per_warp(mode) / 32; }
+__host__ __device__ constexpr int stage_bufs(int mode) { return mlp_mode(mode) ? 1 : 2; }
 __host__ __device__ constexpr int stages_for(int mode) { return staged_mode(mode) ? 3 : STAGES; }
 __host__ __device__ constexpr size_t stg_offset(int mode) {   // from the 1024-aligned base
     return ((size_t)stages_for(mode) * (A_BYTES + B_BYTES) + 256 + PRM_BYTES + 1023) / 1024 * 1024;
 }
 __host__ __device__ constexpr size_t smem_bytes_for(int mode) {
-    return 1024 + stg_offset(mode) + (staged_mode(mode) ? (size_t)EPI_WARPS * STG_WARP : 0);
+    return 1024 + stg_offset(mode) +
+           (staged_mode(mode) ? (size_t)epi_warps(mode) * stage_bufs(mode) * STG_BUF : 0);
 }
-static_assert(smem_bytes_for(MODE_GAP_Z4) <= 232448 && smem_bytes_for(MODE_STORE) <= 232448,
+static_assert(smem_bytes_for(MODE_GAP_Z4) <= 232448 && smem_bytes_for(MODE_STORE) <= 232448 &&
+                  smem_bytes_for(MODE_MLP_L1) <= 232448,
               "shared memory plan exceeds 227 KB");
+static_assert(threads_for(MODE_MLP_L1) <= 1024 && chunks_for(MODE_MLP_L1) >= 1 &&
+                  chunks_for(MODE_GAP_Z4) >= 1,
+              "epilogue warp plan");
 
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
@@ -198,11 +213,24 @@ __device__ __forceinline__ void stage_row(uint32_t buf, int lane, const __nv_bfl
         st_shared_v4(buf + (uint32_t)lane * 64u + (uint32_t)((u ^ ((lane >> 1) & 3)) * 16), v4[u]);
 }
 
-// Before a warp refills staging buffer nbuf & 1: the bulk group that last read it
-// (two chunks ago) has finished reading.
+// Before a warp refills a staging buffer: the bulk group that last read it has
+// finished reading (two chunks ago with two buffers, the previous chunk with one).
+template <int NBUF>
 __device__ __forceinline__ void stage_acquire(int lane) {
-    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+    if (lane == 0) {
+        if constexpr (NBUF == 2) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        else asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
     __syncwarp();
+}
+
+// Lane r's 32 fp32 values as row r of a 32 x 32 fp32 staging block: 128-byte rows
+// with the 128-byte swizzle of the store map (16-byte chunk u at u ^ (r & 7)).
+__device__ __forceinline__ void stage_row_f32(uint32_t buf, int lane, const float (&v)[32]) {
+    const uint4 *v4 = reinterpret_cast<const uint4 *>(v);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+        st_shared_v4(buf + (uint32_t)lane * 128u + (uint32_t)((u ^ (lane & 7)) * 16), v4[u]);
 }
 // After the warp's shared stores: make them visible to the async proxy.
 __device__ __forceinline__ void stage_release() {
@@ -223,11 +251,15 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t sr
 // shared-memory ring run across tiles; accumulator it % 2 is reused every
 // second tile once all epilogue warps have released it.
 template <int MODE>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(threads_for(MODE), 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const __grid_constant__ CUtensorMap tmC, int num_kb, int n_tiles_m, int n_tiles_n,
               GemmEpi ep, unsigned *err) {
     constexpr int NST = stages_for(MODE);
+    constexpr int EPI_WARPS = epi_warps(MODE), GROUPS = epi_groups(MODE);
+    constexpr int COLS_PER_WARP = cols_per_warp(MODE), CHUNKS = chunks_for(MODE);
+    constexpr int NBUF = stage_bufs(MODE);
+    constexpr uint32_t STG_WARP = NBUF * STG_BUF;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -346,37 +378,57 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint32_t use = (uint32_t)(it >> 1);
         const int tile_n = t % n_tiles_n;
         const int m0 = (t / n_tiles_n) * BM, n0 = tile_n * BN;
+        const int row = m0 + q * 32 + lane;
+        const bool row_ok = row < rows;
+        // MLP epilogues: the tile's global inputs (column parameters; the bf16
+        // silu'(z1) factors of L2B) are requested before the wait for the
+        // accumulator, so their latency overlaps the MMA of this tile
+        float a0[mlp_mode(MODE) ? CHUNKS : 1], a1[mlp_mode(MODE) ? CHUNKS : 1];
+        uint4 pre[MODE == MODE_MLP_L2B ? CHUNKS : 1][4];
+        if constexpr (mlp_mode(MODE) && MODE != MODE_MLP_L2B) {
+#pragma unroll
+            for (int c = 0; c < CHUNKS; ++c) {
+                const int cl = n0 + grp * COLS_PER_WARP + c * 32 + lane;
+                a0[c] = 0.f;
+                a1[c] = 0.f;
+                if (cl < ep.cols) {
+                    if (ep.p0) a0[c] = ep.p0[cl];
+                    if constexpr (MODE == MODE_MLP_L2) a1[c] = ep.p1[cl];
+                }
+            }
+        }
+        if constexpr (MODE == MODE_MLP_L2B) {
+#pragma unroll
+            for (int c = 0; c < CHUNKS; ++c) {
+                const int gcol = n0 + grp * COLS_PER_WARP + c * 32;
+                if (row_ok && gcol < ep.cols) {
+                    const uint4 *s4 = reinterpret_cast<const uint4 *>(ep.in_b + (size_t)row * ep.ldi + gcol);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) pre[c][u] = s4[u];
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) pre[c][u] = make_uint4(0, 0, 0, 0);
+                }
+            }
+        }
         const bool ready = mbar_wait(accf0 + 8 * a, use & 1u, err);
         if (!ready) {
             if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_TIMEOUT_EPI);
             break;
         }
         tc_fence_after();
-        const int row = m0 + q * 32 + lane;
-        const bool row_ok = row < rows;
         const uint32_t taddr = tmem + (uint32_t)(a * BN) + ((uint32_t)(q * 32) << 16);
         if constexpr (MODE >= MODE_MLP_L1) {
             // the MLP epilogues: float column parameters staged per warp like the GAP ones
-            // column parameters of all this warp's chunks, loaded together at tile start
             float2 *pfall = reinterpret_cast<float2 *>(prm);
             if constexpr (MODE != MODE_MLP_L2B) {
-                float a0[CHUNKS], a1[CHUNKS];
-#pragma unroll
-                for (int c = 0; c < CHUNKS; ++c) {
-                    const int cl = n0 + grp * COLS_PER_WARP + c * 32 + lane;
-                    a0[c] = 0.f;
-                    a1[c] = 0.f;
-                    if (cl < ep.cols) {
-                        if (ep.p0) a0[c] = ep.p0[cl];
-                        if constexpr (MODE == MODE_MLP_L2) a1[c] = ep.p1[cl];
-                    }
-                }
                 __syncwarp();
 #pragma unroll
                 for (int c = 0; c < CHUNKS; ++c) pfall[c * 32 + lane] = make_float2(a0[c], a1[c]);
                 __syncwarp();
             }
             float racc = 0.f;
+#pragma unroll
             for (int c = 0; c < CHUNKS; ++c) {
                 const int col = grp * COLS_PER_WARP + c * 32;
                 const int gcol = n0 + col;
@@ -393,8 +445,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         sb[j] = __float2bfloat16_rn(sg * (1.f + z * (1.f - sg)));
                     }
                     // h1 and silu'(z1) blocks of one [rows x 2 HH] matrix (s at x2 + col)
-                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
-                    stage_acquire(lane);
+                    const uint32_t sbuf = stg_warp + (NBUF == 2 ? (uint32_t)(nbuf & 1) * STG_BUF : 0u);
+                    stage_acquire<NBUF>(lane);
                     stage_row(sbuf, lane, hb);
                     stage_row(sbuf + STG_HALF, lane, sb);
                     stage_release();
@@ -414,8 +466,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         racc += q2.y * z * sg;
                         ub[j] = __float2bfloat16_rn(q2.y * sg * (1.f + z * (1.f - sg)));
                     }
-                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
-                    stage_acquire(lane);
+                    const uint32_t sbuf = stg_warp + (NBUF == 2 ? (uint32_t)(nbuf & 1) * STG_BUF : 0u);
+                    stage_acquire<NBUF>(lane);
                     stage_row(sbuf, lane, ub);
                     stage_release();
                     const int y = m0 + q * 32;
@@ -427,19 +479,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                 } else if constexpr (MODE == MODE_MLP_L2B) {
                     __align__(16) __nv_bfloat16 sf[32], ub[32];
                     uint4 *t4 = reinterpret_cast<uint4 *>(sf);
-                    if (row_ok) {
-                        const uint4 *s4 = reinterpret_cast<const uint4 *>(ep.in_b + (size_t)row * ep.ldi + gcol);
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) t4[u] = s4[u];
-                    } else {
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) t4[u] = make_uint4(0, 0, 0, 0);
-                    }
+                    for (int u = 0; u < 4; ++u) t4[u] = pre[c][u];
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         ub[j] = __float2bfloat16_rn(v[j] * __bfloat162float(sf[j]));
-                    const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
-                    stage_acquire(lane);
+                    const uint32_t sbuf = stg_warp + (NBUF == 2 ? (uint32_t)(nbuf & 1) * STG_BUF : 0u);
+                    stage_acquire<NBUF>(lane);
                     stage_row(sbuf, lane, ub);
                     stage_release();
                     const int y = m0 + q * 32;
@@ -449,27 +495,39 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     ++nbuf;
                 } else {   // MODE_MLP_L1B
-                    if (row_ok) {
+                    __align__(16) float ov[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) ov[j] = ep.scale * v[j] - pf[j].x;
+                    const int y = m0 + q * 32;   // warp-uniform
+                    if (y + 32 <= rows) {
+                        // a whole 32-row block: staged and written by one TMA store,
+                        // which clips the columns at the map's width (ep.cols)
+                        stage_acquire<NBUF>(lane);
+                        stage_row_f32(stg_warp, lane, ov);
+                        stage_release();
+                        if (lane == 0) {
+                            tma_store_2d(&tmC, stg_warp, gcol, y);
+                            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                        }
+                    } else if (row_ok) {   // the last, partial block: plain stores
                         float *o = ep.out + (size_t)row * ep.ldo + gcol;
                         if (gcol + 32 <= ep.cols) {
                             float4 *o4 = reinterpret_cast<float4 *>(o);
 #pragma unroll
                             for (int j = 0; j < 8; ++j)
-                                o4[j] = make_float4(ep.scale * v[4 * j] - pf[4 * j].x,
-                                                    ep.scale * v[4 * j + 1] - pf[4 * j + 1].x,
-                                                    ep.scale * v[4 * j + 2] - pf[4 * j + 2].x,
-                                                    ep.scale * v[4 * j + 3] - pf[4 * j + 3].x);
+                                o4[j] = make_float4(ov[4 * j], ov[4 * j + 1], ov[4 * j + 2],
+                                                    ov[4 * j + 3]);
                         } else {
 #pragma unroll
                             for (int j = 0; j < 32; ++j)
-                                if (gcol + j < ep.cols) o[j] = ep.scale * v[j] - pf[j].x;
+                                if (gcol + j < ep.cols) o[j] = ov[j];
                         }
                     }
                 }
             }
             if constexpr (MODE == MODE_MLP_L2) {
                 if (row_ok)
-                    ep.rowpart[(size_t)row * ep.rowpart_ld + tile_n * kGemmEpiGroups + grp] = racc;
+                    ep.rowpart[(size_t)row * ep.rowpart_ld + tile_n * GROUPS + grp] = racc;
             }
         } else if constexpr (MODE != MODE_STORE) {
             double e4[4] = {0, 0, 0, 0}, k4[4] = {0, 0, 0, 0};
@@ -512,8 +570,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 // Stage the 32 x 32 hi / lo blocks (64-byte rows, 64-byte swizzle: the
                 // 16-byte chunk u of row r sits at chunk u ^ ((r >> 1) & 3)) and let TMA
                 // write them out as whole lines. Rows past the tensor are clipped by TMA.
-                const uint32_t sbuf = stg_warp + (uint32_t)(nbuf & 1) * STG_BUF;
-                stage_acquire(lane);
+                const uint32_t sbuf = stg_warp + (NBUF == 2 ? (uint32_t)(nbuf & 1) * STG_BUF : 0u);
+                stage_acquire<NBUF>(lane);
                 stage_row(sbuf, lane, hi);
                 if (ep.nsplit == 3) stage_row(sbuf + STG_HALF, lane, lo);
                 stage_release();
@@ -526,7 +584,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 ++nbuf;
             }
             if (row_ok) {
-                const size_t o = ((size_t)row * n_tiles_n + tile_n) * kGemmEpiGroups + grp;
+                const size_t o = ((size_t)row * n_tiles_n + tile_n) * GROUPS + grp;
                 ep.epart[o] = (e4[0] + e4[1]) + (e4[2] + e4[3]);
                 ep.kdsum[o] = ep.c0 * ((k4[0] + k4[1]) + (k4[2] + k4[3]));
             }
@@ -626,6 +684,24 @@ int make_tma_store_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols,
     return TG_OK;
 }
 
+int make_tma_store_f32(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld) {
+    TGB_TRY(get_encoder());
+    TGB_CHECK(((uintptr_t)base & 15) == 0, TG_ERR_ARG, "TMA base address not 16-byte aligned");
+    TGB_CHECK((ld * 4) % 16 == 0, TG_ERR_ARG, "TMA row stride %lld B not a multiple of 16",
+              (long long)(ld * 4));
+    TGB_CHECK(rows >= 1 && cols >= 1, TG_ERR_ARG, "empty TMA extent");
+    cuuint64_t gdim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)(ld * 4)};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(&m->map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base),
+                          gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TGB_CHECK(r == CUDA_SUCCESS, TG_ERR_CUDA, "cuTensorMapEncodeTiled (fp32 store) failed (%d)", (int)r);
+    return TG_OK;
+}
+
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
                    unsigned *err, cudaStream_t st, const TmaMap *C) {
     TGB_CHECK(K % kGemmBK == 0, TG_ERR_ARG, "GEMM K=%d must be a multiple of %d", K, kGemmBK);
@@ -641,8 +717,9 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
               TG_ERR_ARG, "bf16 MLP outputs need a store map, N %% 32 == 0 and x2 %% 32 == 0");
     TGB_CHECK(ep.mode != EPI_MLP_L2B || (ep.ldi % 8 == 0 && ((uintptr_t)ep.in_b & 15) == 0),
               TG_ERR_ARG, "bf16 MLP factor rows must be 16-byte aligned");
-    TGB_CHECK(ep.mode != EPI_MLP_L1B || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
-              TG_ERR_ARG, "fp32 output rows must be 16-byte aligned (ldo %% 4 == 0)");
+    TGB_CHECK(ep.mode != EPI_MLP_L1B || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0 &&
+                                         C != nullptr),
+              TG_ERR_ARG, "MLP fp32 output: 16-byte aligned rows (ldo %% 4 == 0) and a store map");
     int mode = MODE_STORE;
     switch (ep.mode) {
         case EPI_GAP_KERNEL:
@@ -673,7 +750,7 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
     }
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     const int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
-    kerns[mode]<<<grid, THREADS, smem_bytes_for(mode), st>>>(A.map, B.map, C ? C->map : A.map,
+    kerns[mode]<<<grid, threads_for(mode), smem_bytes_for(mode), st>>>(A.map, B.map, C ? C->map : A.map,
                                                              K / kGemmBK, tm, tn, ep, err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;

@@ -23,8 +23,10 @@ namespace tgb {
 //                column x2 + col of the store map
 //   EPI_MLP_L2   z = C + p0[col]: bf16(p1[col] silu' z) through the store map and the
 //                row sums of p1[col] silu z into rowpart[row * rowpart_ld + tile * groups + group]
+//                (groups = kGemmMlpEpiGroups)
 //   EPI_MLP_L2B  bf16(C * in_b[row][col]) through the store map
-//   EPI_MLP_L1B  out[row][col] = scale C - p0[col] (p0 may be null), fp32, cols < cols
+//   EPI_MLP_L1B  out[row][col] = scale C - p0[col] (p0 may be null), fp32, cols < cols,
+//                through the fp32 store map C (make_tma_store_f32 over out)
 enum EpiMode {
     EPI_GAP_KERNEL = 0, EPI_STORE_F32 = 1, EPI_MLP_L1 = 2, EPI_MLP_L2 = 3, EPI_MLP_L2B = 4,
     EPI_MLP_L1B = 5
@@ -70,6 +72,7 @@ constexpr int kGemmBN = 256;
 constexpr int kGemmBK = 64;
 constexpr int kGemmStages = 4;
 constexpr int kGemmEpiGroups = 2;   // epilogue warps per TMEM lane quarter (column groups)
+constexpr int kGemmMlpEpiGroups = 4;   // the same for the MLP epilogues (EPI_MLP_*)
 
 struct TmaMap {
     alignas(64) CUtensorMap map;
@@ -83,6 +86,8 @@ int make_tma_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64
 // 2-D bf16 tensor map for TMA stores of 32 x 32 blocks (64-byte swizzle): the
 // GAP epilogue's kd scratch.
 int make_tma_store_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld);
+// fp32 store map: 32 x 32 boxes, 128-byte swizzle (the EPI_MLP_L1B output)
+int make_tma_store_f32(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld);
 
 // C (map for the GAP epilogue's kd stores) is required in EPI_GAP_KERNEL mode.
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,

@@ -425,7 +425,7 @@ struct MlpInferWork {
     Plan p1, p4;
     std::vector<Plan> p2, p3;
 
-    int npart(const Mlp &m) const { return gemm_n_tiles(m.L.H) * kGemmEpiGroups; }
+    int npart(const Mlp &m) const { return gemm_n_tiles(m.L.H) * kGemmMlpEpiGroups; }
 
     int ensure(Mlp &m, int rows) {
         if (rows > cap) {
@@ -490,6 +490,8 @@ struct MlpInferWork {
         p4.ep.mode = EPI_MLP_L1B;
         p4.ep.scale = 1.f / (float)nm;
         p4.ep.p0 = s;
+        TGB_TRY(make_tma_store_f32(&p4.c, gout, rows, m.L.D, ldgo));
+        p4.has_c = true;
         X = x;
         n = rows;
         ldx = ld;
