@@ -109,6 +109,51 @@ int tg_get_gap_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_ne
                     const int32_t *species_batch, const int32_t *species_all,
                     double *energies0, double *forces0, double *virial);
 
+/* ---- the other GAP families (src/gap_backend_cpu.f90:79-267 add_2b_contribution,
+ *      add_core_pot_contribution, add_3b_contribution; kernels src/gap.f90:400-1042).
+ * tg_family describes one family as read from its .gap block (types.f90
+ * distance_2b / angle_3b / core_pot); species are global ids (1-based
+ * positions in the input's species_types):
+ *   TG_FAMILY_2B        species[0..1] = species1, species2; delta, sigma[0], rcut;
+ *                       n sparse points Qs(n), alphas(n), cutoff(n)
+ *   TG_FAMILY_3B        species[0..2] = species_center, species1, species2; delta,
+ *                       sigma[0..2], rcut, kernel_type (TG_KERNEL_EXP / TG_KERNEL_POL);
+ *                       Qs(n, 3) column-major, alphas(n), cutoff(n)
+ *   TG_FAMILY_CORE_POT  species[0..1]; table x(n), V(n) after the core_pot_cutoff
+ *                       taper (read_files.f90:5425-5447) and the file's end slopes
+ *                       yp1, ypn (> 0.99e30: natural end); the spline second
+ *                       derivatives are made here (read_files.f90:5454-5505)
+ * The cutoff-function buffer of 2b and 3b is 0.5 A, as the reference passes it.
+ * n is at most 4096. */
+enum { TG_FAMILY_2B = 1, TG_FAMILY_3B = 2, TG_FAMILY_CORE_POT = 3 };
+enum { TG_KERNEL_EXP = 0, TG_KERNEL_POL = 1 };
+typedef struct {
+    int32_t kind;
+    int32_t species[3];
+    double delta;
+    double sigma[3];
+    double rcut;
+    int32_t kernel_type;
+    int32_t n;
+    const double *Qs, *alphas, *cutoff;
+    const double *x, *V;
+    double yp1, ypn;
+} tg_family;
+
+/* Uploads a family under key (the key space is shared with tg_soap_begin; an
+ * engine created with the key evaluates the family in every step). */
+int tg_family_begin(int32_t key, const tg_family *family);
+
+/* add_*_contribution for one family and one batch, with the arguments of
+ * tg_get_gap_soap (the site of each list is its self pair's index mod
+ * n_total_sites). ADDS the family's energies0(n_total_sites),
+ * forces0(3, n_total_sites) and virial(3, 3) to the caller's arrays, as the
+ * reference adds this_energies, this_forces, this_virial to its totals. */
+int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                  const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                  const int32_t *species_all, double *energies0, double *forces0,
+                  double *virial);
+
 /* Descriptor only (soap_turbo get_soap as called at gap_interface.f90:320-325,
  * through the same remap): soap(dim, n_central) of the current block's central
  * sites in batch order. The Cartesian derivative array soap_cart_der is never

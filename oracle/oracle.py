@@ -92,6 +92,14 @@ def lib():
                                          C.POINTER(_Block), C.c_void_p, C.c_int, C.c_double,
                                          C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                          C.POINTER(C.c_int64)]
+        L.orc_core_pot_spline.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), _dp]
+        L.orc_family_energy_forces.argtypes = [C.POINTER(_Family), C.c_int, _ip, _ip, _dp, _dp,
+                                               _ip, _ip, C.c_int, _dp, _dp, _dp]
+        L.orc_evaluate_full.argtypes = [C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int,
+                                        C.POINTER(_Block), C.c_int, C.POINTER(_Family),
+                                        C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, _dp, _dp, _dp, C.POINTER(C.c_int64)]
     return _lib
 
 
@@ -101,6 +109,77 @@ def set_threads(n: int) -> int:
 
 def _f64(x):
     return np.ascontiguousarray(x, dtype=np.float64)
+
+
+class _Family(C.Structure):
+    _pd = C.POINTER(C.c_double)
+    _fields_ = [("kind", C.c_int), ("sp", C.c_int * 3), ("delta", C.c_double),
+                ("sigma", C.c_double * 3), ("rcut", C.c_double), ("kernel_pol", C.c_int),
+                ("n", C.c_int), ("Qs", _pd), ("alphas", _pd), ("cutoff", _pd), ("x", _pd),
+                ("V", _pd), ("y2", _pd), ("yp1", C.c_double), ("ypn", C.c_double)]
+
+
+def core_pot_spline(x, V, yp1, ypn):
+    """read_files.f90:5454-5505: (y2, yp1, ypn) of the core_pot table."""
+    x, V = _f64(x), _f64(V)
+    y2 = np.zeros(len(x))
+    a, b = C.c_double(yp1), C.c_double(ypn)
+    lib().orc_core_pot_spline(len(x), x, V, C.byref(a), C.byref(b), y2)
+    return y2, a.value, b.value
+
+
+class FamilyC:
+    """Keeps the buffers behind an ``orc_family`` alive. ``f`` has ``kind``
+    ("distance_2b", "angle_3b" or "core_pot"), ``species`` (global ids) and the
+    family's parameters (turbogap_b200.families)."""
+
+    KINDS = {"distance_2b": 1, "angle_3b": 2, "core_pot": 3}
+
+    def __init__(self, f):
+        s = _Family()
+        s.kind = self.KINDS[f.kind]
+        for q, z in enumerate(f.species):
+            s.sp[q] = int(z)
+        self.keep = []
+
+        def arr(v):
+            a = _f64(v)
+            self.keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+
+        if f.kind == "core_pot":
+            y2, yp1, ypn = core_pot_spline(f.x, f.V, f.yp1, f.ypn)
+            s.n = len(f.x)
+            s.x, s.V, s.y2 = arr(f.x), arr(f.V), arr(y2)
+            s.yp1, s.ypn = yp1, ypn
+        else:
+            s.delta = float(f.delta)
+            sig = np.atleast_1d(np.asarray(f.sigma, dtype=np.float64))
+            for q in range(len(sig)):
+                s.sigma[q] = float(sig[q])
+            s.rcut = float(f.rcut)
+            s.kernel_pol = int(getattr(f, "kernel_type", "exp") == "pol")
+            s.n = len(f.alphas)
+            # angle_3b Qs (n, 3) row-major numpy is Qs(n, 3) column-major transposed
+            Q = np.asarray(f.Qs, dtype=np.float64)
+            s.Qs = arr(Q.T.reshape(-1) if Q.ndim == 2 else Q)
+            s.alphas, s.cutoff = arr(f.alphas), arr(f.cutoff)
+        self.struct = s
+
+
+def family_energy_forces(f, n_neigh, neighbors_list, rjs, xyz, species, neighbor_species,
+                         n_sites0):
+    """gap.f90:400-1042 for one family: energies (n_sites), forces (n_sites0, 3),
+    virial (3, 3)."""
+    fc = FamilyC(f)
+    n = len(n_neigh)
+    e = np.zeros(n)
+    fo = np.zeros((n_sites0, 3))
+    v = np.zeros(9)
+    lib().orc_family_energy_forces(C.byref(fc.struct), n, _i32(n_neigh), _i32(neighbors_list),
+                                   _f64(rjs), _f64(xyz), _i32(species), _i32(neighbor_species),
+                                   int(n_sites0), e, fo, v)
+    return e, fo, v.reshape(3, 3).T.copy()
 
 
 def _i32(x):
@@ -295,7 +374,7 @@ def wrap_pbc(positions, a, b, c):
 
 
 def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max_gbytes=1.0,
-             site_range=None):
+             site_range=None, families=()):
     """Energies (n), forces (n,3), virial (3,3) of one periodic structure.
 
     ``blocks``: sequence of objects with ``hypers`` (attributes as HypersC),
@@ -322,12 +401,16 @@ def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max
     vir = np.zeros(9)
     npairs = C.c_int64(0)
     beg, end = site_range if site_range is not None else (0, n)
-    rc = lib().orc_evaluate_range(n, _f64(positions), _i32(species), _f64(box[0]), _f64(box[1]),
-                                  _f64(box[2]), len(blocks), arr,
-                                  e0a.ctypes.data if e0a is not None else None,
-                                  len(e0a) if e0a is not None else 0, float(neighbors_buffer),
-                                  float(max_gbytes), int(beg), int(end), en, f, vir,
-                                  C.byref(npairs))
+    fams = [FamilyC(q) for q in families]
+    farr = (_Family * max(len(fams), 1))()
+    for i, q in enumerate(fams):
+        farr[i] = q.struct
+    rc = lib().orc_evaluate_full(n, _f64(positions), _i32(species), _f64(box[0]), _f64(box[1]),
+                                 _f64(box[2]), len(blocks), arr, len(fams), farr,
+                                 e0a.ctypes.data if e0a is not None else None,
+                                 len(e0a) if e0a is not None else 0, float(neighbors_buffer),
+                                 float(max_gbytes), int(beg), int(end), en, f, vir,
+                                 C.byref(npairs))
     if rc != 0:
         raise RuntimeError(f"oracle evaluate failed: {rc}")
     return en, f, vir.reshape(3, 3).T, int(npairs.value)

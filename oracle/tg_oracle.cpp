@@ -1023,12 +1023,279 @@ int orc_evaluate_range(int n_sites, const double *positions, const int *species,
                        int n_species_total, double neighbors_buffer, double max_gbytes,
                        int site_beg, int site_end, double *energies, double *forces,
                        double *virial, int64_t *n_pairs_out) {
+    return orc_evaluate_full(n_sites, positions, species, a, b, c, n_blocks, blocks, 0, nullptr,
+                             e0_by_species, n_species_total, neighbors_buffer, max_gbytes,
+                             site_beg, site_end, energies, forces, virial, n_pairs_out);
+}
+
+// read_files.f90:5454-5505
+void orc_core_pot_spline(int n, const double *x, const double *V, double *yp1, double *ypn,
+                         double *y2) {
+    std::vector<double> u(n, 0.0);
+    if (*yp1 > 0.99e30) {
+        y2[0] = 0.0;
+        u[0] = 0.0;
+    } else {
+        y2[0] = -0.5;
+        u[0] = (3.0 / (x[1] - x[0])) * ((V[1] - V[0]) / (x[1] - x[0]) - *yp1);
+    }
+    for (int i = 1; i < n - 1; ++i) {
+        const double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+        const double p = sig * y2[i - 1] + 2.0;
+        y2[i] = (sig - 1.0) / p;
+        u[i] = (V[i + 1] - V[i]) / (x[i + 1] - x[i]) - (V[i] - V[i - 1]) / (x[i] - x[i - 1]);
+        u[i] = (6.0 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+    }
+    double qn, un;
+    if (*ypn > 0.99e30) {
+        qn = 0.0;
+        un = 0.0;
+    } else {
+        qn = 0.5;
+        un = (3.0 / (x[n - 1] - x[n - 2])) * (*ypn - (V[n - 1] - V[n - 2]) / (x[n - 1] - x[n - 2]));
+    }
+    y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0);
+    for (int i = n - 2; i >= 0; --i) y2[i] = y2[i] * y2[i + 1] + u[i];
+    // natural ends: the slope of the spline at the end node (splines.f90:123-183;
+    // at x(n) the last interval is used)
+    auto slope = [&](int j, double r) {
+        const double h = x[j + 1] - x[j], h6 = h / 6.0;
+        const double A = (x[j + 1] - r) / h, B = 1.0 - A;
+        return -1.0 / h * V[j] + 1.0 / h * V[j + 1] + (1.0 - 3.0 * A * A) * h6 * y2[j] +
+               (3.0 * B * B - 1.0) * h6 * y2[j + 1];
+    };
+    if (*yp1 > 0.99e30) *yp1 = slope(0, x[0]);
+    if (*ypn > 0.99e30) *ypn = slope(n - 2, x[n - 1]);
+}
+
+namespace {
+
+// splines.f90:35-121 (value) and 123-183 (derivative), for r < rcut
+int spline_interval(const orc_family *f, double r) {
+    int j = 0;
+    while (j < f->n - 2 && !(r < f->x[j + 1])) ++j;
+    return j;
+}
+double spline_value(const orc_family *f, double r) {
+    const int n = f->n;
+    if (r < f->x[0]) return f->V[0] + (r - f->x[0]) * f->yp1;
+    if (r > f->x[n - 1]) return f->V[n - 1] + (r - f->x[n - 1]) * f->ypn;
+    const int j = spline_interval(f, r);
+    const double h = f->x[j + 1] - f->x[j], h26 = h * h / 6.0;
+    const double A = (f->x[j + 1] - r) / h, B = 1.0 - A;
+    const double C = (A * A * A - A) * h26, D = (B * B * B - B) * h26;
+    return A * f->V[j] + B * f->V[j + 1] + C * f->y2[j] + D * f->y2[j + 1];
+}
+double spline_slope(const orc_family *f, double r) {
+    const int n = f->n;
+    if (r < f->x[0]) return f->yp1;
+    if (r > f->x[n - 1]) return f->ypn;
+    const int j = spline_interval(f, r);
+    const double h = f->x[j + 1] - f->x[j], h6 = h / 6.0;
+    const double A = (f->x[j + 1] - r) / h, B = 1.0 - A;
+    return -1.0 / h * f->V[j] + 1.0 / h * f->V[j + 1] + (1.0 - 3.0 * A * A) * h6 * f->y2[j] +
+           (3.0 * B * B - 1.0) * h6 * f->y2[j + 1];
+}
+
+// gap.f90:1049-1112, d = 3, q = 1 (j = 3)
+double cov_pp(double r) {
+    if (r >= 1.0) return 0.0;
+    if (r <= 0.0) return 1.0;
+    const double om = 1.0 - r;
+    return om * om * om * om * (4.0 * r + 1.0);
+}
+double cov_pp_der(double r) {
+    if (r >= 1.0 || r <= 0.0) return 0.0;
+    const double om = 1.0 - r;
+    return (-4.0 * om * om * om * (4.0 * r + 1.0) + om * om * om * om * 4.0) / r;
+}
+
+}  // namespace
+
+// gap.f90:400-563 (2b), 565-721 (core_pot), 724-1042 (3b)
+void orc_family_energy_forces(const orc_family *f, int n_sites, const int *n_neigh,
+                              const int *neighbors_list, const double *rjs, const double *xyz,
+                              const int *species, const int *neighbor_species, int n_sites0,
+                              double *energies, double *forces, double *virial) {
+    const double pi = std::acos(-1.0);
+    const double buffer = 0.5;   // gap_backend_cpu.f90:152,252 pass 0.5d0
+    for (int i = 0; i < n_sites; ++i) energies[i] = 0.0;
+    for (int i = 0; i < 3 * n_sites0; ++i) forces[i] = 0.0;
+    for (int q = 0; q < 9; ++q) virial[q] = 0.0;
+    auto vir_add = [&](const double *fv, const double *x, double w) {
+        for (int k1 = 0; k1 < 3; ++k1)
+            for (int k2 = 0; k2 < 3; ++k2)
+                virial[k1 + 3 * k2] += w * (fv[k1] * x[k2] + fv[k2] * x[k1]);
+    };
+    if (f->kind == 1 || f->kind == 3) {
+        const int sp1 = f->sp[0], sp2 = f->sp[1];
+        const double rcut = f->kind == 1 ? f->rcut : f->x[f->n - 1];
+        int64_t k = 0;
+        for (int i = 0; i < n_sites; ++i) {
+            if (species[i] != sp1 && species[i] != sp2) {
+                k += n_neigh[i];
+                continue;
+            }
+            ++k;
+            for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+                const int ns = neighbor_species[k];
+                if (!((species[i] == sp1 && ns == sp2) || (species[i] == sp2 && ns == sp1))) continue;
+                const double r = rjs[k];
+                if (!(r < rcut)) continue;
+                const double *x = xyz + 3 * k;
+                double fv[3];
+                if (f->kind == 1) {
+                    double fc = 1.0, dfc = 0.0;
+                    if (!(r < rcut - buffer)) {
+                        fc = (std::cos(pi * (r - rcut + buffer) / buffer) + 1.0) / 2.0;
+                        dfc = pi / 2.0 / buffer * std::sin(pi * (r - rcut + buffer) / buffer);
+                    }
+                    const double d2 = f->delta * f->delta, s2 = f->sigma[0] * f->sigma[0];
+                    for (int s = 0; s < f->n; ++s) {
+                        const double ex = std::exp(-0.5 * (r - f->Qs[s]) * (r - f->Qs[s]) / s2);
+                        energies[i] += d2 * f->alphas[s] * f->cutoff[s] * fc * ex;
+                        const double g = -2.0 * d2 * f->alphas[s] * f->cutoff[s] * ex *
+                                         ((r - f->Qs[s]) / s2 * fc + dfc);
+                        for (int q = 0; q < 3; ++q) fv[q] = g * x[q] / r;
+                        for (int q = 0; q < 3; ++q) forces[3 * i + q] += fv[q];
+                        vir_add(fv, x, -0.25);
+                    }
+                } else {
+                    energies[i] += 0.5 * spline_value(f, r);
+                    const double dv = spline_slope(f, r);
+                    for (int q = 0; q < 3; ++q) fv[q] = dv * x[q] / r;
+                    for (int q = 0; q < 3; ++q) forces[3 * i + q] += fv[q];
+                    vir_add(fv, x, -0.25);
+                }
+            }
+        }
+        return;
+    }
+    // angle_3b
+    const int sp0 = f->sp[0], sp1 = f->sp[1], sp2 = f->sp[2];
+    const double rcut = f->rcut;
+    const int ns = f->n;
+    const double *Q1 = f->Qs, *Q2 = f->Qs + ns, *Q3 = f->Qs + 2 * ns;
+    const double s1 = f->sigma[0] * f->sigma[0], s2 = f->sigma[1] * f->sigma[1],
+                 s3 = f->sigma[2] * f->sigma[2];
+    std::vector<double> pref(ns), rr(ns), kern(ns), kder(ns), dq1(ns), dq2(ns), dq3(ns);
+    for (int s = 0; s < ns; ++s) pref[s] = 2.0 * f->delta * f->delta * f->alphas[s] * f->cutoff[s];
+    int64_t k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp0) {
+            k += n_neigh[i];
+            continue;
+        }
+        const int64_t kself = k;
+        ++k;
+        const int i3 = (neighbors_list[kself] - 1) % n_sites0;
+        for (int j = 1; j < n_neigh[i]; ++j) {
+            const int64_t kj = kself + j;
+            const double r12 = rjs[kj];
+            const int nsj = neighbor_species[kj];
+            if ((nsj != sp1 && nsj != sp2) || r12 > rcut) continue;
+            const int j3 = (neighbors_list[kj] - 1) % n_sites0;
+            const double *x12 = xyz + 3 * kj;
+            double u12[3] = {x12[0] / r12, x12[1] / r12, x12[2] / r12};
+            for (int j2 = j + 1; j2 < n_neigh[i]; ++j2) {
+                const int64_t k2 = kself + j2;
+                const double r13 = rjs[k2];
+                const int nsk = neighbor_species[k2];
+                if (!(((nsj == sp1 && nsk == sp2) || (nsj == sp2 && nsk == sp1)) && r13 < rcut)) continue;
+                const int k3 = (neighbors_list[k2] - 1) % n_sites0;
+                const double *x13 = xyz + 3 * k2;
+                double u13[3] = {x13[0] / r13, x13[1] / r13, x13[2] / r13};
+                double x23[3] = {x13[0] - x12[0], x13[1] - x12[1], x13[2] - x12[2]};
+                const double r23 = std::sqrt(x23[0] * x23[0] + x23[1] * x23[1] + x23[2] * x23[2]);
+                double u23[3] = {x23[0] / r23, x23[1] / r23, x23[2] / r23};
+                if (!(r12 < rcut && r13 < rcut)) continue;
+                double fc12 = 1.0, fc13 = 1.0, df12[3] = {0, 0, 0}, df13[3] = {0, 0, 0};
+                if (!(r12 < rcut - buffer)) {
+                    fc12 = (std::cos(pi * (r12 - rcut + buffer) / buffer) + 1.0) / 2.0;
+                    const double t = std::sin(pi * (r12 - rcut + buffer) / buffer) / 2.0 * pi / buffer;
+                    for (int q = 0; q < 3; ++q) df12[q] = t * u12[q];
+                }
+                if (!(r13 < rcut - buffer)) {
+                    fc13 = (std::cos(pi * (r13 - rcut + buffer) / buffer) + 1.0) / 2.0;
+                    const double t = std::sin(pi * (r13 - rcut + buffer) / buffer) / 2.0 * pi / buffer;
+                    for (int q = 0; q < 3; ++q) df13[q] = t * u13[q];
+                }
+                const double fc = fc12 * fc13;
+                double dfc[3];
+                for (int q = 0; q < 3; ++q) dfc[q] = fc12 * df13[q] + fc13 * df12[q];
+                const double qv1 = r12 + r13, qv2 = (r12 - r13) * (r12 - r13), qv3 = r23;
+                for (int s = 0; s < ns; ++s) {
+                    double t = (qv1 - Q1[s]) * (qv1 - Q1[s]) / s1;
+                    t += (qv2 - Q2[s]) * (qv2 - Q2[s]) / s2;
+                    t += (qv3 - Q3[s]) * (qv3 - Q3[s]) / s3;
+                    rr[s] = std::sqrt(t);
+                    dq1[s] = (qv1 - Q1[s]) / s1;
+                    dq2[s] = (qv2 - Q2[s]) / s2;
+                    dq3[s] = (qv3 - Q3[s]) / s3;
+                }
+                double esum = 0.0;
+                if (!f->kernel_pol) {
+                    for (int s = 0; s < ns; ++s) kern[s] = pref[s] * std::exp(-0.5 * rr[s] * rr[s]);
+                } else {
+                    for (int s = 0; s < ns; ++s) {
+                        kern[s] = pref[s] * cov_pp(rr[s]);
+                        kder[s] = pref[s] * cov_pp_der(rr[s]);
+                    }
+                }
+                for (int s = 0; s < ns; ++s) esum += kern[s];
+                energies[i] += fc * esum;
+                double f1[3], f2[3], f3[3];
+                for (int l = 0; l < 3; ++l) {
+                    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                    for (int s = 0; s < ns; ++s) {
+                        const double d1 = dq1[s] * (u12[l] + u13[l]) +
+                                          dq2[s] * 2.0 * (r12 - r13) * (u12[l] - u13[l]);
+                        const double d2 = -dq1[s] * u12[l] - dq2[s] * 2.0 * (r12 - r13) * u12[l] +
+                                          dq3[s] * u23[l];
+                        const double d3 = -dq1[s] * u13[l] - dq2[s] * 2.0 * (r13 - r12) * u13[l] -
+                                          dq3[s] * u23[l];
+                        if (!f->kernel_pol) {
+                            a1 += kern[s] * (dfc[l] + fc * d1);
+                            a2 += kern[s] * (-fc13 * df12[l] + fc * d2);
+                            a3 += kern[s] * (-fc12 * df13[l] + fc * d3);
+                        } else {
+                            a1 += kern[s] * dfc[l] - kder[s] * fc * d1;
+                            a2 += -kern[s] * fc13 * df12[l] - kder[s] * fc * d2;
+                            a3 += -kern[s] * fc12 * df13[l] - kder[s] * fc * d3;
+                        }
+                    }
+                    f1[l] = -a1;
+                    f2[l] = -a2;
+                    f3[l] = -a3;
+                }
+                for (int q = 0; q < 3; ++q) {
+                    forces[3 * i3 + q] += f1[q];
+                    forces[3 * j3 + q] += f2[q];
+                    forces[3 * k3 + q] += f3[q];
+                }
+                vir_add(f2, x12, 0.5);
+                vir_add(f3, x13, 0.5);
+            }
+        }
+        k = kself + n_neigh[i];
+    }
+}
+
+int orc_evaluate_full(int n_sites, const double *positions, const int *species, const double *a,
+                      const double *b, const double *c, int n_blocks, const orc_gap_block *blocks,
+                      int n_families, const orc_family *families, const double *e0_by_species,
+                      int n_species_total, double neighbors_buffer, double max_gbytes,
+                      int site_beg, int site_end, double *energies, double *forces,
+                      double *virial, int64_t *n_pairs_out) {
     if (site_beg < 0) site_beg = 0;
     if (site_end > n_sites || site_end < 0) site_end = n_sites;
     double rcut_max = 0.0;
     for (int b = 0; b < n_blocks; ++b)
         for (int s = 0; s < blocks[b].hypers.n_species; ++s)
             rcut_max = std::max(rcut_max, blocks[b].hypers.rcut_hard[s]);
+    for (int q = 0; q < n_families; ++q)
+        rcut_max = std::max(rcut_max, families[q].kind == 3 ? families[q].x[families[q].n - 1]
+                                                             : families[q].rcut);
     rcut_max += neighbors_buffer;
     int indices[3];
     orc_number_of_unit_cells(a, b, c, rcut_max, indices);
@@ -1103,6 +1370,27 @@ int orc_evaluate_range(int n_sites, const double *positions, const int *species,
     for (int i = 0; i < n_sites; ++i) energies[i] += e_soap[i];
     for (size_t q = 0; q < f_soap.size(); ++q) forces[q] = f_soap[q];
     for (int q = 0; q < 9; ++q) virial[q] = v_soap[q];
+    // gap_backend_cpu.f90:79-267: every family over this rank's sites and pairs,
+    // added to the totals (neighbor_species from the supercell species)
+    if (n_families > 0) {
+        const int nr = site_end - site_beg;
+        const int64_t p0 = pstart[site_beg];
+        std::vector<double> fe(n_sites), ff(3 * (size_t)n_sites);
+        double fv[9];
+        for (int q = 0; q < n_families; ++q) {
+            orc_family_energy_forces(&families[q], nr, n_neigh.data() + site_beg, nl.data() + p0,
+                                     rjs.data() + p0, xyz.data() + 3 * p0, species + site_beg,
+                                     nspec.data() + p0, n_sites, fe.data(), ff.data(), fv);
+            for (int i = 0; i < nr; ++i) energies[site_beg + i] += fe[i];
+            if (families[q].kind == 2) {
+                for (size_t t = 0; t < ff.size(); ++t) forces[t] += ff[t];
+            } else {
+                for (int i = 0; i < nr; ++i)
+                    for (int t = 0; t < 3; ++t) forces[3 * (site_beg + i) + t] += ff[3 * i + t];
+            }
+            for (int t = 0; t < 9; ++t) virial[t] += fv[t];
+        }
+    }
     return 0;
 }
 

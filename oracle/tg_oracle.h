@@ -171,6 +171,45 @@ int orc_evaluate_range(int n_sites, const double *positions, const int *species,
 
 int orc_set_threads(int n);
 
+/* ---- the other GAP families: distance_2b, angle_3b, core_pot ---------- */
+/* One family (types.f90 distance_2b / angle_3b / core_pot). Species are global
+ * ids (1-based positions in the input's species_types). */
+typedef struct {
+    int kind;               /* 1 = distance_2b, 2 = angle_3b, 3 = core_pot               */
+    int sp[3];              /* 2b, core_pot: species1, species2; 3b: center, 1, 2         */
+    double delta;           /* 2b, 3b                                                     */
+    double sigma[3];        /* 2b: sigma[0]; 3b: sigma(1:3)                               */
+    double rcut;            /* 2b, 3b; core_pot uses maxval(x)                            */
+    int kernel_pol;         /* 3b: 1 = kernel_type "pol", 0 = "exp"                       */
+    int n;                  /* sparse points (2b, 3b) or table nodes (core_pot)           */
+    const double *Qs;       /* 2b: (n); 3b: Qs(n, 3) column-major                          */
+    const double *alphas;   /* (n) */
+    const double *cutoff;   /* (n) */
+    const double *x, *V, *y2;   /* core_pot: nodes, values, spline second derivatives     */
+    double yp1, ypn;        /* core_pot end slopes (after the natural-end replacement)     */
+} orc_family;
+
+/* read_files.f90:5454-5505: spline second derivatives y2(n) of (x, V); end
+ * slopes > 0.99e30 mean a natural end and are replaced by the spline's slope. */
+void orc_core_pot_spline(int n, const double *x, const double *V, double *yp1, double *ypn,
+                         double *y2);
+/* gap.f90:400-1042 for one family over n_sites sites (n_neigh, neighbors_list,
+ * rjs, xyz as build_neighbors_list returns them; species of the sites,
+ * neighbor_species of the pairs). energies(n_sites) assigned; forces(3, n_sites0)
+ * and virial(3, 3) zeroed and accumulated (2b and core_pot on the sites, 3b on
+ * the three atoms of each triplet, by index mod n_sites0). */
+void orc_family_energy_forces(const orc_family *f, int n_sites, const int *n_neigh,
+                              const int *neighbors_list, const double *rjs, const double *xyz,
+                              const int *species, const int *neighbor_species, int n_sites0,
+                              double *energies, double *forces, double *virial);
+/* orc_evaluate_range with the families added (gap_backend_cpu.f90:79-267). */
+int orc_evaluate_full(int n_sites, const double *positions, const int *species, const double *a,
+                      const double *b, const double *c, int n_blocks, const orc_gap_block *blocks,
+                      int n_families, const orc_family *families, const double *e0_by_species,
+                      int n_species_total, double neighbors_buffer, double max_gbytes,
+                      int site_beg, int site_end, double *energies, double *forces,
+                      double *virial, int64_t *n_pairs_out);
+
 #ifdef __cplusplus
 }
 #endif

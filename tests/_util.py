@@ -71,3 +71,27 @@ def sparse_block(h: SoapTurboHypers, n_sparse: int, seed: int, n_atoms=216, L=12
     pick = rng.choice(len(Q), size=n_sparse, replace=False)
     alphas = rng.normal(0.0, sigma_alpha, size=n_sparse)
     return GapBlock(h, Q[pick], alphas, delta=delta, zeta=zeta)
+
+
+def make_families(seed=0, rcut2=4.0, rcut3=3.2):
+    """Seeded distance_2b (C-H), angle_3b (C centre, exp; H centre, pol) and
+    core_pot (C-C) families on species C = 1, H = 2, with sparse points spread
+    over the ranges their descriptors take in the C/H test structures."""
+    from turbogap_b200 import families as FM
+    rng = np.random.default_rng(seed)
+    n2 = 24
+    f2 = FM.Distance2b((1, 2), 0.6, 0.5, rcut2, rng.uniform(0.9, rcut2, n2),
+                       rng.normal(0, 0.05, n2), rng.uniform(0.5, 1.0, n2))
+    def sparse3(n):
+        r1 = rng.uniform(1.0, rcut3, n)
+        r2 = rng.uniform(1.0, rcut3, n)
+        return np.stack([r1 + r2, (r1 - r2) ** 2, rng.uniform(1.0, r1 + r2)], axis=1)
+    n3 = 40
+    f3e = FM.Angle3b((1, 1, 2), 0.3, [1.5, 2.0, 1.2], rcut3, sparse3(n3), rng.normal(0, 0.05, n3),
+                     rng.uniform(0.5, 1.0, n3), "exp")
+    f3p = FM.Angle3b((2, 1, 1), 0.2, [4.0, 4.0, 4.0], rcut3, sparse3(n3), rng.normal(0, 0.05, n3),
+                     rng.uniform(0.5, 1.0, n3), "pol")
+    x = np.linspace(0.6, 2.6, 21)
+    fc = FM.CorePot.from_table((1, 1), x, 3.0 * np.exp(-2.0 * x) / x, 1e50, 0.0,
+                               cutoff=2.6, buffer=0.5)
+    return [f2, f3e, f3p, fc]

@@ -243,13 +243,15 @@ def test_deck_loader(gapdir):
     d, g, data = gapdir
     (d / "input").write_text(DECK)
     (d / "atoms.xyz").write_text(XYZ.split("2\nLattice")[0])
-    with pytest.raises(NotImplementedError, match="distance_2b"):
-        D.Deck(str(d / "input"))
-    text = (d / "ch.gap").read_text()
-    beg = text.index("gap_beg distance_2b")
-    (d / "ch.gap").write_text(text[:beg] + text[text.index("gap_end", beg) + 8:])
+    (d / "a2b.dat").write_text("0.5 1.0\n-0.25 0.75\n0.125 0.5\n")
+    (d / "d2b.dat").write_text("1.5\n2.0\n2.5\n")
     with pytest.warns(UserWarning):
         dk = D.Deck(str(d / "input"))
+    (f2,) = dk.families
+    assert f2.kind == "distance_2b" and f2.species == (1, 2)
+    assert (f2.delta, f2.sigma, f2.rcut) == (0.5, 0.8, 4.5)
+    assert f2.Qs.tolist() == [1.5, 2.0, 2.5] and f2.cutoff.tolist() == [1.0, 0.75, 0.5]
+    assert D.family_key(f2) >= 0x40000000 > D.block_key(dk.blocks[0])
     assert [b.hypers.central_species for b in dk.blocks] == [1, 2]
     fr = dk.frames[0]
     ids = dk.species_ids(fr)
@@ -269,3 +271,39 @@ def test_drawn_velocities():
         T = F.instant_temperature(0.5 * float(np.sum(m[:, None] * v * v)), len(m))
         assert abs(T - 600.0) < (1e-9 if dist == "uniform" else 60.0)
     assert not D.draw_velocities(m[:1], 600.0, "uniform", 0).any()
+
+
+GAP3 = """gap_beg angle_3b
+species_center = C
+species1 = C
+species2 = H
+delta = 0.01
+sigma = 4. 4. 3.
+rcut = 3.5
+kernel_type = "pol"
+desc_sparse = 'd3b.dat'
+alphas_sparse = 'a3b.dat'
+gap_end
+
+gap_beg core_pot
+species1 = H
+species2 = H
+core_pot_file = 'cp.dat'
+gap_end core_pot
+"""
+
+
+def test_three_body_and_core_pot_blocks(tmp_path):
+    (tmp_path / "f.gap").write_text(GAP3)
+    (tmp_path / "a3b.dat").write_text("0.5 1.0\n-0.25 0.5\n")
+    (tmp_path / "d3b.dat").write_text("3.0\n0.25\n2.0\n4.0\n1.0\n2.5\n")
+    (tmp_path / "cp.dat").write_text("4 1.0e50 0.0\n0.5 8.0\n1.0 4.0\n1.5 2.0\n2.0 0.0\n")
+    g = F.read_gap_file(str(tmp_path / "f.gap"))
+    f3 = g.angle_3b[0].load(["C", "H"], str(tmp_path))
+    assert f3.species == (1, 1, 2) and f3.kernel_type == "pol" and f3.sigma == [4.0, 4.0, 3.0]
+    assert f3.Qs.tolist() == [[3.0, 0.25, 2.0], [4.0, 1.0, 2.5]]     # 3 records per point
+    assert f3.alphas.tolist() == [0.5, -0.25] and f3.cutoff.tolist() == [1.0, 0.5]
+    cp = g.core_pot[0].load(["C", "H"], str(tmp_path), core_pot_cutoff=1.5, core_pot_buffer=0.5)
+    assert cp.species == (2, 2) and cp.x.tolist() == [0.5, 1.0, 1.5]
+    assert cp.V[:2].tolist() == [8.0, 4.0] and abs(cp.V[2]) < 1e-15   # tapered to 0 at 1.5
+    assert cp.yp1 == 1e50 and cp.ypn == 0.0 and g.rcut_max == 3.5

@@ -45,6 +45,14 @@ class TgSoapHypers(C.Structure):
     ]
 
 
+class TgFamily(C.Structure):
+    _pd = C.POINTER(C.c_double)
+    _fields_ = [("kind", C.c_int32), ("species", C.c_int32 * 3), ("delta", C.c_double),
+                ("sigma", C.c_double * 3), ("rcut", C.c_double), ("kernel_type", C.c_int32),
+                ("n", C.c_int32), ("Qs", _pd), ("alphas", _pd), ("cutoff", _pd), ("x", _pd),
+                ("V", _pd), ("yp1", C.c_double), ("ypn", C.c_double)]
+
+
 # (name, restype, argtypes) of every C-ABI entry point in include/tgb200.h and
 # include/tgb200_test.h.
 _vp = C.c_void_p
@@ -59,6 +67,8 @@ SIGNATURES = [
     ("tg_get_gap_soap", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, dp, dp, dp]),
     ("tg_get_soap", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, dp,
                               C.POINTER(C.c_int32)]),
+    ("tg_family_begin", C.c_int, [C.c_int32, C.POINTER(TgFamily)]),
+    ("tg_get_family", C.c_int, [C.c_int32, C.c_int32, C.c_int32, ip, ip, dp, dp, ip, dp, dp, dp]),
     ("tg_build_neighbors_list", C.c_int, [C.c_int32, dp, C.c_int32, dp, dp, dp, C.c_double, ip,
                                           ip, _vp, C.c_int64, ip, ip, dp, dp, dp, dp, ip,
                                           C.POINTER(C.c_int64)]),

@@ -104,6 +104,56 @@ def soap_backend_end() -> None:
     check(lib().tg_soap_end())
 
 
+_FAMILY_KIND = {"distance_2b": 1, "angle_3b": 2, "core_pot": 3}
+
+
+def family_begin(family, key: int) -> None:
+    """Upload a distance_2b / angle_3b / core_pot family (turbogap_b200.families)
+    under ``key``; engines created with the key evaluate it every step."""
+    f = _lib.TgFamily()
+    f.kind = _FAMILY_KIND[family.kind]
+    for q, z in enumerate(family.species):
+        f.species[q] = int(z)
+    keep = []
+
+    def arr(v):
+        a = _f64(v)
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    if family.kind == "core_pot":
+        f.n = len(family.x)
+        f.x, f.V = arr(family.x), arr(family.V)
+        f.yp1, f.ypn = float(family.yp1), float(family.ypn)
+    else:
+        f.delta = float(family.delta)
+        sig = np.atleast_1d(np.asarray(family.sigma, dtype=np.float64))
+        for q in range(len(sig)):
+            f.sigma[q] = float(sig[q])
+        f.rcut = float(family.rcut)
+        f.kernel_type = 1 if getattr(family, "kernel_type", "exp") == "pol" else 0
+        f.n = len(family.alphas)
+        Q = np.asarray(family.Qs, dtype=np.float64)
+        f.Qs = arr(Q.T.reshape(-1) if Q.ndim == 2 else Q)   # Qs(n, 3) column-major
+        f.alphas, f.cutoff = arr(family.alphas), arr(family.cutoff)
+    check(lib().tg_family_begin(int(key), C.byref(f)))
+
+
+def get_family(key: int, n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_all,
+               energies0: Optional[np.ndarray] = None, forces0: Optional[np.ndarray] = None,
+               virial: Optional[np.ndarray] = None):
+    """add_*_contribution of one family for one batch: ADDS to energies0
+    (n_total_sites), forces0 (n_total_sites, 3) and virial (3, 3, column-major
+    order), made here when None, and returns them."""
+    e = np.zeros(n_total_sites) if energies0 is None else energies0
+    f = np.zeros((n_total_sites, 3)) if forces0 is None else forces0
+    v = np.zeros(9) if virial is None else virial.T.reshape(-1).copy()
+    check(lib().tg_get_family(int(key), int(n_total_sites), len(n_neigh0), _i32(n_neigh0),
+                              _i32(neighbors_list0), _f64(rjs0), _f64(xyz0), _i32(species_all),
+                              e, f, v))
+    return e, f, v.reshape(3, 3).T.copy()
+
+
 def get_gap_soap(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_batch,
                  species_all, energies0: Optional[np.ndarray] = None,
                  forces0: Optional[np.ndarray] = None):

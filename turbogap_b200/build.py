@@ -30,6 +30,7 @@ SOURCES = {
     "tgb_capi.cu": [],
     "tgb_noalloc.cu": ["--fmad=false"],
     "tgb_comm.cu": [],
+    "tgb_family.cu": [],
 }
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

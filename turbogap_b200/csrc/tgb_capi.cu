@@ -5,6 +5,7 @@
 #include "tgb_gemm.cuh"
 #include "tgb_mlp.cuh"
 #include "tgb_comm.cuh"
+#include "tgb_family.cuh"
 #include "tgb_neighbors.cuh"
 #include "tgb_soap.cuh"
 
@@ -442,6 +443,7 @@ struct Context {
     int device = -1;
     cudaStream_t st = nullptr;
     std::map<int, std::unique_ptr<Block>> blocks;
+    std::map<int, std::unique_ptr<Family>> families;   // 2b / 3b / core_pot, same key space
     std::map<int, std::unique_ptr<Workspace>> ws;
     Block *current = nullptr;
     DBuf<unsigned> err;
@@ -542,6 +544,8 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
                   const double *alphas, double delta, double zeta, int32_t precision) {
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
+    TGB_CHECK(!C.families.count(block_key), TG_ERR_ARG, "key %d already names a 2b/3b/core_pot family",
+              block_key);
     auto it = C.blocks.find(block_key);
     if (it != C.blocks.end() && it->second->M == n_sparse && it->second->precision == precision) {
         C.current = it->second.get();
@@ -895,6 +899,84 @@ int tg_get_gap_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_ne
     return TG_OK;
 }
 
+int tg_family_begin(int32_t key, const tg_family *family) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(family, TG_ERR_ARG, "null family");
+    TGB_CHECK(!C.blocks.count(key), TG_ERR_ARG, "key %d already names a soap_turbo block", key);
+    auto &slot = C.families[key];
+    if (!slot) slot = std::make_unique<Family>();
+    TGB_CUDA(cudaDeviceSynchronize());   // an engine may be using the old parameters
+    const int rc = family_create(*family, *slot);
+    if (rc != TG_OK) {
+        C.families.erase(key);
+        return rc;
+    }
+    slot->key = key;
+    return TG_OK;
+}
+
+int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                  const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                  const int32_t *species_all, double *energies0, double *forces0, double *virial) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    auto fi = C.families.find(key);
+    TGB_CHECK(fi != C.families.end(), TG_ERR_STATE, "family key %d was never begun", key);
+    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0, TG_ERR_ARG, "bad site counts");
+    if (n_sites0 == 0) return TG_OK;
+    TGB_CHECK(n_neigh0 && neighbors_list0 && rjs0 && xyz0 && species_all, TG_ERR_ARG,
+              "null neighbour arrays");
+    // host: list offsets, 0-based neighbours and the site of each list (its self pair)
+    std::vector<int64_t> ps(n_sites0 + 1, 0);
+    for (int i = 0; i < n_sites0; ++i) {
+        TGB_CHECK(n_neigh0[i] >= 1, TG_ERR_ARG, "site %d has no self pair", i);
+        ps[i + 1] = ps[i] + n_neigh0[i];
+    }
+    const int64_t P = ps[n_sites0];
+    std::vector<int> nb(P), rows(n_sites0), atoms(n_sites0);
+    for (int64_t k = 0; k < P; ++k) {
+        TGB_CHECK(neighbors_list0[k] >= 1, TG_ERR_ARG, "neighbour indices are 1-based");
+        nb[k] = neighbors_list0[k] - 1;
+    }
+    for (int i = 0; i < n_sites0; ++i) {
+        rows[i] = i;
+        atoms[i] = nb[ps[i]] % n_total_sites;
+    }
+    cudaStream_t st = C.st;
+    DBuf<int64_t> d_ps;
+    DBuf<int> d_nb, d_rows, d_atoms, d_sp;
+    DBuf<double> d_rjs, d_xyz, d_en, d_fo, d_vir;
+    TGB_TRY(d_ps.ensure(n_sites0 + 1)); TGB_TRY(d_nb.ensure(P)); TGB_TRY(d_rows.ensure(n_sites0));
+    TGB_TRY(d_atoms.ensure(n_sites0)); TGB_TRY(d_sp.ensure(n_total_sites)); TGB_TRY(d_rjs.ensure(P));
+    TGB_TRY(d_xyz.ensure(3 * (size_t)P)); TGB_TRY(d_en.ensure(n_total_sites));
+    TGB_TRY(d_fo.ensure(3 * (size_t)n_total_sites)); TGB_TRY(d_vir.ensure(9));
+    TGB_CUDA(cudaMemcpyAsync(d_ps.p, ps.data(), sizeof(int64_t) * (n_sites0 + 1), cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_nb.p, nb.data(), sizeof(int) * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_rows.p, rows.data(), sizeof(int) * n_sites0, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_atoms.p, atoms.data(), sizeof(int) * n_sites0, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_sp.p, species_all, sizeof(int) * n_total_sites, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_rjs.p, rjs0, sizeof(double) * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemcpyAsync(d_xyz.p, xyz0, sizeof(double) * 3 * P, cudaMemcpyHostToDevice, st));
+    TGB_CUDA(cudaMemsetAsync(d_en.p, 0, sizeof(double) * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(d_fo.p, 0, sizeof(double) * 3 * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(d_vir.p, 0, sizeof(double) * 9, st));
+    SiteArgs S{n_sites0, d_rows.p, d_atoms.p, d_ps.p, d_nb.p, d_xyz.p, d_sp.p};
+    TGB_TRY(evaluate_family(*fi->second, S, d_rjs.p, n_total_sites, d_en.p, d_fo.p, d_vir.p, st));
+    std::vector<double> en(n_total_sites), fo(3 * (size_t)n_total_sites), vr(9);
+    TGB_CUDA(cudaMemcpyAsync(en.data(), d_en.p, sizeof(double) * n_total_sites, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(fo.data(), d_fo.p, sizeof(double) * 3 * n_total_sites, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaMemcpyAsync(vr.data(), d_vir.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    if (energies0)
+        for (int i = 0; i < n_total_sites; ++i) energies0[i] += en[i];
+    if (forces0)
+        for (size_t q = 0; q < fo.size(); ++q) forces0[q] += fo[q];
+    if (virial)
+        for (int q = 0; q < 9; ++q) virial[q] += vr[q];
+    return TG_OK;
+}
+
 int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
                 const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                 const int32_t *species_batch, const int32_t *species_all, double *soap,
@@ -1050,6 +1132,13 @@ struct BlockRun {
     int n_sites = 0;
 };
 
+// a 2b / 3b / core_pot family of an engine and its central sites
+struct FamilyRun {
+    Family *f = nullptr;
+    DBuf<int> sites;
+    int n_sites = 0;
+};
+
 struct Engine {
     int n = 0, nsc = 0, indices[3] = {1, 1, 1};
     bool use_cells = false;
@@ -1062,6 +1151,7 @@ struct Engine {
     DBuf<unsigned> err;
     NeighborList nl;
     std::vector<std::unique_ptr<BlockRun>> runs;
+    std::vector<std::unique_ptr<FamilyRun>> fams;
     cudaGraphExec_t graph = nullptr;
     double graph_dt = 0.0;
     bool first_step = true;
@@ -1139,6 +1229,13 @@ struct Engine {
                 TGB_CUDA(cudaEventRecord(ev_side[k - 1], side[k - 1]));
                 TGB_CUDA(cudaStreamWaitEvent(st, ev_side[k - 1], 0));
             }
+        // the other GAP families on the same lists (gap_backend_cpu.f90:79-267),
+        // timed with the force pass
+        for (auto &fr : fams) {
+            SiteArgs S{fr->n_sites, fr->sites.p, fr->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            TGB_TRY(evaluate_family(*fr->f, S, nl.rjs, n, en.p, f.p, vir.p, st));
+        }
+        if (!fams.empty()) TGB_MARK(log, PASS_FORCE, st);
         // sharded structure: every rank holds its own sites' share; the sum over
         // ranks is the whole (turbogap.f90:1876-1885)
         if (comm) TGB_TRY(comm_allreduce3(comm, f.p, 3 * (size_t)n, en.p, n, vir.p, 9, st));
@@ -1165,6 +1262,15 @@ struct Engine {
                                          cudaMemcpyHostToDevice, st));
             TGB_TRY(run->w->ensure(*b, run->n_sites));
             if (run->mix) TGB_TRY(run->mix->ensure(*b, run->n_sites));
+        }
+        for (auto &fr : fams) {
+            std::vector<int> s;
+            family_sites(*fr->f, species_h.data(), site_beg, site_end, s);
+            fr->n_sites = (int)s.size();
+            TGB_TRY(fr->sites.ensure(std::max<size_t>(s.size(), 1)));
+            if (!s.empty())
+                TGB_CUDA(cudaMemcpyAsync(fr->sites.p, s.data(), sizeof(int) * s.size(),
+                                         cudaMemcpyHostToDevice, st));
         }
         TGB_CUDA(cudaStreamSynchronize(st));
         return TG_OK;
@@ -1204,8 +1310,10 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     double rcut = 0.0;
     for (int k = 0; k < n_blocks; ++k) {
         auto it = C.blocks.find(block_keys[k]);
-        TGB_CHECK(it != C.blocks.end(), TG_ERR_STATE, "block key %d was never begun", block_keys[k]);
-        rcut = std::max(rcut, it->second->rcut_max);
+        auto fi = C.families.find(block_keys[k]);
+        TGB_CHECK(it != C.blocks.end() || fi != C.families.end(), TG_ERR_STATE,
+                  "block key %d was never begun", block_keys[k]);
+        rcut = std::max(rcut, it != C.blocks.end() ? it->second->rcut_max : fi->second->rcut);
     }
     rcut += neighbors_buffer;   // turbogap_setup.f90:284-285
     E.rcut = rcut;
@@ -1249,6 +1357,13 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     E.site_beg = 0;
     E.site_end = n_atoms;
     for (int k = 0; k < n_blocks; ++k) {
+        auto fi = C.families.find(block_keys[k]);
+        if (fi != C.families.end()) {
+            auto fr = std::make_unique<FamilyRun>();
+            fr->f = fi->second.get();
+            E.fams.push_back(std::move(fr));
+            continue;
+        }
         auto run = std::make_unique<BlockRun>();
         run->b = C.blocks[block_keys[k]].get();
         run->w = std::make_unique<Workspace>();
@@ -1814,6 +1929,8 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
     double rcut = 0.0;
     for (int k = 0; k < n_blocks; ++k) {
         auto it = C.blocks.find(block_keys[k]);
+        TGB_CHECK(!C.families.count(block_keys[k]), TG_ERR_ARG,
+                  "key %d is a 2b/3b/core_pot family: batches take soap_turbo blocks", block_keys[k]);
         TGB_CHECK(it != C.blocks.end(), TG_ERR_STATE, "block key %d was never begun", block_keys[k]);
         rcut = std::max(rcut, it->second->rcut_max);
     }

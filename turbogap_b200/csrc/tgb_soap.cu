@@ -557,29 +557,9 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                     : "d"(va), "d"(vb));
             }
         };
-        // pass 1: |p|
-#pragma unroll
-        for (int l = 0; l < NL; ++l)
-#pragma unroll
-            for (int a = 0; a < NB; ++a)
-#pragma unroll
-                for (int b = a; b < NB; ++b) {
-                    double d[2];
-                    gram(l, a, b, d[0], d[1]);
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int n = 8 * a + g8, n2 = 8 * b + 2 * t4 + e;
-                        if (n > n2) continue;
-                        const double v = n != n2 ? d[e] * 1.4142135623730951 : d[e];
-                        nrm2 += v * v;
-                    }
-                }
-        nrm2 = warp_sum(nrm2);
-        inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
-        // pass 2: q = p/|p|, delta = q - mu, delta . mu. The internal order follows
-        // the Gram blocks (internal_pair): an off-diagonal block's entries sit in lane
-        // order (2 lane + e), so its rows are written as pairs; a diagonal block keeps
-        // its upper triangle row by row.
+        // pass 1: p and |p|. Each Gram block is computed once; p goes to the q row in
+        // fp32 at its internal position (an off-diagonal block's entries in lane order
+        // (2 lane + e), a diagonal block's upper triangle row by row), |p|^2 in FP64.
 #pragma unroll
         for (int l = 0; l < NL; ++l)
 #pragma unroll
@@ -590,33 +570,48 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
                     gram(l, a, b, d[0], d[1]);
                     const int base = l * NP + gram_block_start(a, b, NB);
                     if (a != b) {
-                        const int u = base + 2 * lane;   // even: 16-byte mu pairs
-                        const double2 mu2 = __ldg(reinterpret_cast<const double2 *>(P.mu + u));
-                        const double dl0 = d[0] * 1.4142135623730951 * inv - mu2.x;
-                        const double dl1 = d[1] * 1.4142135623730951 * inv - mu2.y;
-                        off += dl0 * mu2.x + dl1 * mu2.y;
-                        const float f0 = (float)dl0, f1 = (float)dl1;
-                        *reinterpret_cast<float2 *>(qrow + u) = make_float2(f0, f1);
-                        __nv_bfloat16 h0, l0, h1, l1;
-                        bf16_split(f0, h0, l0);
-                        bf16_split(f1, h1, l1);
-                        const __nv_bfloat162 hh = __halves2bfloat162(h0, h1);
-                        *reinterpret_cast<__nv_bfloat162 *>(qs + u) = hh;
-                        if (P.nsplit == 3) {
-                            *reinterpret_cast<__nv_bfloat162 *>(qs + DIM + u) = hh;
-                            *reinterpret_cast<__nv_bfloat162 *>(qs + 2 * DIM + u) =
-                                __halves2bfloat162(l0, l1);
-                        }
+                        const double v0 = d[0] * 1.4142135623730951, v1 = d[1] * 1.4142135623730951;
+                        nrm2 += v0 * v0 + v1 * v1;
+                        *reinterpret_cast<float2 *>(qrow + base + 2 * lane) =
+                            make_float2((float)v0, (float)v1);
                     } else {
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
                             const int j = 2 * t4 + e;
                             if (g8 > j) continue;
                             const double v = g8 != j ? d[e] * 1.4142135623730951 : d[e];
-                            emit(base + g8 * 8 - (g8 * (g8 - 1)) / 2 + (j - g8), v, inv, off);
+                            nrm2 += v * v;
+                            qrow[base + g8 * 8 - (g8 * (g8 - 1)) / 2 + (j - g8)] = (float)v;
                         }
                     }
                 }
+        nrm2 = warp_sum(nrm2);
+        inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+        __syncwarp();   // the warp's p entries are visible to every lane
+        // pass 2, streaming: q = p/|p|, delta = q - mu (fp32 row and bf16 split), delta . mu
+        static_assert(DIM % 4 == 0, "four descriptor entries per lane step");
+        for (int u = 4 * lane; u < DIM; u += 128) {
+            const float4 pv = *reinterpret_cast<const float4 *>(qrow + u);
+            const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + u));
+            const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + u + 2));
+            const double dl0 = (double)pv.x * inv - m0.x, dl1 = (double)pv.y * inv - m0.y;
+            const double dl2 = (double)pv.z * inv - m1.x, dl3 = (double)pv.w * inv - m1.y;
+            off += (dl0 * m0.x + dl1 * m0.y) + (dl2 * m1.x + dl3 * m1.y);
+            const float f0 = (float)dl0, f1 = (float)dl1, f2 = (float)dl2, f3 = (float)dl3;
+            *reinterpret_cast<float4 *>(qrow + u) = make_float4(f0, f1, f2, f3);
+            __nv_bfloat16 h0, l0, h1, l1, h2, l2, h3, l3;
+            bf16_split(f0, h0, l0);
+            bf16_split(f1, h1, l1);
+            bf16_split(f2, h2, l2);
+            bf16_split(f3, h3, l3);
+            __nv_bfloat162 hh[2] = {__halves2bfloat162(h0, h1), __halves2bfloat162(h2, h3)};
+            *reinterpret_cast<uint2 *>(qs + u) = *reinterpret_cast<const uint2 *>(hh);
+            if (P.nsplit == 3) {
+                __nv_bfloat162 ll[2] = {__halves2bfloat162(l0, l1), __halves2bfloat162(l2, l3)};
+                *reinterpret_cast<uint2 *>(qs + DIM + u) = *reinterpret_cast<const uint2 *>(hh);
+                *reinterpret_cast<uint2 *>(qs + 2 * DIM + u) = *reinterpret_cast<const uint2 *>(ll);
+            }
+        }
     } else {
         // pass 1: |p| (FP64)
 #pragma unroll

@@ -8,9 +8,10 @@ step 0, the last step and every ``write_xyz`` steps, holding the positions the
 forces were evaluated at (turbogap_md.f90:357-380). ``run_predict`` evaluates
 every frame of the atoms file (``turbogap predict``).
 
-Decks that need anything else (other GAP families, thermostats, barostats,
-adaptive time steps, compressed descriptors, non-orthorhombic boxes) are
-refused with the keyword that needs it. Velocities drawn here (no velocity
+soap_turbo blocks and the distance_2b, angle_3b and core_pot families run on
+the device. Decks that need anything else (thermostats, barostats, adaptive
+time steps, compressed descriptors, non-orthorhombic boxes) are refused with the
+keyword that needs it. Velocities drawn here (no velocity
 column, or ``randomize_velocities``) follow md.f90:95-158 with numpy's
 generator, so they differ from the reference's random stream.
 """
@@ -35,6 +36,19 @@ def block_key(block: GapBlock) -> int:
     c = zlib.crc32(block.alphas.tobytes(), c)
     c = zlib.crc32(repr((vars(h), float(block.delta), float(block.zeta))).encode(), c)
     return int(c & 0x3FFFFFFF) + 1
+
+
+def family_key(f) -> int:
+    """A content key for a 2b / 3b / core_pot family (disjoint from block keys
+    in practice: a different hash input)."""
+    c = zlib.crc32(repr((f.kind, tuple(f.species))).encode())
+    for name in ("Qs", "alphas", "cutoff", "x", "V"):
+        if hasattr(f, name):
+            c = zlib.crc32(np.ascontiguousarray(getattr(f, name)).tobytes(), c)
+    for name in ("delta", "sigma", "rcut", "kernel_type", "yp1", "ypn"):
+        if hasattr(f, name):
+            c = zlib.crc32(repr(getattr(f, name)).encode(), c)
+    return int(c & 0x3FFFFFFF) + 0x40000000
 
 
 def _remove_cm_vel(v: np.ndarray, m: np.ndarray) -> np.ndarray:
@@ -70,18 +84,17 @@ class Deck:
         if d.pot_file is None or d.atoms_file is None:
             raise ValueError("the input file needs pot_file and atoms_file")
         self.gap = F.read_gap_file(os.path.join(self.base, d.pot_file))
-        other = [b.kind for b in self.gap.distance_2b + self.gap.angle_3b + self.gap.core_pot]
-        if other:
-            raise NotImplementedError(f"{sorted(set(other))} blocks are not on the device path "
-                                      "(only soap_turbo is)")
-        if not self.gap.soap_turbo:
-            raise ValueError(f"{d.pot_file} has no soap_turbo block")
+        raw = self.gap.distance_2b + self.gap.angle_3b + self.gap.core_pot
+        if not self.gap.soap_turbo and not raw:
+            raise ValueError(f"{d.pot_file} has no GAP block")
         off = d.off_path()
         if off:
             raise NotImplementedError("not on the device path: " + "; ".join(off))
         self.species_types = d.species
         self.blocks: List[GapBlock] = [s.load(self.species_types, self.base)
                                        for s in self.gap.soap_turbo]
+        self.families = [b.load(self.species_types, self.base, d.core_pot_cutoff,
+                                d.core_pot_buffer) for b in raw]
         self.frames = F.read_extxyz(os.path.join(self.base, d.atoms_file))
         if not self.frames:
             raise ValueError(f"{d.atoms_file} holds no structure")
@@ -111,6 +124,9 @@ class Deck:
             keys.append(block_key(b))
             backend.soap_backend_begin(b, keys[-1])
         backend.soap_backend_end()
+        for f in self.families:
+            keys.append(family_key(f))
+            backend.family_begin(f, keys[-1])
         return keys
 
     def engine(self, frame: F.Frame, keys: List[int]) -> backend.Engine:

@@ -276,9 +276,70 @@ class SoapTurboSpec:
 
 @dataclass
 class RawGapBlock:
-    """A non-soap_turbo block: its type and every ``keyword = values`` line."""
+    """A distance_2b, angle_3b or core_pot block: its type and every
+    ``keyword = values`` line; ``load`` turns it into the family the device
+    evaluates (read_files.f90:5238-5505)."""
     kind: str
     keywords: Dict[str, List[str]]
+
+    def _get(self, names, conv, default, n=1):
+        for k in names:
+            if k in self.keywords:
+                v = _values(["", "="] + self.keywords[k], n, conv, k)
+                return v if n > 1 else v[0]
+        return default
+
+    def _species(self, names, species_types):
+        name = self._get(names, str, None)
+        if name is None:
+            raise ValueError(f"{self.kind} block without {names[-1]}")
+        if name not in species_types:
+            raise ValueError(f"{self.kind} species {name!r} is not among the input species "
+                             f"{list(species_types)}")
+        return list(species_types).index(name) + 1
+
+    def load(self, species_types: Sequence[str], base_dir: str = ".",
+             core_pot_cutoff: float = 1e10, core_pot_buffer: float = 1.0):
+        from . import families as FM
+        s1 = self._species(("Z1", "z1", "species1"), species_types)
+        s2 = self._species(("Z2", "z2", "species2"), species_types)
+        if self.kind == "core_pot":
+            path = self._get(("core_pot_file",), str, None)
+            if path is None:
+                raise ValueError("core_pot block without core_pot_file")
+            return read_core_pot_file(os.path.join(base_dir, path), (s1, s2), core_pot_cutoff,
+                                      core_pot_buffer)
+        fd = self._get(("desc_sparse",), str, None)
+        fa = self._get(("alphas_sparse",), str, None)
+        if fd is None or fa is None:
+            raise ValueError(f"{self.kind} block without desc_sparse / alphas_sparse")
+        rcut = self._get(("rcut",), _real, None)
+        if rcut is None:
+            raise ValueError(f"{self.kind} block without rcut")
+        delta = self._get(("delta",), _real, 1.0)
+        alphas, Qs, cut = read_alphas_and_descriptors(os.path.join(base_dir, fd),
+                                                      os.path.join(base_dir, fa), self.kind)
+        if self.kind == "distance_2b":
+            return FM.Distance2b((s1, s2), delta, self._get(("sigma",), _real, 1.0), rcut,
+                                 Qs[:, 0], alphas, cut)
+        sc = self._species(("Z_center", "z_center", "species_center"), species_types)
+        return FM.Angle3b((sc, s1, s2), delta, self._get(("sigma",), _real, [1.0] * 3, 3), rcut,
+                          Qs, alphas, cut, self._get(("kernel_type",), str, "exp"))
+
+
+def read_core_pot_file(path: str, species, cutoff: float = 1e10, buffer: float = 1.0):
+    """core_pot table: a record ``n yp1 ypn`` then n records ``x V``
+    (read_files.f90:5425-5447), tapered at core_pot_cutoff."""
+    from . import families as FM
+    recs = _records(path)
+    head = _tokens(recs[0])
+    n, yp1, ypn = _int(head[0]), _real(head[1]), _real(head[2])
+    if len(recs) < n + 1:
+        raise ValueError(f"{path}: {n} table records expected")
+    xv = [_tokens(recs[1 + i]) for i in range(n)]
+    x = [_real(t[0]) for t in xv]
+    V = [_real(t[1]) for t in xv]
+    return FM.CorePot.from_table(species, x, V, yp1, ypn, cutoff, buffer)
 
 
 @dataclass
@@ -761,6 +822,8 @@ class InputDeck:
     neighbors_buffer = property(lambda s: s._get("neighbors_buffer", _real, 0.0))
     write_thermo = property(lambda s: s._get("write_thermo", _int, 1))
     write_xyz = property(lambda s: s._get("write_xyz", _int, 0))
+    core_pot_cutoff = property(lambda s: s._get("core_pot_cutoff", _real, 1e10))
+    core_pot_buffer = property(lambda s: s._get("core_pot_buffer", _real, 1.0))
     random_seed = property(lambda s: s._get("random_seed", _int, 0))
 
     def off_path(self) -> List[str]:
