@@ -58,6 +58,9 @@ def parse():
                     help="exact MD snapshots (every 2 steps) the MLPs are trained on")
     ap.add_argument("--mlp-epochs", type=int, default=10)
     ap.add_argument("--gate-ev", type=float, default=0.005)
+    ap.add_argument("--neighbors-buffer", type=float, default=0.0,
+                    help="list skin (A): lists kept until an atom moved sqrt(buffer/2); "
+                         "0 (the reference default) rebuilds every step")
     return ap.parse_args()
 
 
@@ -469,7 +472,8 @@ def run_ours(a):
         B.soap_backend_begin(b, key=i + 1, precision=prec)
         keys.append(i + 1)
     st = w.structure(replica=rank)
-    eng = B.Engine(st.positions, st.species, st.masses, st.box, keys)
+    eng = B.Engine(st.positions, st.species, st.masses, st.box, keys,
+                   neighbors_buffer=a.neighbors_buffer)
     eng.set_state(st.positions, synth.maxwell_velocities(st.masses, w.temperature, w.seed))
     n_pairs = eng.n_pairs()
     ext = torch.cuda.ExternalStream(eng.stream())
@@ -554,8 +558,10 @@ def run_ours(a):
         "warmup": a.warmup, "ms_per_step": 1e3 * t_max / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic",
         "config": {"workload": f"{w.name}: {w.description}", "atoms_per_gpu": st.n,
-                   "pairs": n_pairs, "dt_fs": w.dt, "md": "NVE velocity-Verlet, neighbour list "
-                   "rebuilt every step", "precision": a.precision,
+                   "pairs": n_pairs, "dt_fs": w.dt, "md": "NVE velocity-Verlet, neighbour list " + (
+                       "rebuilt every step" if a.neighbors_buffer <= 0 else
+                       f"built to rcut + {a.neighbors_buffer} A, kept until an atom moved "
+                       f"sqrt({a.neighbors_buffer}/2) A"), "precision": a.precision,
                    "l2": "inputs larger than L2 (GEMM operands and kd scratch > 126 MB)",
                    "parallelism": f"{world} independent replica(s), one per GPU"},
         "roofline": {"kernel": "k_gemm_tn<GAP>: tcgen05 GEMM 1, K = q.Q_s^T with the fused "

@@ -240,6 +240,15 @@ int tg_engine_get_state(tg_engine *e, double *positions, double *velocities, dou
  * positions, velocities, forces (3, n), energies (n), virial (3, 3). */
 int tg_engine_get_frame(tg_engine *e, double *positions, double *velocities, double *forces,
                         double *energies, double *virial);
+/* Neighbour-list reuse with neighbors_buffer > 0 (src/turbogap_md.f90:451-470,
+ * src/neighbors.f90:544-590): the lists are built to rcut + neighbors_buffer
+ * and rebuilt only once some atom's accumulated squared displacement exceeds
+ * neighbors_buffer / 2 (the reference's criterion); in between, the distances
+ * of the kept pairs are recomputed. The decision is taken on the device inside
+ * the captured step. A supercell (box below 2 (rcut + buffer)) rebuilds every
+ * step, as in the reference. Counts of rebuilds and evaluations since
+ * creation; both -1 when every evaluation rebuilds. */
+int tg_engine_neighbor_stats(tg_engine *e, int64_t *n_builds, int64_t *n_evaluations);
 
 /* ---- a structure sharded over ranks (one process per GPU), as the reference
  *      splits central atoms over MPI ranks (src/turbogap.f90:930-942) and sums

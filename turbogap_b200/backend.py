@@ -328,6 +328,13 @@ class Engine:
                                         e.ctypes.data, w.ctypes.data))
         return p, v, f, e, w.reshape(3, 3).T.copy()
 
+    def neighbor_stats(self):
+        """(list rebuilds, evaluations) since creation with neighbors_buffer > 0;
+        (-1, -1) when every evaluation rebuilds its lists."""
+        b, e = C.c_int64(0), C.c_int64(0)
+        check(lib().tg_engine_neighbor_stats(self._h, C.byref(b), C.byref(e)))
+        return int(b.value), int(e.value)
+
     def set_site_range(self, beg: int, end: int):
         """Evaluate only the central sites in [beg, end) (one rank's share)."""
         check(lib().tg_engine_set_site_range(self._h, int(beg), int(end)))

@@ -1155,6 +1155,12 @@ struct Engine {
     cudaGraphExec_t graph = nullptr;
     double graph_dt = 0.0;
     bool first_step = true;
+    // Verlet-skin lists (neighbors_buffer > 0 on the cell path, no supercell)
+    bool skin = false;
+    double skin_thresh = 0.0;            // neighbors_buffer / 2, compared with |displacement|^2
+    DBuf<int> nl_when;                   // nonzero: the next evaluation rebuilds
+    DBuf<double> disp;                   // displacement since the last rebuild (3, n)
+    DBuf<long long> nl_counts;           // rebuilds, evaluations
     std::vector<int> species_h;          // host copy, for the site lists
     int site_beg = 0, site_end = 0;      // central sites of this rank
     Comm *comm = nullptr;                // set: forces/energies/virial summed over ranks
@@ -1202,7 +1208,16 @@ struct Engine {
             TGB_TRY(launch_supercell(n, pos.p, abc.p, indices, pos_sc.p, st));
             p = pos_sc.p;
         }
-        TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        if (skin) {
+            // neighbors_buffer > 0: rebuild only when the previous step asked for it,
+            // otherwise refresh the kept pairs (decided on the device, inside the graph)
+            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st, nl_when.p));
+            TGB_TRY(launch_nl_refresh(n, p, box, nl, nl_when.p, st));
+            TGB_TRY(launch_skin_reset(n, nl_when.p, disp.p, nl_counts.p, st));
+            TGB_CUDA(cudaMemsetAsync(nl_when.p, 0, sizeof(int), st));
+        } else {
+            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        }
         TGB_MARK(log, PASS_NEIGH, st);
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, site_beg, site_end, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
@@ -1282,7 +1297,17 @@ struct Engine {
         TGB_TRY(launch_remove_cm(n, vel.p, mass.p, acc4.p, st));
         TGB_TRY(launch_velocity_verlet(n, pos.p, pos_prev.p, vel.p, f.p, f_prev.p, mass.p, dt,
                                        first ? dt : dt_prev, first ? 1 : 0, st));
+        if (skin) TGB_TRY(launch_skin_check(n, pos.p, pos_prev.p, disp.p, skin_thresh, nl_when.p, st));
         TGB_MARK(log, PASS_INTEGRATE, st);
+        return TG_OK;
+    }
+
+    // the next evaluation rebuilds the list (positions replaced from outside)
+    int force_rebuild() {
+        if (!skin) return TG_OK;
+        const int one = 1;
+        TGB_CUDA(cudaMemcpyAsync(nl_when.p, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+        TGB_CUDA(cudaStreamSynchronize(st));
         return TG_OK;
     }
 };
@@ -1384,6 +1409,18 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     TGB_CUDA(cudaStreamSynchronize(st));
     TGB_TRY(E.nl.reserve(E.n, E.nsc, (int64_t)(P * 1.4) + 64, E.g));
     TGB_CUDA(cudaMemsetAsync(E.nl.err, 0, sizeof(unsigned), st));
+    // turbogap_md.f90:453-470: a supercell always rebuilds; otherwise a positive
+    // buffer keeps the list until an atom has moved far enough
+    E.skin = neighbors_buffer > 0.0 && E.nsc == E.n && E.use_cells;
+    if (E.skin) {
+        E.skin_thresh = neighbors_buffer / 2.0;
+        TGB_TRY(E.nl_when.ensure(1));
+        TGB_TRY(E.disp.ensure(n3));
+        TGB_TRY(E.nl_counts.ensure(2));
+        TGB_CUDA(cudaMemsetAsync(E.disp.p, 0, sizeof(double) * n3, st));
+        TGB_CUDA(cudaMemsetAsync(E.nl_counts.p, 0, sizeof(long long) * 2, st));
+        TGB_TRY(E.force_rebuild());
+    }
     TGB_CUDA(cudaStreamSynchronize(st));
     *out = holder.release();
     return TG_OK;
@@ -1404,6 +1441,7 @@ int tg_engine_set_state(tg_engine *eh, const double *positions, const double *ve
     if (velocities) TGB_CUDA(cudaMemcpyAsync(E.vel.p, velocities, b3, cudaMemcpyHostToDevice, E.st));
     E.first_step = true;
     E.frame_prev = false;
+    if (positions) TGB_TRY(E.force_rebuild());
     TGB_CUDA(cudaStreamSynchronize(E.st));
     return TG_OK;
 }
@@ -1552,6 +1590,19 @@ int tg_engine_set_comm(tg_engine *eh, const void *id128, int32_t n_ranks, int32_
     E.comm = nullptr;
     if (!id128) return TG_OK;
     return comm_init(id128, n_ranks, rank, &E.comm);
+}
+
+int tg_engine_neighbor_stats(tg_engine *eh, int64_t *n_builds, int64_t *n_evaluations) {
+    TGB_CHECK(eh && n_builds && n_evaluations, TG_ERR_ARG, "null argument");
+    Engine &E = eh->e;
+    *n_builds = *n_evaluations = -1;
+    if (!E.skin) return TG_OK;
+    long long c[2] = {0, 0};
+    TGB_CUDA(cudaMemcpyAsync(c, E.nl_counts.p, sizeof(c), cudaMemcpyDeviceToHost, E.st));
+    TGB_CUDA(cudaStreamSynchronize(E.st));
+    *n_builds = c[0];
+    *n_evaluations = c[1];
+    return TG_OK;
 }
 
 int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {

@@ -100,9 +100,10 @@ __device__ __forceinline__ void cell_coords(const double *p, const Box &bx, cons
 }
 
 __global__ void k_cell_assign(int n, const double *__restrict__ pos, Box bx, CellGrid g,
-                              int *__restrict__ cell_xyz, int *__restrict__ cell_count) {
+                              int *__restrict__ cell_xyz, int *__restrict__ cell_count,
+                              const int *__restrict__ when) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (when && !*when)) return;
     int c[3];
     cell_coords(pos + 3 * (size_t)i, bx, g, c);
     cell_xyz[3 * i] = c[0];
@@ -114,9 +115,9 @@ __global__ void k_cell_assign(int n, const double *__restrict__ pos, Box bx, Cel
 
 __global__ void k_cell_fill(int n, const int *__restrict__ cell_xyz, CellGrid g,
                             const int *__restrict__ cell_start, int *__restrict__ cell_fill,
-                            int *__restrict__ cell_atoms) {
+                            int *__restrict__ cell_atoms, const int *__restrict__ when) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (when && !*when)) return;
     const int id = imod(cell_xyz[3 * i], g.mx) + imod(cell_xyz[3 * i + 1], g.my) * g.mx +
                    imod(cell_xyz[3 * i + 2], g.mz) * g.my * g.mx;
     const int slot = atomicAdd(&cell_fill[id], 1);
@@ -126,9 +127,10 @@ __global__ void k_cell_fill(int n, const int *__restrict__ cell_xyz, CellGrid g,
 // The reference links each cell's atoms by head insertion, so a cell is walked
 // in descending atom index (neighbors.f90:398-408, 460-463).
 __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start,
-                            const int *__restrict__ cell_count, int *__restrict__ cell_atoms) {
+                            const int *__restrict__ cell_count, int *__restrict__ cell_atoms,
+                            const int *__restrict__ when) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncells) return;
+    if (c >= ncells || (when && !*when)) return;
     int *a = cell_atoms + cell_start[c];
     const int n = cell_count[c];
     for (int i = 1; i < n; ++i) {
@@ -182,10 +184,11 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
                                 const double *__restrict__ cell_pos, int *__restrict__ n_neigh,
                                 const int64_t *__restrict__ pstart, int64_t cap,
                                 int *__restrict__ nbr, double *__restrict__ rjs,
-                                double *__restrict__ xyz, unsigned *err) {
+                                double *__restrict__ xyz, unsigned *err,
+                                const int *__restrict__ when) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n_sites) return;
+    if (i >= n_sites || (when && !*when)) return;
     if (do_list && !do_list[i]) {
         if (!pstart && lane == 0) n_neigh[i] = 0;
         return;
@@ -318,9 +321,10 @@ __global__ void k_pstart_zero(int64_t *pstart) { pstart[0] = 0; }
 
 // positions in cell order, so that a cell's candidates are read contiguously
 __global__ void k_cell_gather_pos(int n, const int *__restrict__ cell_atoms,
-                                  const double *__restrict__ pos, double *__restrict__ cell_pos) {
+                                  const double *__restrict__ pos, double *__restrict__ cell_pos,
+                                  const int *__restrict__ when) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= n || (when && !*when)) return;
     const int k = cell_atoms[s];
     cell_pos[3 * (size_t)s] = pos[3 * (size_t)k];
     cell_pos[3 * (size_t)s + 1] = pos[3 * (size_t)k + 1];
@@ -574,9 +578,97 @@ CellGrid plan_cells(const Box &bx, double rcut, const int *indices, bool *use_ce
     return g;
 }
 
+namespace {
+
+// build_neighbors_list with rebuild_neighbors_list = .false. (neighbors.f90:544-590):
+// the pair list stays, every pair's MIC vector and distance are recomputed with
+// get_distance from the current positions. Runs only while *when is zero.
+__global__ void k_nl_refresh(int n_sites, const double *__restrict__ pos, Box bx,
+                             const int64_t *__restrict__ pstart, int64_t cap,
+                             const int *__restrict__ nbr, double *__restrict__ rjs,
+                             double *__restrict__ xyz, const int *__restrict__ when) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n_sites || *when) return;
+    const double *pi = pos + 3 * (size_t)i;
+    // a list that overflowed its capacity holds pairs only below cap (the build
+    // raised the capacity error, which the host reports after the step)
+    const int64_t p0 = pstart[i], p1 = min(pstart[i + 1], cap);
+    for (int64_t p = p0 + 1 + lane; p < p1; p += 32) {   // the self pair keeps its zeros
+        double dist[3], d;
+        get_distance(pi, pos + 3 * (size_t)nbr[p], bx, dist, &d);
+        rjs[p] = d;
+        xyz[3 * p] = dist[0];
+        xyz[3 * p + 1] = dist[1];
+        xyz[3 * p + 2] = dist[2];
+    }
+}
+
+// After the list phase of an evaluation: a rebuilt list restarts the displacement
+// accumulation (turbogap_md.f90:464-470 zeroes positions_diff when it decides to
+// rebuild); counters[0] counts rebuilds, counters[1] evaluations.
+__global__ void k_skin_reset(int n, const int *__restrict__ when, double *__restrict__ disp,
+                             long long *__restrict__ counters) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool rebuilt = *when != 0;
+    if (i == 0) {
+        counters[1] += 1;
+        if (rebuilt) counters[0] += 1;
+    }
+    if (i >= n || !rebuilt) return;
+    disp[3 * (size_t)i] = 0.0;
+    disp[3 * (size_t)i + 1] = 0.0;
+    disp[3 * (size_t)i + 2] = 0.0;
+}
+
+// turbogap_md.f90:451-470: positions_diff += positions - positions_prev; the list
+// is rebuilt before the next evaluation once some atom's squared displacement
+// exceeds neighbors_buffer / 2 (the reference compares the square with half
+// the buffer length).
+__global__ void k_skin_check(int n, const double *__restrict__ pos,
+                             const double *__restrict__ pos_prev, double *__restrict__ disp,
+                             double thresh, int *__restrict__ when) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double v = (disp[3 * (size_t)i + q] + pos[3 * (size_t)i + q]) - pos_prev[3 * (size_t)i + q];
+        disp[3 * (size_t)i + q] = v;
+        s = s + v * v;
+    }
+    if (s > thresh) atomicOr(when, 1);
+}
+
+}  // namespace
+
+int launch_nl_refresh(int n_sites, const double *pos, const Box &bx, const NeighborList &nl,
+                      const int *when, cudaStream_t st) {
+    const int TB = 128;
+    const int gw = (int)(((int64_t)n_sites * 32 + TB - 1) / TB);
+    k_nl_refresh<<<gw, TB, 0, st>>>(n_sites, pos, bx, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
+                                    when);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_skin_reset(int n, const int *when, double *disp, long long *counters, cudaStream_t st) {
+    k_skin_reset<<<(n + 255) / 256, 256, 0, st>>>(n, when, disp, counters);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_skin_check(int n, const double *pos, const double *pos_prev, double *disp, double thresh,
+                      int *when, cudaStream_t st) {
+    k_skin_check<<<(n + 255) / 256, 256, 0, st>>>(n, pos, pos_prev, disp, thresh, when);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const Box &bx,
              const CellGrid &g, bool use_cells, double rcut, const int *do_list,
-             cudaStream_t st) {
+             cudaStream_t st, const int *when) {
+    TGB_CHECK(!when || use_cells, TG_ERR_ARG, "a gated list build needs the cell path");
     const int TB = 128;
     const int gb = (n_sites + TB - 1) / TB;
     const int gw = (int)(((int64_t)n_sites * 32 + TB - 1) / TB);   // one warp per site
@@ -584,19 +676,20 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
         const int ncells = g.mx * g.my * g.mz;
         TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
         TGB_CUDA(cudaMemsetAsync(nl.cell_fill, 0, sizeof(int) * ncells, st));
-        k_cell_assign<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, nl.cell_xyz, nl.cell_count);
+        k_cell_assign<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, nl.cell_xyz, nl.cell_count, when);
         size_t bytes = nl.scan_bytes;
         TGB_CUDA(cub::DeviceScan::ExclusiveSum(nl.scan_tmp, bytes, nl.cell_count, nl.cell_start,
                                                ncells, st));
         k_cell_fill<<<gb, TB, 0, st>>>(n_sites, nl.cell_xyz, g, nl.cell_start, nl.cell_fill,
-                                       nl.cell_atoms);
+                                       nl.cell_atoms, when);
         k_cell_sort<<<(ncells + TB - 1) / TB, TB, 0, st>>>(ncells, nl.cell_start, nl.cell_count,
-                                                           nl.cell_atoms);
-        if (nl.cell_pos) k_cell_gather_pos<<<gb, TB, 0, st>>>(n_sites, nl.cell_atoms, pos, nl.cell_pos);
+                                                           nl.cell_atoms, when);
+        if (nl.cell_pos)
+            k_cell_gather_pos<<<gb, TB, 0, st>>>(n_sites, nl.cell_atoms, pos, nl.cell_pos, when);
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
                                            nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
                                            nl.n_neigh, nullptr, nl.cap, nullptr, nullptr, nullptr,
-                                           nl.err);
+                                           nl.err, when);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nullptr,
                                       nl.cap, nullptr, nullptr, nullptr, nl.err);
@@ -609,7 +702,7 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
                                            nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
                                            nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
-                                           nl.err);
+                                           nl.err, when);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nl.pstart,
                                       nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);
@@ -817,7 +910,7 @@ int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st)
         k_bcell_fill<<<gb, TB, 0, st>>>(n, nl.cell_id, nl.cell_start, nl.cell_fill, nl.cell_atoms);
         k_bcell_sort<<<(nl.n_cells + TB - 1) / TB, TB, 0, st>>>(nl.n_cells, nl.cell_start,
                                                                  nl.cell_count, nl.cell_atoms);
-        k_cell_gather_pos<<<gb, TB, 0, st>>>(nl.n_cell_atoms, nl.cell_atoms, pos, nl.cell_pos);
+        k_cell_gather_pos<<<gb, TB, 0, st>>>(nl.n_cell_atoms, nl.cell_atoms, pos, nl.cell_pos, nullptr);
     }
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
                                   nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,

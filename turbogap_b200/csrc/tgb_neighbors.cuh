@@ -71,9 +71,21 @@ CellGrid plan_cells(const Box &bx, double rcut, const int *indices, bool *use_ce
 
 // Count, scan and fill. Pairs beyond nl.cap are dropped and flag
 // DEV_ERR_NEIGH_CAPACITY; pstart[n_sites] is the required capacity.
+// when (device int, optional, cell path only): the list kernels run only while
+// it is nonzero, so a captured step can skip the rebuild on the device.
 int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const Box &bx,
              const CellGrid &g, bool use_cells, double rcut, const int *do_list,
-             cudaStream_t st);
+             cudaStream_t st, const int *when = nullptr);
+
+// Verlet-skin lists (neighbors_buffer > 0, turbogap_md.f90:451-470,
+// neighbors.f90:544-590): refresh distances of the kept pairs while *when is 0;
+// after the list phase restart the displacement sums if the list was rebuilt;
+// after the integrator raise *when once |displacement|^2 > thresh.
+int launch_nl_refresh(int n_sites, const double *pos, const Box &bx, const NeighborList &nl,
+                      const int *when, cudaStream_t st);
+int launch_skin_reset(int n, const int *when, double *disp, long long *counters, cudaStream_t st);
+int launch_skin_check(int n, const double *pos, const double *pos_prev, double *disp, double thresh,
+                      int *when, cudaStream_t st);
 
 // ---- many independent orthorhombic structures at once (batched evaluation).
 // Structure s owns atoms [off, off + n) of the concatenated arrays. Boxes of at
