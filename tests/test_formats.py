@@ -154,6 +154,7 @@ def test_extxyz_read_columns_and_frames(tmp_path):
     assert a.masses.tolist() == [12.011, 1.008, 12.011]
     assert a.fix_atoms[0].tolist() == [False, False, True] and a.fix_atoms[2].all()
     assert a.info["pbc"] == "T T T"
+    assert a.arrays["charge"].tolist() == [9.9, 9.9, 9.9]            # other real columns
     assert b.n == 2 and b.velocities is None and b.masses is None and b.info["step"] == "7"
 
 
@@ -184,6 +185,8 @@ def test_extxyz_write_layout_and_round_trip(tmp_path):
     assert np.allclose(fr[0].positions, pos, atol=5e-9) and np.allclose(fr[0].velocities, vel,
                                                                         atol=5e-9)
     assert np.allclose(fr[1].positions, pos + 1, atol=5e-9)
+    assert np.allclose(fr[0].arrays["forces"], frc, atol=5e-9)
+    assert np.allclose(fr[0].arrays["local_energy"], le, atol=5e-9)
     e = float(fr[0].info["energy"])
     assert abs(e - le.sum()) < 1e-6
     stress = np.array([float(x) for x in fr[0].info["stress"].split()]).reshape(3, 3)

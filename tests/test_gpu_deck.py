@@ -16,7 +16,7 @@ from turbogap_b200.hypers import carbon_hypers
 pytestmark = pytest.mark.gpu
 
 
-def _write_deck(d, nsteps, dt, e0):
+def _write_deck(d, nsteps, dt, e0, extra="", write_xyz=4, temperature=900.0):
     h = carbon_hypers()
     blk = sparse_block(h, 300, seed=61)
     F.write_sparse_set(blk, str(d / "desc_C.dat"), str(d / "alphas_C.dat"))
@@ -24,14 +24,14 @@ def _write_deck(d, nsteps, dt, e0):
         F.write_soap_block(fh, F.spec_from_block(blk, ["C"], "desc_C.dat", "alphas_C.dat"))
     st = synth.random_structure(216, 12.91, 1.2, seed=62)
     m = np.full(st.n, 12.011 * F.AMU_TO_EV_FS2_A2)
-    v = synth.maxwell_velocities(m, 900.0, 63)
+    v = synth.maxwell_velocities(m, temperature, 63)
     F.write_extxyz(str(d / "atoms.xyz"), ["C"] * st.n, st.positions, st.box, step=0, time=0.0,
                    dt=dt, temperature=0.0, pressure=0.0, virial=np.zeros((3, 3)),
                    velocities=v)
     (d / "input").write_text(
         "atoms_file = 'atoms.xyz'\npot_file = 'c.gap'\nn_species = 1\nspecies = C\n"
         f"masses = 12.011\ne0 = {e0!r}\nmd_nsteps = {nsteps}\nmd_step = {dt!r}\n"
-        "write_thermo = 1\nwrite_xyz = 4\n")
+        f"write_thermo = 1\nwrite_xyz = {write_xyz}\n" + extra)
     # the deck's values after the round trip through the files
     fr = F.read_extxyz(str(d / "atoms.xyz"))[0]
     return blk, fr, m
@@ -101,3 +101,30 @@ def test_deck_predict_frames(gpu, tmp_path):
         assert np.abs(r["forces"] - fo).max() < 1e-6
     tr = F.read_extxyz(str(tmp_path / "p" / "trajectory_out.xyz"))
     assert [t.info["i_config"] for t in tr] == ["1", "2"]
+
+
+def test_warm_lists_match_cold_prediction(gpu, tmp_path):
+    """tests/mc_mpi_neighbors of the reference, for MD with kept lists: every
+    frame of a run whose lists live across steps (neighbors_buffer > 0) carries
+    the forces and local energies it was given; a cold prediction of the same
+    frames, with lists built from scratch, must reproduce them (1e-5 eV/A on
+    force components, 1e-6 eV on local energies, as there)."""
+    # The reference rebuilds once a squared displacement exceeds buffer / 2, so an
+    # atom may move sqrt(buffer / 2) first and two atoms closing in on each other
+    # 2 sqrt(buffer / 2); no pair can enter rcut unseen only when that is at most
+    # the buffer, i.e. buffer >= 2 A. A smaller buffer follows the reference and
+    # can drop a pair near the cutoff.
+    nsteps, dt = 30, 1.0
+    _write_deck(tmp_path, nsteps, dt, 0.0, extra="neighbors_buffer = 2.0\n", write_xyz=1,
+                temperature=2500.0)
+    D.run_md(str(tmp_path / "input"), str(tmp_path / "run"))
+    traj = F.read_extxyz(str(tmp_path / "run" / "trajectory_out.xyz"))
+    assert len(traj) == nsteps + 1
+    text = (tmp_path / "input").read_text().replace("atoms_file = 'atoms.xyz'",
+                                                    "atoms_file = 'run/trajectory_out.xyz'")
+    (tmp_path / "input_cold").write_text(text)
+    cold = D.run_predict(str(tmp_path / "input_cold"), str(tmp_path / "cold"))
+    assert len(cold) == len(traj)
+    for k, (fr, c) in enumerate(zip(traj, cold)):
+        assert np.abs(c["forces"] - fr.arrays["forces"]).max() < 1e-5, k
+        assert np.abs(c["energies"] - fr.arrays["local_energy"]).max() < 1e-6, k

@@ -578,6 +578,7 @@ class Frame:
     fix_atoms: Optional[np.ndarray] = None
     properties: str = ""
     info: Dict[str, str] = field(default_factory=dict)
+    arrays: Dict[str, np.ndarray] = field(default_factory=dict)   # other real columns
 
     @property
     def n(self) -> int:
@@ -592,13 +593,15 @@ def _header_pairs(line: str) -> Dict[str, str]:
     return out
 
 
-def _columns(properties: str):
-    """(name, first column, width) of each property of a Properties string."""
+def _columns(properties: str, with_type: bool = False):
+    """(name, first column, width[, type letter]) of each property of a
+    Properties string."""
     parts = properties.split(":")
     cols, c = [], 0
     for k in range(0, len(parts) - 2, 3):
         w = int(parts[k + 2])
-        cols.append((parts[k].lower(), c, w))
+        cols.append((parts[k].lower(), c, w, parts[k + 1].lower()) if with_type else
+                    (parts[k].lower(), c, w))
         c += w
     return cols
 
@@ -606,7 +609,8 @@ def _columns(properties: str):
 def iter_extxyz(path: str) -> Iterator[Frame]:
     """Frames of an extended-XYZ file. Recognised columns, as in read_xyz_line:
     species; pos/positions; vel/velocities; mass/masses; fix_atoms/fix_atom
-    (three logicals). Other columns are skipped by their width."""
+    (three logicals). Other real columns (forces, local_energy, ...) land in
+    ``arrays``; the rest are skipped by their width."""
     recs = _records(path)
     k = 0
     while k < len(recs):
@@ -627,6 +631,11 @@ def iter_extxyz(path: str) -> Iterator[Frame]:
         cols = _columns(props)
         species, pos = [], np.zeros((n, 3))
         vel = mass = fix = None
+        known = ("species", "pos", "positions", "vel", "velocities", "mass", "masses",
+                 "fix_atoms", "fix_atom")
+        extra = {name: (c, w) for name, c, w, ty in _columns(props, True)
+                 if ty == "r" and name not in known}
+        arrays = {name: np.zeros((n, w)) for name, (c, w) in extra.items()}
         for name, c, w in cols:
             if name in ("vel", "velocities"):
                 vel = np.zeros((n, 3))
@@ -647,8 +656,11 @@ def iter_extxyz(path: str) -> Iterator[Frame]:
                     mass[i] = _real(t[c])
                 elif name in ("fix_atoms", "fix_atom"):
                     fix[i] = [_logical(x) for x in t[c:c + 3]]
+            for name, (c, w) in extra.items():
+                arrays[name][i] = [_real(x) for x in t[c:c + w]]
         info = {key: v for key, v in pairs.items() if key.lower() not in ("lattice", "properties")}
-        yield Frame(species, pos, lat.reshape(3, 3), vel, mass, fix, props, info)
+        arrays = {k: (v[:, 0] if v.shape[1] == 1 else v) for k, v in arrays.items()}
+        yield Frame(species, pos, lat.reshape(3, 3), vel, mass, fix, props, info, arrays)
         k += 2 + n
 
 
