@@ -430,6 +430,7 @@ def run_batch(a, w, world, rank, local, dist):
                    "atoms_per_gpu": n, "pairs": bat.n_pairs(),
                    "step": "energies, forces and virials of every cell (batched, one CUDA graph)",
                    "l2": "inputs larger than L2",
+                   "soap_tiles": _tiles_desc(bat.tiles()),
                    "parallelism": f"{world} independent replica(s), one per GPU"},
         "roofline": {"kernel": "k_gemm_tn<GAP>: tcgen05 GEMM 1 (all cells' sites)", "bound": "tensor",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -563,6 +564,7 @@ def run_ours(a):
                        f"built to rcut + {a.neighbors_buffer} A, kept until an atom moved "
                        f"sqrt({a.neighbors_buffer}/2) A"), "precision": a.precision,
                    "l2": "inputs larger than L2 (GEMM operands and kd scratch > 126 MB)",
+                   "soap_tiles": _tiles_desc(eng.tiles()),
                    "parallelism": f"{world} independent replica(s), one per GPU"},
         "roofline": {"kernel": "k_gemm_tn<GAP>: tcgen05 GEMM 1, K = q.Q_s^T with the fused "
                                "K^zeta energy and kd epilogue (all blocks of a step)",
@@ -592,6 +594,13 @@ def run_ours(a):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _tiles_desc(tiles):
+    """Autotuned CTA tiles of the descriptor and force passes, per block."""
+    name = {0: "4 sites/CTA, >=4 CTAs/SM", 1: "4 sites/CTA, >=3 CTAs/SM", 2: "2 sites/CTA, >=8 CTAs/SM",
+            3: "8 sites/CTA, >=2 CTAs/SM"}
+    return [{"descriptor": name[a], "forces": name[b]} for a, b in tiles]
 
 
 def main():

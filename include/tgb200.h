@@ -249,6 +249,14 @@ int tg_engine_get_frame(tg_engine *e, double *positions, double *velocities, dou
  * step, as in the reference. Counts of rebuilds and evaluations since
  * creation; both -1 when every evaluation rebuilds. */
 int tg_engine_neighbor_stats(tg_engine *e, int64_t *n_builds, int64_t *n_evaluations);
+/* CTA tiles of each block's descriptor and force passes, picked at creation by
+ * the autotuner (each of 4 tiles timed on the structure itself; environment
+ * TGB_AUTOTUNE=0 keeps tile 0, TGB_SOAP_TILE=t pins tile t): tiles[2k], tiles[2k+1]
+ * for block k (soap_turbo
+ * blocks in key order). Tile t groups 4, 4, 2, 8 sites per CTA for t = 0..3,
+ * with at least 4, 3, 8, 2 CTAs resident per SM. n >= 2 * blocks; *n_blocks
+ * receives the number of soap_turbo blocks. */
+int tg_engine_tiles(tg_engine *e, int32_t *tiles, int32_t n, int32_t *n_blocks);
 
 /* ---- a structure sharded over ranks (one process per GPU), as the reference
  *      splits central atoms over MPI ranks (src/turbogap.f90:930-942) and sums
@@ -312,6 +320,8 @@ int tg_batch_stream(tg_batch *b, void **stream);
 int tg_batch_profile(tg_batch *b, int32_t n_evals, double *ms_per_pass, int32_t *n_passes);
 /* Kernel launches in one evaluation's CUDA graph. */
 int tg_batch_graph_kernels(tg_batch *b, int32_t *n_kernels);
+/* The autotuned CTA tiles of the batch's blocks, as tg_engine_tiles. */
+int tg_batch_tiles(tg_batch *b, int32_t *tiles, int32_t n, int32_t *n_blocks);
 int tg_batch_n_pairs(tg_batch *b, int64_t *n_pairs);
 
 /* ---- learned surrogate (mixed form). No reference counterpart: TurboGAP has

@@ -88,6 +88,8 @@ SIGNATURES = [
     ("tg_engine_get_frame", C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("tg_engine_set_site_range", C.c_int, [_vp, C.c_int32, C.c_int32]),
     ("tg_engine_neighbor_stats", C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("tg_engine_tiles", C.c_int, [_vp, ip, C.c_int32, C.POINTER(C.c_int32)]),
+    ("tg_batch_tiles", C.c_int, [_vp, ip, C.c_int32, C.POINTER(C.c_int32)]),
     ("tg_nccl_unique_id", C.c_int, [_vp]),
     ("tg_engine_set_comm", C.c_int, [_vp, _vp, C.c_int32, C.c_int32]),
     ("tg_engine_n_pairs", C.c_int, [_vp, C.POINTER(C.c_int64)]),

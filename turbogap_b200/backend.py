@@ -231,6 +231,13 @@ def velocity_verlet(positions, positions_prev, velocities, forces, forces_prev, 
     return float(dtp.value)
 
 
+def _tiles(fn, h):
+    t = np.zeros(64, dtype=np.int32)
+    nb = C.c_int32(0)
+    check(fn(h, t, len(t), C.byref(nb)))
+    return [(int(t[2 * k]), int(t[2 * k + 1])) for k in range(nb.value)]
+
+
 class Engine:
     """Device-resident SOAP-GAP evaluator and NVE integrator for one structure.
 
@@ -327,6 +334,10 @@ class Engine:
         check(lib().tg_engine_get_frame(self._h, p.ctypes.data, v.ctypes.data, f.ctypes.data,
                                         e.ctypes.data, w.ctypes.data))
         return p, v, f, e, w.reshape(3, 3).T.copy()
+
+    def tiles(self):
+        """[(descriptor tile, force tile)] per soap_turbo block, as autotuned."""
+        return _tiles(lib().tg_engine_tiles, self._h)
 
     def neighbor_stats(self):
         """(list rebuilds, evaluations) since creation with neighbors_buffer > 0;
@@ -505,6 +516,10 @@ class Batch:
                                     len(e0) if e0 is not None else 0, C.byref(h)))
         self._h = h
         self._keep = e0
+
+    def tiles(self):
+        """[(descriptor tile, force tile)] per soap_turbo block, as autotuned."""
+        return _tiles(lib().tg_batch_tiles, self._h)
 
     def close(self):
         if self._h:

@@ -12,6 +12,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -101,6 +102,7 @@ struct Workspace {
     TmaMap tmA1{}, tmA2{}, tmKd{};   // tmKd: the GAP epilogue's TMA stores into kd
     int tm_rows = -1;
     const void *tm_p1 = nullptr, *tm_p2 = nullptr;
+    int tile_desc = 0, tile_force = 0;   // CTA tiles of the two SOAP passes (autotuned)
 
     int ensure(const Block &b, int n_sites) {
         const int n = n_sites > 0 ? n_sites : 1;
@@ -117,7 +119,7 @@ struct Workspace {
             TGB_TRY(epart.ensure((size_t)nc * b.n_etiles));
             TGB_TRY(kdsum.ensure((size_t)nc * b.n_etiles));
             TGB_TRY(qoff.ensure(nc));
-            TGB_TRY(vpart.ensure((size_t)9 * ((nc + 3) / 4 + 1)));
+            TGB_TRY(vpart.ensure((size_t)9 * ((nc + 1) / 2 + 1)));   // the 2-site tile
             cap = nc;
         }
         if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p) {
@@ -228,7 +230,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     TGB_TRY(w.ensure(b, S.n_sites));
     const SoapParams P = b.params(n_atoms);
     DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
-    TGB_TRY(launch_soap_expand(P, S, O, st));
+    TGB_TRY(launch_soap_expand(P, S, O, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
     GemmEpi e1{};
     e1.mode = EPI_GAP_KERNEL;
@@ -260,13 +262,78 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct};
     int nblk = 0;
-    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
+    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, w.tile_force));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
     TGB_MARK(log, PASS_FORCE, st);
     return TG_OK;
 }
 
 static unsigned grid_for(int64_t n, int tb = 256) { return (unsigned)((n + tb - 1) / tb); }
+
+// The project's autotuner: with the run's own sites and lists in place, time
+// every CTA tile of the descriptor and the force pass (one warm launch, then
+// `reps` launches between CUDA events) and keep the fastest of each. The tiles
+// change only how central sites are grouped into CTAs and the register budget,
+// so descriptor values do not depend on the choice; the extra force launches
+// add into forces, energies and the virial partials, which every evaluation
+// clears before it starts. TGB_AUTOTUNE=0 keeps the default tiles; TGB_SOAP_TILE
+// pins one.
+bool autotune_enabled() {
+    const char *e = std::getenv("TGB_AUTOTUNE");
+    return !(e && e[0] == '0') && !std::getenv("TGB_SOAP_TILE");
+}
+
+// TGB_SOAP_TILE=t pins every block to tile t (0 .. kSoapTiles - 1) instead of
+// tuning; returns -1 when unset.
+int pinned_tile() {
+    const char *e = std::getenv("TGB_SOAP_TILE");
+    if (!e) return -1;
+    const int t = std::atoi(e);
+    return t < 0 ? 0 : (t >= kSoapTiles ? kSoapTiles - 1 : t);
+}
+
+int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
+                   double *energies, double *virial, unsigned *err, cudaStream_t st, int reps = 3) {
+    if (S.n_sites <= 0) return TG_OK;
+    TGB_TRY(evaluate_block(b, w, S, n_atoms, forces, energies, virial, err, st));
+    const SoapParams P = b.params(n_atoms);
+    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
+    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
+    ForceOut FO{forces, energies, w.vpart.p, err};
+    cudaEvent_t e0, e1;
+    TGB_CUDA(cudaEventCreate(&e0));
+    TGB_CUDA(cudaEventCreate(&e1));
+    auto time_tile = [&](bool force, int t, float &ms) -> int {
+        int nblk = 0;
+        for (int r = 0; r <= reps; ++r) {
+            if (r == 1) TGB_CUDA(cudaEventRecord(e0, st));
+            if (force) TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, t));
+            else TGB_TRY(launch_soap_expand(P, S, O, st, t));
+        }
+        TGB_CUDA(cudaEventRecord(e1, st));
+        TGB_CUDA(cudaEventSynchronize(e1));
+        TGB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return TG_OK;
+    };
+    int rc = TG_OK;
+    for (int pass = 0; pass < 2 && rc == TG_OK; ++pass) {
+        float best = 0.f;
+        int arg = 0;
+        for (int t = 0; t < kSoapTiles && rc == TG_OK; ++t) {
+            float ms = 0.f;
+            rc = time_tile(pass == 1, t, ms);
+            if (rc == TG_OK && (t == 0 || ms < best)) {
+                best = ms;
+                arg = t;
+            }
+        }
+        if (pass == 0) w.tile_desc = arg;
+        else w.tile_force = arg;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
 
 // ---------------------------------------------------------------- mixed form
 // Sites whose ensemble spread exceeds the gate go back to the exact GAP kernel:
@@ -382,7 +449,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
               x.mlp->L.D, b.dim);
     const SoapParams P = b.params(n_atoms);
     DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
-    TGB_TRY(launch_soap_expand(P, S, O, st));
+    TGB_TRY(launch_soap_expand(P, S, O, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
     TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim,
                       b.g0f.p, st));
@@ -430,7 +497,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
     int nblk = 0;
-    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st));
+    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, w.tile_force));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
     TGB_MARK(log, PASS_FORCE, st);
     return TG_OK;
@@ -1302,6 +1369,28 @@ struct Engine {
         return TG_OK;
     }
 
+    // picks the CTA tiles of every block's SOAP passes on this structure
+    int autotune() {
+        if (pinned_tile() >= 0)
+            for (auto &r : runs) r->w->tile_desc = r->w->tile_force = pinned_tile();
+        if (!autotune_enabled() || runs.empty()) return TG_OK;
+        const double *p = pos.p;
+        if (nsc > n) {
+            TGB_TRY(launch_supercell(n, pos.p, abc.p, indices, pos_sc.p, st));
+            p = pos_sc.p;
+        }
+        TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
+        TGB_CUDA(cudaMemsetAsync(en.p, 0, sizeof(double) * n, st));
+        TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
+        for (auto &r : runs) {
+            SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            TGB_TRY(autotune_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
+        }
+        TGB_CUDA(cudaStreamSynchronize(st));
+        return TG_OK;
+    }
+
     // the next evaluation rebuilds the list (positions replaced from outside)
     int force_rebuild() {
         if (!skin) return TG_OK;
@@ -1319,6 +1408,8 @@ struct tg_engine {
 };
 
 extern "C" {
+
+static int engine_errors(Engine &E);
 
 int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *species,
                      const double *masses, const double *a_box, const double *b_box,
@@ -1421,6 +1512,8 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
         TGB_CUDA(cudaMemsetAsync(E.nl_counts.p, 0, sizeof(long long) * 2, st));
         TGB_TRY(E.force_rebuild());
     }
+    TGB_TRY(E.autotune());
+    TGB_TRY(engine_errors(E));
     TGB_CUDA(cudaStreamSynchronize(st));
     *out = holder.release();
     return TG_OK;
@@ -1602,6 +1695,19 @@ int tg_engine_neighbor_stats(tg_engine *eh, int64_t *n_builds, int64_t *n_evalua
     TGB_CUDA(cudaStreamSynchronize(E.st));
     *n_builds = c[0];
     *n_evaluations = c[1];
+    return TG_OK;
+}
+
+int tg_engine_tiles(tg_engine *eh, int32_t *tiles, int32_t n, int32_t *n_blocks) {
+    TGB_CHECK(eh && tiles && n_blocks, TG_ERR_ARG, "null argument");
+    Engine &E = eh->e;
+    TGB_CHECK(n >= 2 * (int)E.runs.size(), TG_ERR_CAPACITY, "tiles needs %d entries",
+              2 * (int)E.runs.size());
+    *n_blocks = (int32_t)E.runs.size();
+    for (size_t k = 0; k < E.runs.size(); ++k) {
+        tiles[2 * k] = E.runs[k]->w->tile_desc;
+        tiles[2 * k + 1] = E.runs[k]->w->tile_force;
+    }
     return TG_OK;
 }
 
@@ -1908,6 +2014,22 @@ struct BatchEngine {
 
     EventLog prof;
 
+    int autotune() {
+        if (pinned_tile() >= 0)
+            for (auto &r : runs) r->w->tile_desc = r->w->tile_force = pinned_tile();
+        if (!autotune_enabled()) return TG_OK;
+        TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
+        TGB_CUDA(cudaMemsetAsync(en.p, 0, sizeof(double) * n, st));
+        TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
+        for (auto &r : runs) {
+            SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            TGB_TRY(autotune_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
+        }
+        TGB_CUDA(cudaStreamSynchronize(st));
+        return TG_OK;
+    }
+
     int compute_ef(EventLog *log = nullptr) {
         TGB_MARK(log, -1, st);
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
@@ -2075,6 +2197,8 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
         E.runs.push_back(std::move(run));
     }
     TGB_TRY(E.size_pairs());
+    TGB_TRY(E.autotune());
+    TGB_TRY(E.errors());
     *out = holder.release();
     return TG_OK;
 }
@@ -2174,6 +2298,19 @@ int tg_batch_graph_kernels(tg_batch *bh, int32_t *n_kernels) {
     cudaGraphDestroy(g);
     TGB_CUDA(ce);
     *n_kernels = k;
+    return TG_OK;
+}
+
+int tg_batch_tiles(tg_batch *bh, int32_t *tiles, int32_t n, int32_t *n_blocks) {
+    TGB_CHECK(bh && tiles && n_blocks, TG_ERR_ARG, "null argument");
+    BatchEngine &E = bh->e;
+    TGB_CHECK(n >= 2 * (int)E.runs.size(), TG_ERR_CAPACITY, "tiles needs %d entries",
+              2 * (int)E.runs.size());
+    *n_blocks = (int32_t)E.runs.size();
+    for (size_t k = 0; k < E.runs.size(); ++k) {
+        tiles[2 * k] = E.runs[k]->w->tile_desc;
+        tiles[2 * k + 1] = E.runs[k]->w->tile_force;
+    }
     return TG_OK;
 }
 

@@ -357,7 +357,10 @@ __device__ __forceinline__ void real_ylm(float x, float y, float z, float *Y) {
 
 // ===================== expansion + power spectrum ===========================
 
-template <int NS, int AMAX, int LMAX>
+// CTA tiles of the descriptor and force passes that the autotuner picks from:
+// tile v runs soap_tile_warps(v) central sites (warps) per CTA with at least
+// soap_tile_minb(v) CTAs resident per SM (the register budget follows).
+template <int NS, int AMAX, int LMAX, int TILE = 0>
 struct DescShape {
     static constexpr int NL = LMAX + 1;
     static constexpr int NLM = NL * NL;
@@ -366,7 +369,7 @@ struct DescShape {
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
     static constexpr int CHUNK = 32;
-    static constexpr int WARPS = 4;
+    static constexpr int WARPS = soap_tile_warps(TILE);
     // per-warp shared memory (floats): Y rows (odd stride NLM), R rows (stride
     // AMAX, read as broadcast float4), a rows (odd stride NL), pair species.
     // The FP64 coefficients of the power-spectrum phase reuse the same area.
@@ -389,9 +392,10 @@ struct DescShape {
 // constant contribution to c_{n,00} is added in FP64 afterwards (it dominates
 // c_{n,00}, and FP32 sums on top of it were the main descriptor error).
 // Power spectrum and |p| in FP64.
-template <int NS, int AMAX, int LMAX>
-__global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
-    using Sh = DescShape<NS, AMAX, LMAX>;
+template <int NS, int AMAX, int LMAX, int TILE>
+__global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
+    k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
+    using Sh = DescShape<NS, AMAX, LMAX, TILE>;
     constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, NF = Sh::NF, DIM = Sh::DIM;
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -638,7 +642,7 @@ __global__ void __launch_bounds__(128, 4) k_soap_expand(SoapParams P, SiteArgs S
 
 // ===================== adjoint force / virial ================================
 
-template <int NS, int AMAX, int LMAX>
+template <int NS, int AMAX, int LMAX, int TILE = 0>
 struct ForceShape {
     static constexpr int NL = LMAX + 1;
     static constexpr int NLM = NL * NL;
@@ -646,7 +650,7 @@ struct ForceShape {
     static constexpr int NF = AMAX + NL;
     static constexpr int DIM = NT * (NT + 1) / 2 * NL;
     static constexpr int SLOTS = (NLM + 31) / 32;
-    static constexpr int WARPS = 4;
+    static constexpr int WARPS = soap_tile_warps(TILE);
     static constexpr int BROW = NT + 4;            // row stride of B_l: rows read as float4, the
                                                    // transposed writes spread over the banks
     static constexpr int BSTRIDE = NT * BROW + 4;  // per-l stride (multiple of 4, 4 mod 32)
@@ -664,9 +668,10 @@ struct ForceShape {
 // One warp per central atom: dE/dq -> dE/dp (normalisation, FP64) -> B_l -> Gamma =
 // dE/dc (shared memory), then one lane per pair contracts Gamma with d(c)/d(r_j)
 // on the fly: F_j -= dE_i/dr_j, F_i += dE_i/dr_j, virial += 1/2 (f x + x f).
-template <int NS, int AMAX, int LMAX>
-__global__ void __launch_bounds__(128, 4) k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
-    using Sh = ForceShape<NS, AMAX, LMAX>;
+template <int NS, int AMAX, int LMAX, int TILE>
+__global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
+    k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
+    using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
     constexpr int NL = Sh::NL, NLM = Sh::NLM, NT = Sh::NT, NF = Sh::NF, DIM = Sh::DIM;
     extern __shared__ __align__(16) float smem[];
     __shared__ double vred[Sh::WARPS][6];
@@ -963,43 +968,66 @@ bool soap_shape_supported(int ns, int amax, int lmax) {
     return false;
 }
 
-template <int NS, int AMAX, int LMAX>
+template <int NS, int AMAX, int LMAX, int TILE>
 static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
-    using Sh = DescShape<NS, AMAX, LMAX>;
+    using Sh = DescShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX, TILE>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
-    if (grid > 0) k_soap_expand<NS, AMAX, LMAX><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
+    if (grid > 0) k_soap_expand<NS, AMAX, LMAX, TILE><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
 
-template <int NS, int AMAX, int LMAX>
+template <int NS, int AMAX, int LMAX, int TILE>
 static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st) {
-    using Sh = ForceShape<NS, AMAX, LMAX>;
+    using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX, TILE>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     *nblk = grid;
-    if (grid > 0) k_soap_force<NS, AMAX, LMAX><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
+    if (grid > 0) k_soap_force<NS, AMAX, LMAX, TILE><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
 
-int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
+template <int NS, int AMAX, int LMAX>
+static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
+                       int tile) {
+    switch (tile) {
+        case 1: return expand_impl<NS, AMAX, LMAX, 1>(P, S, O, st);
+        case 2: return expand_impl<NS, AMAX, LMAX, 2>(P, S, O, st);
+        case 3: return expand_impl<NS, AMAX, LMAX, 3>(P, S, O, st);
+        default: return expand_impl<NS, AMAX, LMAX, 0>(P, S, O, st);
+    }
+}
+
+template <int NS, int AMAX, int LMAX>
+static int force_tile(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
+                      int *nblk, cudaStream_t st, int tile) {
+    switch (tile) {
+        case 1: return force_impl<NS, AMAX, LMAX, 1>(P, S, I, O, nblk, st);
+        case 2: return force_impl<NS, AMAX, LMAX, 2>(P, S, I, O, nblk, st);
+        case 3: return force_impl<NS, AMAX, LMAX, 3>(P, S, I, O, nblk, st);
+        default: return force_impl<NS, AMAX, LMAX, 0>(P, S, I, O, nblk, st);
+    }
+}
+
+int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
+                       int tile) {
 #define X(a, b, c) \
-    if (P.ns == a && P.amax == b && P.lmax == c) return expand_impl<a, b, c>(P, S, O, st);
+    if (P.ns == a && P.amax == b && P.lmax == c) return expand_tile<a, b, c>(P, S, O, st, tile);
     TGB_SOAP_SHAPES(X)
 #undef X
     set_error("unsupported SOAP shape: n_species %d alpha_max %d l_max %d", P.ns, P.amax, P.lmax);
@@ -1007,9 +1035,10 @@ int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O,
 }
 
 int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
-                      int *nblk, cudaStream_t st) {
+                      int *nblk, cudaStream_t st, int tile) {
 #define X(a, b, c) \
-    if (P.ns == a && P.amax == b && P.lmax == c) return force_impl<a, b, c>(P, S, I, O, nblk, st);
+    if (P.ns == a && P.amax == b && P.lmax == c)    \
+        return force_tile<a, b, c>(P, S, I, O, nblk, st, tile);
     TGB_SOAP_SHAPES(X)
 #undef X
     set_error("unsupported SOAP shape: n_species %d alpha_max %d l_max %d", P.ns, P.amax, P.lmax);

@@ -131,9 +131,18 @@ int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cuda
 
 // Launchers; return TG_ERR_ARG for unsupported (ns, amax, lmax).
 bool soap_shape_supported(int ns, int amax, int lmax);
-int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st);
+// CTA tiles of the descriptor and force passes (the autotuner's choices):
+// tile 0: 4 sites per CTA, >= 4 CTAs per SM (128 registers); 1: 4 sites, >= 3
+// CTAs (168 registers); 2: 2 sites, >= 8 CTAs; 3: 8 sites, >= 2 CTAs.
+constexpr int kSoapTiles = 4;
+__host__ __device__ constexpr int soap_tile_warps(int t) { return t == 2 ? 2 : (t == 3 ? 8 : 4); }
+__host__ __device__ constexpr int soap_tile_minb(int t) {
+    return t == 1 ? 3 : (t == 2 ? 8 : (t == 3 ? 2 : 4));
+}
+int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
+                       int tile = 0);
 int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
-                      int *n_vpart_blocks, cudaStream_t st);
+                      int *n_vpart_blocks, cudaStream_t st, int tile = 0);
 int launch_virial_reduce(const double *vpart, int nblk, double *virial_out, cudaStream_t st);
 
 }  // namespace tgb
