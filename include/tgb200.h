@@ -154,6 +154,22 @@ int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const in
                   const int32_t *species_all, double *energies0, double *forces0,
                   double *virial);
 
+/* local_property_predict (src/local_properties.f90:174-294) with the current
+ * block holding the property model (tg_soap_begin with its sparse set, delta
+ * and zeta), through the get_gap_soap remap:
+ *   values(n_central)  V_i = max(0, delta^2 sum_s alpha_s K_is^zeta + v0) of
+ *                      the block's central sites, in batch order;
+ *   value_der(3, P)    (optional) dV_i/dr_j for every pair of those sites' lists,
+ *                      in the order of neighbors_list0 (the self pair holds
+ *                      dV_i/dr_i); zero for pairs the block does not see and
+ *                      for every pair of a site whose value was clamped to 0.
+ * The reference snaps zeta to an integer within 1e-10 here (1e-5 for energies);
+ * the device snaps within 1e-5 in both. */
+int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                          const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                          const int32_t *species_batch, const int32_t *species_all, double v0,
+                          double *values, double *value_der, int32_t *n_central);
+
 /* Descriptor only (soap_turbo get_soap as called at gap_interface.f90:320-325,
  * through the same remap): soap(dim, n_central) of the current block's central
  * sites in batch order. The Cartesian derivative array soap_cart_der is never

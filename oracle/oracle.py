@@ -414,3 +414,24 @@ def evaluate(positions, species, box, blocks, e0=None, neighbors_buffer=0.0, max
     if rc != 0:
         raise RuntimeError(f"oracle evaluate failed: {rc}")
     return en, f, vir.reshape(3, 3).T, int(npairs.value)
+
+
+def local_property_predict(soap, Qs, alphas, V0, delta, zeta, soap_cart_der, n_neigh):
+    """local_properties.f90:174-294 in numpy. soap (n_sites, D) and Qs (M, D) in
+    the same descriptor order; soap_cart_der (P, D, 3) per kept pair, site after
+    site (n_neigh). Returns V (n_sites) and V_der (P, 3), zero for clamped sites."""
+    K = soap @ Qs.T
+    zi = int(round(zeta))
+    z = zi if abs(zi - zeta) < 1e-10 else zeta
+    Kd = z * K ** (z - 1) * alphas[None, :]
+    V = delta ** 2 * (K ** z) @ alphas + V0
+    V = np.where(V < 0.0, 0.0, V)
+    Qss = delta ** 2 * Kd @ Qs
+    der = np.zeros((soap_cart_der.shape[0], 3))
+    k = 0
+    for i, nn in enumerate(n_neigh):
+        for _ in range(nn):
+            if V[i] != 0.0:
+                der[k] = Qss[i] @ soap_cart_der[k]
+            k += 1
+    return V, der

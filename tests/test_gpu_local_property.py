@@ -1,0 +1,58 @@
+"""Local-property prediction (local_properties.f90:174-294, the Hirshfeld-volume
+and dipole predictors' model) on the GPU against the oracle: per-site values
+with the V0 offset and the clamp at zero, and dV_i/dr_j for every pair of the
+caller's lists."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from _util import O, neighbor_data, sparse_block
+from turbogap_b200.hypers import carbon_hypers
+from turbogap_b200.synth import random_structure
+
+pytestmark = pytest.mark.gpu
+
+
+def _kept(st, h, nl):
+    """The block's kept pairs per site (self first), with their global indices."""
+    starts = np.concatenate([[0], np.cumsum(nl["n_neigh"])])
+    nn, idx = [], []
+    for i in range(st.n):
+        c = 0
+        for k in range(starts[i], starts[i + 1]):
+            if nl["rjs"][k] < h.rcut_max:
+                idx.append(k)
+                c += 1
+        nn.append(c)
+    return np.array(nn, np.int32), np.array(idx)
+
+
+@pytest.mark.parametrize("offset", ["none", "median"])
+def test_local_property_matches_oracle(gpu, offset):
+    h = carbon_hypers()
+    blk = sparse_block(h, 250, seed=91, sigma_alpha=0.002)
+    gpu.soap_backend_begin(blk, key=901)
+    st = random_structure(216, 12.91, 1.2, seed=92)
+    nl = neighbor_data(st, h.rcut_max + 0.4)      # lists longer than the block's cutoff
+    nn, idx = _kept(st, h, nl)
+    q, sder, _ = O.get_soap(O.HypersC(h), nn, np.ones((len(idx), 1), np.int32), nl["rjs"][idx],
+                            nl["xyz"][idx], derivatives=True)
+    v0 = 0.0
+    if offset == "median":   # half of the sites fall below zero and are clamped
+        v0 = -float(np.median(O.local_property_predict(q, blk.Qs, blk.alphas, 0.0, blk.delta,
+                                                       blk.zeta, sder, nn)[0]))
+    vals, der = gpu.get_local_property(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"],
+                                       nl["xyz"], st.species, st.species, v0=v0)
+    Vo, Do = O.local_property_predict(q, blk.Qs, blk.alphas, v0, blk.delta, blk.zeta, sder, nn)
+    assert vals.shape == (st.n,)
+    assert (Vo > 0.0).any()
+    if offset == "median":
+        assert (Vo == 0.0).sum() > st.n // 4              # the clamp and its zero derivatives
+    assert np.abs(vals - Vo).max() < 1e-7
+    full = np.zeros((len(nl["rjs"]), 3))
+    full[idx] = Do
+    assert np.abs(der - full).max() < 1e-6 * max(1.0, np.abs(full).max())
+    # pairs beyond the block's cutoff carry nothing
+    far = np.setdiff1d(np.arange(len(nl["rjs"])), idx)
+    assert len(far) > 0 and not der[far].any()

@@ -67,6 +67,8 @@ SIGNATURES = [
     ("tg_get_gap_soap", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, dp, dp, dp]),
     ("tg_get_soap", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, dp,
                               C.POINTER(C.c_int32)]),
+    ("tg_get_local_property", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, C.c_double,
+                                        dp, _vp, C.POINTER(C.c_int32)]),
     ("tg_family_begin", C.c_int, [C.c_int32, C.POINTER(TgFamily)]),
     ("tg_get_family", C.c_int, [C.c_int32, C.c_int32, C.c_int32, ip, ip, dp, dp, ip, dp, dp, dp]),
     ("tg_build_neighbors_list", C.c_int, [C.c_int32, dp, C.c_int32, dp, dp, dp, C.c_double, ip,

@@ -104,6 +104,22 @@ def soap_backend_end() -> None:
     check(lib().tg_soap_end())
 
 
+def get_local_property(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_batch,
+                       species_all, v0: float = 0.0, derivatives: bool = True):
+    """local_property_predict with the current block as the property model:
+    (values of the central sites, dV_i/dr_j per pair (P, 3) or None)."""
+    n = len(n_neigh0)
+    P = int(np.sum(n_neigh0))
+    vals = np.zeros(n)
+    der = np.zeros((P, 3)) if derivatives else None
+    nc = C.c_int32(0)
+    check(lib().tg_get_local_property(int(n_total_sites), n, _i32(n_neigh0), _i32(neighbors_list0),
+                                      _f64(rjs0), _f64(xyz0), _i32(species_batch),
+                                      _i32(species_all), float(v0), vals,
+                                      der.ctypes.data if derivatives else None, C.byref(nc)))
+    return vals[:nc.value], der
+
+
 _FAMILY_KIND = {"distance_2b": 1, "angle_3b": 2, "core_pot": 3}
 
 

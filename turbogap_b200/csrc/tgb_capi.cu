@@ -225,7 +225,7 @@ struct EventLog {
 int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
                    double *energies, double *virial, unsigned *err, cudaStream_t st,
                    EventLog *log = nullptr, const int *atom_struct = nullptr,
-                   double *vir_struct = nullptr) {
+                   double *vir_struct = nullptr, double *pair_grad = nullptr) {
     if (S.n_sites <= 0) return TG_OK;
     TGB_TRY(w.ensure(b, S.n_sites));
     const SoapParams P = b.params(n_atoms);
@@ -260,7 +260,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
     TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
-    ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct};
+    ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct, pair_grad};
     int nblk = 0;
     TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, w.tile_force));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
@@ -1041,6 +1041,69 @@ int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const in
         for (size_t q = 0; q < fo.size(); ++q) forces0[q] += fo[q];
     if (virial)
         for (int q = 0; q < 9; ++q) virial[q] += vr[q];
+    return TG_OK;
+}
+
+int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                          const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                          const int32_t *species_batch, const int32_t *species_all, double v0,
+                          double *values, double *value_der, int32_t *n_central) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
+    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0 && values && n_central, TG_ERR_ARG,
+              "bad local-property arguments");
+    *n_central = 0;
+    if (n_sites0 == 0) return TG_OK;
+    Block &b = *C.current;
+    DBuf<signed char> zf;
+    int64_t P = 0;
+    int nc = 0;
+    TGB_TRY(stage_batch(C, b, n_total_sites, n_sites0, n_neigh0, neighbors_list0, rjs0, xyz0,
+                        species_batch, species_all, &P, &nc, zf));
+    cudaStream_t st = C.st;
+    DBuf<double> pg;
+    TGB_TRY(C.en.ensure(n_total_sites));
+    TGB_TRY(C.fo.ensure(3 * (size_t)n_total_sites));
+    TGB_TRY(C.vir.ensure(9));
+    TGB_CUDA(cudaMemsetAsync(C.en.p, 0, sizeof(double) * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(C.fo.p, 0, sizeof(double) * 3 * n_total_sites, st));
+    TGB_CUDA(cudaMemsetAsync(C.vir.p, 0, sizeof(double) * 9, st));
+    if (value_der) {
+        TGB_TRY(pg.ensure(3 * (size_t)P));
+        TGB_CUDA(cudaMemsetAsync(pg.p, 0, sizeof(double) * 3 * P, st));
+    }
+    auto &wp = C.ws[b.key];
+    if (!wp) wp = std::make_unique<Workspace>();
+    SiteArgs S{nc, C.site_row.p, C.site_atom.p, C.pstart.p, C.nbr.p, C.xyz.p, C.spa.p};
+    TGB_TRY(evaluate_block(b, *wp, S, n_total_sites, C.fo.p, C.en.p, C.vir.p, C.err.p, st, nullptr,
+                           nullptr, nullptr, value_der ? pg.p : nullptr));
+    TGB_TRY(check_err_word(C, C.err.p));
+    std::vector<double> en(n_total_sites);
+    std::vector<int> rows(nc), atoms(nc);
+    std::vector<int64_t> ps(n_sites0 + 1);
+    TGB_CUDA(cudaMemcpyAsync(en.data(), C.en.p, sizeof(double) * n_total_sites, cudaMemcpyDeviceToHost, st));
+    if (nc > 0) {
+        TGB_CUDA(cudaMemcpyAsync(atoms.data(), C.site_atom.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+        TGB_CUDA(cudaMemcpyAsync(rows.data(), C.site_row.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+    }
+    TGB_CUDA(cudaMemcpyAsync(ps.data(), C.pstart.p, sizeof(int64_t) * (n_sites0 + 1), cudaMemcpyDeviceToHost, st));
+    if (value_der)
+        TGB_CUDA(cudaMemcpyAsync(value_der, pg.p, sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, st));
+    TGB_CUDA(cudaStreamSynchronize(st));
+    // local_properties.f90:244-270: V = delta^2 sum_s alpha_s K^zeta + V0, negative
+    // values clamped to zero together with their derivatives
+    for (int i = 0; i < nc; ++i) {
+        double v = en[atoms[i]] + v0;
+        if (v < 0.0) {
+            v = 0.0;
+            if (value_der)
+                for (int64_t p = ps[rows[i]]; p < ps[rows[i] + 1]; ++p)
+                    for (int q = 0; q < 3; ++q) value_der[3 * p + q] = 0.0;
+        }
+        values[i] = v;
+    }
+    *n_central = nc;
     return TG_OK;
 }
 

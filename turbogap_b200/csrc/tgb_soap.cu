@@ -902,6 +902,11 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
             atomicAdd(&O.forces[3 * (size_t)ja], (double)fx);
             atomicAdd(&O.forces[3 * (size_t)ja + 1], (double)fy);
             atomicAdd(&O.forces[3 * (size_t)ja + 2], (double)fz);
+            if (O.pair_grad) {   // d E_i / d r_j = -f_pair
+                O.pair_grad[3 * p] = -(double)fx;
+                O.pair_grad[3 * p + 1] = -(double)fy;
+                O.pair_grad[3 * p + 2] = -(double)fz;
+            }
             fs[0] -= fx; fs[1] -= fy; fs[2] -= fz;
             // virial += 1/2 (f x + x f), packed xx yy zz xy xz yz
             vir[0] += (double)fx * X;
@@ -913,6 +918,8 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         }
 #pragma unroll
         for (int qd = 0; qd < 3; ++qd) fs[qd] = warp_sum(fs[qd]);
+        if (lane == 0 && O.pair_grad)   // the self pair: d E_i / d r_i = -sum_j d E_i / d r_j
+            for (int qd = 0; qd < 3; ++qd) O.pair_grad[3 * p0 + qd] = -fs[qd];
         if (lane == 0) {
             atomicAdd(&O.forces[3 * (size_t)catom], fs[0]);
             atomicAdd(&O.forces[3 * (size_t)catom + 1], fs[1]);

@@ -107,6 +107,9 @@ struct ForceOut {
     // optional (batches): each site's virial is also added to vir_struct[atom_struct[atom]]
     const int *atom_struct = nullptr;
     double *vir_struct = nullptr;   // [n_structs][9]
+    // optional (local properties): d E_site / d r_j per pair of the site lists,
+    // (3, P) in list order; the self pair gets d E_site / d r_site
+    double *pair_grad = nullptr;
 };
 
 // Host-side construction of the FP64 tables on the device.
