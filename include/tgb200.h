@@ -66,6 +66,19 @@ typedef struct {
     const double *atom_sigma_t_scaling;
     const double *amplitude_scaling;
     const double *central_weight;
+    /* SOAP compression: compress_P_nonzero, compress_P_i/j/el (types.f90:92-110,
+     * filled at read_files.f90:5166-5231) and the compressed dim (the file's
+     * header, read_files.f90:5171). compress_P_nonzero = 0 (and dim ignored)
+     * leaves the descriptor uncompressed. Otherwise the descriptor has dim
+     * components, q_c(i) = sum over entries k with compress_P_i[k] = i of
+     * compress_P_el[k] * p(compress_P_j[k]) (1-based; p is the power spectrum in
+     * the uncompressed order n <= n', l), normalised after the map; Qs then has
+     * dim rows. */
+    int32_t dim;
+    int32_t compress_P_nonzero;
+    const int32_t *compress_P_i;
+    const int32_t *compress_P_j;
+    const double *compress_P_el;
 } tg_soap_hypers;
 
 /* ---- device context: gpu_context_init / gpu_context_finalize
@@ -84,8 +97,11 @@ const char *tg_last_error(void);
  *      (src/gap.f90:49-64). Uploads Qs(dim, n_sparse) (column-major, one sparse
  *      point per column, src/read_files.f90:707-720) and alphas(n_sparse), builds
  *      the radial/angular tables, and makes the block current. The upload is
- *      cached by block_key: a later begin with the same key and n_sparse reuses
- *      the device copy (the GPU branch of the reference uploads per call). */
+ *      cached by block_key: a later begin with the same key, n_sparse, precision
+ *      and descriptor shape (species, alpha_max, l_max, central species,
+ *      compression) reuses the device copy (the GPU branch of the reference
+ *      uploads per call); another shape uploads again, and engines made on the
+ *      earlier block keep it. */
 int tg_soap_begin(int32_t block_key, const tg_soap_hypers *hypers, int32_t n_sparse,
                   const double *Qs, const double *alphas, double delta, double zeta,
                   int32_t precision);

@@ -42,6 +42,9 @@ class _Hypers(C.Structure):
         ("atom_sigma_r", C.POINTER(C.c_double)), ("atom_sigma_r_scaling", C.POINTER(C.c_double)),
         ("atom_sigma_t", C.POINTER(C.c_double)), ("atom_sigma_t_scaling", C.POINTER(C.c_double)),
         ("amplitude_scaling", C.POINTER(C.c_double)), ("central_weight", C.POINTER(C.c_double)),
+        ("compress_dim", C.c_int), ("compress_nonzero", C.c_int),
+        ("compress_i", C.POINTER(C.c_int)), ("compress_j", C.POINTER(C.c_int)),
+        ("compress_el", C.POINTER(C.c_double)),
     ]
 
 
@@ -193,7 +196,8 @@ class HypersC:
     (``n_species, l_max, radial_enhancement, central_species, alpha_max,
     species_z, rcut_hard, rcut_soft, nf, global_scaling, atom_sigma_r,
     atom_sigma_r_scaling, atom_sigma_t, atom_sigma_t_scaling,
-    amplitude_scaling, central_weight``)."""
+    amplitude_scaling, central_weight``, and optionally ``compress`` with
+    ``dim, P_i, P_j, P_el``: 1-based compression entries)."""
 
     _dfields = ("rcut_hard", "rcut_soft", "nf", "global_scaling", "atom_sigma_r",
                 "atom_sigma_r_scaling", "atom_sigma_t", "atom_sigma_t_scaling",
@@ -214,6 +218,15 @@ class HypersC:
             a = _f64(getattr(h, name))
             self.keep[name] = a
             setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        comp = getattr(h, "compress", None)
+        if comp is not None and len(comp.P_el) > 0:
+            s.compress_dim = int(comp.dim)
+            s.compress_nonzero = int(len(comp.P_el))
+            for name, arr, ct in (("compress_i", _i32(comp.P_i), C.c_int),
+                                  ("compress_j", _i32(comp.P_j), C.c_int),
+                                  ("compress_el", _f64(comp.P_el), C.c_double)):
+                self.keep[name] = arr
+                setattr(s, name, arr.ctypes.data_as(C.POINTER(ct)))
         self.struct = s
         self.dim = lib().orc_soap_dim(C.byref(s))
 

@@ -376,8 +376,10 @@ int orc_soap_n_tot(const orc_soap_hypers *h) {
     return n;
 }
 
-// read_files.f90:5233-5235
+// read_files.f90:5233-5235; a compressed block has the dim its compression
+// gives (read_files.f90:5171, 5213-5216)
 int orc_soap_dim(const orc_soap_hypers *h) {
+    if (h->compress_nonzero > 0) return h->compress_dim;
     const int n = orc_soap_n_tot(h);
     return n * (n + 1) / 2 * (h->l_max + 1);
 }
@@ -603,13 +605,17 @@ void orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int
                   const int *mask, const double *rjs, const double *xyz, double *soap,
                   double *soap_cart_der, double *sqrt_dot_p) {
     const int ns = h->n_species, L = h->l_max, L2 = (L + 1) * (L + 1);
-    const int n_tot = orc_soap_n_tot(h), dim = orc_soap_dim(h);
+    const int n_tot = orc_soap_n_tot(h), dimf = n_tot * (n_tot + 1) / 2 * (L + 1);
+    // compression: the power spectrum p (dimf entries) is mapped to v = P p
+    // (dim entries) and v is normalised; uncompressed, v = p
+    const bool comp = h->compress_nonzero > 0;
+    const int dim = comp ? h->compress_dim : dimf;
     std::vector<int> ch0(ns + 1, 0);
     for (int s = 0; s < ns; ++s) ch0[s + 1] = ch0[s] + h->alpha_max[s];
     std::vector<int64_t> start(n_sites + 1, 0);
     for (int i = 0; i < n_sites; ++i) start[i + 1] = start[i] + n_neigh[i];
     // power-spectrum index table: d -> (n, n', l)
-    std::vector<int> pn(dim), pn2(dim), pl(dim);
+    std::vector<int> pn(dimf), pn2(dimf), pl(dimf);
     {
         int d = 0;
         for (int n = 0; n < n_tot; ++n)
@@ -620,7 +626,16 @@ void orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int
 #pragma omp parallel
     {
         std::vector<double> c((size_t)n_tot * L2), Y(L2), dY(3 * L2), R(16 * 4), dR(16 * 4),
-            a(L + 1), da(L + 1), p(dim), dc, dp(3 * (size_t)dim);
+            a(L + 1), da(L + 1), p(dimf), dc, dp(3 * (size_t)dimf), v(dim), dv(3 * (size_t)dim);
+        // v = P p over the nonzero entries (1-based i, j), in file order
+        auto compress = [&](const double *x, double *y, int stride) {
+            std::fill(y, y + (size_t)stride * dim, 0.0);
+            for (int k = 0; k < h->compress_nonzero; ++k) {
+                const int i = h->compress_i[k] - 1, j = h->compress_j[k] - 1;
+                for (int q = 0; q < stride; ++q)
+                    y[(size_t)stride * i + q] += h->compress_el[k] * x[(size_t)stride * j + q];
+            }
+        };
 #pragma omp for schedule(dynamic, 4)
         for (int i = 0; i < n_sites; ++i) {
             const int64_t k0 = start[i], nn = n_neigh[i];
@@ -666,22 +681,24 @@ void orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int
                     }
                 }
             }
-            // power spectrum and normalisation
-            double nrm2 = 0.0;
-            for (int d = 0; d < dim; ++d) {
+            // power spectrum, compression and normalisation
+            for (int d = 0; d < dimf; ++d) {
                 const int n = pn[d], n2 = pn2[d], l = pl[d];
-                double v = 0.0;
+                double pv = 0.0;
                 for (int m = -l; m <= l; ++m) {
                     const int lm = l * l + l + m;
-                    v += c[(size_t)n * L2 + lm] * c[(size_t)n2 * L2 + lm];
+                    pv += c[(size_t)n * L2 + lm] * c[(size_t)n2 * L2 + lm];
                 }
-                if (n != n2) v *= sqrt2;
-                p[d] = v;
-                nrm2 += v * v;
+                if (n != n2) pv *= sqrt2;
+                p[d] = pv;
             }
+            if (comp) compress(p.data(), v.data(), 1);
+            else std::copy(p.begin(), p.end(), v.begin());
+            double nrm2 = 0.0;
+            for (int d = 0; d < dim; ++d) nrm2 += v[d] * v[d];
             const double nrm = std::sqrt(nrm2);
             if (sqrt_dot_p) sqrt_dot_p[i] = nrm;
-            for (int d = 0; d < dim; ++d) soap[(size_t)i * dim + d] = nrm > 0.0 ? p[d] / nrm : 0.0;
+            for (int d = 0; d < dim; ++d) soap[(size_t)i * dim + d] = nrm > 0.0 ? v[d] / nrm : 0.0;
             if (!soap_cart_der) continue;
             double *self_der = soap_cart_der + (size_t)k0 * 3 * dim;
             std::fill(self_der, self_der + 3 * (size_t)dim, 0.0);
@@ -689,27 +706,28 @@ void orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int
                 double *out = soap_cart_der + (size_t)(k0 + kk) * 3 * dim;
                 if (nrm == 0.0) { std::fill(out, out + 3 * (size_t)dim, 0.0); continue; }
                 const double *dck = &dc[(size_t)kk * n_tot * L2 * 3];
-                double qdp[3] = {0, 0, 0};
-                for (int d = 0; d < dim; ++d) {
+                for (int d = 0; d < dimf; ++d) {
                     const int n = pn[d], n2 = pn2[d], l = pl[d];
-                    double v[3] = {0, 0, 0};
+                    double g[3] = {0, 0, 0};
                     for (int m = -l; m <= l; ++m) {
                         const int lm = l * l + l + m;
                         const double *g1 = &dck[((size_t)n * L2 + lm) * 3];
                         const double *g2 = &dck[((size_t)n2 * L2 + lm) * 3];
                         const double c1 = c[(size_t)n * L2 + lm], c2 = c[(size_t)n2 * L2 + lm];
-                        for (int q = 0; q < 3; ++q) v[q] += g1[q] * c2 + c1 * g2[q];
+                        for (int q = 0; q < 3; ++q) g[q] += g1[q] * c2 + c1 * g2[q];
                     }
                     const double mu = (n != n2) ? sqrt2 : 1.0;
-                    for (int q = 0; q < 3; ++q) {
-                        dp[3 * (size_t)d + q] = mu * v[q];
-                        qdp[q] += (p[d] / nrm) * mu * v[q];
-                    }
+                    for (int q = 0; q < 3; ++q) dp[3 * (size_t)d + q] = mu * g[q];
                 }
+                if (comp) compress(dp.data(), dv.data(), 3);
+                else std::copy(dp.begin(), dp.end(), dv.begin());
+                double qdp[3] = {0, 0, 0};
+                for (int d = 0; d < dim; ++d)
+                    for (int q = 0; q < 3; ++q) qdp[q] += (v[d] / nrm) * dv[3 * (size_t)d + q];
                 for (int d = 0; d < dim; ++d) {
-                    const double qd = p[d] / nrm;
+                    const double qd = v[d] / nrm;
                     for (int q = 0; q < 3; ++q) {
-                        const double val = (dp[3 * (size_t)d + q] - qd * qdp[q]) / nrm;
+                        const double val = (dv[3 * (size_t)d + q] - qd * qdp[q]) / nrm;
                         out[3 * (size_t)d + q] = val;
                         self_der[3 * (size_t)d + q] -= val;
                     }

@@ -54,6 +54,17 @@ typedef struct {
     const double *atom_sigma_t_scaling;
     const double *amplitude_scaling;
     const double *central_weight;
+    /* SOAP compression (types.f90:92-110 compress_P_*, filled at
+     * read_files.f90:5166-5231). compress_nonzero = 0: uncompressed. Otherwise
+     * the descriptor has compress_dim components, q_c(i) = sum over entries k
+     * with compress_i[k] = i of compress_el[k] * p(compress_j[k]) (1-based; j
+     * in the uncompressed order n <= n', l), and q_c is normalised after the map
+     * (parity unpinned: soap_turbo is absent). */
+    int compress_dim;
+    int compress_nonzero;
+    const int *compress_i;
+    const int *compress_j;
+    const double *compress_el;
 } orc_soap_hypers;
 
 /* ---- geometry: neighbors.f90 ------------------------------------------- */

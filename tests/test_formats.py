@@ -122,9 +122,9 @@ def test_compress_file_both_forms(tmp_path):
                            [1.0], [1.0], [1.0], l_max=2, compress_soap=True,
                            file_compress=p2.name)
     assert spec.compression(str(tmp_path)).dim == 2
-    with pytest.raises(NotImplementedError):
-        spec.load(["C"], str(tmp_path))
     spec.file_compress, spec.compress_mode = "none", "trivial"
+    assert spec.compression(str(tmp_path)).dim == 8 * 9 // 2 * 3 - 7 * 8 // 2 * 3
+    spec.compress_mode = "0_0"
     with pytest.raises(NotImplementedError, match="get_compress_indices"):
         spec.compression(str(tmp_path))
 

@@ -42,6 +42,9 @@ class TgSoapHypers(C.Structure):
         ("atom_sigma_r", C.POINTER(C.c_double)), ("atom_sigma_r_scaling", C.POINTER(C.c_double)),
         ("atom_sigma_t", C.POINTER(C.c_double)), ("atom_sigma_t_scaling", C.POINTER(C.c_double)),
         ("amplitude_scaling", C.POINTER(C.c_double)), ("central_weight", C.POINTER(C.c_double)),
+        ("dim", C.c_int32), ("compress_P_nonzero", C.c_int32),
+        ("compress_P_i", C.POINTER(C.c_int32)), ("compress_P_j", C.POINTER(C.c_int32)),
+        ("compress_P_el", C.POINTER(C.c_double)),
     ]
 
 

@@ -88,6 +88,12 @@ class _HypersC:
         s.atom_sigma_t_scaling = darr(h.atom_sigma_t_scaling)
         s.amplitude_scaling = darr(h.amplitude_scaling)
         s.central_weight = darr(h.central_weight)
+        if h.compress is not None:
+            s.dim = h.compress.dim
+            s.compress_P_nonzero = len(h.compress.P_el)
+            s.compress_P_i = iarr(h.compress.P_i)
+            s.compress_P_j = iarr(h.compress.P_j)
+            s.compress_P_el = darr(h.compress.P_el)
         self.struct = s
 
 

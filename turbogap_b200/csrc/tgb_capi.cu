@@ -56,11 +56,18 @@ struct DBuf {
 
 static int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// Largest compressed descriptor accepted (the GEMM operands grow with it).
+constexpr int kMaxCompressedDim = 16384;
+
 // ---------------------------------------------------------------- blocks
 struct Block {
     int key = 0, precision = TG_PREC_BF16X3;
     SoapHostHypers hh{};
     int ns = 0, amax = 0, lmax = 0, ntot = 0, nlm = 0, dim = 0;
+    // dim: entries of the descriptor rows the GEMMs see. Uncompressed, dim = dimf
+    // (the power spectrum); compressed, dim = dimc (the transformation's own dim)
+    // rounded up to a multiple of 8 with zero entries.
+    int dimf = 0, dimc = 0;
     int M = 0, Mpad = 0, K1 = 0, K2 = 0, nsplit = 3, n_etiles = 0, tw = 0;
     int KD = 0;   // stored kd row: [hi | lo] (bf16x3) or [hi]; GEMM 2 reads hi twice
     double delta = 1.0, zeta = 1.0, rcut_max = 0.0;
@@ -71,8 +78,17 @@ struct Block {
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
     DBuf<float> g0f;       // g0 in fp32: subtracted from the MLP's dE/dq rows
-    DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d
+    DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d (-1: padding)
     TmaMap tmB1{}, tmB2{};
+    // compression matrix C (dim x dimf) as CSR by row and by column
+    DBuf<int> c_row_ptr, c_row_col, c_col_ptr, c_col_row;
+    DBuf<double> c_row_val, c_col_val;
+
+    bool compressed() const { return dimc > 0; }
+    CompressArgs cargs() const {
+        return CompressArgs{dimf, c_row_ptr.p, c_row_col.p, c_row_val.p,
+                            c_col_ptr.p, c_col_row.p, c_col_val.p};
+    }
 
     SoapParams params(int n_atoms) const {
         SoapParams P{};
@@ -89,6 +105,7 @@ struct Block {
         P.self_R = selfR.p;
         P.mu = mu.p;
         P.g0 = g0.p;
+        P.raw = compressed() ? 1 : 0;
         return P;
     }
 };
@@ -98,9 +115,11 @@ struct Workspace {
     int cap = 0;
     DBuf<__nv_bfloat16> qsplit, kd;
     DBuf<float> q, c, g;
+    DBuf<double> praw;         // compressed blocks: p, [n][dimf]
+    DBuf<float> gfull;         //   and dE/dp
     DBuf<double> pnorm, epart, kdsum, qoff, vpart;
     TmaMap tmA1{}, tmA2{}, tmKd{};   // tmKd: the GAP epilogue's TMA stores into kd
-    int tm_rows = -1;
+    int tm_rows = -1, tm_k1 = -1, tm_kd = -1;
     const void *tm_p1 = nullptr, *tm_p2 = nullptr;
     int tile_desc = 0, tile_force = 0;   // CTA tiles of the two SOAP passes (autotuned)
 
@@ -108,7 +127,8 @@ struct Workspace {
         const int n = n_sites > 0 ? n_sites : 1;
         if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.KD ||
             qsplit.n < (size_t)n * b.K1 || c.n < (size_t)n * b.ntot * b.nlm ||
-            epart.n < (size_t)n * b.n_etiles || kdsum.n < (size_t)n * b.n_etiles) {
+            epart.n < (size_t)n * b.n_etiles || kdsum.n < (size_t)n * b.n_etiles ||
+            (b.compressed() && (praw.n < (size_t)n * b.dimf || gfull.n < (size_t)n * b.dimf))) {
             const int nc = n > cap ? n : cap;
             TGB_TRY(qsplit.ensure((size_t)nc * b.K1));
             TGB_TRY(kd.ensure((size_t)nc * b.KD));
@@ -120,15 +140,21 @@ struct Workspace {
             TGB_TRY(kdsum.ensure((size_t)nc * b.n_etiles));
             TGB_TRY(qoff.ensure(nc));
             TGB_TRY(vpart.ensure((size_t)9 * ((nc + 1) / 2 + 1)));   // the 2-site tile
+            if (b.compressed()) {
+                TGB_TRY(praw.ensure((size_t)nc * b.dimf));
+                TGB_TRY(gfull.ensure((size_t)nc * b.dimf));
+            }
             cap = nc;
         }
-        if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p) {
+        if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p || tm_k1 != b.K1 || tm_kd != b.KD) {
             TGB_TRY(make_tma_bf16(&tmA1, qsplit.p, n, b.K1, b.K1, kGemmBM));
             TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.KD, b.KD, kGemmBM));
             TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, n, b.KD, b.KD));
             tm_rows = n;
             tm_p1 = qsplit.p;
             tm_p2 = kd.p;
+            tm_k1 = b.K1;
+            tm_kd = b.KD;
         }
         return TG_OK;
     }
@@ -221,6 +247,27 @@ struct EventLog {
         if (log) TGB_TRY((log)->mark((p), (st))); \
     } while (0)
 
+// The descriptor pass: the SOAP expansion and power spectrum, and for a
+// compressed block the compression after it (the expansion then leaves the raw
+// power spectrum in praw).
+int descriptor_pass(const Block &b, Workspace &w, const SoapParams &P, const SiteArgs &S,
+                    cudaStream_t st, int tile) {
+    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p, w.praw.p};
+    TGB_TRY(launch_soap_expand(P, S, O, st, tile));
+    if (!b.compressed()) return TG_OK;
+    return launch_compress_forward(P, b.cargs(), S.n_sites, w.praw.p, O, st);
+}
+
+// The force pass; a compressed block first takes dE/dq back to dE/dp.
+int force_pass(const Block &b, Workspace &w, const SoapParams &P, const SiteArgs &S, ForceIn I,
+               const ForceOut &FO, int *nblk, cudaStream_t st, int tile) {
+    if (b.compressed()) {
+        TGB_TRY(launch_compress_adjoint(P, b.cargs(), S.n_sites, I, w.gfull.p, st));
+        I.g = w.gfull.p;
+    }
+    return launch_soap_force(P, S, I, FO, nblk, st, tile);
+}
+
 // Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces.
 int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
                    double *energies, double *virial, unsigned *err, cudaStream_t st,
@@ -229,8 +276,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     if (S.n_sites <= 0) return TG_OK;
     TGB_TRY(w.ensure(b, S.n_sites));
     const SoapParams P = b.params(n_atoms);
-    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
-    TGB_TRY(launch_soap_expand(P, S, O, st, w.tile_desc));
+    TGB_TRY(descriptor_pass(b, w, P, S, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
     GemmEpi e1{};
     e1.mode = EPI_GAP_KERNEL;
@@ -262,7 +308,7 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct, pair_grad};
     int nblk = 0;
-    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, w.tile_force));
+    TGB_TRY(force_pass(b, w, P, S, I, FO, &nblk, st, w.tile_force));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
     TGB_MARK(log, PASS_FORCE, st);
     return TG_OK;
@@ -297,8 +343,11 @@ int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     if (S.n_sites <= 0) return TG_OK;
     TGB_TRY(evaluate_block(b, w, S, n_atoms, forces, energies, virial, err, st));
     const SoapParams P = b.params(n_atoms);
-    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
-    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
+    // the tiles apply to the expansion and force kernels (a compressed block's
+    // expansion writes praw and its force kernel reads gfull)
+    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p, w.praw.p};
+    ForceIn I{b.compressed() ? w.gfull.p : w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p,
+              b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
     cudaEvent_t e0, e1;
     TGB_CUDA(cudaEventCreate(&e0));
@@ -448,8 +497,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     TGB_CHECK(x.mlp->L.D == b.dim, TG_ERR_ARG, "MLP input size %d does not match block dim %d",
               x.mlp->L.D, b.dim);
     const SoapParams P = b.params(n_atoms);
-    DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p};
-    TGB_TRY(launch_soap_expand(P, S, O, st, w.tile_desc));
+    TGB_TRY(descriptor_pass(b, w, P, S, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
     TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim,
                       b.g0f.p, st));
@@ -497,7 +545,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
     ForceOut FO{forces, energies, w.vpart.p, err};
     int nblk = 0;
-    TGB_TRY(launch_soap_force(P, S, I, FO, &nblk, st, w.tile_force));
+    TGB_TRY(force_pass(b, w, P, S, I, FO, &nblk, st, w.tile_force));
     TGB_TRY(launch_virial_reduce(w.vpart.p, nblk, virial, st));
     TGB_MARK(log, PASS_FORCE, st);
     return TG_OK;
@@ -510,6 +558,9 @@ struct Context {
     int device = -1;
     cudaStream_t st = nullptr;
     std::map<int, std::unique_ptr<Block>> blocks;
+    // blocks replaced under their key by a begin of another shape: engines made
+    // before the replacement still point at them, so they live until finalize
+    std::vector<std::unique_ptr<Block>> retired;
     std::map<int, std::unique_ptr<Family>> families;   // 2b / 3b / core_pot, same key space
     std::map<int, std::unique_ptr<Workspace>> ws;
     Block *current = nullptr;
@@ -607,18 +658,69 @@ int tg_memory_budget(double *max_gbytes) {
     return TG_OK;
 }
 
+// Whether a cached block can stand for a begin with these arguments: the same
+// sparse-set size, precision and descriptor shape (species, alpha_max, l_max,
+// compression), so that every buffer a caller sizes from the hypers matches.
+static bool same_shape(const Block &b, const tg_soap_hypers &h, int n_sparse, int precision) {
+    if (b.M != n_sparse || b.precision != precision || b.hh.ns != h.n_species ||
+        b.hh.lmax != h.l_max || b.hh.central_species != h.central_species)
+        return false;
+    for (int s = 0; s < b.hh.ns; ++s)
+        if (b.hh.alpha_max[s] != h.alpha_max[s] || b.hh.species_z[s] != h.species_z[s]) return false;
+    const int dimc = h.compress_P_nonzero > 0 ? h.dim : 0;
+    return b.dimc == dimc && (dimc == 0 || b.c_row_col.n == (size_t)h.compress_P_nonzero);
+}
+
+// The compression matrix of a block as two CSR copies on the device: by
+// compressed row (forward pass) and by internal power-spectrum column (adjoint).
+// Entries keep the caller's order within a row or column.
+static int upload_compression(Block &b, const tg_soap_hypers &h) {
+    std::vector<int> inv(b.dimf);
+    for (int d = 0; d < b.dimf; ++d) inv[descriptor_ref_index(d, b.ntot, b.lmax + 1)] = d;
+    const int nz = h.compress_P_nonzero;
+    std::vector<int> rp(b.dim + 1, 0), cp(b.dimf + 1, 0), rc(nz), cr(nz);
+    std::vector<double> rv(nz), cv(nz);
+    for (int k = 0; k < nz; ++k) {
+        ++rp[h.compress_P_i[k]];
+        ++cp[inv[h.compress_P_j[k] - 1] + 1];
+    }
+    for (int i = 0; i < b.dim; ++i) rp[i + 1] += rp[i];
+    for (int j = 0; j < b.dimf; ++j) cp[j + 1] += cp[j];
+    std::vector<int> rf(rp.begin(), rp.end() - 1), cf(cp.begin(), cp.end() - 1);
+    for (int k = 0; k < nz; ++k) {
+        const int i = h.compress_P_i[k] - 1, j = inv[h.compress_P_j[k] - 1];
+        rc[rf[i]] = j;
+        rv[rf[i]++] = h.compress_P_el[k];
+        cr[cf[j]] = i;
+        cv[cf[j]++] = h.compress_P_el[k];
+    }
+    TGB_TRY(b.c_row_ptr.ensure(b.dim + 1));
+    TGB_TRY(b.c_col_ptr.ensure(b.dimf + 1));
+    TGB_TRY(b.c_row_col.ensure(nz));
+    TGB_TRY(b.c_col_row.ensure(nz));
+    TGB_TRY(b.c_row_val.ensure(nz));
+    TGB_TRY(b.c_col_val.ensure(nz));
+    TGB_CUDA(cudaMemcpy(b.c_row_ptr.p, rp.data(), sizeof(int) * rp.size(), cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_col_ptr.p, cp.data(), sizeof(int) * cp.size(), cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_row_col.p, rc.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_col_row.p, cr.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_row_val.p, rv.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_col_val.p, cv.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    return TG_OK;
+}
+
 int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, const double *Qs,
                   const double *alphas, double delta, double zeta, int32_t precision) {
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(!C.families.count(block_key), TG_ERR_ARG, "key %d already names a 2b/3b/core_pot family",
               block_key);
+    TGB_CHECK(h && Qs && alphas, TG_ERR_ARG, "null hypers/Qs/alphas");
     auto it = C.blocks.find(block_key);
-    if (it != C.blocks.end() && it->second->M == n_sparse && it->second->precision == precision) {
+    if (it != C.blocks.end() && same_shape(*it->second, *h, n_sparse, precision)) {
         C.current = it->second.get();
         return TG_OK;
     }
-    TGB_CHECK(h && Qs && alphas, TG_ERR_ARG, "null hypers/Qs/alphas");
     TGB_CHECK(h->n_species >= 1 && h->n_species <= kMaxSpecies, TG_ERR_ARG,
               "n_species %d outside 1..%d", h->n_species, kMaxSpecies);
     TGB_CHECK(precision == TG_PREC_BF16X3 || precision == TG_PREC_BF16, TG_ERR_ARG,
@@ -666,7 +768,23 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
               "unsupported SOAP shape: n_species %d alpha_max %d l_max %d", b->ns, b->amax, b->lmax);
     b->ntot = b->ns * b->amax;
     b->nlm = (b->lmax + 1) * (b->lmax + 1);
-    b->dim = b->ntot * (b->ntot + 1) / 2 * (b->lmax + 1);
+    b->dimf = b->ntot * (b->ntot + 1) / 2 * (b->lmax + 1);
+    b->dimc = 0;
+    b->dim = b->dimf;
+    if (h->compress_P_nonzero > 0) {
+        // read_files.f90:5166-5231: q_c(i) = sum P_el p(P_j) over P_i = i (1-based)
+        TGB_CHECK(h->compress_P_i && h->compress_P_j && h->compress_P_el, TG_ERR_ARG,
+                  "compression entries are null");
+        TGB_CHECK(h->dim >= 1 && h->dim <= kMaxCompressedDim, TG_ERR_ARG,
+                  "compressed dim %d outside 1..%d", h->dim, kMaxCompressedDim);
+        for (int k = 0; k < h->compress_P_nonzero; ++k)
+            TGB_CHECK(h->compress_P_i[k] >= 1 && h->compress_P_i[k] <= h->dim &&
+                          h->compress_P_j[k] >= 1 && h->compress_P_j[k] <= b->dimf,
+                      TG_ERR_ARG, "compression entry %d (%d, %d) outside %d x %d", k + 1,
+                      h->compress_P_i[k], h->compress_P_j[k], h->dim, b->dimf);
+        b->dimc = h->dim;
+        b->dim = round_up(h->dim, 8);
+    }
     b->nsplit = precision == TG_PREC_BF16X3 ? 3 : 1;
     b->M = n_sparse;
     b->Mpad = round_up(n_sparse, 64);
@@ -697,14 +815,22 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     TGB_TRY(b->aoff.ensure(b->Mpad));
     TGB_TRY(b->g0.ensure(b->dim));
     TGB_TRY(b->ref_index.ensure(b->dim));
-    // The device keeps descriptor entries in its internal order (l-major); the
-    // sparse set is permuted into that order once here.
+    // The device keeps power-spectrum entries in its internal order (l-major);
+    // the sparse set is permuted into that order once here. A compressed block's
+    // entries stay in the transformation's order, padded with zeros to dim, and
+    // the transformation's columns are permuted instead.
     std::vector<int> ref(b->dim);
-    for (int d = 0; d < b->dim; ++d) ref[d] = descriptor_ref_index(d, b->ntot, b->lmax + 1);
-    std::vector<double> Qi((size_t)n_sparse * b->dim);
+    const int qdim = b->compressed() ? b->dimc : b->dim;   // rows of the caller's Qs
+    if (b->compressed()) {
+        for (int d = 0; d < b->dim; ++d) ref[d] = d < b->dimc ? d : -1;
+        TGB_TRY(upload_compression(*b, *h));
+    } else {
+        for (int d = 0; d < b->dim; ++d) ref[d] = descriptor_ref_index(d, b->ntot, b->lmax + 1);
+    }
+    std::vector<double> Qi((size_t)n_sparse * b->dim, 0.0);
     for (int s = 0; s < n_sparse; ++s)
         for (int d = 0; d < b->dim; ++d)
-            Qi[(size_t)s * b->dim + d] = Qs[(size_t)s * b->dim + ref[d]];
+            if (ref[d] >= 0) Qi[(size_t)s * b->dim + d] = Qs[(size_t)s * qdim + ref[d]];
     Qs = Qi.data();
     TGB_CUDA(cudaMemcpy(b->ref_index.p, ref.data(), sizeof(int) * b->dim, cudaMemcpyHostToDevice));
     // Centre of the sparse set (FP64): the GEMMs run on q - mu and q_s - mu, the
@@ -751,6 +877,8 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     TGB_TRY(make_tma_bf16(&b->tmB2, b->QsT.p, b->dim, b->K2, b->K2, kGemmBN));
     TGB_CUDA(cudaStreamSynchronize(C.st));
     C.current = b.get();
+    auto old = C.blocks.find(block_key);
+    if (old != C.blocks.end()) C.retired.push_back(std::move(old->second));
     C.blocks[block_key] = std::move(b);
     return TG_OK;
 }
@@ -807,13 +935,15 @@ __global__ void k_seen(int n_sites, const int *__restrict__ site_row, const int6
 
 // q = mu + delta (rows of dim)
 // q = mu + delta, written back in the reference order of the descriptor entries.
-__global__ void k_d2f(int64_t n, int dim, const float *__restrict__ a, const double *__restrict__ mu,
-                      const int *__restrict__ ref_index, double *__restrict__ b) {
+__global__ void k_d2f(int64_t n, int dim, int dim_out, const float *__restrict__ a,
+                      const double *__restrict__ mu, const int *__restrict__ ref_index,
+                      double *__restrict__ b) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t site = i / dim;
     const int d = (int)(i - site * dim);
-    b[site * dim + ref_index[d]] = mu[d] + (double)a[i];
+    const int r = ref_index[d];
+    if (r >= 0) b[site * dim_out + r] = mu[d] + (double)a[i];
 }
 
 __global__ void k_gather_species(int64_t P, const int *__restrict__ nbr, const int *__restrict__ sp,
@@ -1129,14 +1259,14 @@ int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0
     TGB_TRY(wp->ensure(b, nc));
     SiteArgs S{nc, C.site_row.p, C.site_atom.p, C.pstart.p, C.nbr.p, C.xyz.p, C.spa.p};
     const SoapParams Pm = b.params(n_total_sites);
-    DescOut O{wp->qsplit.p, wp->q.p, wp->qoff.p, wp->pnorm.p, wp->c.p};
-    TGB_TRY(launch_soap_expand(Pm, S, O, C.st));
+    TGB_TRY(descriptor_pass(b, *wp, Pm, S, C.st, 0));
+    const int dout = b.compressed() ? b.dimc : b.dim;
     DBuf<double> out;
-    TGB_TRY(out.ensure((size_t)nc * b.dim));
-    k_d2f<<<grid_for((int64_t)nc * b.dim), 256, 0, C.st>>>((int64_t)nc * b.dim, b.dim, wp->q.p,
+    TGB_TRY(out.ensure((size_t)nc * dout));
+    k_d2f<<<grid_for((int64_t)nc * b.dim), 256, 0, C.st>>>((int64_t)nc * b.dim, b.dim, dout, wp->q.p,
                                                             b.mu.p, b.ref_index.p, out.p);
     TGB_CUDA(cudaGetLastError());
-    TGB_CUDA(cudaMemcpyAsync(soap, out.p, sizeof(double) * nc * b.dim, cudaMemcpyDeviceToHost, C.st));
+    TGB_CUDA(cudaMemcpyAsync(soap, out.p, sizeof(double) * nc * dout, cudaMemcpyDeviceToHost, C.st));
     TGB_CUDA(cudaStreamSynchronize(C.st));
     return TG_OK;
 }

@@ -391,8 +391,10 @@ struct DescShape {
 // accumulates c_{n,lm} over the chunk's pairs in FP32. The central atom's
 // constant contribution to c_{n,00} is added in FP64 afterwards (it dominates
 // c_{n,00}, and FP32 sums on top of it were the main descriptor error).
-// Power spectrum and |p| in FP64.
-template <int NS, int AMAX, int LMAX, int TILE>
+// Power spectrum and |p| in FP64. RAW (compressed blocks, P.raw): the power
+// spectrum goes to O.praw in FP64 for the compression pass, and the kernel stops
+// there; a separate instantiation, so the uncompressed kernels keep their code.
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
 __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
     k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
     using Sh = DescShape<NS, AMAX, LMAX, TILE>;
@@ -576,8 +578,12 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                     if (a != b) {
                         const double v0 = d[0] * 1.4142135623730951, v1 = d[1] * 1.4142135623730951;
                         nrm2 += v0 * v0 + v1 * v1;
-                        *reinterpret_cast<float2 *>(qrow + base + 2 * lane) =
-                            make_float2((float)v0, (float)v1);
+                        if constexpr (RAW)
+                            *reinterpret_cast<double2 *>(O.praw + (size_t)site * DIM + base +
+                                                         2 * lane) = make_double2(v0, v1);
+                        else
+                            *reinterpret_cast<float2 *>(qrow + base + 2 * lane) =
+                                make_float2((float)v0, (float)v1);
                     } else {
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
@@ -585,10 +591,13 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                             if (g8 > j) continue;
                             const double v = g8 != j ? d[e] * 1.4142135623730951 : d[e];
                             nrm2 += v * v;
-                            qrow[base + g8 * 8 - (g8 * (g8 - 1)) / 2 + (j - g8)] = (float)v;
+                            const int u = base + g8 * 8 - (g8 * (g8 - 1)) / 2 + (j - g8);
+                            if constexpr (RAW) O.praw[(size_t)site * DIM + u] = v;
+                            else qrow[u] = (float)v;
                         }
                     }
                 }
+        if constexpr (RAW) return;
         nrm2 = warp_sum(nrm2);
         inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
         __syncwarp();   // the warp's p entries are visible to every lane
@@ -617,6 +626,13 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
             }
         }
     } else {
+        if constexpr (RAW) {
+#pragma unroll
+            for (int l = 0; l < NL; ++l)
+                for (int pi = lane; pi < NP; pi += 32)
+                    O.praw[(size_t)site * DIM + l * NP + pi] = power(l, pi);
+            return;
+        }
         // pass 1: |p| (FP64)
 #pragma unroll
         for (int l = 0; l < NL; ++l)
@@ -668,7 +684,9 @@ struct ForceShape {
 // One warp per central atom: dE/dq -> dE/dp (normalisation, FP64) -> B_l -> Gamma =
 // dE/dc (shared memory), then one lane per pair contracts Gamma with d(c)/d(r_j)
 // on the fly: F_j -= dE_i/dr_j, F_i += dE_i/dr_j, virial += 1/2 (f x + x f).
-template <int NS, int AMAX, int LMAX, int TILE>
+// RAW (compressed blocks, P.raw): I.g already holds dE/dp, from the compression's
+// adjoint; a separate instantiation, so the uncompressed kernels keep their code.
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
 __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
     k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
     using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
@@ -725,46 +743,50 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                 Bl[n2 * Sh::BROW + n] = v;
             }
         };
-        double dot = 0.0;
-        if constexpr (VEC) {
-            for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
-                const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
-                const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
-                const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
-                const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
-                const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
-                dot += (ksum * m0.x + z0.x + (double)gv.x) * (m0.x + (double)qv.x);
-                dot += (ksum * m0.y + z0.y + (double)gv.y) * (m0.y + (double)qv.y);
-                dot += (ksum * m1.x + z1.x + (double)gv.z) * (m1.x + (double)qv.z);
-                dot += (ksum * m1.y + z1.y + (double)gv.w) * (m1.y + (double)qv.w);
-            }
+        if constexpr (RAW) {
+            for (int d = lane; d < DIM; d += 32) put_b(d, (double)g[d], 0.0, 0.0, 1.0);
         } else {
-            for (int d = lane; d < DIM; d += 32) {
-                const double mu = P.mu[d];
-                dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
+            double dot = 0.0;
+            if constexpr (VEC) {
+                for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
+                    const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
+                    const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
+                    const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
+                    const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                    const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
+                    const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                    dot += (ksum * m0.x + z0.x + (double)gv.x) * (m0.x + (double)qv.x);
+                    dot += (ksum * m0.y + z0.y + (double)gv.y) * (m0.y + (double)qv.y);
+                    dot += (ksum * m1.x + z1.x + (double)gv.z) * (m1.x + (double)qv.z);
+                    dot += (ksum * m1.y + z1.y + (double)gv.w) * (m1.y + (double)qv.w);
+                }
+            } else {
+                for (int d = lane; d < DIM; d += 32) {
+                    const double mu = P.mu[d];
+                    dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
+                }
             }
-        }
-        dot = warp_sum(dot);
-        const double nrm = I.pnorm[site];
-        const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-        if constexpr (VEC) {
-            for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
-                const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
-                const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
-                const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
-                const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
-                const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
-                put_b(d0, ksum * m0.x + z0.x + (double)gv.x, m0.x + (double)qv.x, dot, inv);
-                put_b(d0 + 1, ksum * m0.y + z0.y + (double)gv.y, m0.y + (double)qv.y, dot, inv);
-                put_b(d0 + 2, ksum * m1.x + z1.x + (double)gv.z, m1.x + (double)qv.z, dot, inv);
-                put_b(d0 + 3, ksum * m1.y + z1.y + (double)gv.w, m1.y + (double)qv.w, dot, inv);
-            }
-        } else {
-            for (int d = lane; d < DIM; d += 32) {
-                const double mu = P.mu[d];
-                put_b(d, ksum * mu + P.g0[d] + (double)g[d], mu + (double)q[d], dot, inv);
+            dot = warp_sum(dot);
+            const double nrm = I.pnorm[site];
+            const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+            if constexpr (VEC) {
+                for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
+                    const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
+                    const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
+                    const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
+                    const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                    const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
+                    const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                    put_b(d0, ksum * m0.x + z0.x + (double)gv.x, m0.x + (double)qv.x, dot, inv);
+                    put_b(d0 + 1, ksum * m0.y + z0.y + (double)gv.y, m0.y + (double)qv.y, dot, inv);
+                    put_b(d0 + 2, ksum * m1.x + z1.x + (double)gv.z, m1.x + (double)qv.z, dot, inv);
+                    put_b(d0 + 3, ksum * m1.y + z1.y + (double)gv.w, m1.y + (double)qv.w, dot, inv);
+                }
+            } else {
+                for (int d = lane; d < DIM; d += 32) {
+                    const double mu = P.mu[d];
+                    put_b(d, ksum * mu + P.g0[d] + (double)g[d], mu + (double)q[d], dot, inv);
+                }
             }
         }
         __syncwarp();
@@ -964,6 +986,106 @@ __global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, doub
     if (threadIdx.x == 0) atomicAdd(out + q, s);   // blocks may reduce concurrently
 }
 
+// ===================== SOAP compression =====================================
+
+// One warp per site: v = C p (FP64), |v| in FP64, then
+// q = v / |v| leaves as the uncompressed pass leaves it: delta = q - mu (fp32
+// row, bf16 split rows) and delta . mu. v is formed twice (once for |v|, once
+// for the output) instead of being staged: a row of C has a handful of entries.
+__global__ void __launch_bounds__(256) k_compress_fwd(SoapParams P, CompressArgs C, int n_sites,
+                                                      const double *__restrict__ praw, DescOut O) {
+    const int lane = threadIdx.x & 31;
+    const int site = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (site >= n_sites) return;
+    const double *p = praw + (size_t)site * C.dimf;
+    const int D = P.dim;
+    auto row = [&](int i) {
+        double v = 0.0;
+        for (int k = C.row_ptr[i]; k < C.row_ptr[i + 1]; ++k)
+            v += C.row_val[k] * p[C.row_col[k]];
+        return v;
+    };
+    double nrm2 = 0.0;
+    for (int i = lane; i < D; i += 32) {
+        const double v = row(i);
+        nrm2 += v * v;
+    }
+    nrm2 = warp_sum(nrm2);
+    const double inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
+    __nv_bfloat16 *qs = O.qsplit + (size_t)site * P.K1;
+    float *qrow = O.q + (size_t)site * D;
+    double off = 0.0;
+    for (int i = lane; i < D; i += 32) {
+        const double mu = P.mu[i];
+        const double dl = row(i) * inv - mu;
+        off += dl * mu;
+        const float df = (float)dl;
+        qrow[i] = df;
+        __nv_bfloat16 hi, lo;
+        bf16_split(df, hi, lo);
+        qs[i] = hi;
+        if (P.nsplit == 3) {
+            qs[D + i] = hi;
+            qs[2 * D + i] = lo;
+        }
+    }
+    for (int k = P.nsplit * D + lane; k < P.K1; k += 32) qs[k] = __float2bfloat16_rn(0.f);
+    off = warp_sum(off);
+    if (lane == 0) {
+        O.pnorm[site] = sqrt(nrm2);
+        O.qoff[site] = off;
+    }
+}
+
+// One warp per site: dE/dq = ksum mu + g0 + g (as the force pass forms it),
+// dE/dv = (dE/dq - (dE/dq . q) q) / |v| in FP64, and dE/dp = C^T dE/dv, one
+// column of C per lane step (dE/dv is re-formed per entry from the rows).
+__global__ void __launch_bounds__(256) k_compress_adj(SoapParams P, CompressArgs C, int n_sites,
+                                                      ForceIn I, float *__restrict__ gfull) {
+    const int lane = threadIdx.x & 31;
+    const int site = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (site >= n_sites) return;
+    const int D = P.dim;
+    const float *g = I.g + (size_t)site * D;
+    const float *q = I.q + (size_t)site * D;
+    double ksum = 0.0;
+    for (int t = lane; t < I.n_etiles; t += 32) ksum += I.kdsum[(size_t)site * I.n_etiles + t];
+    ksum = warp_sum(ksum);
+    double dot = 0.0;
+    for (int i = lane; i < D; i += 32) {
+        const double mu = P.mu[i];
+        dot += (ksum * mu + P.g0[i] + (double)g[i]) * (mu + (double)q[i]);
+    }
+    dot = warp_sum(dot);
+    const double nrm = I.pnorm[site];
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    float *out = gfull + (size_t)site * C.dimf;
+    for (int j = lane; j < C.dimf; j += 32) {
+        double acc = 0.0;
+        for (int k = C.col_ptr[j]; k < C.col_ptr[j + 1]; ++k) {
+            const int i = C.col_row[k];
+            const double mu = P.mu[i];
+            const double gi = ksum * mu + P.g0[i] + (double)g[i];
+            acc += C.col_val[k] * (gi - dot * (mu + (double)q[i])) * inv;
+        }
+        out[j] = (float)acc;
+    }
+}
+
+int launch_compress_forward(const SoapParams &P, const CompressArgs &C, int n_sites,
+                            const double *praw, const DescOut &O, cudaStream_t st) {
+    if (n_sites > 0) k_compress_fwd<<<(n_sites + 7) / 8, 256, 0, st>>>(P, C, n_sites, praw, O);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_compress_adjoint(const SoapParams &P, const CompressArgs &C, int n_sites,
+                            const ForceIn &I, float *gfull, cudaStream_t st) {
+    if (n_sites > 0) k_compress_adj<<<(n_sites + 7) / 8, 256, 0, st>>>(P, C, n_sites, I, gfull);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
 // ===================== launchers ============================================
 
 #define TGB_SOAP_SHAPES(X) X(1, 8, 8) X(2, 8, 8) X(1, 8, 6) X(2, 8, 6) X(1, 4, 4) X(2, 4, 4)
@@ -975,36 +1097,38 @@ bool soap_shape_supported(int ns, int amax, int lmax) {
     return false;
 }
 
-template <int NS, int AMAX, int LMAX, int TILE>
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
 static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
     using Sh = DescShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX, TILE>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX, TILE, RAW>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
-    if (grid > 0) k_soap_expand<NS, AMAX, LMAX, TILE><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
+    if (grid > 0)
+        k_soap_expand<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
 
-template <int NS, int AMAX, int LMAX, int TILE>
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
 static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st) {
     using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX, TILE>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX, TILE, RAW>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     *nblk = grid;
-    if (grid > 0) k_soap_force<NS, AMAX, LMAX, TILE><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
+    if (grid > 0)
+        k_soap_force<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -1012,6 +1136,11 @@ static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, 
 template <int NS, int AMAX, int LMAX>
 static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
                        int tile) {
+    // compressed blocks: one tile (the compression passes dominate their cost)
+    if (P.raw) {
+        TGB_CHECK(O.praw != nullptr, TG_ERR_ARG, "a compressed block needs DescOut::praw");
+        return expand_impl<NS, AMAX, LMAX, 0, true>(P, S, O, st);
+    }
     switch (tile) {
         case 1: return expand_impl<NS, AMAX, LMAX, 1>(P, S, O, st);
         case 2: return expand_impl<NS, AMAX, LMAX, 2>(P, S, O, st);
@@ -1023,6 +1152,8 @@ static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O,
 template <int NS, int AMAX, int LMAX>
 static int force_tile(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st, int tile) {
+    // compressed blocks: one tile (the compression passes dominate their cost)
+    if (P.raw) return force_impl<NS, AMAX, LMAX, 0, true>(P, S, I, O, nblk, st);
     switch (tile) {
         case 1: return force_impl<NS, AMAX, LMAX, 1>(P, S, I, O, nblk, st);
         case 2: return force_impl<NS, AMAX, LMAX, 2>(P, S, I, O, nblk, st);

@@ -23,6 +23,12 @@ struct SoapParams {
     const float *self_R;       // [ns][amax]: central-atom contribution to c_{n,00}
     const double *mu;          // [dim]: mean of the sparse set; the GEMMs see q - mu
     const double *g0;          // [dim]: sum_s kcoef_s (q_s - mu), the K = 1 part of dE/dq
+    // 1 for a compressed block: the descriptor pass writes the raw power spectrum
+    // p (FP64, all NT (NT + 1) / 2 (l_max + 1) entries, internal order) to
+    // DescOut::praw and stops there, and the force pass reads ForceIn::g as dE/dp
+    // in that order; both run their tile 0. The compression passes between them
+    // work in the compressed space of dim.
+    int raw;
 };
 
 // Per-launch site addressing: site i reads CSR row site_row[i] of the pair
@@ -86,6 +92,7 @@ struct DescOut {
     double *qoff;            // [n_sites]: delta . mu (FP64)
     double *pnorm;           // [n_sites]
     float *c;                // [n_sites][ntot][nlm]
+    double *praw = nullptr;  // compressed blocks: [n_sites][NT (NT + 1) / 2 (l_max + 1)], p
 };
 
 struct ForceIn {
@@ -147,5 +154,27 @@ int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O,
 int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *n_vpart_blocks, cudaStream_t st, int tile = 0);
 int launch_virial_reduce(const double *vpart, int nblk, double *virial_out, cudaStream_t st);
+
+// SOAP compression (soap_turbo's compress_P_*): q = v / |v| with v = C p, C a
+// sparse (dim x dimf) matrix, p the raw power spectrum in the internal order.
+// Rows of C at or above the transformation's own dim are empty (zero padding to
+// the GEMM row length).
+struct CompressArgs {
+    int dimf;                 // uncompressed entries per site (columns of C)
+    const int *row_ptr;       // [dim + 1]: CSR of C by compressed index
+    const int *row_col;       //   internal index of p
+    const double *row_val;
+    const int *col_ptr;       // [dimf + 1]: CSR of C^T by internal index of p
+    const int *col_row;       //   compressed index
+    const double *col_val;
+};
+// praw [n_sites][dimf] -> O.q, O.qsplit, O.qoff, O.pnorm in the compressed space
+// (the outputs of the uncompressed descriptor pass, same layouts, P.dim entries).
+int launch_compress_forward(const SoapParams &P, const CompressArgs &C, int n_sites,
+                            const double *praw, const DescOut &O, cudaStream_t st);
+// dE/dq (I.g, I.kdsum, I.q, I.pnorm in the compressed space) -> dE/dp
+// [n_sites][dimf] through the normalisation and C^T.
+int launch_compress_adjoint(const SoapParams &P, const CompressArgs &C, int n_sites,
+                            const ForceIn &I, float *gfull, cudaStream_t st);
 
 }  // namespace tgb

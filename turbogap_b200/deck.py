@@ -8,10 +8,10 @@ step 0, the last step and every ``write_xyz`` steps, holding the positions the
 forces were evaluated at (turbogap_md.f90:357-380). ``run_predict`` evaluates
 every frame of the atoms file (``turbogap predict``).
 
-soap_turbo blocks and the distance_2b, angle_3b and core_pot families run on
-the device. Decks that need anything else (thermostats, barostats, adaptive
-time steps, compressed descriptors, non-orthorhombic boxes) are refused with the
-keyword that needs it. Velocities drawn here (no velocity
+soap_turbo blocks (compressed ones included) and the distance_2b, angle_3b and
+core_pot families run on the device. Decks that need anything else
+(thermostats, barostats, adaptive time steps, non-orthorhombic boxes) are
+refused with the keyword that needs it. Velocities drawn here (no velocity
 column, or ``randomize_velocities``) follow md.f90:95-158 with numpy's
 generator, so they differ from the reference's random stream.
 """

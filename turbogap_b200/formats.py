@@ -27,7 +27,7 @@ from typing import Dict, Iterator, List, Optional, Sequence
 
 import numpy as np
 
-from .hypers import GapBlock, SoapTurboHypers
+from .hypers import GapBlock, SoapCompression, SoapTurboHypers, trivial_compression
 
 AMU_TO_EV_FS2_A2 = 103.6426965268      # read_files.f90:1301, xyz.f90:466
 EV_PER_A3_TO_BAR = 1602176.6208        # turbogap.f90:95
@@ -122,9 +122,12 @@ class CompressSpec:
 
     def matrix(self, full_dim: int) -> np.ndarray:
         """The dense (dim, full_dim) transformation."""
-        P = np.zeros((self.dim, full_dim))
-        np.add.at(P, (self.P_i - 1, self.P_j - 1), self.P_el)
-        return P
+        return self.compression().matrix(full_dim)
+
+    def compression(self) -> SoapCompression:
+        """The transformation as the block's hyperparameters carry it (the
+        header's alpha_max and l_max are read and not used, as in the reference)."""
+        return SoapCompression(self.dim, self.P_i, self.P_j, self.P_el)
 
 
 def read_compress_file(path: str, n_species: int) -> CompressSpec:
@@ -241,28 +244,37 @@ class SoapTurboSpec:
             central_species=self.central_species, basis=self.basis,
             scaling_mode=self.scaling_mode)
 
-    def compression(self, base_dir: str = ".") -> Optional[CompressSpec]:
+    def compression(self, base_dir: str = ".") -> Optional[SoapCompression]:
         """The compression transformation when compress_soap is set. A file
-        takes precedence over compress_mode (read_files.f90:5162-5165)."""
+        takes precedence over compress_mode (read_files.f90:5162-5165). Of the
+        named modes (get_compress_indices in soap_turbo, which is not part of
+        the reference tree) "trivial" is built as the reference's generator of
+        compress files writes it; other modes are refused."""
         if not self.compress_soap:
             return None
         if self.file_compress != "none":
-            return read_compress_file(os.path.join(base_dir, self.file_compress), self.n_species)
+            return read_compress_file(os.path.join(base_dir, self.file_compress),
+                                      self.n_species).compression()
+        if self.compress_mode == "trivial":
+            if self.l_max is None:
+                raise ValueError("soap_turbo block without l_max")
+            return trivial_compression(self.alpha_max, self.l_max)
         if self.compress_mode != "none":
             raise NotImplementedError(
-                f"compress_mode {self.compress_mode!r}: the recipes live in soap_turbo's "
-                "get_compress_indices, which is not part of the reference tree; give a "
-                "file_compress_soap instead")
+                f"compress_mode {self.compress_mode!r}: only \"trivial\" is available (the "
+                "other recipes live in soap_turbo's get_compress_indices, which is not part "
+                "of the reference tree); give a file_compress_soap instead")
         raise ValueError("compress_soap needs file_compress_soap or compress_mode")
 
     def load(self, species_types: Sequence[str], base_dir: str = ".") -> GapBlock:
         """The block with its sparse set, ready for soap_backend_begin.
 
         Paths in the file are relative to the directory the run starts in
-        (``base_dir``). Compressed descriptors are not on the device path."""
+        (``base_dir``). A compressed block carries its transformation, and its
+        sparse descriptors have the compressed dim."""
         h = self.hypers(species_types)
         if self.compress_soap:
-            raise NotImplementedError("compress_soap blocks are not on the device path")
+            h.compress = self.compression(base_dir)
         if self.file_desc is None or self.file_alphas is None:
             raise ValueError("soap_turbo block without desc_sparse / alphas_sparse")
         alphas, Qs, _ = read_alphas_and_descriptors(os.path.join(base_dir, self.file_desc),

@@ -11,9 +11,57 @@ rcut_hard - buffer (read_files.f90:5101-5108).
 from __future__ import annotations
 
 from dataclasses import dataclass, field
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
+
+
+@dataclass
+class SoapCompression:
+    """soap_turbo compression (``compress_P_*``, types.f90:92-110, filled at
+    read_files.f90:5166-5231): the descriptor has ``dim`` components,
+    q_c(i) = sum of P_el(k) p(P_j(k)) over the entries k with P_i(k) = i
+    (1-based; p in the uncompressed order n <= n', l), normalised after the map."""
+    dim: int
+    P_i: np.ndarray
+    P_j: np.ndarray
+    P_el: np.ndarray
+
+    def __post_init__(self):
+        self.dim = int(self.dim)
+        self.P_i = np.ascontiguousarray(self.P_i, dtype=np.int32)
+        self.P_j = np.ascontiguousarray(self.P_j, dtype=np.int32)
+        self.P_el = np.ascontiguousarray(self.P_el, dtype=np.float64)
+        if not (self.P_i.shape == self.P_j.shape == self.P_el.shape) or self.P_i.ndim != 1:
+            raise ValueError("compression entries need matching P_i, P_j, P_el")
+        if self.dim < 1 or len(self.P_el) < 1:
+            raise ValueError("compression needs dim >= 1 and at least one entry")
+
+    def matrix(self, full_dim: int) -> np.ndarray:
+        """The dense (dim, full_dim) transformation."""
+        P = np.zeros((self.dim, full_dim))
+        np.add.at(P, (self.P_i.astype(np.int64) - 1, self.P_j.astype(np.int64) - 1), self.P_el)
+        return P
+
+
+def trivial_compression(alpha_max: Sequence[int], l_max: int) -> SoapCompression:
+    """compress_mode "trivial", as the reference's generator of compress files
+    writes it (tools/compress_indices/compress_indices.py:39-57): keep the
+    components (n, n', l), n <= n', in which n or n' is the first radial
+    channel of some species; P_el = 1."""
+    nmax = [int(a) for a in alpha_max]
+    pivots = set(np.cumsum([0] + nmax[:-1]).tolist())    # 0-based first channel per species
+    ntot = sum(nmax)
+    keep = []
+    k = 0
+    for n in range(ntot):
+        for n2 in range(n, ntot):
+            for _ in range(l_max + 1):
+                k += 1
+                if n in pivots or n2 in pivots:
+                    keep.append(k)
+    d = len(keep)
+    return SoapCompression(d, np.arange(1, d + 1), np.array(keep), np.ones(d))
 
 
 @dataclass
@@ -35,6 +83,7 @@ class SoapTurboHypers:
     central_species: int = 0        # 1-based index into species_z; 0 = every atom
     basis: str = "poly3"
     scaling_mode: str = "polynomial"
+    compress: Optional[SoapCompression] = None
 
     def __post_init__(self):
         n = len(self.species_z)
@@ -85,10 +134,23 @@ class SoapTurboHypers:
         return int(sum(self.alpha_max))
 
     @property
-    def dim(self) -> int:
+    def uncompressed_dim(self) -> int:
         # read_files.f90:5233-5235
         n = self.n_max
         return n * (n + 1) // 2 * (self.l_max + 1)
+
+    @property
+    def dim(self) -> int:
+        """Components of the descriptor the kernel sees: the compressed dim when
+        the block is compressed (read_files.f90:5171, 5213-5216)."""
+        return self.compress.dim if self.compress is not None else self.uncompressed_dim
+
+    @property
+    def device_dim(self) -> int:
+        """Row length of descriptor and dE/dq rows on the device (the input size
+        of a mixed-form MLP): dim, or a compressed dim rounded up to a multiple
+        of 8 with zero components."""
+        return self.dim if self.compress is None else (self.dim + 7) // 8 * 8
 
     @property
     def n_lm(self) -> int:
