@@ -310,3 +310,27 @@ def test_three_body_and_core_pot_blocks(tmp_path):
     assert cp.species == (2, 2) and cp.x.tolist() == [0.5, 1.0, 1.5]
     assert cp.V[:2].tolist() == [8.0, 4.0] and abs(cp.V[2]) < 1e-15   # tapered to 0 at 1.5
     assert cp.yp1 == 1e50 and cp.ypn == 0.0 and g.rcut_max == 3.5
+
+
+def test_compressed_block_round_trip(tmp_path):
+    """A compressed block written as .gap + sparse set + compress file loads back
+    with the same transformation and descriptors."""
+    from turbogap_b200.hypers import GapBlock, SoapCompression, carbon_hypers
+    rng = np.random.default_rng(5)
+    comp = SoapCompression(20, np.arange(1, 21).repeat(2), rng.integers(1, 325, size=40),
+                           rng.normal(size=40))
+    h = carbon_hypers()
+    h.compress = comp
+    blk = GapBlock(h, rng.normal(size=(6, 20)), rng.normal(size=6))
+    F.write_sparse_set(blk, str(tmp_path / "d.dat"), str(tmp_path / "a.dat"))
+    F.write_compress_file(str(tmp_path / "c.dat"), comp, h.alpha_max, h.l_max)
+    with open(tmp_path / "x.gap", "w") as fh:
+        F.write_soap_block(fh, F.spec_from_block(blk, ["C"], "d.dat", "a.dat", "c.dat"))
+    b2 = F.read_gap_file(str(tmp_path / "x.gap")).soap_turbo[0].load(["C"], str(tmp_path))
+    assert b2.hypers.dim == 20 and b2.hypers.uncompressed_dim == 324
+    assert np.array_equal(b2.hypers.compress.P_i, comp.P_i)
+    assert np.array_equal(b2.hypers.compress.P_j, comp.P_j)
+    assert np.array_equal(b2.hypers.compress.P_el, comp.P_el)
+    assert np.array_equal(b2.Qs, blk.Qs)
+    with pytest.raises(ValueError, match="compress file"):
+        F.spec_from_block(blk, ["C"], "d.dat", "a.dat")

@@ -11,17 +11,21 @@ from _util import O, sparse_block
 from turbogap_b200 import deck as D
 from turbogap_b200 import formats as F
 from turbogap_b200 import synth
-from turbogap_b200.hypers import carbon_hypers
+from turbogap_b200.hypers import SoapCompression, carbon_hypers
 
 pytestmark = pytest.mark.gpu
 
 
-def _write_deck(d, nsteps, dt, e0, extra="", write_xyz=4, temperature=900.0):
+def _write_deck(d, nsteps, dt, e0, extra="", write_xyz=4, temperature=900.0, compress=None):
     h = carbon_hypers()
+    h.compress = compress
     blk = sparse_block(h, 300, seed=61)
     F.write_sparse_set(blk, str(d / "desc_C.dat"), str(d / "alphas_C.dat"))
+    if compress is not None:
+        F.write_compress_file(str(d / "compress_C.dat"), compress, h.alpha_max, h.l_max)
     with open(d / "c.gap", "w") as fh:
-        F.write_soap_block(fh, F.spec_from_block(blk, ["C"], "desc_C.dat", "alphas_C.dat"))
+        F.write_soap_block(fh, F.spec_from_block(blk, ["C"], "desc_C.dat", "alphas_C.dat",
+                                                 "compress_C.dat" if compress else None))
     st = synth.random_structure(216, 12.91, 1.2, seed=62)
     m = np.full(st.n, 12.011 * F.AMU_TO_EV_FS2_A2)
     v = synth.maxwell_velocities(m, temperature, 63)
@@ -57,9 +61,24 @@ def _oracle_md(blk, fr, m, nsteps, dt, e0):
     return np.array(rows), frames
 
 
-def test_deck_md_matches_oracle(gpu, tmp_path):
+def _transformation(full_dim, dim, seed):
+    rng = np.random.default_rng(seed)
+    P_i = np.concatenate([np.arange(1, dim + 1), rng.integers(1, dim + 1, size=dim)])
+    P_j = rng.integers(1, full_dim + 1, size=2 * dim)
+    return SoapCompression(dim, P_i, P_j, rng.uniform(0.2, 1.0, size=2 * dim))
+
+
+@pytest.mark.parametrize("compressed", [False, True])
+def test_deck_md_matches_oracle(gpu, tmp_path, compressed):
+    """compressed: the potential's block names a compress file (P_transformation
+    of 50 rows over the 324 components), which the deck loader hands to the
+    device with the sparse set."""
     nsteps, dt, e0 = 9, 1.0, -0.125
-    blk, fr, m = _write_deck(tmp_path, nsteps, dt, e0)
+    comp = _transformation(324, 50, 65) if compressed else None
+    blk, fr, m = _write_deck(tmp_path, nsteps, dt, e0, compress=comp)
+    if compressed:
+        g = F.read_gap_file(str(tmp_path / "c.gap"))
+        assert g.soap_turbo[0].compress_soap and g.soap_turbo[0].file_compress == "compress_C.dat"
     out = tmp_path / "run"
     res = D.run_md(str(tmp_path / "input"), str(out))
     ref, frames = _oracle_md(blk, fr, m, nsteps, dt, e0)

@@ -81,13 +81,14 @@ struct Block {
     DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d (-1: padding)
     TmaMap tmB1{}, tmB2{};
     // compression matrix C (dim x dimf) as CSR by row and by column
-    DBuf<int> c_row_ptr, c_row_col, c_col_ptr, c_col_row;
+    DBuf<int> c_row_ptr, c_row_col, c_col_idx, c_col_ptr, c_col_row;
     DBuf<double> c_row_val, c_col_val;
+    int c_ncols = 0;
 
     bool compressed() const { return dimc > 0; }
     CompressArgs cargs() const {
         return CompressArgs{dimf, c_row_ptr.p, c_row_col.p, c_row_val.p,
-                            c_col_ptr.p, c_col_row.p, c_col_val.p};
+                            c_ncols, c_col_idx.p, c_col_ptr.p, c_col_row.p, c_col_val.p};
     }
 
     SoapParams params(int n_atoms) const {
@@ -694,14 +695,24 @@ static int upload_compression(Block &b, const tg_soap_hypers &h) {
         cr[cf[j]] = i;
         cv[cf[j]++] = h.compress_P_el[k];
     }
+    // the adjoint walks only the columns that have entries
+    std::vector<int> cidx, cptr(1, 0);
+    for (int j = 0; j < b.dimf; ++j)
+        if (cp[j + 1] > cp[j]) {
+            cidx.push_back(j);
+            cptr.push_back(cp[j + 1]);
+        }
+    b.c_ncols = (int)cidx.size();
     TGB_TRY(b.c_row_ptr.ensure(b.dim + 1));
-    TGB_TRY(b.c_col_ptr.ensure(b.dimf + 1));
+    TGB_TRY(b.c_col_idx.ensure(b.c_ncols));
+    TGB_TRY(b.c_col_ptr.ensure(b.c_ncols + 1));
     TGB_TRY(b.c_row_col.ensure(nz));
     TGB_TRY(b.c_col_row.ensure(nz));
     TGB_TRY(b.c_row_val.ensure(nz));
     TGB_TRY(b.c_col_val.ensure(nz));
     TGB_CUDA(cudaMemcpy(b.c_row_ptr.p, rp.data(), sizeof(int) * rp.size(), cudaMemcpyHostToDevice));
-    TGB_CUDA(cudaMemcpy(b.c_col_ptr.p, cp.data(), sizeof(int) * cp.size(), cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_col_idx.p, cidx.data(), sizeof(int) * cidx.size(), cudaMemcpyHostToDevice));
+    TGB_CUDA(cudaMemcpy(b.c_col_ptr.p, cptr.data(), sizeof(int) * cptr.size(), cudaMemcpyHostToDevice));
     TGB_CUDA(cudaMemcpy(b.c_row_col.p, rc.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
     TGB_CUDA(cudaMemcpy(b.c_col_row.p, cr.data(), sizeof(int) * nz, cudaMemcpyHostToDevice));
     TGB_CUDA(cudaMemcpy(b.c_row_val.p, rv.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));

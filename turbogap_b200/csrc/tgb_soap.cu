@@ -14,6 +14,7 @@
 
 #include "tgb_soap.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -988,27 +989,28 @@ __global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, doub
 
 // ===================== SOAP compression =====================================
 
-// One warp per site: v = C p (FP64), |v| in FP64, then
-// q = v / |v| leaves as the uncompressed pass leaves it: delta = q - mu (fp32
-// row, bf16 split rows) and delta . mu. v is formed twice (once for |v|, once
-// for the output) instead of being staged: a row of C has a handful of entries.
+// Both compression kernels run one warp per site and stage a row of D FP64
+// values per warp in shared memory; W warps per CTA with W * 8 * D bytes within
+// the default 48 KB where D allows, else one warp with opt-in shared memory.
+
+// v = C p (FP64, from a CSR copy of C by row), |v| in FP64, then q = v / |v|
+// leaves as the uncompressed pass leaves it: delta = q - mu (fp32 row, bf16
+// split rows) and delta . mu. Each lane reads back only the v entries it wrote.
 __global__ void __launch_bounds__(256) k_compress_fwd(SoapParams P, CompressArgs C, int n_sites,
                                                       const double *__restrict__ praw, DescOut O) {
-    const int lane = threadIdx.x & 31;
-    const int site = blockIdx.x * 8 + (threadIdx.x >> 5);
+    extern __shared__ double vsh[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int site = blockIdx.x * (blockDim.x >> 5) + warp;
     if (site >= n_sites) return;
-    const double *p = praw + (size_t)site * C.dimf;
     const int D = P.dim;
-    auto row = [&](int i) {
-        double v = 0.0;
-        for (int k = C.row_ptr[i]; k < C.row_ptr[i + 1]; ++k)
-            v += C.row_val[k] * p[C.row_col[k]];
-        return v;
-    };
+    double *v = vsh + (size_t)warp * D;
+    const double *p = praw + (size_t)site * C.dimf;
     double nrm2 = 0.0;
     for (int i = lane; i < D; i += 32) {
-        const double v = row(i);
-        nrm2 += v * v;
+        double x = 0.0;
+        for (int k = C.row_ptr[i]; k < C.row_ptr[i + 1]; ++k) x += C.row_val[k] * p[C.row_col[k]];
+        v[i] = x;
+        nrm2 += x * x;
     }
     nrm2 = warp_sum(nrm2);
     const double inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
@@ -1017,7 +1019,7 @@ __global__ void __launch_bounds__(256) k_compress_fwd(SoapParams P, CompressArgs
     double off = 0.0;
     for (int i = lane; i < D; i += 32) {
         const double mu = P.mu[i];
-        const double dl = row(i) * inv - mu;
+        const double dl = v[i] * inv - mu;
         off += dl * mu;
         const float df = (float)dl;
         qrow[i] = df;
@@ -1037,15 +1039,18 @@ __global__ void __launch_bounds__(256) k_compress_fwd(SoapParams P, CompressArgs
     }
 }
 
-// One warp per site: dE/dq = ksum mu + g0 + g (as the force pass forms it),
-// dE/dv = (dE/dq - (dE/dq . q) q) / |v| in FP64, and dE/dp = C^T dE/dv, one
-// column of C per lane step (dE/dv is re-formed per entry from the rows).
+// dE/dq = ksum mu + g0 + g (as the force pass forms it), dE/dv = (dE/dq -
+// (dE/dq . q) q) / |v| in FP64 into shared memory, then dE/dp = C^T dE/dv (fp32
+// out): the row is zeroed, and the columns of C that have entries (a CSR copy of
+// C by column) are written one per lane step.
 __global__ void __launch_bounds__(256) k_compress_adj(SoapParams P, CompressArgs C, int n_sites,
                                                       ForceIn I, float *__restrict__ gfull) {
-    const int lane = threadIdx.x & 31;
-    const int site = blockIdx.x * 8 + (threadIdx.x >> 5);
+    extern __shared__ double hsh[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int site = blockIdx.x * (blockDim.x >> 5) + warp;
     if (site >= n_sites) return;
     const int D = P.dim;
+    double *h = hsh + (size_t)warp * D;
     const float *g = I.g + (size_t)site * D;
     const float *q = I.q + (size_t)site * D;
     double ksum = 0.0;
@@ -1054,34 +1059,64 @@ __global__ void __launch_bounds__(256) k_compress_adj(SoapParams P, CompressArgs
     double dot = 0.0;
     for (int i = lane; i < D; i += 32) {
         const double mu = P.mu[i];
-        dot += (ksum * mu + P.g0[i] + (double)g[i]) * (mu + (double)q[i]);
+        const double gi = ksum * mu + P.g0[i] + (double)g[i];
+        h[i] = gi;
+        dot += gi * (mu + (double)q[i]);
     }
     dot = warp_sum(dot);
     const double nrm = I.pnorm[site];
     const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    for (int i = lane; i < D; i += 32) h[i] = (h[i] - dot * (P.mu[i] + (double)q[i])) * inv;
+    __syncwarp();   // every lane reads every entry of h below
     float *out = gfull + (size_t)site * C.dimf;
-    for (int j = lane; j < C.dimf; j += 32) {
-        double acc = 0.0;
-        for (int k = C.col_ptr[j]; k < C.col_ptr[j + 1]; ++k) {
-            const int i = C.col_row[k];
-            const double mu = P.mu[i];
-            const double gi = ksum * mu + P.g0[i] + (double)g[i];
-            acc += C.col_val[k] * (gi - dot * (mu + (double)q[i])) * inv;
-        }
-        out[j] = (float)acc;
+    if ((C.dimf & 3) == 0) {
+        float4 *o4 = reinterpret_cast<float4 *>(out);
+        for (int j = lane; j < C.dimf / 4; j += 32) o4[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        for (int j = lane; j < C.dimf; j += 32) out[j] = 0.f;
     }
+    __syncwarp();   // the zeros land before the columns below overwrite theirs
+    for (int t = lane; t < C.ncols; t += 32) {
+        double acc = 0.0;
+        for (int k = C.col_ptr[t]; k < C.col_ptr[t + 1]; ++k) acc += C.col_val[k] * h[C.col_row[k]];
+        out[C.col_idx[t]] = (float)acc;
+    }
+}
+
+// Warps per CTA and shared bytes for the compression kernels at row length D.
+static void compress_launch_shape(int D, int &warps, size_t &smem) {
+    const size_t row = sizeof(double) * (size_t)D;
+    warps = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / row));
+    smem = row * warps;
+}
+
+template <typename K>
+static int compress_smem_attr(K kernel, size_t smem) {
+    if (smem > 48 * 1024)
+        TGB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return TG_OK;
 }
 
 int launch_compress_forward(const SoapParams &P, const CompressArgs &C, int n_sites,
                             const double *praw, const DescOut &O, cudaStream_t st) {
-    if (n_sites > 0) k_compress_fwd<<<(n_sites + 7) / 8, 256, 0, st>>>(P, C, n_sites, praw, O);
+    int w = 0;
+    size_t smem = 0;
+    compress_launch_shape(P.dim, w, smem);
+    TGB_TRY(compress_smem_attr(k_compress_fwd, smem));
+    if (n_sites > 0)
+        k_compress_fwd<<<(n_sites + w - 1) / w, 32 * w, smem, st>>>(P, C, n_sites, praw, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
 
 int launch_compress_adjoint(const SoapParams &P, const CompressArgs &C, int n_sites,
                             const ForceIn &I, float *gfull, cudaStream_t st) {
-    if (n_sites > 0) k_compress_adj<<<(n_sites + 7) / 8, 256, 0, st>>>(P, C, n_sites, I, gfull);
+    int w = 0;
+    size_t smem = 0;
+    compress_launch_shape(P.dim, w, smem);
+    TGB_TRY(compress_smem_attr(k_compress_adj, smem));
+    if (n_sites > 0)
+        k_compress_adj<<<(n_sites + w - 1) / w, 32 * w, smem, st>>>(P, C, n_sites, I, gfull);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -1133,33 +1168,43 @@ static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, 
     return TG_OK;
 }
 
+template <int NS, int AMAX, int LMAX, bool RAW>
+static int expand_tiles(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
+                        int tile) {
+    switch (tile) {
+        case 1: return expand_impl<NS, AMAX, LMAX, 1, RAW>(P, S, O, st);
+        case 2: return expand_impl<NS, AMAX, LMAX, 2, RAW>(P, S, O, st);
+        case 3: return expand_impl<NS, AMAX, LMAX, 3, RAW>(P, S, O, st);
+        default: return expand_impl<NS, AMAX, LMAX, 0, RAW>(P, S, O, st);
+    }
+}
+
 template <int NS, int AMAX, int LMAX>
 static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
                        int tile) {
-    // compressed blocks: one tile (the compression passes dominate their cost)
     if (P.raw) {
         TGB_CHECK(O.praw != nullptr, TG_ERR_ARG, "a compressed block needs DescOut::praw");
-        return expand_impl<NS, AMAX, LMAX, 0, true>(P, S, O, st);
+        return expand_tiles<NS, AMAX, LMAX, true>(P, S, O, st, tile);
     }
+    return expand_tiles<NS, AMAX, LMAX, false>(P, S, O, st, tile);
+}
+
+template <int NS, int AMAX, int LMAX, bool RAW>
+static int force_tiles(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
+                       int *nblk, cudaStream_t st, int tile) {
     switch (tile) {
-        case 1: return expand_impl<NS, AMAX, LMAX, 1>(P, S, O, st);
-        case 2: return expand_impl<NS, AMAX, LMAX, 2>(P, S, O, st);
-        case 3: return expand_impl<NS, AMAX, LMAX, 3>(P, S, O, st);
-        default: return expand_impl<NS, AMAX, LMAX, 0>(P, S, O, st);
+        case 1: return force_impl<NS, AMAX, LMAX, 1, RAW>(P, S, I, O, nblk, st);
+        case 2: return force_impl<NS, AMAX, LMAX, 2, RAW>(P, S, I, O, nblk, st);
+        case 3: return force_impl<NS, AMAX, LMAX, 3, RAW>(P, S, I, O, nblk, st);
+        default: return force_impl<NS, AMAX, LMAX, 0, RAW>(P, S, I, O, nblk, st);
     }
 }
 
 template <int NS, int AMAX, int LMAX>
 static int force_tile(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st, int tile) {
-    // compressed blocks: one tile (the compression passes dominate their cost)
-    if (P.raw) return force_impl<NS, AMAX, LMAX, 0, true>(P, S, I, O, nblk, st);
-    switch (tile) {
-        case 1: return force_impl<NS, AMAX, LMAX, 1>(P, S, I, O, nblk, st);
-        case 2: return force_impl<NS, AMAX, LMAX, 2>(P, S, I, O, nblk, st);
-        case 3: return force_impl<NS, AMAX, LMAX, 3>(P, S, I, O, nblk, st);
-        default: return force_impl<NS, AMAX, LMAX, 0>(P, S, I, O, nblk, st);
-    }
+    if (P.raw) return force_tiles<NS, AMAX, LMAX, true>(P, S, I, O, nblk, st, tile);
+    return force_tiles<NS, AMAX, LMAX, false>(P, S, I, O, nblk, st, tile);
 }
 
 int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,

@@ -26,8 +26,8 @@ struct SoapParams {
     // 1 for a compressed block: the descriptor pass writes the raw power spectrum
     // p (FP64, all NT (NT + 1) / 2 (l_max + 1) entries, internal order) to
     // DescOut::praw and stops there, and the force pass reads ForceIn::g as dE/dp
-    // in that order; both run their tile 0. The compression passes between them
-    // work in the compressed space of dim.
+    // in that order (separate instantiations of both kernels, every tile). The
+    // compression passes between them work in the compressed space of dim.
     int raw;
 };
 
@@ -164,7 +164,9 @@ struct CompressArgs {
     const int *row_ptr;       // [dim + 1]: CSR of C by compressed index
     const int *row_col;       //   internal index of p
     const double *row_val;
-    const int *col_ptr;       // [dimf + 1]: CSR of C^T by internal index of p
+    int ncols;                // columns of C with at least one entry
+    const int *col_idx;       // [ncols]: their internal index of p
+    const int *col_ptr;       // [ncols + 1]: CSR of C^T over those columns
     const int *col_row;       //   compressed index
     const double *col_val;
 };

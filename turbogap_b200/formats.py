@@ -550,6 +550,12 @@ def write_soap_block(fh, spec: SoapTurboSpec) -> None:
     line("scaling_mode", spec.scaling_mode)
     line("zeta", repr(float(spec.zeta)))
     line("delta", repr(float(spec.delta)))
+    if spec.compress_soap:
+        line("compress_soap", ".true.")
+        if spec.file_compress != "none":
+            line("file_compress_soap", f"'{spec.file_compress}'")
+        if spec.compress_mode != "none":
+            line("compress_mode", spec.compress_mode)
     if spec.file_desc:
         line("desc_sparse", f"'{spec.file_desc}'")
     if spec.file_alphas:
@@ -557,10 +563,27 @@ def write_soap_block(fh, spec: SoapTurboSpec) -> None:
     fh.write("gap_end\n")
 
 
+def write_compress_file(path: str, comp: SoapCompression, alpha_max: Sequence[int],
+                        l_max: int) -> None:
+    """A compress file in its ``P_transformation`` form, as read_files.f90:5166-5194
+    reads it: alpha_max per species, l_max and dim, then one ``i j value`` line
+    per entry between ``P_transformation`` and ``end_transformation``."""
+    with open(path, "w") as fh:
+        fh.write(" ".join(str(int(a)) for a in alpha_max) + f" {int(l_max)} {comp.dim}\n")
+        fh.write("P_transformation\n")
+        for i, j, v in zip(comp.P_i.tolist(), comp.P_j.tolist(), comp.P_el.tolist()):
+            fh.write(f"{i} {j} {v!r}\n")
+        fh.write("end_transformation\n")
+
+
 def spec_from_block(block: GapBlock, species_types: Sequence[str], file_desc: str,
-                    file_alphas: str) -> SoapTurboSpec:
-    """The file form of a GapBlock whose species_z index ``species_types``."""
+                    file_alphas: str, file_compress: Optional[str] = None) -> SoapTurboSpec:
+    """The file form of a GapBlock whose species_z index ``species_types``. A
+    compressed block names the compress file its transformation was written to
+    (``write_compress_file``)."""
     h = block.hypers
+    if h.compress is not None and not file_compress:
+        raise ValueError("a compressed block needs the name of its compress file")
     return SoapTurboSpec(
         n_species=h.n_species, species=[species_types[z - 1] for z in h.species_z],
         alpha_max=list(h.alpha_max), rcut_hard=list(h.rcut_hard), buffer=list(h.buffer),
@@ -571,7 +594,8 @@ def spec_from_block(block: GapBlock, species_types: Sequence[str], file_desc: st
         global_scaling=list(h.global_scaling), l_max=h.l_max,
         radial_enhancement=h.radial_enhancement, basis=h.basis, scaling_mode=h.scaling_mode,
         zeta=float(block.zeta), delta=float(block.delta), central_species=h.central_species,
-        file_desc=file_desc, file_alphas=file_alphas)
+        file_desc=file_desc, file_alphas=file_alphas, compress_soap=h.compress is not None,
+        file_compress=file_compress if h.compress is not None else "none")
 
 
 # --------------------------------------------------------------------------

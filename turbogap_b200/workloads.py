@@ -11,6 +11,8 @@ atoms of further seeded structures of the same kind, computed by this backend
   ch1m       2 blocks (C and H), D = 1224, M = 4000 each, dt 0.5 fs, 300 K
   cells512   512 independent C cells (64-2048 atoms, 1.5-3.5 g/cm3), 1 block D = 324,
              M = 2000; one step = energies and forces of every cell (batched)
+  ch32k_trivial  the ch32k structure and seeds with both blocks under the
+             "trivial" SOAP compression (D = 279 of 1224), M = 4000 each
 """
 from __future__ import annotations
 
@@ -20,7 +22,7 @@ from typing import Callable, List
 import numpy as np
 
 from . import synth
-from .hypers import GapBlock, SoapTurboHypers, carbon_hypers, ch_hypers
+from .hypers import GapBlock, SoapTurboHypers, carbon_hypers, ch_hypers, trivial_compression
 
 
 @dataclass
@@ -74,6 +76,17 @@ WORKLOADS = {
                      "1048576 atoms C:H=3:1 at 0.12 /A3, D=1224 per block, M=4000 per block",
                      source=lambda s: _ch(1048576, s)),
 }
+
+
+def _trivial(h: SoapTurboHypers) -> SoapTurboHypers:
+    h.compress = trivial_compression(h.alpha_max, h.l_max)
+    return h
+
+
+WORKLOADS["ch32k_trivial"] = Workload(
+    "ch32k_trivial", 1, [_trivial(ch_hypers(1)), _trivial(ch_hypers(2))], [4000, 4000], 1.0,
+    300.0, "the ch32k structure with both blocks under the trivial SOAP compression "
+    "(D=279 of 1224 each), zeta 4, M=4000 per block", source=lambda s: _ch(32768, s))
 
 
 def uneven_cells(n_cells: int, seed: int):
