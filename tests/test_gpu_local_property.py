@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from _util import O, neighbor_data, sparse_block
-from turbogap_b200.hypers import carbon_hypers
+from turbogap_b200.hypers import SoapCompression, carbon_hypers
 from turbogap_b200.synth import random_structure
 
 pytestmark = pytest.mark.gpu
@@ -28,11 +28,22 @@ def _kept(st, h, nl):
     return np.array(nn, np.int32), np.array(idx)
 
 
+def _transformation(full_dim, dim, seed):
+    rng = np.random.default_rng(seed)
+    P_i = np.concatenate([np.arange(1, dim + 1), rng.integers(1, dim + 1, size=dim)])
+    P_j = rng.integers(1, full_dim + 1, size=2 * dim)
+    return SoapCompression(dim, P_i, P_j, rng.uniform(0.2, 1.0, size=2 * dim))
+
+
+@pytest.mark.parametrize("compressed", [False, True])
 @pytest.mark.parametrize("offset", ["none", "median"])
-def test_local_property_matches_oracle(gpu, offset):
+def test_local_property_matches_oracle(gpu, offset, compressed):
+    """compressed: the property's block under a 45-row P_transformation."""
     h = carbon_hypers()
+    if compressed:
+        h.compress = _transformation(h.uncompressed_dim, 45, seed=93)
     blk = sparse_block(h, 250, seed=91, sigma_alpha=0.002)
-    gpu.soap_backend_begin(blk, key=901)
+    gpu.soap_backend_begin(blk, key=903 if compressed else 901)
     st = random_structure(216, 12.91, 1.2, seed=92)
     nl = neighbor_data(st, h.rcut_max + 0.4)      # lists longer than the block's cutoff
     nn, idx = _kept(st, h, nl)

@@ -78,6 +78,8 @@ struct Block {
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
     DBuf<float> g0f;       // g0 in fp32: subtracted from the MLP's dE/dq rows
+    DBuf<float> muf;       // mu in fp32
+    double mu2 = 0.0, g0mu = 0.0;   // mu . mu, g0 . mu
     DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d (-1: padding)
     TmaMap tmB1{}, tmB2{};
     // compression matrix C (dim x dimf) as CSR by row and by column
@@ -106,6 +108,10 @@ struct Block {
         P.self_R = selfR.p;
         P.mu = mu.p;
         P.g0 = g0.p;
+        P.muf = muf.p;
+        P.g0f = g0f.p;
+        P.mu2 = mu2;
+        P.g0mu = g0mu;
         P.raw = compressed() ? 1 : 0;
         return P;
     }
@@ -306,7 +312,8 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
     TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
     TGB_MARK(log, PASS_GEMM2, st);
-    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
+    ForceIn I{w.g.p,     w.q.p,      w.pnorm.p,         w.c.p,   w.epart.p,
+              w.kdsum.p, b.n_etiles, b.delta * b.delta, w.qoff.p};
     ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct, pair_grad};
     int nblk = 0;
     TGB_TRY(force_pass(b, w, P, S, I, FO, &nblk, st, w.tile_force));
@@ -348,7 +355,7 @@ int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     // expansion writes praw and its force kernel reads gfull)
     DescOut O{w.qsplit.p, w.q.p, w.qoff.p, w.pnorm.p, w.c.p, w.praw.p};
     ForceIn I{b.compressed() ? w.gfull.p : w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p,
-              b.n_etiles, b.delta * b.delta};
+              b.n_etiles, b.delta * b.delta, w.qoff.p};
     ForceOut FO{forces, energies, w.vpart.p, err};
     cudaEvent_t e0, e1;
     TGB_CUDA(cudaEventCreate(&e0));
@@ -543,7 +550,8 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
                                        x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
     TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_GEMM2, st);
-    ForceIn I{w.g.p, w.q.p, w.pnorm.p, w.c.p, w.epart.p, w.kdsum.p, b.n_etiles, b.delta * b.delta};
+    ForceIn I{w.g.p,     w.q.p,      w.pnorm.p,         w.c.p,   w.epart.p,
+              w.kdsum.p, b.n_etiles, b.delta * b.delta, w.qoff.p};
     ForceOut FO{forces, energies, w.vpart.p, err};
     int nblk = 0;
     TGB_TRY(force_pass(b, w, P, S, I, FO, &nblk, st, w.tile_force));
@@ -865,9 +873,17 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
             for (int d = 0; d < b->dim; ++d) g0[d] += c * (Qs[(size_t)s * b->dim + d] - mu[d]);
         }
         TGB_CUDA(cudaMemcpy(b->g0.p, g0.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
-        std::vector<float> g0f(g0.begin(), g0.end());
+        std::vector<float> g0f(g0.begin(), g0.end()), muf(mu.begin(), mu.end());
         TGB_TRY(b->g0f.ensure(b->dim));
+        TGB_TRY(b->muf.ensure(b->dim));
         TGB_CUDA(cudaMemcpy(b->g0f.p, g0f.data(), sizeof(float) * b->dim, cudaMemcpyHostToDevice));
+        TGB_CUDA(cudaMemcpy(b->muf.p, muf.data(), sizeof(float) * b->dim, cudaMemcpyHostToDevice));
+        b->mu2 = 0.0;
+        b->g0mu = 0.0;
+        for (int d = 0; d < b->dim; ++d) {
+            b->mu2 += mu[d] * mu[d];
+            b->g0mu += g0[d] * mu[d];
+        }
         TGB_CUDA(cudaMemcpy(b->mu.p, mu.data(), sizeof(double) * b->dim, cudaMemcpyHostToDevice));
         TGB_CUDA(cudaMemcpy(b->aoff.p, aoff.data(), sizeof(double) * b->Mpad, cudaMemcpyHostToDevice));
     }

@@ -713,9 +713,13 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         const int catom = S.site_atom[site];
         const int64_t p0 = S.pstart[row];
         const int np = (int)(S.pstart[row + 1] - p0);
-        // dE/dq = ksum mu + g0 + g_delta: ksum = sum_s kd_s (FP64, GEMM-1 epilogue),
-        // g0 = sum_s kcoef_s (q_s - mu) (FP64, per block), g_delta from GEMM 2;
-        // q = mu + delta. dE/dp = (dE/dq - (dE/dq . q) q) / |p|, all in FP64.
+        // dE/dq = G = ksum mu + g0 + g: ksum = sum_s kd_s (FP64, GEMM-1 epilogue),
+        // g0 = sum_s kcoef_s (q_s - mu) (per block), g from GEMM 2; q = mu + delta.
+        // dE/dp = (G - (G . q) q) / |p| = (a mu + g0 + g - dot delta) / |p| with
+        // dot = G . q and a = ksum - dot. The large parts, ksum mu . mu against dot,
+        // cancel only in the FP64 scalars dot = ksum (mu . mu + delta . mu) + g0 . mu
+        // + sum (g0 delta + g q) and a; the per-entry terms are all small and run in
+        // fp32.
         const float *g = I.g + (size_t)site * DIM;
         const float *q = I.q + (size_t)site * DIM;
         // per-slice partial sums: lanes load in parallel, a butterfly adds them
@@ -731,10 +735,9 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         // Four consecutive entries per lane and 16-byte loads; a group of four never
         // crosses an l boundary because NP % 4 == 0.
         constexpr bool VEC = (DIM % 4 == 0) && (NP % 4 == 0);
-        auto put_b = [&](int d, double gd, double qd, double dotv, double invv) {
+        auto put_b = [&](int d, float h) {
             const int l = d / NP, pi = d - l * NP;
             float *Bl = Bm + l * Sh::BSTRIDE;
-            const float h = (float)((gd - dotv * qd) * invv);
             const int n = pair_n[pi], n2 = pair_n2[pi];
             if (n == n2) {
                 Bl[n * Sh::BROW + n] = 2.f * h;
@@ -745,49 +748,42 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
             }
         };
         if constexpr (RAW) {
-            for (int d = lane; d < DIM; d += 32) put_b(d, (double)g[d], 0.0, 0.0, 1.0);
+            for (int d = lane; d < DIM; d += 32) put_b(d, g[d]);
         } else {
-            double dot = 0.0;
+            float sp = 0.f;   // sum (g0 delta + g q), a small sum
             if constexpr (VEC) {
                 for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                    const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
-                    const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
-                    const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
-                    const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                    const float4 m = __ldg(reinterpret_cast<const float4 *>(P.muf + d0));
+                    const float4 z = __ldg(reinterpret_cast<const float4 *>(P.g0f + d0));
                     const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
                     const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
-                    dot += (ksum * m0.x + z0.x + (double)gv.x) * (m0.x + (double)qv.x);
-                    dot += (ksum * m0.y + z0.y + (double)gv.y) * (m0.y + (double)qv.y);
-                    dot += (ksum * m1.x + z1.x + (double)gv.z) * (m1.x + (double)qv.z);
-                    dot += (ksum * m1.y + z1.y + (double)gv.w) * (m1.y + (double)qv.w);
+                    sp += z.x * qv.x + gv.x * (m.x + qv.x);
+                    sp += z.y * qv.y + gv.y * (m.y + qv.y);
+                    sp += z.z * qv.z + gv.z * (m.z + qv.z);
+                    sp += z.w * qv.w + gv.w * (m.w + qv.w);
                 }
             } else {
-                for (int d = lane; d < DIM; d += 32) {
-                    const double mu = P.mu[d];
-                    dot += (ksum * mu + P.g0[d] + (double)g[d]) * (mu + (double)q[d]);
-                }
+                for (int d = lane; d < DIM; d += 32)
+                    sp += P.g0f[d] * q[d] + g[d] * (P.muf[d] + q[d]);
             }
-            dot = warp_sum(dot);
+            const double dot = ksum * (P.mu2 + I.qoff[site]) + P.g0mu + warp_sum((double)sp);
             const double nrm = I.pnorm[site];
             const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+            const float fa = (float)((ksum - dot) * inv), fi = (float)inv, fd = (float)(dot * inv);
             if constexpr (VEC) {
                 for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                    const double2 m0 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0));
-                    const double2 m1 = __ldg(reinterpret_cast<const double2 *>(P.mu + d0 + 2));
-                    const double2 z0 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0));
-                    const double2 z1 = __ldg(reinterpret_cast<const double2 *>(P.g0 + d0 + 2));
+                    const float4 m = __ldg(reinterpret_cast<const float4 *>(P.muf + d0));
+                    const float4 z = __ldg(reinterpret_cast<const float4 *>(P.g0f + d0));
                     const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
                     const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
-                    put_b(d0, ksum * m0.x + z0.x + (double)gv.x, m0.x + (double)qv.x, dot, inv);
-                    put_b(d0 + 1, ksum * m0.y + z0.y + (double)gv.y, m0.y + (double)qv.y, dot, inv);
-                    put_b(d0 + 2, ksum * m1.x + z1.x + (double)gv.z, m1.x + (double)qv.z, dot, inv);
-                    put_b(d0 + 3, ksum * m1.y + z1.y + (double)gv.w, m1.y + (double)qv.w, dot, inv);
+                    put_b(d0, fa * m.x + fi * (z.x + gv.x) - fd * qv.x);
+                    put_b(d0 + 1, fa * m.y + fi * (z.y + gv.y) - fd * qv.y);
+                    put_b(d0 + 2, fa * m.z + fi * (z.z + gv.z) - fd * qv.z);
+                    put_b(d0 + 3, fa * m.w + fi * (z.w + gv.w) - fd * qv.w);
                 }
             } else {
-                for (int d = lane; d < DIM; d += 32) {
-                    const double mu = P.mu[d];
-                    put_b(d, ksum * mu + P.g0[d] + (double)g[d], mu + (double)q[d], dot, inv);
-                }
+                for (int d = lane; d < DIM; d += 32)
+                    put_b(d, fa * P.muf[d] + fi * (P.g0f[d] + g[d]) - fd * q[d]);
             }
         }
         __syncwarp();
@@ -1204,6 +1200,7 @@ template <int NS, int AMAX, int LMAX>
 static int force_tile(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st, int tile) {
     if (P.raw) return force_tiles<NS, AMAX, LMAX, true>(P, S, I, O, nblk, st, tile);
+    TGB_CHECK(I.qoff && P.muf && P.g0f, TG_ERR_ARG, "the force pass needs qoff, muf and g0f");
     return force_tiles<NS, AMAX, LMAX, false>(P, S, I, O, nblk, st, tile);
 }
 

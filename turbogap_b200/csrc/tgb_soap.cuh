@@ -23,6 +23,8 @@ struct SoapParams {
     const float *self_R;       // [ns][amax]: central-atom contribution to c_{n,00}
     const double *mu;          // [dim]: mean of the sparse set; the GEMMs see q - mu
     const double *g0;          // [dim]: sum_s kcoef_s (q_s - mu), the K = 1 part of dE/dq
+    const float *muf, *g0f;    // fp32 copies (the force pass's per-entry terms)
+    double mu2, g0mu;          // mu . mu and g0 . mu (FP64)
     // 1 for a compressed block: the descriptor pass writes the raw power spectrum
     // p (FP64, all NT (NT + 1) / 2 (l_max + 1) entries, internal order) to
     // DescOut::praw and stops there, and the force pass reads ForceIn::g as dE/dp
@@ -104,6 +106,7 @@ struct ForceIn {
     const double *kdsum;     // [n_sites][n_etiles]: sum_s kd_s per tile
     int n_etiles;
     double delta2;
+    const double *qoff;      // [n_sites]: delta . mu (FP64, from the descriptor pass)
 };
 
 struct ForceOut {
