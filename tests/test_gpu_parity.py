@@ -29,8 +29,10 @@ def _f32(u):
     return (u.astype(np.uint32) << 16).view(np.float32)
 
 
+# the last two: more tiles than SMs with a short last column tile, where the
+# waves rotate the column tiles over the CTAs
 @pytest.mark.parametrize("M,N,K", [(128, 256, 64), (257, 516, 192), (1000, 700, 640),
-                                   (33, 1224, 3712)])
+                                   (33, 1224, 3712), (10240, 324, 128), (7680, 700, 192)])
 def test_tcgen05_gemm(gpu, M, N, K):
     rng = np.random.default_rng(M + N + K)
     A = _bf16(rng.normal(size=(M, K)))

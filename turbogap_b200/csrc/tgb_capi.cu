@@ -82,6 +82,9 @@ struct Block {
     double mu2 = 0.0, g0mu = 0.0;   // mu . mu, g0 . mu
     DBuf<int> ref_index;   // [dim]: reference position of internal descriptor entry d (-1: padding)
     TmaMap tmB1{}, tmB2{};
+    TmaMap tmB1l{}, tmB2l{};   // the short last column tile's B maps (N % kGemmBN != 0)
+    const TmaMap *last1() const { return gemm_last_box_rows(Mpad) ? &tmB1l : nullptr; }
+    const TmaMap *last2() const { return gemm_last_box_rows(dim) ? &tmB2l : nullptr; }
     // compression matrix C (dim x dimf) as CSR by row and by column
     DBuf<int> c_row_ptr, c_row_col, c_col_idx, c_col_ptr, c_col_row;
     DBuf<double> c_row_val, c_col_val;
@@ -301,7 +304,8 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e1.K2 = b.KD;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st, &w.tmKd));
+    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st, &w.tmKd,
+                           b.last1()));
     TGB_MARK(log, PASS_GEMM1, st);
     GemmEpi e2{};
     e2.mode = EPI_STORE_F32;
@@ -310,7 +314,8 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     e2.out = w.g.p;
     e2.ldo = b.dim;
     e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
-    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st));
+    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st, nullptr,
+                           b.last2()));
     TGB_MARK(log, PASS_GEMM2, st);
     ForceIn I{w.g.p,     w.q.p,      w.pnorm.p,         w.c.p,   w.epart.p,
               w.kdsum.p, b.n_etiles, b.delta * b.delta, w.qoff.p};
@@ -535,7 +540,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e1.K2 = b.KD;
     e1.Mpad = b.Mpad;
     e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st, &w.tmKd));
+    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st, &w.tmKd, b.last1()));
     TGB_MARK(log, PASS_GEMM1, st);
     GemmEpi e2{};
     e2.mode = EPI_STORE_F32;
@@ -545,7 +550,7 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     e2.out = x.g_g.p;
     e2.ldo = b.dim;
     e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
-    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st));
+    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st, nullptr, b.last2()));
     k_scatter_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
                                        x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
     TGB_CUDA(cudaGetLastError());
@@ -902,6 +907,12 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
     TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st, b->table_fd.p));
     TGB_TRY(make_tma_bf16(&b->tmB1, b->QsA.p, b->Mpad, b->K1, b->K1, kGemmBN));
     TGB_TRY(make_tma_bf16(&b->tmB2, b->QsT.p, b->dim, b->K2, b->K2, kGemmBN));
+    if (b->last1())
+        TGB_TRY(make_tma_bf16(&b->tmB1l, b->QsA.p, b->Mpad, b->K1, b->K1,
+                              gemm_last_box_rows(b->Mpad)));
+    if (b->last2())
+        TGB_TRY(make_tma_bf16(&b->tmB2l, b->QsT.p, b->dim, b->K2, b->K2,
+                              gemm_last_box_rows(b->dim)));
     TGB_CUDA(cudaStreamSynchronize(C.st));
     C.current = b.get();
     auto old = C.blocks.find(block_key);
@@ -2560,16 +2571,18 @@ extern "C" int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t 
     TGB_CUDA(cudaMemcpyAsync(a.p, A, sizeof(uint16_t) * M * K, cudaMemcpyHostToDevice, C.st));
     TGB_CUDA(cudaMemcpyAsync(b.p, B, sizeof(uint16_t) * N * K, cudaMemcpyHostToDevice, C.st));
     TGB_CUDA(cudaMemsetAsync(c.p, 0, sizeof(float) * M * N, C.st));
-    TmaMap ta{}, tb{};
+    TmaMap ta{}, tb{}, tl{};
     TGB_TRY(make_tma_bf16(&ta, a.p, M, K, K, kGemmBM));
     TGB_TRY(make_tma_bf16(&tb, b.p, N, K, K, kGemmBN));
+    const int lr = gemm_last_box_rows(N);   // the short last column tile, as the blocks run it
+    if (lr) TGB_TRY(make_tma_bf16(&tl, b.p, N, K, K, lr));
     GemmEpi ep{};
     ep.mode = EPI_STORE_F32;
     ep.rows = M;
     ep.cols = N;
     ep.out = c.p;
     ep.ldo = N;
-    TGB_TRY(launch_gemm_tn(ta, tb, M, N, K, ep, C.err.p, C.st));
+    TGB_TRY(launch_gemm_tn(ta, tb, M, N, K, ep, C.err.p, C.st, nullptr, lr ? &tl : nullptr));
     TGB_TRY(check_err_word(C, C.err.p));
     TGB_CUDA(cudaMemcpyAsync(Cout, c.p, sizeof(float) * M * N, cudaMemcpyDeviceToHost, C.st));
     TGB_CUDA(cudaStreamSynchronize(C.st));

@@ -246,15 +246,28 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t sr
                  : "memory");
 }
 
-// Persistent: CTA b processes tiles b, b + gridDim.x, ... (column tile fastest,
-// so concurrently resident CTAs share A rows in L2). Stage counters of the
-// shared-memory ring run across tiles; accumulator it % 2 is reused every
-// second tile once all epilogue warps have released it.
+// Column tile of linear tile t. Column tiles run fastest, so the CTAs of one
+// wave that share a row tile read its A rows from L2 once. With rotate set (the
+// grid is then a multiple of n_tiles_n, so a row tile never straddles two waves)
+// wave w shifts the column tiles of every row by w, and the short last column
+// tile moves from CTA to CTA instead of always landing on the same ones.
+__device__ __forceinline__ int tile_col(int t, int n_tiles_n, int rotate) {
+    const int n = t % n_tiles_n;
+    return rotate ? (n + t / (int)gridDim.x) % n_tiles_n : n;
+}
+
+// Persistent: CTA b processes tiles b, b + gridDim.x, ... (see tile_col). Stage
+// counters of the shared-memory ring run across tiles; accumulator it % 2 is
+// reused every second tile once all epilogue warps have released it. With
+// last_rows > 0 the last column tile loads its B operand through tmBl (a box of
+// last_rows rows) and its MMAs are last_rows wide; the epilogues read no column
+// past N.
 template <int MODE>
 __global__ void __launch_bounds__(threads_for(MODE), 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-              const __grid_constant__ CUtensorMap tmC, int num_kb, int n_tiles_m, int n_tiles_n,
-              GemmEpi ep, unsigned *err) {
+              const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmBl,
+              int num_kb, int n_tiles_m, int n_tiles_n, int last_rows, int rotate, GemmEpi ep,
+              unsigned *err) {
     constexpr int NST = stages_for(MODE);
     constexpr int EPI_WARPS = epi_warps(MODE), GROUPS = epi_groups(MODE);
     constexpr int COLS_PER_WARP = cols_per_warp(MODE), CHUNKS = chunks_for(MODE);
@@ -311,7 +324,10 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
         int g = 0;   // k-blocks issued so far (all tiles)
         bool ok = true;
         for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
-            const int m0 = (t / n_tiles_n) * BM, n0 = (t % n_tiles_n) * BN;
+            const int tn = tile_col(t, n_tiles_n, rotate);
+            const int m0 = (t / n_tiles_n) * BM, n0 = tn * BN;
+            const bool short_tile = last_rows > 0 && tn == n_tiles_n - 1;
+            const uint32_t b_bytes = short_tile ? (uint32_t)last_rows * BK * 2 : B_BYTES;
             const int ak = ep.bd_block > 0 ? (n0 / ep.bd_block) * ep.bd_block : 0;
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
                 const int s = g % NST;
@@ -321,11 +337,12 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
                     ok = false;
                     break;
                 }
-                mbar_expect_tx(full0 + 8 * s, A_BYTES + B_BYTES);
+                mbar_expect_tx(full0 + 8 * s, A_BYTES + b_bytes);
                 int ax = ak + kb * BK;
                 if (ep.a_krep > 0 && ax >= ep.a_krep) ax -= ep.a_krep;
                 tma_load_2d(sA + s * A_BYTES, &tmA, ax, m0, full0 + 8 * s);
-                tma_load_2d(sB + s * B_BYTES, &tmB, kb * BK, n0, full0 + 8 * s);
+                tma_load_2d(sB + s * B_BYTES, short_tile ? &tmBl : &tmB, kb * BK, n0,
+                            full0 + 8 * s);
             }
         }
         // Drain: the last load of every stage has landed before the CTA may exit
@@ -334,10 +351,12 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
             (void)mbar_wait(full0 + 8 * (k % NST), (uint32_t)(k / NST) & 1u, err);
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer
-        constexpr uint32_t idesc = make_idesc(BM, BN);
+        constexpr uint32_t idesc_full = make_idesc(BM, BN);
         int g = 0, it = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++it) {
+            const bool short_tile = last_rows > 0 && tile_col(t, n_tiles_n, rotate) == n_tiles_n - 1;
+            const uint32_t idesc = short_tile ? make_idesc(BM, last_rows) : idesc_full;
             const int a = it & 1;
             const uint32_t use = (uint32_t)(it >> 1);
             if (!mbar_wait(acce0 + 8 * a, (use & 1u) ^ 1u, err)) {
@@ -376,7 +395,7 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
       for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
         const int a = it & 1;
         const uint32_t use = (uint32_t)(it >> 1);
-        const int tile_n = t % n_tiles_n;
+        const int tile_n = tile_col(t, n_tiles_n, rotate);
         const int m0 = (t / n_tiles_n) * BM, n0 = tile_n * BN;
         const int row = m0 + q * 32 + lane;
         const bool row_ok = row < rows;
@@ -703,7 +722,7 @@ int make_tma_store_f32(TmaMap *m, const void *base, int64_t rows, int64_t cols, 
 }
 
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
-                   unsigned *err, cudaStream_t st, const TmaMap *C) {
+                   unsigned *err, cudaStream_t st, const TmaMap *C, const TmaMap *Blast) {
     TGB_CHECK(K % kGemmBK == 0, TG_ERR_ARG, "GEMM K=%d must be a multiple of %d", K, kGemmBK);
     // 16-byte vector stores in the epilogues
     TGB_CHECK(ep.mode != EPI_STORE_F32 || (ep.ldo % 4 == 0 && ((uintptr_t)ep.out & 15) == 0),
@@ -731,7 +750,8 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
         case EPI_MLP_L1B: mode = MODE_MLP_L1B; break;
         default: mode = MODE_STORE;
     }
-    using Kern = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, int, int, int, GemmEpi, unsigned *);
+    using Kern = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, CUtensorMap, int, int, int, int,
+                          int, GemmEpi, unsigned *);
     static const Kern kerns[N_MODES] = {
         k_gemm_tn<MODE_GAP_Z4>, k_gemm_tn<MODE_GAP_ZINT>, k_gemm_tn<MODE_GAP_ZREAL>,
         k_gemm_tn<MODE_STORE>, k_gemm_tn<MODE_MLP_L1>, k_gemm_tn<MODE_MLP_L2>,
@@ -749,9 +769,16 @@ int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const 
         TGB_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     }
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
-    const int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
-    kerns[mode]<<<grid, threads_for(mode), smem_bytes_for(mode), st>>>(A.map, B.map, C ? C->map : A.map,
-                                                             K / kGemmBK, tm, tn, ep, err);
+    int grid = std::min(tm * tn, n_sm);   // persistent: one CTA per SM
+    const int last_rows = Blast ? gemm_last_box_rows(N) : 0;
+    // A short last column tile among at most four pays for the SMs a grid that is
+    // a multiple of the column-tile count may leave idle (none with two tiles on
+    // 148 SMs): the waves then rotate the short tile over the CTAs.
+    const int rotate = (last_rows > 0 && tn > 1 && tn <= 4 && grid == n_sm) ? 1 : 0;
+    if (rotate) grid = n_sm / tn * tn;
+    kerns[mode]<<<grid, threads_for(mode), smem_bytes_for(mode), st>>>(
+        A.map, B.map, C ? C->map : A.map, Blast ? Blast->map : B.map, K / kGemmBK, tm, tn, last_rows,
+        rotate, ep, err);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

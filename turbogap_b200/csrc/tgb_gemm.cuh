@@ -90,10 +90,20 @@ int make_tma_store_bf16(TmaMap *m, const void *base, int64_t rows, int64_t cols,
 int make_tma_store_f32(TmaMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld);
 
 // C (map for the GAP epilogue's kd stores) is required in EPI_GAP_KERNEL mode.
+// Blast, optional: a second map over B whose box is gemm_last_box_rows(N) rows
+// tall; the last column tile of an N that is not a multiple of kGemmBN then
+// loads and multiplies only those rows instead of a full kGemmBN-row box.
 int launch_gemm_tn(const TmaMap &A, const TmaMap &B, int M, int N, int K, const GemmEpi &ep,
-                   unsigned *err, cudaStream_t st, const TmaMap *C = nullptr);
+                   unsigned *err, cudaStream_t st, const TmaMap *C = nullptr,
+                   const TmaMap *Blast = nullptr);
 
 inline int gemm_n_tiles(int N) { return (N + kGemmBN - 1) / kGemmBN; }
+// Rows of the last column tile, rounded up to the MMA's N step of 16; 0 when N
+// is a multiple of kGemmBN (no short tile).
+inline int gemm_last_box_rows(int N) {
+    const int r = N % kGemmBN;
+    return r == 0 ? 0 : (r + 15) / 16 * 16;
+}
 // Number of column slices the energy partials are split into.
 inline int gemm_n_etiles(int N) { return gemm_n_tiles(N) * kGemmEpiGroups; }
 
