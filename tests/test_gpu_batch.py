@@ -47,3 +47,26 @@ def test_batch_matches_oracle_per_structure(gpu):
         assert np.max(np.abs(v[s] - vo)) < V_TOL * max(1.0, np.max(np.abs(vo))), s
         off += st.n
     bat.close()
+
+
+@pytest.mark.parametrize("slots", ["0", "8"])
+def test_batch_list_builds_agree(gpu, monkeypatch, slots):
+    """The one-pass list build (pairs counted into fixed rows, then compacted)
+    against the two-pass build (TGB_BATCH_SLOTS=0) and against rows too short for
+    every atom (8), where each step falls back to the second search: the same
+    energies, forces and virials."""
+    h = carbon_hypers()
+    blk = sparse_block(h, 300, seed=41)
+    gpu.soap_backend_begin(blk, key=4242)
+    cells = _cells()
+    ref = gpu.Batch(cells, [4242])
+    e1, f1, v1 = ref.compute()
+    ref.close()
+    monkeypatch.setenv("TGB_BATCH_SLOTS", slots)
+    bat = gpu.Batch(cells, [4242])
+    for _ in range(2):                      # the second call replays the CUDA graph
+        e, f, v = bat.compute()
+        assert np.max(np.abs(e - e1)) < 1e-12 and np.max(np.abs(f - f1)) < 1e-9
+        assert np.max(np.abs(v - v1)) < 1e-9
+    bat.close()
+

@@ -2227,7 +2227,8 @@ struct BatchEngine {
     double rcut = 0.0;
     DBuf<double> pos, f, en, vir, vir_s, e0, xyz, cell_pos;
     DBuf<int> species, atom_struct, cell_id, cell_count, cell_start, cell_fill, cell_atoms, n_neigh,
-        nbr;
+        nbr, snbr, ovf;
+    DBuf<double> sxyz;
     DBuf<int64_t> pstart;
     DBuf<BatchStruct> sdev;
     DBuf<char> scan_tmp;
@@ -2304,6 +2305,28 @@ struct BatchEngine {
         nl.nbr = nbr.p;
         nl.xyz = xyz.p;
         nl.cap = cap;
+        // slot rows of the one-pass build: the largest count with 25 % headroom
+        // (an atom that outgrows them sends that build to the second search)
+        std::vector<int> cnt(n);
+        TGB_CUDA(cudaMemcpyAsync(cnt.data(), nl.n_neigh, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                                 st));
+        TGB_CUDA(cudaStreamSynchronize(st));
+        int mx = 1;
+        for (int c : cnt) mx = std::max(mx, c);
+        int slots = (mx + mx / 4 + 8 + 15) / 16 * 16;
+        // TGB_BATCH_SLOTS=s sets the rows (0: the two-pass build), e.g. to make
+        // the overflow fallback run
+        if (const char *e = std::getenv("TGB_BATCH_SLOTS")) slots = std::max(0, std::atoi(e));
+        nl.slots = 0;
+        if (slots > 0 && slots <= 256) {
+            TGB_TRY(snbr.ensure((size_t)n * slots));
+            TGB_TRY(sxyz.ensure((size_t)3 * n * slots));
+            TGB_TRY(ovf.ensure(1));
+            nl.snbr = snbr.p;
+            nl.sxyz = sxyz.p;
+            nl.ovf = ovf.p;
+            nl.slots = slots;
+        }
         TGB_CUDA(cudaMemsetAsync(nl.err, 0, sizeof(unsigned), st));
         TGB_CUDA(cudaStreamSynchronize(st));
         return TG_OK;

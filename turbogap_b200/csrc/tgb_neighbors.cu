@@ -785,16 +785,23 @@ __global__ void k_bcell_sort(int ncells, const int *__restrict__ cell_start,
 // the atom's cell, or (image, atom) pairs of the structure); lanes test 32 at a
 // time and emit accepted pairs in sequence order (ballot + prefix popcount).
 // Count mode when pstart is null.
+// Three uses: count (pstart and slots unset), count into slot rows (slots > 0:
+// pair e of atom i at row i * slots + e while e < slots, *ovf set past it), and
+// fill the compact arrays at pstart (run only when *gate is set, if gate given).
 __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStruct *__restrict__ st,
                            const int *__restrict__ atom_struct, const int *__restrict__ cell_id,
                            const int *__restrict__ cell_start, const int *__restrict__ cell_count,
                            const int *__restrict__ cell_atoms, const double *__restrict__ cell_pos,
                            double rcut, int *__restrict__ n_neigh,
                            const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
-                           double *__restrict__ xyz, unsigned *err) {
+                           double *__restrict__ xyz, unsigned *err, int slots,
+                           int *__restrict__ ovf, const int *__restrict__ gate) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
+    if (i >= n || (gate && !*gate)) return;
+    // where pair e goes, and whether it fits
+    const bool slotted = !pstart && slots > 0;
+    const bool writes = pstart || slotted;
     const BatchStruct b = st[atom_struct[i]];
     const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
     // candidate segments: lane c < 27 describes cell c (mode 0); mode 1 has one
@@ -820,9 +827,10 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
         if (lane >= o) incl += v;
     }
     const int total = b.mode == 0 ? __shfl_sync(0xffffffffu, incl, 31) : b.n * nimg;
-    const int64_t base = pstart ? pstart[i] : 0;
-    if (pstart && lane == 0) {   // self pair first
-        if (base < cap) {
+    const int64_t base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
+    const int64_t lim = pstart ? cap : base + slots;
+    if (writes && lane == 0) {   // self pair first
+        if (base < lim) {
             nbr[base] = i;
             xyz[3 * base] = 0.0;
             xyz[3 * base + 1] = 0.0;
@@ -876,13 +884,15 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
             take = !self && d2 < rcut * rcut;
         }
         const unsigned msk = __ballot_sync(0xffffffffu, take);
-        if (pstart && take) {
+        if (writes && take) {
             const int64_t p = base + count + __popc(msk & ((1u << lane) - 1u));
-            if (p < cap) {
+            if (p < lim) {
                 nbr[p] = k;
                 xyz[3 * p] = dist[0];
                 xyz[3 * p + 1] = dist[1];
                 xyz[3 * p + 2] = dist[2];
+            } else if (slotted) {
+                *ovf = 1;   // the fallback search fills this build
             } else {
                 atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
             }
@@ -890,6 +900,25 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
         count += __popc(msk);
     }
     if (!pstart && lane == 0) n_neigh[i] = count;
+}
+
+// Slot rows to the compact arrays (a warp per atom), unless a row overflowed.
+__global__ void k_bnl_compact(int n, int slots, const int *__restrict__ n_neigh,
+                              const int64_t *__restrict__ pstart, const int *__restrict__ snbr,
+                              const double *__restrict__ sxyz, const int *__restrict__ ovf,
+                              int64_t cap, int *__restrict__ nbr, double *__restrict__ xyz,
+                              unsigned *err) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n || *ovf) return;
+    const int cnt = n_neigh[i];
+    const int64_t dst = pstart[i], src = (int64_t)i * slots;
+    if (dst + cnt > cap) {
+        if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+        return;
+    }
+    for (int e = lane; e < cnt; e += 32) nbr[dst + e] = snbr[src + e];
+    for (int e = lane; e < 3 * cnt; e += 32) xyz[3 * dst + e] = sxyz[3 * src + e];
 }
 
 }  // namespace
@@ -912,15 +941,24 @@ int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st)
                                                                  nl.cell_count, nl.cell_atoms);
         k_cell_gather_pos<<<gb, TB, 0, st>>>(nl.n_cell_atoms, nl.cell_atoms, pos, nl.cell_pos, nullptr);
     }
+    const bool one_pass = nl.slots > 0 && nl.cap > 0;
+    if (one_pass) TGB_CUDA(cudaMemsetAsync(nl.ovf, 0, sizeof(int), st));
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
                                   nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
-                                  nullptr, nl.cap, nullptr, nullptr, nl.err);
+                                  nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
+                                  one_pass ? nl.sxyz : nullptr, nl.err, one_pass ? nl.slots : 0,
+                                  nl.ovf, nullptr);
     k_pstart_zero<<<1, 1, 0, st>>>(nl.pstart);
     size_t bytes = nl.scan_bytes;
     TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n, st));
+    if (one_pass)
+        k_bnl_compact<<<gw, TB, 0, st>>>(n, nl.slots, nl.n_neigh, nl.pstart, nl.snbr, nl.sxyz,
+                                         nl.ovf, nl.cap, nl.nbr, nl.xyz, nl.err);
+    // the filling search: always in the two-pass build, after an overflow in the other
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
                                   nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
-                                  nl.pstart, nl.cap, nl.nbr, nl.xyz, nl.err);
+                                  nl.pstart, nl.cap, nl.nbr, nl.xyz, nl.err, 0, nullptr,
+                                  one_pass ? nl.ovf : nullptr);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

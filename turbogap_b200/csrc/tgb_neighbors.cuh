@@ -121,6 +121,15 @@ struct BatchNL {
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
     unsigned *err = nullptr;
+    // One-pass build: with slots > 0 (and pair arrays, cap > 0) the search writes
+    // each atom's pairs into slots fixed-size rows of snbr / sxyz while it counts
+    // them, and a copy compacts the rows after the scan. An atom with more than
+    // slots pairs sets *ovf, and the build then falls back to a second search
+    // that fills the compact arrays directly; no host round trip either way.
+    int slots = 0;
+    int *snbr = nullptr;           // [n_atoms * slots]
+    double *sxyz = nullptr;        // [n_atoms * slots * 3]
+    int *ovf = nullptr;
 };
 
 // Count, scan and fill (pairs beyond nl.cap are dropped and flag DEV_ERR_NEIGH_CAPACITY;
