@@ -211,3 +211,31 @@ def test_engine_nve_energy_conservation(gpu, ch_blocks):
     assert abs((ep1 + ek1) - (ep0 + ek0)) / st.n < 1e-5
     assert ek1 > 0
     eng.close()
+
+
+@pytest.mark.parametrize("slots", ["0", "8"])
+def test_engine_list_builds_agree(gpu, ch_blocks, monkeypatch, slots):
+    """The engine's one-pass list build (pairs counted into fixed rows, then
+    compacted) against the two-pass build (TGB_NL_SLOTS=0) and against rows too
+    short for every site (8, each build falls back to the filling search): the
+    same energies, forces and virial, also over MD steps."""
+    bC, bH = ch_blocks
+    gpu.soap_backend_begin(bC, key=201)
+    gpu.soap_backend_begin(bH, key=202)
+    st = random_structure(300, (300 / 0.12) ** (1 / 3), 1.0, seed=13, h_fraction=0.25)
+    vel = maxwell_velocities(st.masses, 600.0, 14)
+    out = []
+    for env in (None, slots):
+        if env is not None:
+            monkeypatch.setenv("TGB_NL_SLOTS", env)
+        eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [201, 202])
+        e, f, v = eng.compute()
+        eng.set_state(st.positions, vel)
+        eng.md(3, 1.0)
+        p, _, f2 = eng.get_state()
+        out.append((e, f, v, p, f2))
+        eng.close()
+    (e1, f1, v1, p1, g1), (e2, f2, v2, p2, g2) = out
+    assert np.abs(e1 - e2).max() < 1e-12 and np.abs(f1 - f2).max() < 1e-12
+    assert np.abs(v1 - v2).max() < 1e-12
+    assert np.abs(p1 - p2).max() < 1e-12 and np.abs(g1 - g2).max() < 1e-10

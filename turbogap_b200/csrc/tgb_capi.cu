@@ -1730,6 +1730,20 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     TGB_CUDA(cudaMemcpyAsync(&P, E.nl.pstart + E.n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     TGB_CUDA(cudaStreamSynchronize(st));
     TGB_TRY(E.nl.reserve(E.n, E.nsc, (int64_t)(P * 1.4) + 64, E.g));
+    if (E.use_cells) {
+        // slot rows of the one-pass build: the largest count with 25 % headroom (a
+        // site that outgrows them sends that build to the filling search);
+        // TGB_NL_SLOTS=s sets the rows, 0 keeps the two-pass build
+        std::vector<int> cnt(E.n);
+        TGB_CUDA(cudaMemcpyAsync(cnt.data(), E.nl.n_neigh, sizeof(int) * E.n,
+                                 cudaMemcpyDeviceToHost, st));
+        TGB_CUDA(cudaStreamSynchronize(st));
+        int mx = 1;
+        for (int c : cnt) mx = std::max(mx, c);
+        int slots = (mx + mx / 4 + 8 + 15) / 16 * 16;
+        if (const char *e = std::getenv("TGB_NL_SLOTS")) slots = std::max(0, std::atoi(e));
+        if (slots > 0 && slots <= 256) TGB_TRY(E.nl.reserve_slots(E.n, slots));
+    }
     TGB_CUDA(cudaMemsetAsync(E.nl.err, 0, sizeof(unsigned), st));
     // turbogap_md.f90:453-470: a supercell always rebuilds; otherwise a positive
     // buffer keeps the list until an atom has moved far enough

@@ -176,6 +176,9 @@ struct PairSink {
 // 27 cells form one flattened sequence in that order; lanes test 32 consecutive
 // candidates at a time and emit the accepted ones in sequence order (ballot +
 // prefix popcount), so the pairs come out exactly in the reference's order.
+// Three uses, as in the batched search: count (pstart and slots unset), count
+// into slot rows (slots > 0: pair e of site i at row i * slots + e while e <
+// slots, *ovf set past it), and fill at pstart (only when *gate is set, if given).
 __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box bx, CellGrid g,
                                 double rcut, const int *__restrict__ do_list,
                                 const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
@@ -185,10 +188,14 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
                                 const int64_t *__restrict__ pstart, int64_t cap,
                                 int *__restrict__ nbr, double *__restrict__ rjs,
                                 double *__restrict__ xyz, unsigned *err,
-                                const int *__restrict__ when) {
+                                const int *__restrict__ when, int slots = 0,
+                                int *__restrict__ ovf = nullptr,
+                                const int *__restrict__ gate = nullptr) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n_sites || (when && !*when)) return;
+    if (i >= n_sites || (when && !*when) || (gate && !*gate)) return;
+    const bool slotted = !pstart && slots > 0;
+    const bool writes = pstart || slotted;
     if (do_list && !do_list[i]) {
         if (!pstart && lane == 0) n_neigh[i] = 0;
         return;
@@ -219,9 +226,10 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
     const double rc2 = rcut * rcut, rc2_lo = rc2 * (1.0 - 1e-12), rc2_hi = rc2 * (1.0 + 1e-12);
-    const int64_t base = pstart ? pstart[i] : 0;
-    if (pstart && lane == 0) {   // self pair first
-        if (base < cap) {
+    const int64_t base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
+    const int64_t lim = pstart ? cap : base + slots;
+    if (writes && lane == 0) {   // self pair first
+        if (base < lim) {
             nbr[base] = i;
             rjs[base] = 0.0;
             xyz[3 * base] = 0.0;
@@ -268,7 +276,7 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
                 }
                 if (d2 < rc2_lo) {
                     take = true;
-                    if (pstart) d = sqrt(d2);
+                    if (writes) d = sqrt(d2);
                 } else if (d2 <= rc2_hi) {
                     d = sqrt(d2);
                     take = d < rcut;
@@ -276,14 +284,16 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, take);
-        if (pstart && take) {
+        if (writes && take) {
             const int64_t p = base + count + __popc(m & ((1u << lane) - 1u));
-            if (p < cap) {
+            if (p < lim) {
                 nbr[p] = k;
                 rjs[p] = d;
                 xyz[3 * p] = dist[0];
                 xyz[3 * p + 1] = dist[1];
                 xyz[3 * p + 2] = dist[2];
+            } else if (slotted) {
+                *ovf = 1;   // the filling search makes this build
             } else {
                 atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
             }
@@ -291,6 +301,29 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
         count += __popc(m);
     }
     if (!pstart && lane == 0) n_neigh[i] = count;
+}
+
+// Slot rows to the compact arrays (a warp per site), unless a row overflowed.
+__global__ void k_nl_compact(int n_sites, int slots, const int *__restrict__ n_neigh,
+                             const int64_t *__restrict__ pstart, const int *__restrict__ snbr,
+                             const double *__restrict__ srjs, const double *__restrict__ sxyz,
+                             const int *__restrict__ ovf, const int *__restrict__ when, int64_t cap,
+                             int *__restrict__ nbr, double *__restrict__ rjs,
+                             double *__restrict__ xyz, unsigned *err) {
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n_sites || *ovf || (when && !*when)) return;
+    const int cnt = n_neigh[i];
+    const int64_t dst = pstart[i], src = (int64_t)i * slots;
+    if (dst + cnt > cap) {
+        if (lane == 0) atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+        return;
+    }
+    for (int e = lane; e < cnt; e += 32) {
+        nbr[dst + e] = snbr[src + e];
+        rjs[dst + e] = srjs[src + e];
+    }
+    for (int e = lane; e < 3 * cnt; e += 32) xyz[3 * dst + e] = sxyz[3 * src + e];
 }
 
 // O(N * N_supercell) search (neighbors.f90:474-514): ascending supercell index.
@@ -557,7 +590,19 @@ int NeighborList::reserve(int ns, int nsc, int64_t pair_cap, const CellGrid &g) 
     return TG_OK;
 }
 
+int NeighborList::reserve_slots(int ns, int s) {
+    dev_free(snbr); dev_free(srjs); dev_free(sxyz);
+    slots = 0;
+    TGB_TRY(dev_alloc(&snbr, (size_t)ns * s));
+    TGB_TRY(dev_alloc(&srjs, (size_t)ns * s));
+    TGB_TRY(dev_alloc(&sxyz, (size_t)3 * ns * s));
+    if (!ovf) TGB_TRY(dev_alloc(&ovf, 1));
+    slots = s;
+    return TG_OK;
+}
+
 void NeighborList::release() {
+    dev_free(snbr); dev_free(srjs); dev_free(sxyz); dev_free(ovf);
     dev_free(n_neigh); dev_free(pstart); dev_free(cell_xyz); dev_free(cell_atoms);
     dev_free(cell_count); dev_free(cell_start); dev_free(cell_fill); dev_free(nbr);
     dev_free(rjs); dev_free(xyz); dev_free(scan_tmp); dev_free(err); dev_free(cell_pos);
@@ -672,6 +717,8 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     const int TB = 128;
     const int gb = (n_sites + TB - 1) / TB;
     const int gw = (int)(((int64_t)n_sites * 32 + TB - 1) / TB);   // one warp per site
+    const bool one_pass = use_cells && nl.slots > 0 && nl.cap > 0;
+    if (one_pass) TGB_CUDA(cudaMemsetAsync(nl.ovf, 0, sizeof(int), st));
     if (use_cells) {
         const int ncells = g.mx * g.my * g.mz;
         TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
@@ -688,8 +735,10 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
             k_cell_gather_pos<<<gb, TB, 0, st>>>(n_sites, nl.cell_atoms, pos, nl.cell_pos, when);
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
                                            nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
-                                           nl.n_neigh, nullptr, nl.cap, nullptr, nullptr, nullptr,
-                                           nl.err, when);
+                                           nl.n_neigh, nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
+                                           one_pass ? nl.srjs : nullptr,
+                                           one_pass ? nl.sxyz : nullptr, nl.err, when,
+                                           one_pass ? nl.slots : 0, nl.ovf);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nullptr,
                                       nl.cap, nullptr, nullptr, nullptr, nl.err);
@@ -699,10 +748,15 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n_sites,
                                            st));
     if (use_cells) {
+        if (one_pass)
+            k_nl_compact<<<gw, TB, 0, st>>>(n_sites, nl.slots, nl.n_neigh, nl.pstart, nl.snbr,
+                                            nl.srjs, nl.sxyz, nl.ovf, when, nl.cap, nl.nbr, nl.rjs,
+                                            nl.xyz, nl.err);
+        // the filling search: always in the two-pass build, after an overflow in the other
         k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
                                            nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
                                            nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
-                                           nl.err, when);
+                                           nl.err, when, 0, nullptr, one_pass ? nl.ovf : nullptr);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nl.pstart,
                                       nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);

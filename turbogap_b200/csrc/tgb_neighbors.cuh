@@ -58,8 +58,17 @@ struct NeighborList {
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
     unsigned *err = nullptr;
+    // One search pass on the cell path (as in the batched build): with slots > 0
+    // and cap > 0 the search writes each site's pairs into fixed rows while it
+    // counts them, a copy compacts the rows after the scan, and a site with more
+    // than slots pairs sets *ovf, which sends the build to the filling search.
+    int slots = 0;
+    int *snbr = nullptr;
+    double *srjs = nullptr, *sxyz = nullptr;
+    int *ovf = nullptr;
 
     int reserve(int n_sites, int n_sc, int64_t pair_cap, const CellGrid &g);
+    int reserve_slots(int n_sites, int slots);
     void release();
 };
 
