@@ -48,3 +48,17 @@ def test_maxwell_velocity_distribution_shape():
     # fourth moment of a Gaussian (kurtosis 3): the shape, not only the width
     assert abs((z ** 4).mean() - 3.0) < 0.1
     assert np.abs((m[:, None] * v).sum(0)).max() < 1e-9 * m.sum()
+
+
+def test_wrap_triclinic_lands_in_the_cell():
+    """wrap_pbc in a sheared box: the fractional coordinates end in [0, 1)."""
+    rng = np.random.default_rng(3)
+    box = np.array([[8.0, 0.0, 0.0], [2.4, 7.5, 0.0], [-1.1, 1.6, 9.0]])
+    p = rng.uniform(-25, 25, size=(60, 3))
+    q = p.copy()
+    O.wrap_pbc(q, box[0], box[1], box[2])
+    frac = q @ np.linalg.inv(box)
+    assert frac.min() > -1e-12 and frac.max() < 1.0 + 1e-12
+    # a whole-cell shift of the original
+    shift = (p - q) @ np.linalg.inv(box)
+    assert np.abs(shift - np.round(shift)).max() < 1e-9

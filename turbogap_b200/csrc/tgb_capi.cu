@@ -1666,8 +1666,9 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
     E.rcut = rcut;
     // read_files.f90:320-380: supercell when the box cannot hold a cutoff sphere
     host_unit_cells(a_box, b_box, c_box, rcut, E.indices);
+    // a triclinic box takes the reference's O(N N_supercell) list search
+    // (neighbors.f90:474-514) and its triclinic wrap_pbc
     E.box_prim = make_box(a_box, b_box, c_box);
-    TGB_CHECK(E.box_prim.ortho, TG_ERR_ARG, "the device engine supports orthorhombic boxes");
     double A[3], B[3], Cc[3];
     for (int q = 0; q < 3; ++q) {
         A[q] = a_box[q] * E.indices[0];

@@ -426,6 +426,27 @@ __global__ void k_wrap_ortho(int n, double *__restrict__ pos, Box bx) {
                (double)(int)s2 * bx.c[q];
 }
 
+// wrap_pbc (md.f90:348-380), triclinic: i_shift from get_distance of the origin
+// and the atom (neighbors.f90:107-140): floor of minus the Gram-inverse solution,
+// in the reference's operation order.
+__global__ void k_wrap_tri(int n, double *__restrict__ pos, Box bx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *p = pos + 3 * (size_t)i;
+    const double dd[3] = {p[0], p[1], p[2]};   // posj - posi with posi = 0
+    const double v[3] = {-1.0 * dot3(dd, bx.a), -1.0 * dot3(dd, bx.b), -1.0 * dot3(dd, bx.c)};
+    int sh[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) s = s + bx.inv[r][j] * v[j];
+        sh[r] = (int)floor(-s);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        p[q] = p[q] - (double)sh[0] * bx.a[q] - (double)sh[1] * bx.b[q] - (double)sh[2] * bx.c[q];
+}
+
 // sum_i m_i v_i (3) and sum_i m_i (1) into acc[4] (FP64 atomics, then apply)
 __global__ void k_cm_accumulate(int n, const double *__restrict__ vel, const double *__restrict__ m,
                                 double *acc) {
@@ -1044,11 +1065,8 @@ int launch_velocity_verlet(int n, double *pos, double *pos_prev, double *vel, co
 }
 
 int launch_wrap(int n, double *pos, const Box &bx, cudaStream_t st) {
-    if (!bx.ortho) {
-        set_error("wrap_pbc on device supports orthorhombic boxes only");
-        return TG_ERR_ARG;
-    }
-    k_wrap_ortho<<<(n + 255) / 256, 256, 0, st>>>(n, pos, bx);
+    if (bx.ortho) k_wrap_ortho<<<(n + 255) / 256, 256, 0, st>>>(n, pos, bx);
+    else k_wrap_tri<<<(n + 255) / 256, 256, 0, st>>>(n, pos, bx);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }

@@ -9,8 +9,8 @@ forces were evaluated at (turbogap_md.f90:357-380). ``run_predict`` evaluates
 every frame of the atoms file (``turbogap predict``).
 
 soap_turbo blocks (compressed ones included) and the distance_2b, angle_3b and
-core_pot families run on the device. Decks that need anything else
-(thermostats, barostats, adaptive time steps, non-orthorhombic boxes) are
+core_pot families run on the device, in orthorhombic and triclinic boxes. Decks
+that need anything else (thermostats, barostats, adaptive time steps) are
 refused with the keyword that needs it. Velocities drawn here (no velocity
 column, or ``randomize_velocities``) follow md.f90:95-158 with numpy's
 generator, so they differ from the reference's random stream.
@@ -205,8 +205,6 @@ def run_predict(input_path: str, out_dir: Optional[str] = None) -> List[Dict[str
     keys = deck.begin()
     res = []
     for k, frame in enumerate(deck.frames):
-        if not np.allclose(frame.lattice, np.diag(np.diag(frame.lattice))):
-            raise NotImplementedError("the device path takes orthorhombic boxes")
         ids = deck.species_ids(frame)
         eng = deck.engine(frame, keys)
         e, f, vir = eng.compute()
