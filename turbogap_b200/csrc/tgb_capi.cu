@@ -74,7 +74,7 @@ struct Block {
     int zeta_int = 0;
     signed char zmap[kMaxZ];
     DBuf<float> table, selfR;
-    DBuf<float2> table_fd;   // the descriptor's (f, f') copy, function-major
+    DBuf<float4> table_fd;   // the descriptor's (f, f') interval copy
     DBuf<__nv_bfloat16> QsA, QsT;
     DBuf<double> alpha, mu, aoff, g0;
     DBuf<float> g0f;       // g0 in fp32: subtracted from the MLP's dE/dq rows
@@ -903,7 +903,7 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
                                                                    b->QsA.p, b->QsT.p);
     k_prep_alpha<<<(b->Mpad + 255) / 256, 256, 0, C.st>>>(ta.p, b->M, b->Mpad, b->alpha.p);
     TGB_CUDA(cudaGetLastError());
-    TGB_TRY(b->table_fd.ensure((size_t)hh.ns * (b->amax + b->lmax + 1) * (kTableIntervals + 1)));
+    TGB_TRY(b->table_fd.ensure((size_t)hh.ns * (b->amax + b->lmax + 1) * kTableIntervals));
     TGB_TRY(build_soap_tables(hh, b->table.p, b->selfR.p, C.st, b->table_fd.p));
     TGB_TRY(make_tma_bf16(&b->tmB1, b->QsA.p, b->Mpad, b->K1, b->K1, kGemmBN));
     TGB_TRY(make_tma_bf16(&b->tmB2, b->QsT.p, b->dim, b->K2, b->K2, kGemmBN));

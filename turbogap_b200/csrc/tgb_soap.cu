@@ -235,17 +235,18 @@ int descriptor_ref_index(int d_internal, int nt, int nl) {
     return pi_ref * nl + l;
 }
 
-// (f, f') of every function and node (node-major, like the float4 table): the
-// descriptor's gathers touch half the bytes
-__global__ void k_table_fd(int nf, const float4 *__restrict__ T, float2 *__restrict__ out) {
+// (f, f') at both ends of every interval and function, (f_k, f'_k, f_k+1, f'_k+1),
+// interval-major: the descriptor's Hermite value is one 16-byte gather per
+// function instead of two 8-byte ones
+__global__ void k_table_fd(int nf, const float4 *__restrict__ T, float4 *__restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nf * (kTableIntervals + 1)) return;
-    const float4 v = T[i];
-    out[i] = make_float2(v.x, v.y);
+    if (i >= nf * kTableIntervals) return;
+    const float4 a = T[i], b = T[i + nf];   // node k and node k + 1 of function j
+    out[i] = make_float4(a.x, a.y, b.x, b.y);
 }
 
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st,
-                      float2 *table_fd) {
+                      float4 *table_fd) {
     const int amax = h.alpha_max[0];
     const int tw = table_width(amax, h.lmax);
     std::vector<double> W(amax * amax);
@@ -263,9 +264,9 @@ int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cuda
         k_build_self<<<1, 32, 0, st>>>(th, dW, self_R + s * amax);
         if (table_fd) {
             const int nf = amax + h.lmax + 1, nodes = kTableIntervals + 1;
-            k_table_fd<<<(nf * nodes + 255) / 256, 256, 0, st>>>(
+            k_table_fd<<<(nf * kTableIntervals + 255) / 256, 256, 0, st>>>(
                 nf, reinterpret_cast<const float4 *>(table + (size_t)s * nodes * tw),
-                table_fd + (size_t)s * nf * nodes);
+                table_fd + (size_t)s * nf * kTableIntervals);
         }
     }
     cudaError_t e = cudaGetLastError();
@@ -296,10 +297,10 @@ struct Hermite {
         h01 = -2.f * t3 + 3.f * t2;
         h11 = (t3 - t2) * h;
     }
-    // value from the (f, f') table of function j
-    __device__ __forceinline__ float value_fd(const float2 *T, int nf, int j) const {
-        const float2 a = __ldg(T + (size_t)k * nf + j), b = __ldg(T + (size_t)(k + 1) * nf + j);
-        return h00 * a.x + h10 * a.y + h01 * b.x + h11 * b.y;
+    // value from the interval table (f_k, f'_k, f_k+1, f'_k+1) of function j
+    __device__ __forceinline__ float value_fd(const float4 *T, int nf, int j) const {
+        const float4 a = __ldg(T + (size_t)k * nf + j);
+        return h00 * a.x + h10 * a.y + h01 * a.z + h11 * a.w;
     }
     // value from (f, f') and, when wanted, first derivative from (f', f'') of function j
     __device__ __forceinline__ float value(const float4 *T, int nf, int j) const {
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                         z = (float)S.xyz[3 * p + 2];
             const float r = sqrtf(x * x + y * y + z * z);
             if (s >= 0 && r < P.rcut[s] && r > 0.f) {
-                const float2 *Tf = P.table_fd + (size_t)s * NF * (kTableIntervals + 1);
+                const float4 *Tf = P.table_fd + (size_t)s * NF * kTableIntervals;
                 const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
                 float rv[AMAX];
 #pragma unroll

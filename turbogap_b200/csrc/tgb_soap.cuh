@@ -19,7 +19,7 @@ struct SoapParams {
     float tab_h[kMaxSpecies];  // node spacing (A)
     float tab_inv_h[kMaxSpecies];
     const float *table;        // [ns][kTableIntervals + 1][tw]
-    const float2 *table_fd;    // [ns][kTableIntervals + 1][functions]: (f, f') only
+    const float4 *table_fd;    // [ns][kTableIntervals][functions]: (f, f') at both ends
     const float *self_R;       // [ns][amax]: central-atom contribution to c_{n,00}
     const double *mu;          // [dim]: mean of the sparse set; the GEMMs see q - mu
     const double *g0;          // [dim]: sum_s kcoef_s (q_s - mu), the K = 1 part of dE/dq
@@ -137,10 +137,10 @@ struct SoapHostHypers {
 int table_width(int amax, int lmax);
 
 // Builds table and self_R (device buffers owned by the caller) in FP64 on the GPU,
-// and, when table_fd is given, the descriptor's (f, f') copy
-// ([ns][kTableIntervals + 1][amax + lmax + 1] float2).
+// and, when table_fd is given, the descriptor's interval copy
+// ([ns][kTableIntervals][amax + lmax + 1] float4: f, f' at both ends).
 int build_soap_tables(const SoapHostHypers &h, float *table, float *self_R, cudaStream_t st,
-                      float2 *table_fd = nullptr);
+                      float4 *table_fd = nullptr);
 
 // Launchers; return TG_ERR_ARG for unsupported (ns, amax, lmax).
 bool soap_shape_supported(int ns, int amax, int lmax);
