@@ -144,3 +144,30 @@ def test_key_reuse_with_another_shape(gpu, blocks):
     assert np.array_equal(e_again, e_old)
     eng.close()
 
+
+
+def test_repeated_entries_add(gpu):
+    """A transformation with an entry split in two gives the descriptors of the
+    one with the summed weight (entries add, in both CSR copies on the device)."""
+    full = ch_hypers(1)
+    base = random_transformation(full.uncompressed_dim, 40, seed=91, per_row=2)
+    split = SoapCompression(base.dim, np.concatenate([base.P_i, base.P_i[:7]]),
+                            np.concatenate([base.P_j, base.P_j[:7]]),
+                            np.concatenate([base.P_el, base.P_el[:7] * 0.75]))
+    split.P_el[:7] = base.P_el[:7] * 0.25
+    st = synth.random_structure(300, L, 1.0, seed=92, h_fraction=0.25)
+    nl = neighbor_data(st, 3.7)
+    out = []
+    for key, comp in ((1804, base), (1805, split)):
+        h = ch_hypers(1)
+        h.compress = comp
+        b = sparse_block(h, 100, seed=93, n_atoms=300, L=L, d_min=1.0, h_fraction=0.25,
+                         n_structs=1)
+        gpu.soap_backend_begin(b, key=key)
+        out.append(gpu.get_soap(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"], nl["xyz"],
+                                st.species, st.species, h.dim))
+    h = ch_hypers(1)
+    h.compress = base
+    qo, _, _ = oracle_descriptors(st, h, nl)
+    assert np.abs(out[0] - out[1]).max() < 1e-7
+    assert np.abs(out[0] - qo).max() < Q_TOL and np.abs(out[1] - qo).max() < Q_TOL

@@ -125,3 +125,21 @@ def test_compressed_forces_and_virial_match_finite_differences(compressed_blocks
             return _energy(st, blocks, pos=st.positions @ eps.T, box=st.box @ eps.T)
         dE = (strained(1e-4) - strained(-1e-4)) / 2e-4
         assert abs(-dE - vir[a, b]) <= 1e-4 * np.abs(vir).max()
+
+
+def test_repeated_entries_add():
+    """Entries of a transformation add up (q_c(i) += P_el p(P_j) per entry, the
+    loop the file format implies): a list with an entry split in two gives the
+    same descriptor as the list with the summed weight."""
+    st = random_structure(90, L, 1.0, seed=97, h_fraction=0.25)
+    nl = neighbor_data(st, 3.7)
+    full = ch_small(1)
+    base = random_transformation(full.uncompressed_dim, 20, seed=98, per_row=2)
+    split = SoapCompression(base.dim, np.concatenate([base.P_i, base.P_i[:5]]),
+                            np.concatenate([base.P_j, base.P_j[:5]]),
+                            np.concatenate([base.P_el * 1.0, np.zeros(5)]))
+    split.P_el[:5] = base.P_el[:5] * 0.25
+    split.P_el[-5:] = base.P_el[:5] * 0.75
+    q1, n1, _ = oracle_descriptors(st, ch_small(1, base), nl)
+    q2, n2, _ = oracle_descriptors(st, ch_small(1, split), nl)
+    assert np.allclose(q1, q2, atol=1e-14) and np.allclose(n1, n2, rtol=1e-14)
