@@ -150,7 +150,13 @@ def test_repeated_entries_add(gpu):
     """A transformation with an entry split in two gives the descriptors of the
     one with the summed weight (entries add, in both CSR copies on the device)."""
     full = ch_hypers(1)
-    base = random_transformation(full.uncompressed_dim, 40, seed=91, per_row=2)
+    rng = np.random.default_rng(91)
+    # the first 80 components (n = 0 with every n', all l: the large ones) in
+    # pairs with positive weights, so that |v| is of the size of |p| and the 1e-7
+    # descriptor bar applies as for the power spectrum itself (a few random
+    # small components would make |v| small and magnify the fp32 error of c)
+    base = SoapCompression(40, np.repeat(np.arange(1, 41), 2), rng.permutation(80) + 1,
+                           rng.uniform(0.2, 1.0, size=80))
     split = SoapCompression(base.dim, np.concatenate([base.P_i, base.P_i[:7]]),
                             np.concatenate([base.P_j, base.P_j[:7]]),
                             np.concatenate([base.P_el, base.P_el[:7] * 0.75]))
