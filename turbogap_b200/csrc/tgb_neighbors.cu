@@ -879,6 +879,7 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
     const bool writes = pstart || slotted;
     const BatchStruct b = st[atom_struct[i]];
     const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    const double invL[3] = {1.0 / b.L[0], 1.0 / b.L[1], 1.0 / b.L[2]};
     // candidate segments: lane c < 27 describes cell c (mode 0); mode 1 has one
     // segment per image
     const int nimg = (2 * b.img[0] + 1) * (2 * b.img[1] + 1) * (2 * b.img[2] + 1);
@@ -950,7 +951,10 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 double v = pk[q] - pi[q];
-                v -= b.L[q] * rint(v / b.L[q]);   // minimum image
+                // minimum image, by the reciprocal: rint differs from that of the
+                // quotient only within an ulp of |v| = L / 2, a tie between two
+                // images at the same distance
+                v -= b.L[q] * rint(v * invL[q]);
                 v += t[q] * b.L[q];
                 dist[q] = v;
                 d2 += v * v;
