@@ -115,3 +115,35 @@ def test_energy_continuous_across_cutoff():
         es.append(O.evaluate(pos, np.array([1, 1], np.int32), np.eye(3) * 12.0, [blk])[0].sum())
     es = np.array(es)
     assert np.abs(np.diff(es)).max() < 1e-12
+
+
+def test_triclinic_forces_and_virial_match_finite_differences():
+    """A sheared cell through the reference's triclinic path (Gram-inverse
+    get_distance, brute-force lists, supercell replicas): forces and virial
+    against central finite differences of the oracle's own energy."""
+    from turbogap_b200.hypers import SoapTurboHypers
+    from turbogap_b200.synth import Structure
+    h = SoapTurboHypers(species_z=[1, 2], alpha_max=[4, 4], l_max=4, central_species=1)
+    L0 = (60 / 0.12) ** (1 / 3)
+    blk = sparse_block(h, 40, seed=26, n_atoms=60, L=L0, d_min=1.0, h_fraction=0.25,
+                       n_structs=2)
+    cube = random_structure(60, L0, 1.0, seed=27, h_fraction=0.25)
+    box = np.array([[1.0, 0.0, 0.0], [0.2, 1.0, 0.0], [-0.15, 0.1, 1.0]]) * L0
+    st = Structure((cube.positions / L0) @ box, cube.species, box)
+    _, f, vir, _ = O.evaluate(st.positions, st.species, st.box, [blk])
+    for i in (0, 17, 42):
+        for q in range(3):
+            p = st.positions.copy()
+            p[i, q] += H_FD
+            ep = _energy(st, [blk], pos=p)
+            p[i, q] -= 2 * H_FD
+            em = _energy(st, [blk], pos=p)
+            fd = -(ep - em) / (2 * H_FD)
+            assert abs(fd - f[i, q]) <= 1e-4 * max(abs(f[i, q]), 1e-3 * np.abs(f).max())
+    for a, b in ((0, 0), (0, 1), (2, 1)):
+        def strained(s):
+            eps = np.eye(3)
+            eps[a, b] += s
+            return _energy(st, [blk], pos=st.positions @ eps.T, box=st.box @ eps.T)
+        dE = (strained(STRAIN) - strained(-STRAIN)) / (2 * STRAIN)
+        assert abs(-dE - vir[a, b]) <= 1e-4 * np.abs(vir).max()
