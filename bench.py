@@ -2,7 +2,7 @@
 """SOAP-GAP E+F atom-steps/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ch32k] [--precision bf16x3|bf16]
+                    [--workload ch1m] [--precision bf16x3|bf16]
 
 One step is one NVE velocity-Verlet MD step of the workload through the
 device-resident engine: neighbour list rebuild, every soap_turbo block
@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ch32k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ch1m", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "bf16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=10)
@@ -242,9 +242,7 @@ def mixed_leg(B, eng, blocks, w, a, ext, dist, plain_ms):
                      "final_loss": [float(l_[-1]) for l_ in losses]},
         "ms_per_step_by_pass": prof,
     }
-    for m in mlps:
-        m.close()
-    return out
+    return out, mlps
 
 
 # ------------------------------------------------------------------ CPU (oracle)
@@ -266,15 +264,107 @@ def calibrate_sample(O, st, blocks, target_s):
     return int(max(64, min(st.n, round(target_s / per_site)))), per_site
 
 
-def cpu_baseline_leg(w, st, target_s=15.0):
+def cpu_baseline_leg(w, st, blocks, target_s=15.0, single_core_s=5.0):
+    """The FP64 oracle port on the host cores: E+F of central sites 0..n-1 of the
+    workload's structure (one MPI rank's share, all blocks, the share's lists),
+    with the sparse sets the GPU arm uses, so the same share on the GPU is a
+    parity check. The sample is sized to about target_s; the rate is sites per
+    second, a full step of the structure taking N / rate. Also a single-thread
+    rate on a smaller share. Returns the cpu_baseline object and the oracle's
+    share (n, energies, forces, virial)."""
     import oracle as O
-    blocks = oracle_blocks(w)
+    cores = O.set_threads(0)
     n, per = calibrate_sample(O, st, blocks, target_s)
-    t = time_oracle_sample(O, st, blocks, n)
-    cores = os.cpu_count()
-    return {"value": n / t, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"E+F of sites 0..{n - 1} of the {w.name} structure (the share of one "
-                      f"MPI rank, all blocks), FP64 oracle port, {cores} OpenMP threads, {t:.1f} s"}
+    t0 = time.perf_counter()
+    e, f, v, _ = O.evaluate(st.positions, st.species, st.box, blocks, site_range=(0, n))
+    t = time.perf_counter() - t0
+    O.set_threads(1)
+    try:
+        n1 = int(max(32, min(n, round(single_core_s / (per * cores)))))
+        t1 = time_oracle_sample(O, st, blocks, n1)
+    finally:
+        O.set_threads(cores)
+    cpu = {"value": n / t, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"E+F of central sites 0..{n - 1} of the {w.name} structure (one MPI "
+                     f"rank's share, all blocks), FP64 oracle port, {cores} OpenMP threads, "
+                     f"{t:.1f} s; the rate is sites per second, so a full step of the "
+                     f"{st.n}-atom structure would take {st.n * t / n:.0f} s",
+           "host_cpu": _host_cpu(),
+           "single_core": {"value": n1 / t1, "unit": UNIT, "cores": 1,
+                           "sample": f"central sites 0..{n1 - 1}, 1 thread, {t1:.1f} s"}}
+    return cpu, (n, e, f, v)
+
+
+def _host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def parity_leg(B, eng, st, oracle_share, blocks, keys, mlps, gate_ev):
+    """The plain form against the FP64 oracle on the CPU baseline's share (the
+    same central sites, the same structure and sparse sets): max |dE| per site,
+    max |dF| over the share's force contributions, the virial relative to its
+    largest component. The mixed form on the same share (energy RMSE over the
+    share's sites), and the mixed form's full-force RMSE on a held-out cell of
+    the workload's kind (2048 atoms, another seed), where the oracle evaluates
+    every site."""
+    import oracle as O
+    n, eo, fo, vo = oracle_share
+    eng.set_state(st.positions, np.zeros_like(st.positions))
+    eng.set_site_range(0, n)
+    e, f, v = eng.compute()
+    out = {"sites": n, "structure": "the benchmark structure at its initial positions",
+           "max_dE_eV_per_atom": float(np.abs(e - eo)[:n].max()),
+           "max_dF_eV_per_A": float(np.abs(f - fo).max()),
+           "virial_rel": float(np.abs(v - vo).max() / max(np.abs(vo).max(), 1e-300)),
+           "bounds": {"dE_eV_per_atom": 1e-6, "dF_eV_per_A": 1e-6, "virial_rel": 1e-6}}
+    if mlps:
+        for i, m in enumerate(mlps):
+            B.engine_set_mlp(eng, i, m, gate_ev=gate_ev)
+        em, fm, _ = eng.compute()
+        gated = sum(B.engine_mlp_stats(eng, i)[0] for i in range(len(mlps)))
+        for i in range(len(mlps)):
+            B.engine_set_mlp(eng, i, None)
+        out["mixed_share"] = {"rmse_e_mev_per_atom": 1e3 * float(np.sqrt(np.mean((em - eo)[:n] ** 2))),
+                              "max_e_mev_per_atom": 1e3 * float(np.abs(em - eo)[:n].max()),
+                              "gated_sites": int(gated)}
+        # held-out cell: full forces
+        held = _held_out_cell(st)
+        if held is not None:
+            eh, fh, _, _ = O.evaluate(held.positions, held.species, held.box, blocks)
+            e2 = B.Engine(held.positions, held.species, held.masses, held.box, keys)
+            ep, fp, _ = e2.compute()
+            for i, m in enumerate(mlps):
+                B.engine_set_mlp(e2, i, m, gate_ev=gate_ev)
+            em2, fm2, _ = e2.compute()
+            g2 = sum(B.engine_mlp_stats(e2, i)[0] for i in range(len(mlps)))
+            e2.close()
+            out["held_out_cell"] = {
+                "atoms": held.n,
+                "plain_max_dE_eV_per_atom": float(np.abs(ep - eh).max()),
+                "plain_max_dF_eV_per_A": float(np.abs(fp - fh).max()),
+                "mixed_rmse_e_mev_per_atom": 1e3 * float(np.sqrt(np.mean((em2 - eh) ** 2))),
+                "mixed_rmse_f_mev_per_A": 1e3 * float(np.sqrt(np.mean((fm2 - fh) ** 2))),
+                "mixed_gated_sites": int(g2),
+                "mixed_bounds": {"rmse_e_mev_per_atom": 1.0, "rmse_f_mev_per_A": 30.0}}
+    eng.set_site_range(0, st.n)
+    return out
+
+
+def _held_out_cell(st):
+    """A 2048-atom cell of the benchmark structure's kind (density, composition,
+    minimum distance), from another seed; None for kinds not covered."""
+    n = 2048
+    dens = st.n / abs(np.linalg.det(st.box))
+    hfrac = float(np.mean(st.species == 2))
+    dmin = 1.0 if hfrac > 0 else 1.2
+    return synth.random_structure(n, (n / dens) ** (1 / 3), dmin, seed=777001,
+                                  h_fraction=round(hfrac, 4))
 
 
 def run_reference_batch(a, w, world):
@@ -542,17 +632,21 @@ def run_ours(a):
            "api": "tg_engine_set_state + tg_engine_compute (host positions in, host energies/"
                   "forces/virial out)"}
 
-    mixed = None
+    mixed, mlps = None, []
     if not a.no_mixed:
-        mixed = mixed_leg(B, eng, blocks, w, a, ext, dist, 1e3 * t_max / a.steps)
+        mixed, mlps = mixed_leg(B, eng, blocks, w, a, ext, dist, 1e3 * t_max / a.steps)
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_leg(w, w.structure())
+            cpu, share = cpu_baseline_leg(w, st, blocks)
         except Exception as ex:  # keep the bench line even if the oracle cannot run
-            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"failed: {ex}"}
+            cpu, share = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                          "sample": f"failed: {ex}"}, None
+        if share is not None:
+            parity = parity_leg(B, eng, st, share, blocks, keys, mlps, a.gate_ev)
+    for m in mlps:
+        m.close()
 
     # the per-site DRAM bytes were captured at D = 1224, M = 4000 (ch16k)
     same_gemm = all(b.hypers.dim == 1224 and b.n_sparse == 4000 for b in blocks)
@@ -586,6 +680,7 @@ def run_ours(a):
                                "issue_rate_tflops": achieved2 * nsplit},
                      "ms_per_step_by_pass": prof},
         "cpu_baseline": cpu,
+        "parity": parity,
         "mixed": mixed,
         "e2e": e2e,
         "gpu_launches": kernels_per_step * a.steps,

@@ -226,8 +226,11 @@ int tg_build_neighbors_list(int32_t n_sites_supercell, const double *positions,
  *   pstart[i] + k; neighbors_list (cap) 1-based; rjs (cap); xyz (3, cap).
  *   stream: a cudaStream_t (NULL = legacy default stream); the call
  *   synchronises it before returning. *n_pairs = pairs needed; more than cap
- *   gives TG_ERR_CAPACITY. Make the first call on a device outside stream
- *   capture (it resolves the scratch address). Calls that overlap on one
+ *   gives TG_ERR_CAPACITY. rcut_max must be positive and finite. Make the
+ *   first call on a device outside stream capture: it resolves the scratch
+ *   address and, under lazy module loading, loads the module that holds the
+ *   array, so the device memory it takes appears at that call, once per
+ *   device. Calls that overlap on one
  *   device share the scratch and race: serialise them. Needs no
  *   tg_context_init. */
 int tg_build_neighbors_list_noalloc(int32_t n_sites, const double *positions,

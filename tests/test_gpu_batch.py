@@ -1,4 +1,4 @@
-"""Batched evaluation of independent structures of uneven size (BASELINE config 2
+"""Batched evaluation of independent structures of uneven size (the batched
 kind) against the FP64 oracle, structure by structure: boxes below 2 rcut (several
 images of a neighbour), between 2 and 3 rcut (minimum image) and above 3 rcut
 (cell lists)."""

@@ -74,7 +74,9 @@ def test_noalloc_matches_allocating_entry_twice(gpu):
     st_b = random_structure(3000, 31.0, 1.1, seed=72)
     ref_a, ref_b = _reference(st_a), _reference(st_b)
     cap = 60 * 3000
-    rc, P, out_a, _ = _noalloc(st_a, cap, stream)          # first call: per-device set-up
+    # first call: the per-device set-up, which (lazy module loading) may load the
+    # module and its fixed array, so its memory change is not checked
+    rc, P, out_a, _ = _noalloc(st_a, cap, stream)
     assert rc == 0, lib().tg_last_error()
     assert P == len(ref_a["neighbors_list"])
     _same(ref_a, out_a)
@@ -108,3 +110,12 @@ def test_noalloc_limits(gpu):
     rc = lib().tg_build_neighbors_list_noalloc(10, 1, tri[0], tri[1], tri[2], RCUT,
                                                1, 1, 1, 1, 1, 1, C.byref(Pn), nul)
     assert rc == -1 and b"orthorhombic" in lib().tg_last_error()
+    cube = [np.eye(3)[k] * 20.0 for k in range(3)]
+    for bad in (0.0, -1.0, float("nan"), float("inf")):        # rcut_max checked first
+        rc = lib().tg_build_neighbors_list_noalloc(10, 1, cube[0], cube[1], cube[2], bad,
+                                                   1, 1, 1, 1, 1, 1, C.byref(Pn), nul)
+        assert rc == -1 and b"rcut_max" in lib().tg_last_error()
+    huge = [np.eye(3)[k] * 1e12 for k in range(3)]             # cells per axis overflow int
+    rc = lib().tg_build_neighbors_list_noalloc(10, 1, huge[0], huge[1], huge[2], RCUT,
+                                               1, 1, 1, 1, 1, 1, C.byref(Pn), nul)
+    assert rc == -3 and b"no-allocation limit" in lib().tg_last_error()

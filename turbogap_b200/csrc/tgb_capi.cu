@@ -120,28 +120,47 @@ struct Block {
     }
 };
 
+// The kd scratch (GEMM 1's split kernel derivative, GEMM 2's A operand) is
+// bounded: the two GEMMs run over row chunks of kd_chunk_rows() sites, so kd
+// holds one chunk. Chunks are whole 128-row tiles; the per-row arithmetic does
+// not depend on the chunking.
+constexpr size_t kKdScratchBytes = size_t(1) << 30;
+
+static int kd_chunk_rows(const Block &b, int n_sites) {
+    long long rows = (long long)(kKdScratchBytes / (sizeof(__nv_bfloat16) * (size_t)b.KD));
+    if (const char *e = std::getenv("TGB_KD_CHUNK_ROWS")) {   // tests: force several chunks
+        const long long v = std::atoll(e);
+        if (v > 0) rows = v;
+    }
+    rows = std::max<long long>(kGemmBM, rows / kGemmBM * kGemmBM);
+    const long long n = std::max(n_sites, 1);
+    return (int)std::min<long long>(rows, (n + kGemmBM - 1) / kGemmBM * kGemmBM);
+}
+
 // Per-block evaluation buffers, sized by the number of central sites.
 struct Workspace {
     int cap = 0;
+    int kd_rows = 0;           // rows of kd (one GEMM row chunk)
     DBuf<__nv_bfloat16> qsplit, kd;
     DBuf<float> q, c, g;
     DBuf<double> praw;         // compressed blocks: p, [n][dimf]
     DBuf<float> gfull;         //   and dE/dp
     DBuf<double> pnorm, epart, kdsum, qoff, vpart;
     TmaMap tmA1{}, tmA2{}, tmKd{};   // tmKd: the GAP epilogue's TMA stores into kd
-    int tm_rows = -1, tm_k1 = -1, tm_kd = -1;
+    int tm_rows = -1, tm_k1 = -1, tm_kd = -1, tm_kdrows = -1;
     const void *tm_p1 = nullptr, *tm_p2 = nullptr;
     int tile_desc = 0, tile_force = 0;   // CTA tiles of the two SOAP passes (autotuned)
 
     int ensure(const Block &b, int n_sites) {
         const int n = n_sites > 0 ? n_sites : 1;
-        if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)n * b.KD ||
+        const int R = kd_chunk_rows(b, n);
+        if (n > cap || q.n < (size_t)n * b.dim || kd.n < (size_t)R * b.KD ||
             qsplit.n < (size_t)n * b.K1 || c.n < (size_t)n * b.ntot * b.nlm ||
             epart.n < (size_t)n * b.n_etiles || kdsum.n < (size_t)n * b.n_etiles ||
             (b.compressed() && (praw.n < (size_t)n * b.dimf || gfull.n < (size_t)n * b.dimf))) {
             const int nc = n > cap ? n : cap;
             TGB_TRY(qsplit.ensure((size_t)nc * b.K1));
-            TGB_TRY(kd.ensure((size_t)nc * b.KD));
+            TGB_TRY(kd.ensure((size_t)R * b.KD));
             TGB_TRY(q.ensure((size_t)nc * b.dim));
             TGB_TRY(g.ensure((size_t)nc * b.dim));
             TGB_TRY(c.ensure((size_t)nc * b.ntot * b.nlm));
@@ -156,15 +175,18 @@ struct Workspace {
             }
             cap = nc;
         }
-        if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p || tm_k1 != b.K1 || tm_kd != b.KD) {
+        kd_rows = R;
+        if (tm_rows != n || tm_p1 != qsplit.p || tm_p2 != kd.p || tm_k1 != b.K1 || tm_kd != b.KD ||
+            tm_kdrows != R) {
             TGB_TRY(make_tma_bf16(&tmA1, qsplit.p, n, b.K1, b.K1, kGemmBM));
-            TGB_TRY(make_tma_bf16(&tmA2, kd.p, n, b.KD, b.KD, kGemmBM));
-            TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, n, b.KD, b.KD));
+            TGB_TRY(make_tma_bf16(&tmA2, kd.p, R, b.KD, b.KD, kGemmBM));
+            TGB_TRY(make_tma_store_bf16(&tmKd, kd.p, R, b.KD, b.KD));
             tm_rows = n;
             tm_p1 = qsplit.p;
             tm_p2 = kd.p;
             tm_k1 = b.K1;
             tm_kd = b.KD;
+            tm_kdrows = R;
         }
         return TG_OK;
     }
@@ -278,7 +300,26 @@ int force_pass(const Block &b, Workspace &w, const SoapParams &P, const SiteArgs
     return launch_soap_force(P, S, I, FO, nblk, st, tile);
 }
 
-// Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces.
+// GEMM 1's epilogue parameters for a block (rows and per-row outputs set by the caller).
+static GemmEpi gap_epilogue(const Block &b, const Workspace &w) {
+    GemmEpi e1{};
+    e1.mode = EPI_GAP_KERNEL;
+    e1.cols = b.Mpad;
+    e1.alpha = b.alpha.p;
+    e1.c0 = b.zeta * b.delta * b.delta;
+    e1.zeta_int = b.zeta_int;
+    e1.zeta_f = b.zeta;
+    e1.aoff = b.aoff.p;
+    e1.kd = w.kd.p;
+    e1.K2 = b.KD;
+    e1.Mpad = b.Mpad;
+    e1.nsplit = b.nsplit;
+    return e1;
+}
+
+// Descriptor, GEMM 1 (kernel + energy epilogue), GEMM 2 (dE/dq), forces. The
+// GEMMs run chunk by chunk over w.kd_rows sites, GEMM 2 of a chunk right after
+// its GEMM 1, so kd holds one chunk.
 int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
                    double *energies, double *virial, unsigned *err, cudaStream_t st,
                    EventLog *log = nullptr, const int *atom_struct = nullptr,
@@ -288,35 +329,32 @@ int evaluate_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     const SoapParams P = b.params(n_atoms);
     TGB_TRY(descriptor_pass(b, w, P, S, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
-    GemmEpi e1{};
-    e1.mode = EPI_GAP_KERNEL;
-    e1.rows = S.n_sites;
-    e1.cols = b.Mpad;
-    e1.alpha = b.alpha.p;
-    e1.c0 = b.zeta * b.delta * b.delta;
-    e1.zeta_int = b.zeta_int;
-    e1.zeta_f = b.zeta;
-    e1.epart = w.epart.p;
-    e1.kdsum = w.kdsum.p;
-    e1.aoff = b.aoff.p;
-    e1.qoff = w.qoff.p;
-    e1.kd = w.kd.p;
-    e1.K2 = b.KD;
-    e1.Mpad = b.Mpad;
-    e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(w.tmA1, b.tmB1, S.n_sites, b.Mpad, b.K1, e1, err, st, &w.tmKd,
-                           b.last1()));
-    TGB_MARK(log, PASS_GEMM1, st);
-    GemmEpi e2{};
-    e2.mode = EPI_STORE_F32;
-    e2.rows = S.n_sites;
-    e2.cols = b.dim;
-    e2.out = w.g.p;
-    e2.ldo = b.dim;
-    e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
-    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, S.n_sites, b.dim, b.K2, e2, err, st, nullptr,
-                           b.last2()));
-    TGB_MARK(log, PASS_GEMM2, st);
+    const int n = S.n_sites, R = w.kd_rows;
+    for (int r0 = 0; r0 < n; r0 += R) {
+        const int nr = std::min(R, n - r0);
+        TmaMap a1c;
+        const TmaMap *a1 = &w.tmA1;
+        if (nr < n) {   // this chunk's rows of the split-q operand
+            TGB_TRY(make_tma_bf16(&a1c, w.qsplit.p + (size_t)r0 * b.K1, nr, b.K1, b.K1, kGemmBM));
+            a1 = &a1c;
+        }
+        GemmEpi e1 = gap_epilogue(b, w);
+        e1.rows = nr;
+        e1.epart = w.epart.p + (size_t)r0 * b.n_etiles;
+        e1.kdsum = w.kdsum.p + (size_t)r0 * b.n_etiles;
+        e1.qoff = w.qoff.p + r0;
+        TGB_TRY(launch_gemm_tn(*a1, b.tmB1, nr, b.Mpad, b.K1, e1, err, st, &w.tmKd, b.last1()));
+        TGB_MARK(log, PASS_GEMM1, st);
+        GemmEpi e2{};
+        e2.mode = EPI_STORE_F32;
+        e2.rows = nr;
+        e2.cols = b.dim;
+        e2.out = w.g.p + (size_t)r0 * b.dim;
+        e2.ldo = b.dim;
+        e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
+        TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, nr, b.dim, b.K2, e2, err, st, nullptr, b.last2()));
+        TGB_MARK(log, PASS_GEMM2, st);
+    }
     ForceIn I{w.g.p,     w.q.p,      w.pnorm.p,         w.c.p,   w.epart.p,
               w.kdsum.p, b.n_etiles, b.delta * b.delta, w.qoff.p};
     ForceOut FO{forces, energies, w.vpart.p, err, atom_struct, vir_struct, pair_grad};
@@ -469,6 +507,14 @@ __global__ void k_collect(int n, int D, int n_et, double delta2, const double *_
     if (lane == 0) E[row] = delta2 * e;
 }
 
+// gated rows of each GEMM row chunk: min(R, max(0, count - c R))
+__global__ void k_chunk_counts(const int *__restrict__ gcount, int R, int nch,
+                               int *__restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    out[c] = max(0, min(R, *gcount - c * R));
+}
+
 struct MixedRun {
     Mlp *mlp = nullptr;
     MlpInferWork *iw = nullptr;   // this block's inference buffers
@@ -477,7 +523,7 @@ struct MixedRun {
     DBuf<__nv_bfloat16> Qg;
     DBuf<double> qoff_g, epart_g, kdsum_g, emean, estd;
     DBuf<float> g_g;
-    DBuf<int> gidx, gcount;
+    DBuf<int> gidx, gcount, chunk_cnt;
     TmaMap tmQg{};
 
     int ensure(const Block &b, int n_sites) {
@@ -492,6 +538,7 @@ struct MixedRun {
         TGB_TRY(g_g.ensure((size_t)n * b.dim));
         TGB_TRY(gidx.ensure(n));
         TGB_TRY(gcount.ensure(1));
+        TGB_TRY(chunk_cnt.ensure((size_t)(n + kGemmBM - 1) / kGemmBM));
         TGB_TRY(make_tma_bf16(&tmQg, Qg.p, n, b.K1, b.K1, kGemmBM));
         cap = n;
         return TG_OK;
@@ -523,34 +570,38 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
                                       x.qoff_g.p);
     TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_MLP, st);
-    GemmEpi e1{};
-    e1.mode = EPI_GAP_KERNEL;
-    e1.rows = n;
-    e1.rows_dev = x.gcount.p;
-    e1.cols = b.Mpad;
-    e1.alpha = b.alpha.p;
-    e1.c0 = b.zeta * b.delta * b.delta;
-    e1.zeta_int = b.zeta_int;
-    e1.zeta_f = b.zeta;
-    e1.epart = x.epart_g.p;
-    e1.kdsum = x.kdsum_g.p;
-    e1.aoff = b.aoff.p;
-    e1.qoff = x.qoff_g.p;
-    e1.kd = w.kd.p;
-    e1.K2 = b.KD;
-    e1.Mpad = b.Mpad;
-    e1.nsplit = b.nsplit;
-    TGB_TRY(launch_gemm_tn(x.tmQg, b.tmB1, n, b.Mpad, b.K1, e1, err, st, &w.tmKd, b.last1()));
-    TGB_MARK(log, PASS_GEMM1, st);
-    GemmEpi e2{};
-    e2.mode = EPI_STORE_F32;
-    e2.rows = n;
-    e2.rows_dev = x.gcount.p;
-    e2.cols = b.dim;
-    e2.out = x.g_g.p;
-    e2.ldo = b.dim;
-    e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
-    TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, n, b.dim, b.K2, e2, err, st, nullptr, b.last2()));
+    // both GEMMs over the compacted gated rows in chunks of w.kd_rows, each chunk's
+    // row count taken on the device from the gated count
+    const int R = w.kd_rows, nch = (n + R - 1) / R;
+    k_chunk_counts<<<grid_for(nch), 256, 0, st>>>(x.gcount.p, R, nch, x.chunk_cnt.p);
+    TGB_CUDA(cudaGetLastError());
+    for (int c = 0; c < nch; ++c) {
+        const int r0 = c * R, nr = std::min(R, n - r0);
+        TmaMap a1c;
+        const TmaMap *a1 = &x.tmQg;
+        if (nr < n) {
+            TGB_TRY(make_tma_bf16(&a1c, x.Qg.p + (size_t)r0 * b.K1, nr, b.K1, b.K1, kGemmBM));
+            a1 = &a1c;
+        }
+        GemmEpi e1 = gap_epilogue(b, w);
+        e1.rows = nr;
+        e1.rows_dev = x.chunk_cnt.p + c;
+        e1.epart = x.epart_g.p + (size_t)r0 * b.n_etiles;
+        e1.kdsum = x.kdsum_g.p + (size_t)r0 * b.n_etiles;
+        e1.qoff = x.qoff_g.p + r0;
+        TGB_TRY(launch_gemm_tn(*a1, b.tmB1, nr, b.Mpad, b.K1, e1, err, st, &w.tmKd, b.last1()));
+        TGB_MARK(log, PASS_GEMM1, st);
+        GemmEpi e2{};
+        e2.mode = EPI_STORE_F32;
+        e2.rows = nr;
+        e2.rows_dev = x.chunk_cnt.p + c;
+        e2.cols = b.dim;
+        e2.out = x.g_g.p + (size_t)r0 * b.dim;
+        e2.ldo = b.dim;
+        e2.a_krep = b.nsplit == 3 ? b.Mpad : 0;
+        TGB_TRY(launch_gemm_tn(w.tmA2, b.tmB2, nr, b.dim, b.K2, e2, err, st, nullptr, b.last2()));
+        TGB_MARK(log, PASS_GEMM2, st);
+    }
     k_scatter_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.n_etiles, x.epart_g.p,
                                        x.kdsum_g.p, x.g_g.p, w.epart.p, w.kdsum.p, w.g.p);
     TGB_CUDA(cudaGetLastError());

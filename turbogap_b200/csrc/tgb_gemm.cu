@@ -1,11 +1,16 @@
 // tgb_gemm.cu -- Blackwell (sm_100a) GEMM for the GAP sparse-set kernel.
 //
-// One CTA computes one 128 x 256 tile of C = A . B^T:
-//   warp 0  : TMA producer (one lane) feeding a 4-stage shared-memory ring,
-//   warp 1  : allocates 256 TMEM columns; one lane issues tcgen05.mma
-//             (M=128, N=256, K=16, bf16 -> fp32) and tcgen05.commit,
-//   warps 2-5: epilogue, tcgen05.ld of the accumulator (warp w reads TMEM lanes
-//             32*(w%4) .. +31) and the fused GAP epilogue.
+// A persistent CTA per SM walks 128 x 256 tiles of C = A . B^T:
+//   warp 0  : TMA producer (one lane) feeding a shared-memory operand ring of
+//             3 stages (modes whose epilogue stages bf16 or fp32 outputs for TMA
+//             stores) or 4 stages (the plain fp32 store),
+//   warp 1  : allocates 512 TMEM columns (two 256-column accumulators, so one
+//             tile's epilogue overlaps the next tile's MMAs); one lane issues
+//             tcgen05.mma (M=128, N=256, K=16, bf16 -> fp32) and tcgen05.commit,
+//   warps 2.. : epilogue, kGemmEpiGroups (GAP, plain store: 8 warps) or
+//             kGemmMlpEpiGroups (MLP modes: 16 warps) warps per TMEM lane
+//             quarter; warp w reads TMEM lanes 32*(w%4) .. +31 and its column
+//             group of the tile with tcgen05.ld, then runs the fused epilogue.
 // Operand tiles are [rows x 64] bf16 with the 128-byte swizzle, which is the
 // canonical K-major layout of the UMMA shared-memory descriptor.
 // Every mbarrier wait is bounded by wall time; on expiry the waiting role sets

@@ -16,7 +16,10 @@
 //
 // The first call on a device resolves the array's device address with
 // cudaGetSymbolAddress (and sizes the scan workspace); make that first call
-// outside any stream capture. Every call shares the array and leaves its
+// outside any stream capture. Under lazy module loading (the CUDA 12 default)
+// that first call is also what loads this file's module, and with it the
+// array and the kernels: the device memory they take appears then, once per
+// device, and no later call changes it. Every call shares the array and leaves its
 // contents behind, so the counters that must start at zero are cleared on each
 // call; calls that overlap on the GPU (different streams, or another thread)
 // race on the shared array and must be serialised by the caller.
@@ -25,6 +28,7 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <cmath>
 #include <mutex>
 
 namespace tgb {
@@ -65,6 +69,8 @@ int scratch_for_current_device(unsigned char **out) {
     if (!g_scratch_dev[dev]) {
         void *p = nullptr;
         TGB_CUDA(cudaGetSymbolAddress(&p, g_nl_scratch));
+        cudaFuncAttributes fa;   // loads the module's kernels now, not inside a later call
+        TGB_CUDA(cudaFuncGetAttributes(&fa, k_to_one_based));
         // the scan workspace must fit its region for the largest sizes allowed
         size_t need_sites = 0, need_cells = 0;
         TGB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, need_sites, (const int *)nullptr,
@@ -97,8 +103,26 @@ extern "C" int tg_build_neighbors_list_noalloc(int32_t n_sites, const double *po
     TGB_CHECK(n_sites <= kNoAllocMaxSites, TG_ERR_CAPACITY,
               "%d sites exceed the no-allocation limit of %d (use tg_build_neighbors_list)",
               n_sites, kNoAllocMaxSites);
+    TGB_CHECK(std::isfinite(rcut_max) && rcut_max > 0.0, TG_ERR_ARG,
+              "rcut_max must be positive and finite (got %g)", rcut_max);
     double a[3], b[3], c[3];
     for (int k = 0; k < 3; ++k) a[k] = a_box[k], b[k] = b_box[k], c[k] = c_box[k];
+    for (int k = 0; k < 3; ++k)
+        TGB_CHECK(std::isfinite(a[k]) && std::isfinite(b[k]) && std::isfinite(c[k]), TG_ERR_ARG,
+                  "non-finite lattice vector component");
+    TGB_CHECK(a[0] > 0.0 && b[1] > 0.0 && c[2] > 0.0, TG_ERR_ARG,
+              "the no-allocation entry point takes orthorhombic boxes with positive edges");
+    // Cells per axis are int(L / rcut) (neighbors.f90:391-396); bound them, and
+    // their product, in floating point before any integer conversion, so that the
+    // grid can never outgrow the fixed scratch array.
+    {
+        const double lx = std::fabs(a[0]) / rcut_max, ly = std::fabs(b[1]) / rcut_max,
+                     lz = std::fabs(c[2]) / rcut_max;
+        TGB_CHECK(lx <= kNoAllocMaxCells && ly <= kNoAllocMaxCells && lz <= kNoAllocMaxCells &&
+                      std::floor(lx) * std::floor(ly) * std::floor(lz) <= (double)kNoAllocMaxCells,
+                  TG_ERR_CAPACITY, "box / rcut_max gives more cells than the no-allocation limit of %d",
+                  kNoAllocMaxCells);
+    }
     Box bx = make_box(a, b, c);
     if (bx.ortho) {   // neighbors.f90:372-384: snap the off-diagonal noise to zero
         a[1] = a[2] = b[0] = b[2] = c[0] = c[1] = 0.0;

@@ -4,7 +4,7 @@ Every structure is a periodic cubic box filled with uniformly random atoms
 subject to a minimum pair distance under the minimum-image convention.
 Seeds: workload k uses 1000 + k; sub-structures use (1000 + k) * 100 + i.
 
-Workloads (BASELINE configs):
+Workloads:
   carbon216   216 C, L = 12.91 A (2.0 g/cm^3), d_min 1.2 A          (k = 0)
   ch32k       32,768 atoms C:H = 3:1, 0.12 atoms/A^3, d_min 1.0 A   (k = 1)
   cells512    512 C cells, N log-uniform 64..2048, 1.5..3.5 g/cm^3  (k = 2)
