@@ -380,13 +380,20 @@ bool autotune_enabled() {
     return !(e && e[0] == '0') && !std::getenv("TGB_SOAP_TILE");
 }
 
-// TGB_SOAP_TILE=t pins every block to tile t (0 .. kSoapTiles - 1) instead of
+// TGB_SOAP_TILE=t pins every block to tile t (0 .. kForceTiles - 1) instead of
 // tuning; returns -1 when unset.
 int pinned_tile() {
     const char *e = std::getenv("TGB_SOAP_TILE");
     if (!e) return -1;
     const int t = std::atoi(e);
-    return t < 0 ? 0 : (t >= kSoapTiles ? kSoapTiles - 1 : t);
+    return t < 0 ? 0 : (t >= kForceTiles ? kForceTiles - 1 : t);
+}
+
+// A pinned tile for a block: the descriptor pass has tiles 0 .. kSoapTiles - 1,
+// the force pass also the tensor-core tile where the block's shape allows it.
+void pin_tiles(const Block &b, Workspace &w, int t) {
+    w.tile_desc = std::min(t, kSoapTiles - 1);
+    w.tile_force = (t == kForceTileMma && !soap_force_mma_supported(b.params(1))) ? 0 : t;
 }
 
 int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, double *forces,
@@ -419,7 +426,9 @@ int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
     for (int pass = 0; pass < 2 && rc == TG_OK; ++pass) {
         float best = 0.f;
         int arg = 0;
-        for (int t = 0; t < kSoapTiles && rc == TG_OK; ++t) {
+        const int n_tiles = pass == 1 ? kForceTiles : kSoapTiles;
+        for (int t = 0; t < n_tiles && rc == TG_OK; ++t) {
+            if (pass == 1 && t == kForceTileMma && !soap_force_mma_supported(P)) continue;
             float ms = 0.f;
             rc = time_tile(pass == 1, t, ms);
             if (rc == TG_OK && (t == 0 || ms < best)) {
@@ -1654,7 +1663,7 @@ struct Engine {
     // picks the CTA tiles of every block's SOAP passes on this structure
     int autotune() {
         if (pinned_tile() >= 0)
-            for (auto &r : runs) r->w->tile_desc = r->w->tile_force = pinned_tile();
+            for (auto &r : runs) pin_tiles(*r->b, *r->w, pinned_tile());
         if (!autotune_enabled() || runs.empty()) return TG_OK;
         const double *p = pos.p;
         if (nsc > n) {
@@ -2314,7 +2323,7 @@ struct BatchEngine {
 
     int autotune() {
         if (pinned_tile() >= 0)
-            for (auto &r : runs) r->w->tile_desc = r->w->tile_force = pinned_tile();
+            for (auto &r : runs) pin_tiles(*r->b, *r->w, pinned_tile());
         if (!autotune_enabled()) return TG_OK;
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));

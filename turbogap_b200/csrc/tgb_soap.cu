@@ -15,6 +15,7 @@
 #include "tgb_soap.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <vector>
 
@@ -25,6 +26,69 @@ __constant__ float cYn[kMaxL + 1][kMaxL + 1];   // N_l0, sqrt2 N_lm (m > 0)
 __constant__ float cRa[kMaxL + 1][kMaxL + 1];   // (2l-1)/(l-m)
 __constant__ float cRb[kMaxL + 1][kMaxL + 1];   // (l+m-1)/(l-m)
 __constant__ float cDf[kMaxL + 2];              // (2m-1)!!
+
+// ---- column order of the tensor-core pair contraction (l_max = 8) ----------
+// G_lm = sum_n Gamma_{n,lm} R_n(r_pair) is an MMA whose 96 accumulator columns
+// hold the 81 lm of Gamma. A lane with t = lane % 4 owns columns 8k + 2t and
+// 8k + 2t + 1 of every n-tile k: at step k they hold the (cos, sin) pair of one
+// (l, m), and the steps of a lane walk whole m-chains (l = m .. 8 at fixed m), so
+// the lane evaluates Y_lm and its gradient with the Legendre recurrence in l.
+// Chains per lane group: t = 0: m = 0, 7, 8 (the m = 0 sin column is empty);
+// t = 1: m = 1, 6; t = 2: m = 2, 5; t = 3: m = 3, 4 (the last step is empty).
+constexpr int kMmaSteps = 12, kMmaCols = 8 * kMmaSteps;
+// step record: qa = Aa z qa1 - Ba qa2 + Ca (Q_l^m), qb likewise (Q_l^{m+1}),
+// f = the Y_lm normalisation, m; an empty step has f = 0
+struct MmaStep {
+    float Aa, Ba, Ca, Ab, Bb, Cb, f, m;
+};
+__constant__ MmaStep cStep[kMmaSteps][4];
+__constant__ signed char cStepL[kMmaSteps][4];   // l of the step, -1 when empty
+__constant__ unsigned char cLm2Col[81];          // accumulator column of lm
+
+static int init_mma_steps(const float yn[kMaxL + 1][kMaxL + 1], const float ra[kMaxL + 1][kMaxL + 1],
+                          const float rb[kMaxL + 1][kMaxL + 1], const float *df) {
+    const int chains[4][3] = {{0, 7, 8}, {1, 6, -1}, {2, 5, -1}, {3, 4, -1}};
+    MmaStep st[kMmaSteps][4] = {};
+    signed char sl[kMmaSteps][4];
+    unsigned char lm2col[81];
+    std::memset(sl, -1, sizeof(sl));
+    std::memset(lm2col, 0xff, sizeof(lm2col));
+    for (int t = 0; t < 4; ++t) {
+        int k = 0;
+        for (int c = 0; c < 3; ++c) {
+            const int m = chains[t][c];
+            if (m < 0) continue;
+            for (int l = m; l <= 8; ++l, ++k) {
+                MmaStep &r = st[k][t];
+                if (l == m) { r.Aa = 0.f; r.Ba = 0.f; r.Ca = df[m]; }
+                else if (l == m + 1) { r.Aa = (float)(2 * m + 1); r.Ba = 0.f; r.Ca = 0.f; }
+                else { r.Aa = ra[l][m]; r.Ba = rb[l][m]; r.Ca = 0.f; }
+                if (l == m) { r.Ab = 0.f; r.Bb = 0.f; r.Cb = 0.f; }
+                else if (l == m + 1) { r.Ab = 0.f; r.Bb = 0.f; r.Cb = df[m + 1]; }
+                else if (l == m + 2) { r.Ab = (float)(2 * m + 3); r.Bb = 0.f; r.Cb = 0.f; }
+                else { r.Ab = ra[l][m + 1]; r.Bb = rb[l][m + 1]; r.Cb = 0.f; }
+                r.f = yn[l][m];
+                r.m = (float)m;
+                sl[k][t] = (signed char)l;
+                lm2col[l * l + l + m] = (unsigned char)(8 * k + 2 * t);
+                if (m > 0) lm2col[l * l + l - m] = (unsigned char)(8 * k + 2 * t + 1);
+            }
+        }
+        if (k > kMmaSteps) {
+            set_error("tensor-core step plan overflows (%d steps)", k);
+            return TG_ERR_STATE;
+        }
+    }
+    for (int lm = 0; lm < 81; ++lm)
+        if (lm2col[lm] == 0xff) {
+            set_error("tensor-core step plan misses lm %d", lm);
+            return TG_ERR_STATE;
+        }
+    TGB_CUDA(cudaMemcpyToSymbol(cStep, st, sizeof(st)));
+    TGB_CUDA(cudaMemcpyToSymbol(cStepL, sl, sizeof(sl)));
+    TGB_CUDA(cudaMemcpyToSymbol(cLm2Col, lm2col, sizeof(lm2col)));
+    return TG_OK;
+}
 
 int init_soap_constants() {
     float yn[kMaxL + 1][kMaxL + 1] = {}, ra[kMaxL + 1][kMaxL + 1] = {},
@@ -49,7 +113,7 @@ int init_soap_constants() {
     TGB_CUDA(cudaMemcpyToSymbol(cRa, ra, sizeof(ra)));
     TGB_CUDA(cudaMemcpyToSymbol(cRb, rb, sizeof(rb)));
     TGB_CUDA(cudaMemcpyToSymbol(cDf, df, sizeof(df)));
-    return TG_OK;
+    return init_mma_steps(yn, ra, rb, df);
 }
 
 // ===================== FP64 table construction ==============================
@@ -319,6 +383,39 @@ __device__ __forceinline__ int fold_index(int j, int n) {
     return j < n ? j : j % n;
 }
 
+// Bulk prefetch of [p, p + bytes) into L2 (a hint; nothing is written). The range
+// shrinks to whole 16-byte units inside it, so it never leaves the buffer.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+    const uintptr_t e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a))
+                     : "memory");
+}
+
+// The rows a site's force pass reads (g, q, c) and its pair records, prefetched
+// into L2 by the warp that runs `ahead` sites earlier: sites run in about index
+// order, so when the site's own warp starts, its rows come from L2, not DRAM.
+// RAW (compressed blocks): g is dE/dp in rows of DIM, and q (rows of the
+// compressed dim) is not read.
+template <int DIM, int NT, int NLM, bool RAW>
+__device__ __forceinline__ void prefetch_force_site(const SiteArgs &S, const ForceIn &I, int site,
+                                                    int lane) {
+    const int fs = site + I.ahead;
+    if (I.ahead <= 0 || fs >= S.n_sites || lane >= 4) return;
+    if (lane == 0) prefetch_l2(I.g + (size_t)fs * DIM, sizeof(float) * DIM);
+    else if (lane == 1) {
+        if (!RAW) prefetch_l2(I.q + (size_t)fs * DIM, sizeof(float) * DIM);
+    }
+    else if (lane == 2) prefetch_l2(I.c + (size_t)fs * NT * NLM, sizeof(float) * NT * NLM);
+    else {
+        const int row = S.site_row[fs];
+        const int64_t p0 = S.pstart[row], p1 = S.pstart[row + 1];
+        prefetch_l2(S.xyz + 3 * p0, sizeof(double) * 3 * (size_t)(p1 - p0));
+        prefetch_l2(S.nbr + p0, sizeof(int) * (size_t)(p1 - p0));
+    }
+}
+
 // Descriptor species of a global species id, -1 when the block does not see it.
 __device__ __forceinline__ int zlookup(const SoapParams &P, int z) {
     return (z >= 0 && z < kMaxZ) ? (int)P.zmap[z] : -1;
@@ -417,6 +514,13 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
     __syncthreads();
     const int site = blockIdx.x * Sh::WARPS + warp;
     if (site >= S.n_sites) return;
+    if (lane == 0 && S.ahead > 0 && site + S.ahead < S.n_sites) {
+        // the pair records of the site `ahead` sites on, into L2 for its warp
+        const int fr = S.site_row[site + S.ahead];
+        const int64_t f0 = S.pstart[fr], f1 = S.pstart[fr + 1];
+        prefetch_l2(S.xyz + 3 * f0, sizeof(double) * 3 * (size_t)(f1 - f0));
+        prefetch_l2(S.nbr + f0, sizeof(int) * (size_t)(f1 - f0));
+    }
     const int row = S.site_row[site];
     const int catom = S.site_atom[site];
     const int64_t p0 = S.pstart[row];
@@ -710,10 +814,14 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
     const int site = blockIdx.x * Sh::WARPS + warp;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     if (site < S.n_sites) {
+        prefetch_force_site<DIM, NT, NLM, RAW>(S, I, site, lane);
         const int row = S.site_row[site];
         const int catom = S.site_atom[site];
         const int64_t p0 = S.pstart[row];
         const int np = (int)(S.pstart[row + 1] - p0);
+        // the c row is read after the dE/dp phase: request its lines into L1 now
+        for (int o = 32 * lane; o < NT * NLM; o += 32 * 32)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(I.c + (size_t)site * NT * NLM + o));
         // dE/dq = G = ksum mu + g0 + g: ksum = sum_s kd_s (FP64, GEMM-1 epilogue),
         // g0 = sum_s kcoef_s (q_s - mu) (per block), g from GEMM 2; q = mu + delta.
         // dE/dp = (G - (G . q) q) / |p| = (a mu + g0 + g - dot delta) / |p| with
@@ -753,36 +861,56 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         } else {
             float sp = 0.f;   // sum (g0 delta + g q), a small sum
             if constexpr (VEC) {
-                for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                    const float4 m = __ldg(reinterpret_cast<const float4 *>(P.muf + d0));
-                    const float4 z = __ldg(reinterpret_cast<const float4 *>(P.g0f + d0));
-                    const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
-                    const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                // the site's g and q rows go to registers in one round trip and are
+                // read once; mu and g0 (per block, L1-resident) are read twice
+                constexpr int NV4 = DIM / 4, NV = (NV4 + 31) / 32;
+                const float4 *g4 = reinterpret_cast<const float4 *>(g);
+                const float4 *q4 = reinterpret_cast<const float4 *>(q);
+                const float4 *m4 = reinterpret_cast<const float4 *>(P.muf);
+                const float4 *z4 = reinterpret_cast<const float4 *>(P.g0f);
+                float4 gr[NV], qr[NV];
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const int i4 = lane + 32 * k;
+                    gr[k] = i4 < NV4 ? g4[i4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    qr[k] = i4 < NV4 ? q4[i4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const int i4 = lane + 32 * k;
+                    if (i4 >= NV4) continue;
+                    const float4 m = __ldg(m4 + i4), z = __ldg(z4 + i4);
+                    const float4 gv = gr[k], qv = qr[k];
                     sp += z.x * qv.x + gv.x * (m.x + qv.x);
                     sp += z.y * qv.y + gv.y * (m.y + qv.y);
                     sp += z.z * qv.z + gv.z * (m.z + qv.z);
                     sp += z.w * qv.w + gv.w * (m.w + qv.w);
                 }
-            } else {
-                for (int d = lane; d < DIM; d += 32)
-                    sp += P.g0f[d] * q[d] + g[d] * (P.muf[d] + q[d]);
-            }
-            const double dot = ksum * (P.mu2 + I.qoff[site]) + P.g0mu + warp_sum((double)sp);
-            const double nrm = I.pnorm[site];
-            const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-            const float fa = (float)((ksum - dot) * inv), fi = (float)inv, fd = (float)(dot * inv);
-            if constexpr (VEC) {
-                for (int d0 = 4 * lane; d0 < DIM; d0 += 128) {
-                    const float4 m = __ldg(reinterpret_cast<const float4 *>(P.muf + d0));
-                    const float4 z = __ldg(reinterpret_cast<const float4 *>(P.g0f + d0));
-                    const float4 gv = *reinterpret_cast<const float4 *>(g + d0);
-                    const float4 qv = *reinterpret_cast<const float4 *>(q + d0);
+                const double dot = ksum * (P.mu2 + I.qoff[site]) + P.g0mu + warp_sum((double)sp);
+                const double nrm = I.pnorm[site];
+                const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+                const float fa = (float)((ksum - dot) * inv), fi = (float)inv,
+                            fd = (float)(dot * inv);
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const int i4 = lane + 32 * k;
+                    if (i4 >= NV4) continue;
+                    const float4 m = __ldg(m4 + i4), z = __ldg(z4 + i4);
+                    const float4 gv = gr[k], qv = qr[k];
+                    const int d0 = 4 * i4;
                     put_b(d0, fa * m.x + fi * (z.x + gv.x) - fd * qv.x);
                     put_b(d0 + 1, fa * m.y + fi * (z.y + gv.y) - fd * qv.y);
                     put_b(d0 + 2, fa * m.z + fi * (z.z + gv.z) - fd * qv.z);
                     put_b(d0 + 3, fa * m.w + fi * (z.w + gv.w) - fd * qv.w);
                 }
             } else {
+                for (int d = lane; d < DIM; d += 32)
+                    sp += P.g0f[d] * q[d] + g[d] * (P.muf[d] + q[d]);
+                const double dot = ksum * (P.mu2 + I.qoff[site]) + P.g0mu + warp_sum((double)sp);
+                const double nrm = I.pnorm[site];
+                const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+                const float fa = (float)((ksum - dot) * inv), fi = (float)inv,
+                            fd = (float)(dot * inv);
                 for (int d = lane; d < DIM; d += 32)
                     put_b(d, fa * P.muf[d] + fi * (P.g0f[d] + g[d]) - fd * q[d]);
             }
@@ -976,6 +1104,435 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
     }
 }
 
+// ===================== adjoint forces on the tensor cores =====================
+//
+// The same contraction as k_soap_force, with its two dense products on the
+// tensor cores (mma.sync m16n8k8, TF32 operands, fp32 accumulation):
+//   Gamma_l = B_l C_l              [NT x NT] . [NT x (2l+1)] per l,
+//   G = R Gamma, G' = R' Gamma     [16 pairs x NT] . [NT x 96 columns] per 16 pairs,
+// where row p of R (R') holds R~_n (R~'_n) of pair p in its species' channels.
+// PREC 3 splits every operand into TF32 hi + lo and runs hi.hi + hi.lo + lo.hi
+// (about fp32 accuracy: the plain form); PREC 1 runs hi.hi (the mixed form).
+// The accumulators stay in registers: the lane owning columns (8k + 2t, +1)
+// walks its m-chains over the steps k (see init_mma_steps) for the rows g and
+// g + 8 of the tile and sums its part of T1 = sum Y (a G' + a' G) and
+// T2 = sum a G grad Y; a quad shuffle adds the four lanes' parts.
+
+template <int PREC>
+__device__ __forceinline__ void tf32_split(float x, uint32_t &hi, uint32_t &lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    if constexpr (PREC == 3) {
+        const float r = x - __uint_as_float(hi);
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+    } else {
+        lo = 0u;
+    }
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+        "{%8, %9}, {%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// d += a . b with the TF32 split of both (PREC 3) or the leading parts only
+template <int PREC>
+__device__ __forceinline__ void mma_split(float (&d)[4], const uint32_t (&ah)[4],
+                                          const uint32_t (&al)[4], uint32_t bh0, uint32_t bh1,
+                                          uint32_t bl0, uint32_t bl1) {
+    if constexpr (PREC == 3) {
+        mma_tf32(d, al[0], al[1], al[2], al[3], bh0, bh1);
+        mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bl0, bl1);
+    }
+    mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bh0, bh1);
+}
+
+template <int NS>
+struct MmaForceShape {
+    static constexpr int NT = NS * 8, NL = 9, NLM = 81;
+    static constexpr int NP = NT * (NT + 1) / 2, DIM = NP * NL;
+    static constexpr int BROW = NT + 4;               // B_l rows: A-fragment loads conflict-free
+    static constexpr int BSTRIDE = NT * BROW + 4;
+    static constexpr int BAREA = NL * BSTRIDE;
+    static constexpr int CROW = 88;                   // staged c rows: B-fragment loads conflict-free
+    static constexpr int CAREA = NT * CROW;
+    static constexpr int AROW = NT + 4;               // pair rows of R~ and R~'
+    static constexpr int AUX = 44;                    // a_l, a'_l, u, 1/r, (x+iy)^m per pair
+    static constexpr int STAGE = 32 * (2 * AROW + AUX);
+    static constexpr int XAREA = (BAREA + CAREA > STAGE ? BAREA + CAREA : STAGE);
+    static constexpr int GROW = 104;                  // Gamma rows (96 columns), 8 mod 32
+    static constexpr int GAREA = NT * GROW;
+    static constexpr int WARP_FLOATS = (XAREA + GAREA + 3) / 4 * 4;
+    static constexpr int WARPS = 4;
+};
+
+template <int NS, int PREC>
+__global__ void __launch_bounds__(128, 2)
+    k_soap_force_mma(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
+    using Sh = MmaForceShape<NS>;
+    constexpr int NT = Sh::NT, NL = Sh::NL, NLM = Sh::NLM, NP = Sh::NP, DIM = Sh::DIM;
+    constexpr int AMAX = 8, NF = AMAX + NL, KS = NT / 8;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ double vred[Sh::WARPS][6];
+    __shared__ unsigned char pair_n[NP], pair_n2[NP];
+    __shared__ float4 stepc[kMmaSteps * 4 * 2];
+    __shared__ int stepl[kMmaSteps * 4];
+    __shared__ unsigned char lm2col[NLM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+        int n = 0, n2 = 0;
+        internal_pair(i, NT, n, n2);
+        pair_n[i] = (unsigned char)n;
+        pair_n2[i] = (unsigned char)n2;
+    }
+    for (int i = threadIdx.x; i < kMmaSteps * 4; i += blockDim.x) {
+        const MmaStep &r = cStep[i / 4][i % 4];
+        stepc[2 * i] = make_float4(r.Aa, r.Ba, r.Ca, r.Ab);
+        stepc[2 * i + 1] = make_float4(r.Bb, r.Cb, r.f, r.m);
+        stepl[i] = cStepL[i / 4][i % 4];
+    }
+    for (int i = threadIdx.x; i < NLM; i += blockDim.x) lm2col[i] = cLm2Col[i];
+    if (lane < 6) vred[warp][lane] = 0.0;
+    float *X = smem + warp * Sh::WARP_FLOATS;
+    float *Bm = X;                    // [l][n][n2], phases A and B
+    float *cs = X + Sh::BAREA;        // [n][lm] (row CROW), phase B
+    float *Ag = X;                    // [pair][n] R~ (row AROW), phase C
+    float *Ad = X + 32 * Sh::AROW;    // [pair][n] R~'
+    float *aux = X + 64 * Sh::AROW;   // [pair][AUX]
+    float *Gs = X + Sh::XAREA;        // Gamma [n][column] (row GROW)
+    // columns without an lm stay zero: zero the whole Gamma area once
+    for (int i = lane; i < Sh::GAREA; i += 32) Gs[i] = 0.f;
+    __syncthreads();
+    const int site = blockIdx.x * Sh::WARPS + warp;
+    double vir[6] = {0, 0, 0, 0, 0, 0};
+    if (site < S.n_sites) {
+        prefetch_force_site<DIM, NT, NLM, false>(S, I, site, lane);
+        const int row = S.site_row[site];
+        const int catom = S.site_atom[site];
+        const int64_t p0 = S.pstart[row];
+        const int np = (int)(S.pstart[row + 1] - p0);
+        const float *g_row = I.g + (size_t)site * DIM;
+        const float *q_row = I.q + (size_t)site * DIM;
+        const float *c_row = I.c + (size_t)site * NT * NLM;
+        // ---- every row of the site in one round trip: c (to shared memory), g and q
+        constexpr int NV4 = DIM / 4, NV = (NV4 + 31) / 32;
+        constexpr int NC4 = NT * NLM / 4, NCV = (NC4 + 31) / 32;
+        static_assert(DIM % 4 == 0 && NP % 4 == 0 && (NT * NLM) % 4 == 0, "vector rows");
+        float4 cv[NCV], gr[NV], qr[NV];
+#pragma unroll
+        for (int k = 0; k < NCV; ++k) {
+            const int i4 = lane + 32 * k;
+            cv[k] = i4 < NC4 ? reinterpret_cast<const float4 *>(c_row)[i4]
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const int i4 = lane + 32 * k;
+            gr[k] = i4 < NV4 ? reinterpret_cast<const float4 *>(g_row)[i4]
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            qr[k] = i4 < NV4 ? reinterpret_cast<const float4 *>(q_row)[i4]
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        double ksum = 0.0, esum = 0.0;
+        for (int k = lane; k < I.n_etiles; k += 32) {
+            ksum += I.kdsum[(size_t)site * I.n_etiles + k];
+            esum += I.epart[(size_t)site * I.n_etiles + k];
+        }
+        ksum = warp_sum(ksum);
+        esum = warp_sum(esum);
+#pragma unroll
+        for (int k = 0; k < NCV; ++k) {
+            const int i4 = lane + 32 * k;
+            if (i4 >= NC4) continue;
+            const float v[4] = {cv[k].x, cv[k].y, cv[k].z, cv[k].w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = 4 * i4 + u, n2 = e / NLM;
+                cs[n2 * Sh::CROW + (e - n2 * NLM)] = v[u];
+            }
+        }
+        // ---- dE/dp, as in k_soap_force, into the symmetric B_l
+        auto put_b = [&](int d, float h) {
+            const int l = d / NP, pi = d - l * NP;
+            float *Bl = Bm + l * Sh::BSTRIDE;
+            const int n = pair_n[pi], n2 = pair_n2[pi];
+            if (n == n2) {
+                Bl[n * Sh::BROW + n] = 2.f * h;
+            } else {
+                const float v = 1.41421356237309515f * h;
+                Bl[n * Sh::BROW + n2] = v;
+                Bl[n2 * Sh::BROW + n] = v;
+            }
+        };
+        {
+            const float4 *m4 = reinterpret_cast<const float4 *>(P.muf);
+            const float4 *z4 = reinterpret_cast<const float4 *>(P.g0f);
+            float sp = 0.f;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const int i4 = lane + 32 * k;
+                if (i4 >= NV4) continue;
+                const float4 m = __ldg(m4 + i4), z = __ldg(z4 + i4);
+                const float4 gv = gr[k], qv = qr[k];
+                sp += z.x * qv.x + gv.x * (m.x + qv.x);
+                sp += z.y * qv.y + gv.y * (m.y + qv.y);
+                sp += z.z * qv.z + gv.z * (m.z + qv.z);
+                sp += z.w * qv.w + gv.w * (m.w + qv.w);
+            }
+            const double dot = ksum * (P.mu2 + I.qoff[site]) + P.g0mu + warp_sum((double)sp);
+            const double nrm = I.pnorm[site];
+            const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+            const float fa = (float)((ksum - dot) * inv), fi = (float)inv, fd = (float)(dot * inv);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const int i4 = lane + 32 * k;
+                if (i4 >= NV4) continue;
+                const float4 m = __ldg(m4 + i4), z = __ldg(z4 + i4);
+                const float4 gv = gr[k], qv = qr[k];
+                const int d0 = 4 * i4;
+                put_b(d0, fa * m.x + fi * (z.x + gv.x) - fd * qv.x);
+                put_b(d0 + 1, fa * m.y + fi * (z.y + gv.y) - fd * qv.y);
+                put_b(d0 + 2, fa * m.z + fi * (z.z + gv.z) - fd * qv.z);
+                put_b(d0 + 3, fa * m.w + fi * (z.w + gv.w) - fd * qv.w);
+            }
+        }
+        __syncwarp();
+        // ---- Gamma_l = B_l C_l: rows n (g, g + 8), columns m-index (8 jj + 2t, +1)
+#pragma unroll 1
+        for (int l = 0; l < NL; ++l) {
+            const float *Bl = Bm + l * Sh::BSTRIDE;
+            uint32_t ah[KS][4], al[KS][4];
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const int c0 = 8 * ks + t;
+                if constexpr (NT == 16) {
+                    tf32_split<PREC>(Bl[g * Sh::BROW + c0], ah[ks][0], al[ks][0]);
+                    tf32_split<PREC>(Bl[(g + 8) * Sh::BROW + c0], ah[ks][1], al[ks][1]);
+                    tf32_split<PREC>(Bl[g * Sh::BROW + c0 + 4], ah[ks][2], al[ks][2]);
+                    tf32_split<PREC>(Bl[(g + 8) * Sh::BROW + c0 + 4], ah[ks][3], al[ks][3]);
+                } else {   // 8 channels: rows 8..15 of the tile are zero
+                    tf32_split<PREC>(Bl[g * Sh::BROW + c0], ah[ks][0], al[ks][0]);
+                    tf32_split<PREC>(Bl[g * Sh::BROW + c0 + 4], ah[ks][2], al[ks][2]);
+                    ah[ks][1] = al[ks][1] = ah[ks][3] = al[ks][3] = 0u;
+                }
+            }
+            const int nm = 2 * l + 1;
+            for (int jj = 0; 8 * jj < nm; ++jj) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+                const int col = 8 * jj + g;   // this lane's B-fragment column (m-index)
+#pragma unroll
+                for (int ks = 0; ks < KS; ++ks) {
+                    const int k0 = 8 * ks + t;
+                    const float b0 = col < nm ? cs[k0 * Sh::CROW + l * l + col] : 0.f;
+                    const float b1 = col < nm ? cs[(k0 + 4) * Sh::CROW + l * l + col] : 0.f;
+                    uint32_t bh0, bl0, bh1, bl1;
+                    tf32_split<PREC>(b0, bh0, bl0);
+                    tf32_split<PREC>(b1, bh1, bl1);
+                    mma_split<PREC>(d, ah[ks], al[ks], bh0, bh1, bl0, bl1);
+                }
+                // d: rows n = g (d0, d1), g + 8 (d2, d3); m-index 8 jj + 2t (+1)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int mi = 8 * jj + 2 * t + e;
+                    if (mi < nm) {
+                        const int c = lm2col[l * l + mi];
+                        Gs[g * Sh::GROW + c] = d[e];
+                        if (NT == 16) Gs[(g + 8) * Sh::GROW + c] = d[2 + e];
+                    }
+                }
+            }
+        }
+        __syncwarp();   // Gamma complete; B_l and c are dead: the pair staging goes over them
+        // ---- pairs, 32 at a time: lane-per-pair set-up, then two 16-pair MMA tiles
+        double fs[3] = {0, 0, 0};
+        for (int base = 1; base < np; base += 32) {
+            {
+                const int pp = base + lane;
+                float *ag = Ag + lane * Sh::AROW, *ad = Ad + lane * Sh::AROW, *ax = aux + lane * Sh::AUX;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) { ag[n] = 0.f; ad[n] = 0.f; }
+#pragma unroll
+                for (int k = 0; k <= 40; ++k) ax[k] = 0.f;   // [40]: the valid flag
+                if (pp < np) {
+                    const int64_t p = p0 + pp;
+                    const int ja = fold_index(S.nbr[p], P.n_atoms);
+                    const int s = zlookup(P, S.species[ja]);
+                    const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
+                                z = (float)S.xyz[3 * p + 2];
+                    const float r = sqrtf(x * x + y * y + z * z);
+                    if (s >= 0 && r < P.rcut[s] && r > 0.f) {
+                        const float4 *T = reinterpret_cast<const float4 *>(
+                            P.table + (size_t)s * (kTableIntervals + 1) * (4 * NF));
+                        const Hermite hm(r, P.tab_h[s], P.tab_inv_h[s]);
+#pragma unroll
+                        for (int n = 0; n < AMAX; ++n)
+                            hm.value_deriv(T, NF, n, ag[s * AMAX + n], ad[s * AMAX + n]);
+#pragma unroll
+                        for (int l = 0; l < NL; ++l) hm.value_deriv(T, NF, AMAX + l, ax[l], ax[9 + l]);
+                        const float ir = 1.f / r, u0 = x * ir, u1 = y * ir, u2 = z * ir;
+                        ax[18] = u0; ax[19] = u1; ax[20] = u2; ax[21] = ir;
+                        float cm = 1.f, sm = 0.f;
+#pragma unroll
+                        for (int m = 0; m <= 8; ++m) {
+                            ax[22 + m] = cm;
+                            ax[31 + m] = sm;
+                            const float c2 = u0 * cm - u1 * sm;
+                            sm = u0 * sm + u1 * cm;
+                            cm = c2;
+                        }
+                        ax[40] = 1.f;
+                    }
+                }
+            }
+            __syncwarp();
+#pragma unroll 1
+            for (int mt = 0; mt < 2; ++mt) {
+                if (base + 16 * mt >= np) break;   // warp-uniform
+                const int r0 = 16 * mt + g, r1 = r0 + 8;
+                float accG[kMmaSteps][4], accD[kMmaSteps][4];
+#pragma unroll
+                for (int j = 0; j < kMmaSteps; ++j)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) accG[j][e] = accD[j][e] = 0.f;
+#pragma unroll
+                for (int ks = 0; ks < KS; ++ks) {
+                    const int k0 = 8 * ks + t;
+                    uint32_t gh[4], gl[4], dh[4], dl[4];
+                    tf32_split<PREC>(Ag[r0 * Sh::AROW + k0], gh[0], gl[0]);
+                    tf32_split<PREC>(Ag[r1 * Sh::AROW + k0], gh[1], gl[1]);
+                    tf32_split<PREC>(Ag[r0 * Sh::AROW + k0 + 4], gh[2], gl[2]);
+                    tf32_split<PREC>(Ag[r1 * Sh::AROW + k0 + 4], gh[3], gl[3]);
+                    tf32_split<PREC>(Ad[r0 * Sh::AROW + k0], dh[0], dl[0]);
+                    tf32_split<PREC>(Ad[r1 * Sh::AROW + k0], dh[1], dl[1]);
+                    tf32_split<PREC>(Ad[r0 * Sh::AROW + k0 + 4], dh[2], dl[2]);
+                    tf32_split<PREC>(Ad[r1 * Sh::AROW + k0 + 4], dh[3], dl[3]);
+#pragma unroll
+                    for (int j = 0; j < kMmaSteps; ++j) {
+                        uint32_t bh0, bl0, bh1, bl1;
+                        tf32_split<PREC>(Gs[k0 * Sh::GROW + 8 * j + g], bh0, bl0);
+                        tf32_split<PREC>(Gs[(k0 + 4) * Sh::GROW + 8 * j + g], bh1, bl1);
+                        mma_split<PREC>(accG[j], gh, gl, bh0, bh1, bl0, bl1);
+                        mma_split<PREC>(accD[j], dh, dl, bh0, bh1, bl0, bl1);
+                    }
+                }
+                // post-processing: rows r0 (accumulator elements 0, 1) and r1 (2, 3)
+                float T[2][4];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float *ax = aux + (h ? r1 : r0) * Sh::AUX;
+                    const float z = ax[20];
+                    float qa1 = 0.f, qa2 = 0.f, qb1 = 0.f, qb2 = 0.f;
+                    float T1 = 0.f, T2x = 0.f, T2y = 0.f, T2z = 0.f;
+#pragma unroll
+                    for (int k = 0; k < kMmaSteps; ++k) {
+                        const float4 c1 = stepc[2 * (4 * k + t)], c2 = stepc[2 * (4 * k + t) + 1];
+                        const int l = stepl[4 * k + t];
+                        const int m = (int)c2.w;
+                        const float qa = c1.x * z * qa1 - c1.y * qa2 + c1.z;
+                        const float qb = c1.w * z * qb1 - c2.x * qb2 + c2.y;
+                        qa2 = qa1; qa1 = qa;
+                        qb2 = qb1; qb1 = qb;
+                        if (l < 0) continue;   // an empty step (lane-group uniform)
+                        const float a = ax[l], da = ax[9 + l];
+                        const float cm = ax[22 + m], sm = ax[31 + m];
+                        const float cm1 = ax[22 + (m > 0 ? m - 1 : 0)], sm1 = ax[31 + (m > 0 ? m - 1 : 0)];
+                        const float Gp = accG[k][2 * h], Gn = accG[k][2 * h + 1];
+                        const float dGp = accD[k][2 * h], dGn = accD[k][2 * h + 1];
+                        const float y = c2.z * qa;
+                        T1 += y * (cm * (a * dGp + da * Gp) + sm * (a * dGn + da * Gn));
+                        const float wc = a * Gp, ws = a * Gn, fm = y * c2.w;
+                        T2x += fm * (wc * cm1 + ws * sm1);
+                        T2y += fm * (ws * cm1 - wc * sm1);
+                        T2z += c2.z * qb * (wc * cm + ws * sm);
+                    }
+                    T[h][0] = T1; T[h][1] = T2x; T[h][2] = T2y; T[h][3] = T2z;
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        T[h][c] += __shfl_xor_sync(0xffffffffu, T[h][c], 1);
+                        T[h][c] += __shfl_xor_sync(0xffffffffu, T[h][c], 2);
+                    }
+                // lane t = 0 takes row r0's pair, t = 1 row r1's
+                if (t < 2) {
+                    const int rr = t == 0 ? r0 : r1;
+                    const float *ax = aux + rr * Sh::AUX;
+                    const int pp = base + rr;
+                    if (pp < np && ax[40] != 0.f) {
+                        const int64_t p = p0 + pp;
+                        const int ja = fold_index(S.nbr[p], P.n_atoms);
+                        const float u0 = ax[18], u1 = ax[19], u2 = ax[20], ir = ax[21];
+                        const float T1 = T[t][0], T2x = T[t][1], T2y = T[t][2], T2z = T[t][3];
+                        const float ut2 = u0 * T2x + u1 * T2y + u2 * T2z;
+                        const float fx = -(T1 * u0 + (T2x - ut2 * u0) * ir);
+                        const float fy = -(T1 * u1 + (T2y - ut2 * u1) * ir);
+                        const float fz = -(T1 * u2 + (T2z - ut2 * u2) * ir);
+                        const double X3 = S.xyz[3 * p], Y3 = S.xyz[3 * p + 1], Z3 = S.xyz[3 * p + 2];
+                        atomicAdd(&O.forces[3 * (size_t)ja], (double)fx);
+                        atomicAdd(&O.forces[3 * (size_t)ja + 1], (double)fy);
+                        atomicAdd(&O.forces[3 * (size_t)ja + 2], (double)fz);
+                        if (O.pair_grad) {
+                            O.pair_grad[3 * p] = -(double)fx;
+                            O.pair_grad[3 * p + 1] = -(double)fy;
+                            O.pair_grad[3 * p + 2] = -(double)fz;
+                        }
+                        fs[0] -= fx; fs[1] -= fy; fs[2] -= fz;
+                        vir[0] += (double)fx * X3;
+                        vir[1] += (double)fy * Y3;
+                        vir[2] += (double)fz * Z3;
+                        vir[3] += 0.5 * ((double)fx * Y3 + (double)fy * X3);
+                        vir[4] += 0.5 * ((double)fx * Z3 + (double)fz * X3);
+                        vir[5] += 0.5 * ((double)fy * Z3 + (double)fz * Y3);
+                    }
+                }
+            }
+            __syncwarp();   // the next 32 pairs overwrite the staging
+        }
+#pragma unroll
+        for (int qd = 0; qd < 3; ++qd) fs[qd] = warp_sum(fs[qd]);
+        if (lane == 0 && O.pair_grad)
+            for (int qd = 0; qd < 3; ++qd) O.pair_grad[3 * p0 + qd] = -fs[qd];
+        if (lane == 0) {
+            atomicAdd(&O.forces[3 * (size_t)catom], fs[0]);
+            atomicAdd(&O.forces[3 * (size_t)catom + 1], fs[1]);
+            atomicAdd(&O.forces[3 * (size_t)catom + 2], fs[2]);
+            O.energies[catom] += I.delta2 * esum;
+        }
+    }
+#pragma unroll
+    for (int qd = 0; qd < 6; ++qd) vir[qd] = warp_sum(vir[qd]);
+    if (lane == 0)
+        for (int qd = 0; qd < 6; ++qd) vred[warp][qd] = vir[qd];
+    if (O.vir_struct && lane == 0 && site < S.n_sites) {
+        double *o = O.vir_struct + 9 * (size_t)O.atom_struct[S.site_atom[site]];
+        atomicAdd(o + 0, vir[0]);
+        atomicAdd(o + 4, vir[1]);
+        atomicAdd(o + 8, vir[2]);
+        atomicAdd(o + 1, vir[3]);
+        atomicAdd(o + 3, vir[3]);
+        atomicAdd(o + 2, vir[4]);
+        atomicAdd(o + 6, vir[4]);
+        atomicAdd(o + 5, vir[5]);
+        atomicAdd(o + 7, vir[5]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < Sh::WARPS; ++w)
+            for (int qd = 0; qd < 6; ++qd) v[qd] += vred[w][qd];
+        double *o = O.vpart + (size_t)blockIdx.x * 9;
+        o[0] = v[0]; o[4] = v[1]; o[8] = v[2];
+        o[1] = o[3] = v[3];
+        o[2] = o[6] = v[4];
+        o[5] = o[7] = v[5];
+    }
+}
+
 __global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, double *out) {
     const int q = threadIdx.y;   // 9 components
     double s = 0.0;
@@ -1129,6 +1686,17 @@ bool soap_shape_supported(int ns, int amax, int lmax) {
     return false;
 }
 
+// Warps of a kernel resident on the whole GPU at once (one site per warp).
+template <typename K>
+static int resident_warps(K kernel, int threads, size_t smem, int *out) {
+    int per_sm = 0, dev = 0, n_sm = 0;
+    TGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    TGB_CUDA(cudaGetDevice(&dev));
+    TGB_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    *out = std::max(1, per_sm * n_sm * (threads / 32));
+    return TG_OK;
+}
+
 template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
 static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
     using Sh = DescShape<NS, AMAX, LMAX, TILE>;
@@ -1139,9 +1707,15 @@ static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
+    static int resident = 0;   // sites in flight at once: the L2 prefetch distance
+    if (!resident)
+        TGB_TRY(resident_warps(k_soap_expand<NS, AMAX, LMAX, TILE, RAW>, 32 * Sh::WARPS, smem,
+                               &resident));
+    SiteArgs S2 = S;
+    S2.ahead = resident;
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     if (grid > 0)
-        k_soap_expand<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, O);
+        k_soap_expand<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S2, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -1157,10 +1731,16 @@ static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, 
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
+    static int resident = 0;   // sites in flight at once: the L2 prefetch distance
+    if (!resident)
+        TGB_TRY(resident_warps(k_soap_force<NS, AMAX, LMAX, TILE, RAW>, 32 * Sh::WARPS, smem,
+                               &resident));
+    ForceIn I2 = I;
+    I2.ahead = resident;
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     *nblk = grid;
     if (grid > 0)
-        k_soap_force<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I, O);
+        k_soap_force<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I2, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -1184,6 +1764,44 @@ static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O,
         return expand_tiles<NS, AMAX, LMAX, true>(P, S, O, st, tile);
     }
     return expand_tiles<NS, AMAX, LMAX, false>(P, S, O, st, tile);
+}
+
+template <int NS, int PREC>
+static int force_mma_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I,
+                          const ForceOut &O, int *nblk, cudaStream_t st) {
+    using Sh = MmaForceShape<NS>;
+    const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
+    static bool attr = false;
+    if (!attr) {
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_force_mma<NS, PREC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    static int resident = 0;   // sites in flight at once: the L2 prefetch distance
+    if (!resident)
+        TGB_TRY(resident_warps(k_soap_force_mma<NS, PREC>, 32 * Sh::WARPS, smem, &resident));
+    ForceIn I2 = I;
+    I2.ahead = resident;
+    const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
+    *nblk = grid;
+    if (grid > 0) k_soap_force_mma<NS, PREC><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I2, O);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+bool soap_force_mma_supported(const SoapParams &P) {
+    return !P.raw && P.amax == 8 && P.lmax == 8 && (P.ns == 1 || P.ns == 2);
+}
+
+static int launch_soap_force_mma(const SoapParams &P, const SiteArgs &S, const ForceIn &I,
+                                 const ForceOut &O, int *nblk, cudaStream_t st) {
+    TGB_CHECK(I.qoff && P.muf && P.g0f, TG_ERR_ARG, "the force pass needs qoff, muf and g0f");
+    const bool fast = P.force_prec == 1;
+    if (P.ns == 1)
+        return fast ? force_mma_impl<1, 1>(P, S, I, O, nblk, st)
+                    : force_mma_impl<1, 3>(P, S, I, O, nblk, st);
+    return fast ? force_mma_impl<2, 1>(P, S, I, O, nblk, st)
+                : force_mma_impl<2, 3>(P, S, I, O, nblk, st);
 }
 
 template <int NS, int AMAX, int LMAX, bool RAW>
@@ -1217,6 +1835,12 @@ int launch_soap_expand(const SoapParams &P, const SiteArgs &S, const DescOut &O,
 
 int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st, int tile) {
+    if (tile == kForceTileMma) {
+        TGB_CHECK(soap_force_mma_supported(P), TG_ERR_ARG,
+                  "the tensor-core force tile needs alpha_max 8, l_max 8, 1 or 2 species and no "
+                  "compression");
+        return launch_soap_force_mma(P, S, I, O, nblk, st);
+    }
 #define X(a, b, c) \
     if (P.ns == a && P.amax == b && P.lmax == c)    \
         return force_tile<a, b, c>(P, S, I, O, nblk, st, tile);

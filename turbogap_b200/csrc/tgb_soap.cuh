@@ -31,6 +31,9 @@ struct SoapParams {
     // in that order (separate instantiations of both kernels, every tile). The
     // compression passes between them work in the compressed space of dim.
     int raw;
+    // precision of the tensor-core force tile: 3 = TF32 hi/lo split (about fp32,
+    // the plain form), 1 = single TF32 products (the mixed form's budget)
+    int force_prec = 3;
 };
 
 // Per-launch site addressing: site i reads CSR row site_row[i] of the pair
@@ -43,6 +46,7 @@ struct SiteArgs {
     const int *nbr;          // 0-based supercell index per pair
     const double *xyz;       // (3, P) MIC vectors r_j - r_i
     const int *species;      // global species id per unit-cell atom
+    int ahead = 0;           // set by the launchers: sites in flight at once (L2 prefetch distance)
 };
 
 // Descriptor entries on the device run in the internal order d = l * NP + pi
@@ -107,6 +111,7 @@ struct ForceIn {
     int n_etiles;
     double delta2;
     const double *qoff;      // [n_sites]: delta . mu (FP64, from the descriptor pass)
+    int ahead = 0;           // set by the launcher: sites in flight at once (L2 prefetch distance)
 };
 
 struct ForceOut {
@@ -148,6 +153,11 @@ bool soap_shape_supported(int ns, int amax, int lmax);
 // tile 0: 4 sites per CTA, >= 4 CTAs per SM (128 registers); 1: 4 sites, >= 3
 // CTAs (168 registers); 2: 2 sites, >= 8 CTAs; 3: 8 sites, >= 2 CTAs.
 constexpr int kSoapTiles = 4;
+// The force pass has one more tile: the tensor-core kernel (mma.sync TF32, 4 sites
+// per CTA), for alpha_max 8, l_max 8, 1 or 2 species, uncompressed blocks.
+constexpr int kForceTileMma = 4;
+constexpr int kForceTiles = 5;
+bool soap_force_mma_supported(const SoapParams &P);
 __host__ __device__ constexpr int soap_tile_warps(int t) { return t == 2 ? 2 : (t == 3 ? 8 : 4); }
 __host__ __device__ constexpr int soap_tile_minb(int t) {
     return t == 1 ? 3 : (t == 2 ? 8 : (t == 3 ? 2 : 4));
