@@ -20,6 +20,18 @@ extern "C" {
 int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t *A, const uint16_t *B,
                      float *C);
 
+/* Failure test: the same GEMM with its TMA producer silenced (zero operands,
+ * nothing loaded). The MMA issuer's bounded mbarrier wait runs out after 2 s,
+ * the kernel sets its timeout bits and returns, TMEM freed, no fault. Returns
+ * TG_ERR_TIMEOUT (and the device error word in *err_word). */
+int tgx_gemm_stall_probe(int32_t M, int32_t N, int32_t K, uint32_t *err_word);
+
+/* Failure test, host code only: NCCL communicator initialisation over the id
+ * (from tg_nccl_unique_id), one grouped all-reduce without data, destruction.
+ * Each step is polled with the deadline of TGB_NCCL_TIMEOUT_S: TG_ERR_TIMEOUT
+ * when a rank never arrives. TGB_NCCL_LIBRARY selects the NCCL build. */
+int tgx_comm_probe(const void *id128, int32_t n_ranks, int32_t rank);
+
 struct tg_mlp;
 /* Loss and parameter gradients of one member on one batch of B normalised
  * samples (x (B, dim), y (B), gref (B, dim) fp32), without updating it. grads

@@ -3,8 +3,9 @@
 The oracle rounds every GEMM operand to bf16 where the GPU does, so training
 gradients, energies and input gradients agree to fp32-accumulation level.
 The engine tests show the gate (gate 0 = exact GAP everywhere) and what the
-trained ensemble gains over the method without it: a low error and a small
-gated fraction, where an untrained ensemble sends every site back to GAP."""
+trained ensemble gains over the method without it, on a cell held out of the
+training data: a low error and a small gated fraction, where an untrained
+ensemble sends every site back to GAP."""
 from __future__ import annotations
 
 import numpy as np
@@ -140,14 +141,21 @@ def _carbon_engine(gpu, n_sparse=300, seed=31):
 
 
 def test_engine_mixed_form(gpu):
-    eng, h, st = _carbon_engine(gpu)
+    train_eng, h, st = _carbon_engine(gpu)
     D = h.dim
-    # training data: exact steps of a 600 K run
+    # training data: exact steps of a 600 K run of one cell
     m = gpu.Mlp(D, 256, 4, seed=5)
     for _ in range(40):
-        eng.md(1, 1.0)
-        m.add_engine_samples(eng, 0)
+        train_eng.md(1, 1.0)
+        m.add_engine_samples(train_eng, 0)
     assert m.n_samples() == 40 * 216
+    train_eng.close()
+    # evaluated on a held-out cell (another seed, 10 steps into its own 600 K run)
+    held = synth.random_structure(216, 12.91, 1.2, seed=977)
+    masses = np.full(216, 12.011 * 103.6426965268)
+    eng = gpu.Engine(held.positions, held.species, masses, held.box, [777])
+    eng.set_state(held.positions, synth.maxwell_velocities(masses, 600.0, 978))
+    eng.md(10, 1.0)
     e_ref, f_ref, v_ref = eng.compute()
 
     # gate 0: every site goes back to the exact kernel -> the exact result

@@ -128,6 +128,8 @@ SIGNATURES = [
     ("tg_batch_profile", C.c_int, [_vp, C.c_int32, dp, C.POINTER(C.c_int32)]),
     ("tg_batch_graph_kernels", C.c_int, [_vp, C.POINTER(C.c_int32)]),
     ("tgx_gemm_bf16_tn", C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16p, u16p, f32p]),
+    ("tgx_gemm_stall_probe", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32)]),
+    ("tgx_comm_probe", C.c_int, [_vp, C.c_int32, C.c_int32]),
     ("tgx_mlp_batch_grads", C.c_int, [_vp, C.c_int32, C.c_int32, f32p, f32p, f32p, C.c_double, dp,
                                       C.POINTER(C.c_double), f32p, f32p]),
     ("tgx_mlp_layout", C.c_int, [_vp, i64p]),

@@ -2687,6 +2687,40 @@ extern "C" int tgx_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const uint16_t 
     return TG_OK;
 }
 
+// The GEMM with its producer silenced: the MMA issuer's first bounded wait
+// (2 s) runs out, every role leaves, TMEM is freed and the call returns
+// TG_ERR_TIMEOUT with the device error word in *err_word; nothing faults and
+// the context stays usable.
+extern "C" int tgx_gemm_stall_probe(int32_t M, int32_t N, int32_t K, uint32_t *err_word) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(M > 0 && N > 0 && K > 0 && K % kGemmBK == 0 && err_word, TG_ERR_ARG,
+              "bad GEMM shape");
+    DBuf<__nv_bfloat16> a, b;
+    DBuf<float> c;
+    TGB_TRY(a.ensure((size_t)M * K));
+    TGB_TRY(b.ensure((size_t)N * K));
+    TGB_TRY(c.ensure((size_t)M * N));
+    TGB_CUDA(cudaMemsetAsync(a.p, 0, sizeof(__nv_bfloat16) * M * K, C.st));
+    TGB_CUDA(cudaMemsetAsync(b.p, 0, sizeof(__nv_bfloat16) * N * K, C.st));
+    TmaMap ta{}, tb{};
+    TGB_TRY(make_tma_bf16(&ta, a.p, M, K, K, kGemmBM));
+    TGB_TRY(make_tma_bf16(&tb, b.p, N, K, K, kGemmBN));
+    GemmEpi ep{};
+    ep.mode = EPI_STORE_F32;
+    ep.rows = M;
+    ep.cols = N;
+    ep.out = c.p;
+    ep.ldo = N;
+    ep.stall_test = 1;
+    TGB_TRY(launch_gemm_tn(ta, tb, M, N, K, ep, C.err.p, C.st));
+    unsigned e = 0;
+    TGB_CUDA(cudaMemcpyAsync(&e, C.err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, C.st));
+    TGB_CUDA(cudaStreamSynchronize(C.st));
+    *err_word = e;
+    return check_err_word(C, C.err.p);
+}
+
 extern "C" int tgx_mlp_batch_grads(tg_mlp *h, int32_t member, int32_t B, const float *x,
                                    const float *y, const float *gref, double lam, double *grads,
                                    double *loss, float *E, float *G) {

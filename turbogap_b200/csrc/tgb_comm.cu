@@ -5,6 +5,7 @@
 // grouped all-reduce are polled on the host with a deadline (default 120 s,
 // TGB_NCCL_TIMEOUT_S), after which the communicator is aborted and the call
 // returns TG_ERR_TIMEOUT instead of waiting for a rank that never arrives.
+// TGB_NCCL_LIBRARY selects the library to load (default libnccl.so.2).
 #include "tgb_comm.cuh"
 #include "tgb_common.cuh"
 
@@ -47,8 +48,13 @@ int api(NcclApi **out) {
     std::lock_guard<std::mutex> lk(g_api_mu);
     if (!g_api.h) {
         void *h = nullptr;
+        // TGB_NCCL_LIBRARY names another build of the library (a path or a soname)
+        if (const char *lib = std::getenv("TGB_NCCL_LIBRARY")) {
+            h = dlopen(lib, RTLD_NOW | RTLD_GLOBAL);
+            TGB_CHECK(h, TG_ERR_STATE, "NCCL library %s could not be loaded: %s", lib, dlerror());
+        }
         for (const char *name : {"libnccl.so.2", "libnccl.so"})
-            if ((h = dlopen(name, RTLD_NOW | RTLD_GLOBAL))) break;
+            if (h || (h = dlopen(name, RTLD_NOW | RTLD_GLOBAL))) break;
         TGB_CHECK(h, TG_ERR_STATE, "NCCL (libnccl.so.2) could not be loaded: %s", dlerror());
         NcclApi a;
         a.h = h;
@@ -173,3 +179,15 @@ int comm_allreduce3(Comm *c, double *x, size_t nx, double *y, size_t ny, double 
 }
 
 }  // namespace tgb
+
+// Failure test: a communicator of n_ranks, then one grouped all-reduce with no
+// data, then its destruction, host code only (the deadline logic of a sharded
+// engine's exchange step without a GPU). Returns the first failing status.
+extern "C" int tgx_comm_probe(const void *id128, int32_t n_ranks, int32_t rank) {
+    tgb::Comm *c = nullptr;
+    int rc = tgb::comm_init(id128, n_ranks, rank, &c);
+    if (rc != TG_OK) return rc;
+    rc = tgb::comm_allreduce3(c, nullptr, 0, nullptr, 0, nullptr, 0, nullptr);
+    tgb::comm_destroy(c);
+    return rc;
+}

@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
     if (warp == 0 && lane == 0) {
         // ---- TMA producer
         int g = 0;   // k-blocks issued so far (all tiles)
-        bool ok = true;
+        bool ok = ep.stall_test == 0;   // the failure test issues nothing
         for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
             const int tn = tile_col(t, n_tiles_n, rotate);
             const int m0 = (t / n_tiles_n) * BM, n0 = tn * BN;

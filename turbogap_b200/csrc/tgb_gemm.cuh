@@ -65,6 +65,10 @@ struct GemmEpi {
     float scale;
     float *rowpart;                 // fp32 row partial sums (EPI_MLP_L2)
     int rowpart_ld;
+    // failure test only (tgx_gemm_stall_probe): nonzero makes the producer issue
+    // no loads, so the MMA issuer's first bounded wait runs out and every role
+    // leaves with DEV_ERR_TIMEOUT_* set; zero in every production launch
+    int stall_test;
 };
 
 constexpr int kGemmBM = 128;
