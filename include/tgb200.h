@@ -186,6 +186,45 @@ int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t
                           const int32_t *species_batch, const int32_t *species_all, double v0,
                           double *values, double *value_der, int32_t *n_central);
 
+/* get_soap_dipole (src/gap.f90:261-398) with the current block holding a dipole
+ * GAP (tg_soap_begin: its sparse set, delta and zeta), through the get_gap_soap
+ * remap, with the arguments of tg_get_local_property:
+ *   dipoles(3, n_central)  mu_i = dE_i/dr_i, the gradient of the block's local
+ *                          fictitious energy E_i with respect to the central
+ *                          atom's own position (the self pair of its list);
+ *   energies(n_central)    (optional) E_i = delta^2 sum_s alpha_s K_is^zeta, no
+ *                          e0 and no clamp: a fitting artefact that is never
+ *                          added to the energy or its gradient to the forces.
+ * Central sites in batch order; zeta snapped to an integer within 1e-5 as the
+ * reference does here. The total dipole is the sum of mu_i. */
+int tg_get_soap_dipole(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                       const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                       const int32_t *species_batch, const int32_t *species_all,
+                       double *dipoles, double *energies, int32_t *n_central);
+
+/* get_ts_energy_and_forces (src/vdw.f90:163-493): Tkatchenko-Scheffler
+ * dispersion from Hirshfeld volumes, with the reference's arguments (host
+ * arrays, Fortran layouts, 1-based neighbour indices and species):
+ *   hirshfeld_v(n_sites) of this batch's sites and hirshfeld_v_cart_der(3, P)
+ *   per pair of their lists (tg_get_local_property gives both), n_neigh(n_sites),
+ *   neighbors_list(P), neighbor_species(P), rjs(P), xyz(3, P), the neighbours'
+ *   volumes hirshfeld_v_neigh(P), c6_ref/r0_ref/alpha0_ref(n_species),
+ *   mbd_ts_scaling(n_sites0) by atom.
+ * Outputs are assigned as the reference assigns them: energies(n_sites); with
+ * do_forces, forces0(3, n_sites0), virial(3, 3) and local_virial_diag0(3,
+ * n_sites0). Pairs count where rcut_inner < rjs < rcut, smoothed over the two
+ * buffers. FP64 on the device. */
+int tg_get_ts_energy_and_forces(int32_t n_sites, int32_t n_sites0, const double *hirshfeld_v,
+                                const double *hirshfeld_v_cart_der, const int32_t *n_neigh,
+                                const int32_t *neighbors_list, const int32_t *neighbor_species,
+                                double rcut, double buffer, double rcut_inner, double buffer_inner,
+                                const double *rjs, const double *xyz,
+                                const double *hirshfeld_v_neigh, double sR, double d,
+                                int32_t n_species, const double *c6_ref, const double *r0_ref,
+                                const double *alpha0_ref, int32_t do_forces, double x_min,
+                                double x_max, const double *mbd_ts_scaling, double *energies,
+                                double *forces0, double *virial, double *local_virial_diag0);
+
 /* Descriptor only (soap_turbo get_soap as called at gap_interface.f90:320-325,
  * through the same remap): soap(dim, n_central) of the current block's central
  * sites in batch order. The Cartesian derivative array soap_cart_der is never

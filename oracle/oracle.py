@@ -448,3 +448,151 @@ def local_property_predict(soap, Qs, alphas, V0, delta, zeta, soap_cart_der, n_n
                 der[k] = Qss[i] @ soap_cart_der[k]
             k += 1
     return V, der
+
+
+def soap_dipole(soap, soap_cart_der, Qs, alphas, delta, zeta, n_neigh):
+    """get_soap_dipole (gap.f90:261-398) in numpy: zeta snapped within 1e-5;
+    energies = delta^2 K^zeta . alphas (no e0); Qss = zeta delta^2 (K^(zeta-1)
+    alphas) Qs; mu_i = Qss_i . soap_cart_der of the site's first (self) pair.
+    soap (n_sites, D), Qs (M, D), soap_cart_der (P, D, 3) per kept pair, site
+    after site (n_neigh). Returns (dipoles (n_sites, 3), energies (n_sites))."""
+    zi = int(zeta)
+    z = float(zi) if abs(zeta - zi) < 1e-5 else zeta
+    K = soap @ Qs.T
+    energies = delta ** 2 * (K ** z) @ alphas
+    Qss = z * delta ** 2 * (K ** (z - 1.0) * alphas[None, :]) @ Qs
+    mu = np.zeros((soap.shape[0], 3))
+    k = 0
+    for i, nn in enumerate(n_neigh):
+        mu[i] = Qss[i] @ soap_cart_der[k]
+        k += nn
+    return mu, energies
+
+
+def poly_cut(x, x_min, x_max):
+    """misc.f90:479-494."""
+    if x < x_min:
+        return 0.0
+    if x >= x_max:
+        return 1.0
+    c = x - (x_max + x_min) / 2.0
+    w = x_max - x_min
+    return 0.5 + 1.5 * c / w - 2.0 * c ** 3 / w ** 3
+
+
+def ts_energy_and_forces(hirshfeld_v, hirshfeld_v_cart_der, n_neigh, neighbors_list,
+                         neighbor_species, rcut, buffer, rcut_inner, buffer_inner, rjs, xyz,
+                         hirshfeld_v_neigh, sR, d, c6_ref, r0_ref, alpha0_ref, n_sites0,
+                         mbd_ts_scaling, x_min=0.0, x_max=0.0):
+    """get_ts_energy_and_forces (vdw.f90:163-493), statement by statement in
+    Python loops (FP64). Pairs-major arrays (xyz, hirshfeld_v_cart_der (P, 3)),
+    1-based neighbours and species. Returns (energies, forces (n_sites0, 3),
+    virial (3, 3), local virial diagonal (n_sites0, 3))."""
+    n_sites = len(n_neigh)
+    P = len(neighbors_list)
+    rjs = np.asarray(rjs, float)
+    # buffer flags (:259-280)
+    in_buf = np.zeros(P, bool)
+    if buffer > 0.0 or buffer_inner > 0.0:
+        for k in range(P):
+            if (rcut - buffer < rjs[k] < rcut) or (rcut_inner < rjs[k] < rcut_inner + buffer_inner):
+                in_buf[k] = True
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r6 = 1.0 / rjs ** 6
+        r6_der = -6.0 / rjs * r6
+    for k in np.nonzero(in_buf)[0]:                  # :287-300, from the unsmoothed r6
+        if rjs[k] <= rcut_inner + buffer_inner:
+            rb = -(rjs[k] - rcut_inner - buffer_inner) / buffer_inner
+            r6_der[k] += 6.0 * r6[k] / (-buffer_inner) * (-rb + rb ** 2)
+        else:
+            rb = (rjs[k] - rcut + buffer) / buffer
+            r6_der[k] += 6.0 * r6[k] / buffer * (-rb + rb ** 2)
+    for k in np.nonzero(in_buf)[0]:                  # :302-310
+        if rjs[k] <= rcut_inner + buffer_inner:
+            rb = (rjs[k] - rcut_inner - buffer_inner) / (-buffer_inner)
+        else:
+            rb = (rjs[k] - rcut + buffer) / buffer
+        r6[k] *= 1.0 - 3.0 * rb ** 2 + 2.0 * rb ** 3
+    sp = np.asarray(neighbor_species) - 1
+    vn = np.asarray(hirshfeld_v_neigh, float)
+    c6_ii_n = np.asarray(c6_ref)[sp] * vn ** 2       # :329-332
+    r0_ii_n = np.asarray(r0_ref)[sp] * vn ** (1.0 / 3.0)
+    a0_n = np.asarray(alpha0_ref)[sp] * vn
+    c6_ij = np.zeros(P)
+    r0_ij = np.zeros(P)
+    k = 0
+    for i in range(n_sites):                         # :341-367
+        i2 = (neighbors_list[k] - 1) % n_sites0
+        c6_ii = c6_ii_n[k] * mbd_ts_scaling[i2]
+        r0_i, a0_i = r0_ii_n[k], a0_n[k]
+        c6_ij[k], r0_ij[k] = c6_ii, r0_i
+        k += 1
+        for _ in range(1, n_neigh[i]):
+            j2 = (neighbors_list[k] - 1) % n_sites0
+            c6_jj = c6_ii_n[k] * mbd_ts_scaling[j2]
+            a0_j = a0_n[k]
+            if c6_ii == 0.0 or c6_jj == 0.0:
+                c6_ij[k] = 0.0
+            else:
+                c6_ij[k] = 2.0 * c6_ii * c6_jj / (a0_j / a0_i * c6_ii + a0_i / a0_j * c6_jj)
+            r0_ij[k] = r0_i + r0_ii_n[k]
+            k += 1
+    energies = np.zeros(n_sites)
+    f_damp = np.zeros(P)
+    exp_damp = np.zeros(P)
+    k = 0
+    for i in range(n_sites):                         # :375-388
+        k += 1
+        for _ in range(1, n_neigh[i]):
+            if rcut_inner < rjs[k] < rcut:
+                with np.errstate(divide="ignore", over="ignore"):
+                    exp_damp[k] = np.exp(-d * (rjs[k] / (sR * r0_ij[k]) - 1.0))
+                f_damp[k] = 1.0 / (1.0 + exp_damp[k])
+                energies[i] += c6_ij[k] * r6[k] * f_damp[k]
+            k += 1
+    energies *= -0.5
+    forces = np.zeros((n_sites0, 3))
+    virial = np.zeros((3, 3))
+    lvir = np.zeros((n_sites0, 3))
+    pf1 = np.zeros(n_sites)
+    pf2 = np.zeros(n_sites)
+    k = 0
+    for i in range(n_sites):                         # :402-421
+        i2s = sp[k]
+        k += 1
+        for _ in range(1, n_neigh[i]):
+            if rcut_inner < rjs[k] < rcut:
+                pf1[i] += c6_ij[k] * f_damp[k] * r6[k]
+                pf2[i] -= (c6_ij[k] * f_damp[k] ** 2 * rjs[k] * r6[k] * exp_damp[k] * d / sR
+                           / r0_ij[k] ** 2)
+            k += 1
+        if hirshfeld_v[i] == 0.0:
+            pf1[i] = pf2[i] = 0.0
+        else:
+            pf1[i] = pf1[i] / hirshfeld_v[i]
+            pf2[i] = pf2[i] * r0_ref[i2s] / 3.0 / hirshfeld_v[i] ** (2.0 / 3.0)
+    vd = np.asarray(hirshfeld_v_cart_der, float)
+    x = np.asarray(xyz, float)
+    k = 0
+    for i in range(n_sites):                         # :422-486
+        i2 = (neighbors_list[k] - 1) % n_sites0
+        for _ in range(n_neigh[i]):
+            j2 = (neighbors_list[k] - 1) % n_sites0
+            if rcut_inner < rjs[k] < rcut:
+                pc = poly_cut(rjs[k], x_min, x_max)
+                if not np.all(vd[k] == 0.0):
+                    f = vd[k] * (pf1[i] + pf2[i])
+                    forces[j2] += f
+                    lvir[j2] += f * x[k] * pc
+                    virial += 0.5 * (np.outer(f, x[k]) + np.outer(x[k], f))
+                if r0_ij[k] == 0.0:
+                    f = np.zeros(3)
+                else:
+                    f = (c6_ij[k] / rjs[k] * x[k] * f_damp[k]
+                         * (-r6_der[k] - r6[k] * f_damp[k] * exp_damp[k] * d / sR / r0_ij[k]))
+                if j2 != i2:
+                    forces[i2] += f
+                lvir[j2] -= 0.5 * f * x[k] * pc
+                virial -= 0.25 * (np.outer(f, x[k]) + np.outer(x[k], f))
+            k += 1
+    return energies, forces, virial, lvir

@@ -67,3 +67,28 @@ def test_local_property_matches_oracle(gpu, offset, compressed):
     # pairs beyond the block's cutoff carry nothing
     far = np.setdiff1d(np.arange(len(nl["rjs"])), idx)
     assert len(far) > 0 and not der[far].any()
+
+
+@pytest.mark.parametrize("zeta", [4.0, 2.5])
+def test_soap_dipole_matches_oracle(gpu, zeta):
+    """get_soap_dipole (gap.f90:261-398): the self pair's gradient of a dipole
+    GAP's fictitious local energy, mu_i = dE_i/dr_i, and E_i itself (no e0, no
+    clamp), against the oracle's restatement on the materialised derivatives."""
+    from turbogap_b200.hypers import GapBlock
+    h = carbon_hypers()
+    base = sparse_block(h, 200, seed=95, sigma_alpha=0.01)
+    blk = GapBlock(h, base.Qs, base.alphas, delta=0.7, zeta=zeta)
+    gpu.soap_backend_begin(blk, key=905 if zeta == 4.0 else 906)
+    st = random_structure(216, 12.91, 1.2, seed=96)
+    nl = neighbor_data(st, h.rcut_max + 0.3)
+    nn, idx = _kept(st, h, nl)
+    q, sder, _ = O.get_soap(O.HypersC(h), nn, np.ones((len(idx), 1), np.int32), nl["rjs"][idx],
+                            nl["xyz"][idx], derivatives=True)
+    mu, en = gpu.get_soap_dipole(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"], nl["xyz"],
+                                 st.species, st.species)
+    mo, eo = O.soap_dipole(q, sder, blk.Qs, blk.alphas, blk.delta, blk.zeta, nn)
+    assert mu.shape == (st.n, 3) and en.shape == (st.n,)
+    assert np.abs(en - eo).max() < 1e-7
+    assert np.abs(mu - mo).max() < 1e-6 * max(1.0, np.abs(mo).max())
+    # the total dipole
+    assert np.abs(mu.sum(0) - mo.sum(0)).max() < 1e-5 * max(1.0, np.abs(mo).max())

@@ -72,6 +72,13 @@ SIGNATURES = [
                               C.POINTER(C.c_int32)]),
     ("tg_get_local_property", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, C.c_double,
                                         dp, _vp, C.POINTER(C.c_int32)]),
+    ("tg_get_soap_dipole", C.c_int, [C.c_int32, C.c_int32, ip, ip, dp, dp, ip, ip, dp, _vp,
+                                     C.POINTER(C.c_int32)]),
+    ("tg_get_ts_energy_and_forces", C.c_int, [C.c_int32, C.c_int32, dp, _vp, ip, ip, ip, C.c_double,
+                                              C.c_double, C.c_double, C.c_double, dp, dp, dp,
+                                              C.c_double, C.c_double, C.c_int32, dp, dp, dp,
+                                              C.c_int32, C.c_double, C.c_double, dp, dp, _vp, _vp,
+                                              _vp]),
     ("tg_family_begin", C.c_int, [C.c_int32, C.POINTER(TgFamily)]),
     ("tg_get_family", C.c_int, [C.c_int32, C.c_int32, C.c_int32, ip, ip, dp, dp, ip, dp, dp, dp]),
     ("tg_build_neighbors_list", C.c_int, [C.c_int32, dp, C.c_int32, dp, dp, dp, C.c_double, ip,

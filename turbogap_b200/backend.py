@@ -126,6 +126,48 @@ def get_local_property(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0
     return vals[:nc.value], der
 
 
+def get_soap_dipole(n_total_sites: int, n_neigh0, neighbors_list0, rjs0, xyz0, species_batch,
+                    species_all):
+    """get_soap_dipole (gap.f90:261-398) with the current block as the dipole
+    model: (local dipoles mu_i = dE_i/dr_i (n_central, 3), the fictitious local
+    energies E_i (n_central)) of the block's central sites."""
+    n = len(n_neigh0)
+    mu = np.zeros((n, 3))
+    en = np.zeros(n)
+    nc = C.c_int32(0)
+    check(lib().tg_get_soap_dipole(int(n_total_sites), n, _i32(n_neigh0), _i32(neighbors_list0),
+                                   _f64(rjs0), _f64(xyz0), _i32(species_batch), _i32(species_all),
+                                   mu, en.ctypes.data, C.byref(nc)))
+    return mu[:nc.value], en[:nc.value]
+
+
+def get_ts_energy_and_forces(hirshfeld_v, hirshfeld_v_cart_der, n_neigh, neighbors_list,
+                             neighbor_species, rcut, buffer, rcut_inner, buffer_inner, rjs, xyz,
+                             hirshfeld_v_neigh, sR, d, c6_ref, r0_ref, alpha0_ref, n_sites0,
+                             mbd_ts_scaling=None, do_forces=True, x_min=0.0, x_max=0.0):
+    """get_ts_energy_and_forces (vdw.f90:163-493) on the device. Arrays as numpy
+    (pairs-major: hirshfeld_v_cart_der and xyz (P, 3)); 1-based neighbours and
+    species. Returns (energies (n_sites), forces (n_sites0, 3), virial (3, 3),
+    local virial diagonal (n_sites0, 3)); the last three are None without forces."""
+    n = len(n_neigh)
+    sc = _f64(mbd_ts_scaling) if mbd_ts_scaling is not None else np.ones(n_sites0)
+    en = np.zeros(n)
+    f = np.zeros((n_sites0, 3)) if do_forces else None
+    v = np.zeros(9) if do_forces else None
+    lv = np.zeros((n_sites0, 3)) if do_forces else None
+    vd = _f64(hirshfeld_v_cart_der) if do_forces else None
+    check(lib().tg_get_ts_energy_and_forces(
+        n, int(n_sites0), _f64(hirshfeld_v), vd.ctypes.data if do_forces else None, _i32(n_neigh),
+        _i32(neighbors_list), _i32(neighbor_species), float(rcut), float(buffer), float(rcut_inner),
+        float(buffer_inner), _f64(rjs), _f64(xyz), _f64(hirshfeld_v_neigh), float(sR), float(d),
+        len(c6_ref), _f64(c6_ref), _f64(r0_ref), _f64(alpha0_ref), 1 if do_forces else 0,
+        float(x_min), float(x_max), sc, en, f.ctypes.data if do_forces else None,
+        v.ctypes.data if do_forces else None, lv.ctypes.data if do_forces else None))
+    if not do_forces:
+        return en, None, None, None
+    return en, f, v.reshape(3, 3).T.copy(), lv
+
+
 _FAMILY_KIND = {"distance_2b": 1, "angle_3b": 2, "core_pot": 3}
 
 

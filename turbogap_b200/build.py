@@ -31,6 +31,7 @@ SOURCES = {
     "tgb_noalloc.cu": ["--fmad=false"],
     "tgb_comm.cu": [],
     "tgb_family.cu": [],
+    "tgb_vdw.cu": [],
 }
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

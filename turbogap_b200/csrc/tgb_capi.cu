@@ -1272,17 +1272,17 @@ int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const in
     return TG_OK;
 }
 
-int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
-                          const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
-                          const int32_t *species_batch, const int32_t *species_all, double v0,
-                          double *values, double *value_der, int32_t *n_central) {
-    TGB_TRY(need_ctx());
+// One block's GAP sum delta^2 sum_s alpha_s K_is^zeta (no e0) per central site and,
+// when der is given, its gradient d/dr_j for every pair of the sites' lists (the
+// self pair holding d/dr_i), through the get_gap_soap remap. Host outputs: the
+// sums by atom (en, n_total_sites), the sites' batch rows and atoms, the list
+// starts (ps, n_sites0 + 1) and der (3 P).
+static int property_eval(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                         const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                         const int32_t *species_batch, const int32_t *species_all, double *der,
+                         std::vector<double> &en, std::vector<int> &rows, std::vector<int> &atoms,
+                         std::vector<int64_t> &ps, int *n_central) {
     Context &C = *g_ctx;
-    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
-    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0 && values && n_central, TG_ERR_ARG,
-              "bad local-property arguments");
-    *n_central = 0;
-    if (n_sites0 == 0) return TG_OK;
     Block &b = *C.current;
     DBuf<signed char> zf;
     int64_t P = 0;
@@ -1297,7 +1297,7 @@ int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t
     TGB_CUDA(cudaMemsetAsync(C.en.p, 0, sizeof(double) * n_total_sites, st));
     TGB_CUDA(cudaMemsetAsync(C.fo.p, 0, sizeof(double) * 3 * n_total_sites, st));
     TGB_CUDA(cudaMemsetAsync(C.vir.p, 0, sizeof(double) * 9, st));
-    if (value_der) {
+    if (der) {
         TGB_TRY(pg.ensure(3 * (size_t)P));
         TGB_CUDA(cudaMemsetAsync(pg.p, 0, sizeof(double) * 3 * P, st));
     }
@@ -1305,22 +1305,44 @@ int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t
     if (!wp) wp = std::make_unique<Workspace>();
     SiteArgs S{nc, C.site_row.p, C.site_atom.p, C.pstart.p, C.nbr.p, C.xyz.p, C.spa.p};
     TGB_TRY(evaluate_block(b, *wp, S, n_total_sites, C.fo.p, C.en.p, C.vir.p, C.err.p, st, nullptr,
-                           nullptr, nullptr, value_der ? pg.p : nullptr));
+                           nullptr, nullptr, der ? pg.p : nullptr));
     TGB_TRY(check_err_word(C, C.err.p));
-    std::vector<double> en(n_total_sites);
-    std::vector<int> rows(nc), atoms(nc);
-    std::vector<int64_t> ps(n_sites0 + 1);
+    en.assign(n_total_sites, 0.0);
+    rows.assign(nc, 0);
+    atoms.assign(nc, 0);
+    ps.assign(n_sites0 + 1, 0);
     TGB_CUDA(cudaMemcpyAsync(en.data(), C.en.p, sizeof(double) * n_total_sites, cudaMemcpyDeviceToHost, st));
     if (nc > 0) {
         TGB_CUDA(cudaMemcpyAsync(atoms.data(), C.site_atom.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
         TGB_CUDA(cudaMemcpyAsync(rows.data(), C.site_row.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
     }
     TGB_CUDA(cudaMemcpyAsync(ps.data(), C.pstart.p, sizeof(int64_t) * (n_sites0 + 1), cudaMemcpyDeviceToHost, st));
-    if (value_der)
-        TGB_CUDA(cudaMemcpyAsync(value_der, pg.p, sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, st));
+    if (der) TGB_CUDA(cudaMemcpyAsync(der, pg.p, sizeof(double) * 3 * P, cudaMemcpyDeviceToHost, st));
     TGB_CUDA(cudaStreamSynchronize(st));
-    // local_properties.f90:244-270: V = delta^2 sum_s alpha_s K^zeta + V0, negative
-    // values clamped to zero together with their derivatives
+    *n_central = nc;
+    return TG_OK;
+}
+
+int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                          const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                          const int32_t *species_batch, const int32_t *species_all, double v0,
+                          double *values, double *value_der, int32_t *n_central) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
+    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0 && values && n_central, TG_ERR_ARG,
+              "bad local-property arguments");
+    *n_central = 0;
+    if (n_sites0 == 0) return TG_OK;
+    std::vector<double> en;
+    std::vector<int> rows, atoms;
+    std::vector<int64_t> ps;
+    int nc = 0;
+    TGB_TRY(property_eval(n_total_sites, n_sites0, n_neigh0, neighbors_list0, rjs0, xyz0,
+                          species_batch, species_all, value_der, en, rows, atoms, ps, &nc));
+    // local_properties.f90:244-270 (and hirshfeld_predict, vdw.f90:39-159): V =
+    // delta^2 sum_s alpha_s K^zeta + V0, negative values clamped to zero together
+    // with their derivatives
     for (int i = 0; i < nc; ++i) {
         double v = en[atoms[i]] + v0;
         if (v < 0.0) {
@@ -1330,6 +1352,36 @@ int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t
                     for (int q = 0; q < 3; ++q) value_der[3 * p + q] = 0.0;
         }
         values[i] = v;
+    }
+    *n_central = nc;
+    return TG_OK;
+}
+
+int tg_get_soap_dipole(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
+                       const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
+                       const int32_t *species_batch, const int32_t *species_all, double *dipoles,
+                       double *energies, int32_t *n_central) {
+    TGB_TRY(need_ctx());
+    Context &C = *g_ctx;
+    TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
+    TGB_CHECK(n_total_sites >= 1 && n_sites0 >= 0 && dipoles && n_central, TG_ERR_ARG,
+              "bad dipole arguments");
+    *n_central = 0;
+    if (n_sites0 == 0) return TG_OK;
+    int64_t P = 0;
+    for (int i = 0; i < n_sites0; ++i) P += n_neigh0[i];
+    std::vector<double> der(3 * (size_t)std::max<int64_t>(P, 1)), en;
+    std::vector<int> rows, atoms;
+    std::vector<int64_t> ps;
+    int nc = 0;
+    TGB_TRY(property_eval(n_total_sites, n_sites0, n_neigh0, neighbors_list0, rjs0, xyz0,
+                          species_batch, species_all, der.data(), en, rows, atoms, ps, &nc));
+    // gap.f90:378-387: mu_i = Qss_i . d(soap_i)/d(r_i), the self pair (first of
+    // the site's list) of the fictitious energy's gradient; no e0, no clamp
+    for (int i = 0; i < nc; ++i) {
+        const int64_t self = ps[rows[i]];
+        for (int q = 0; q < 3; ++q) dipoles[3 * (size_t)i + q] = der[3 * self + q];
+        if (energies) energies[i] = en[atoms[i]];
     }
     *n_central = nc;
     return TG_OK;
