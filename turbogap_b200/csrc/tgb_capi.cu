@@ -466,17 +466,29 @@ __global__ void k_mlp_mix(int n, int n_et, const double *__restrict__ emean,
     }
 }
 
-// compacted GEMM-1 operand rows and delta.mu of the gated sites
-__global__ void k_gather_gated(const int *__restrict__ gcount, const int *__restrict__ gidx, int K1,
-                               const __nv_bfloat16 *__restrict__ qsplit,
+// compacted GEMM-1 operand rows of the gated sites and their delta.mu. The mixed
+// form's descriptor writes only its network's bf16 input, so the rows are split
+// here from the fp32 delta rows, exactly as the descriptor splits them.
+__global__ void k_gather_gated(const int *__restrict__ gcount, const int *__restrict__ gidx, int D,
+                               int K1, int nsplit, const float *__restrict__ q,
                                const double *__restrict__ qoff, __nv_bfloat16 *__restrict__ Qg,
                                double *__restrict__ qoff_g) {
     const int cnt = *gcount;
     for (int r = blockIdx.x; r < cnt; r += gridDim.x) {
         const int site = gidx[r];
-        const uint4 *src = reinterpret_cast<const uint4 *>(qsplit + (size_t)site * K1);
-        uint4 *dst = reinterpret_cast<uint4 *>(Qg + (size_t)r * K1);
-        for (int k = threadIdx.x; k < K1 / 8; k += blockDim.x) dst[k] = src[k];
+        const float *src = q + (size_t)site * D;
+        __nv_bfloat16 *dst = Qg + (size_t)r * K1;
+        for (int d = threadIdx.x; d < D; d += blockDim.x) {
+            __nv_bfloat16 hi, lo;
+            bf16_split(src[d], hi, lo);
+            dst[d] = hi;
+            if (nsplit == 3) {
+                dst[D + d] = hi;
+                dst[2 * D + d] = lo;
+            }
+        }
+        for (int k = nsplit * D + threadIdx.x; k < K1; k += blockDim.x)
+            dst[k] = __float2bfloat16_rn(0.f);
         if (threadIdx.x == 0) qoff_g[r] = qoff[site];
     }
 }
@@ -565,7 +577,13 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     TGB_TRY(x.ensure(b, n));
     TGB_CHECK(x.mlp->L.D == b.dim, TG_ERR_ARG, "MLP input size %d does not match block dim %d",
               x.mlp->L.D, b.dim);
-    const SoapParams P = b.params(n_atoms);
+    // the descriptor writes the network's input only: the bf16 row of delta,
+    // zero-padded to the network's input length (the gated rows are split below)
+    TGB_CHECK(x.mlp->L.Dp <= b.K1, TG_ERR_ARG, "MLP input length %d exceeds the row length %d",
+              x.mlp->L.Dp, b.K1);
+    SoapParams P = b.params(n_atoms);
+    P.nsplit = 1;
+    P.fill_to = x.mlp->L.Dp;
     TGB_TRY(descriptor_pass(b, w, P, S, st, w.tile_desc));
     TGB_MARK(log, PASS_DESC, st);
     TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim,
@@ -575,8 +593,8 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
                                            1.0 / (b.delta * b.delta), w.epart.p, w.kdsum.p,
                                            x.gidx.p, x.gcount.p);
     const unsigned gg = (unsigned)std::min(n, 1184);   // grid-stride over the gated rows
-    k_gather_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.K1, w.qsplit.p, w.qoff.p, x.Qg.p,
-                                      x.qoff_g.p);
+    k_gather_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.K1, b.nsplit, w.q.p,
+                                      w.qoff.p, x.Qg.p, x.qoff_g.p);
     TGB_CUDA(cudaGetLastError());
     TGB_MARK(log, PASS_MLP, st);
     // both GEMMs over the compacted gated rows in chunks of w.kd_rows, each chunk's

@@ -755,7 +755,8 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
     }
     const double nrm = sqrt(nrm2);
     off = warp_sum(off);
-    for (int d = P.nsplit * DIM + lane; d < K1; d += 32) qs[d] = __float2bfloat16_rn(0.f);
+    const int fill = P.fill_to > 0 ? P.fill_to : K1;
+    for (int d = P.nsplit * DIM + lane; d < fill; d += 32) qs[d] = __float2bfloat16_rn(0.f);
     if (lane == 0) {
         O.pnorm[site] = nrm;
         O.qoff[site] = off;
@@ -1585,7 +1586,8 @@ __global__ void __launch_bounds__(256) k_compress_fwd(SoapParams P, CompressArgs
             qs[2 * D + i] = lo;
         }
     }
-    for (int k = P.nsplit * D + lane; k < P.K1; k += 32) qs[k] = __float2bfloat16_rn(0.f);
+    const int fill = P.fill_to > 0 ? P.fill_to : P.K1;
+    for (int k = P.nsplit * D + lane; k < fill; k += 32) qs[k] = __float2bfloat16_rn(0.f);
     off = warp_sum(off);
     if (lane == 0) {
         O.pnorm[site] = sqrt(nrm2);

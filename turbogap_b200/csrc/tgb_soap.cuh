@@ -34,6 +34,10 @@ struct SoapParams {
     // precision of the tensor-core force tile: 3 = TF32 hi/lo split (about fp32,
     // the plain form), 1 = single TF32 products (the mixed form's budget)
     int force_prec = 3;
+    // columns of the split-q row the descriptor writes (the parts, then zeros up
+    // to fill_to); 0 means the whole row K1. The mixed form writes nsplit 1 and
+    // fills to its network's padded input length.
+    int fill_to = 0;
 };
 
 // Per-launch site addressing: site i reads CSR row site_row[i] of the pair
