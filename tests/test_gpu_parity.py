@@ -239,3 +239,20 @@ def test_engine_list_builds_agree(gpu, ch_blocks, monkeypatch, slots):
     assert np.abs(e1 - e2).max() < 1e-12 and np.abs(f1 - f2).max() < 1e-12
     assert np.abs(v1 - v2).max() < 1e-12
     assert np.abs(p1 - p2).max() < 1e-12 and np.abs(g1 - g2).max() < 1e-10
+
+
+def test_engine_parity_real_zeta(gpu, carbon_block):
+    """A non-integer zeta (gap.f90:115-121 keeps it real beyond 1e-5 of an
+    integer): the real-power epilogue, whose padding columns must add nothing."""
+    from turbogap_b200.hypers import GapBlock
+    blk = GapBlock(carbon_block.hypers, carbon_block.Qs, carbon_block.alphas, delta=1.0, zeta=2.5)
+    gpu.soap_backend_begin(blk, key=111)
+    st = random_structure(216, 12.91, 1.2, seed=1000)
+    eo, fo, vo, _ = O.evaluate(st.positions, st.species, st.box, [blk])
+    eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [111])
+    e, f, v = eng.compute()
+    eng.close()
+    assert np.all(np.isfinite(eo))
+    assert np.abs(e - eo).max() < E_TOL
+    assert np.abs(f - fo).max() < F_TOL
+    assert np.abs(v - vo).max() < V_TOL * np.abs(vo).max()

@@ -585,7 +585,11 @@ __global__ void __launch_bounds__(threads_for(MODE), 1)
                 for (int j = 0; j < 32; ++j) {
                     const double2 p = pc[j];
                     const double K = ((double)v[j] + p.y) + qo;
-                    const double t1 = p.x * kpow_m1<MODE>(K, ep);   // alpha_s K^(zeta-1)
+                    // alpha_s K^(zeta-1); with a real zeta a padding column (alpha 0,
+                    // K = delta . mu, which may be negative) must give 0, not 0 x NaN
+                    double t1;
+                    if constexpr (MODE == MODE_GAP_ZREAL) t1 = p.x != 0.0 ? p.x * kpow_m1<MODE>(K, ep) : 0.0;
+                    else t1 = p.x * kpow_m1<MODE>(K, ep);
                     k4[j & 3] += t1;
                     e4[j & 3] = fma(t1, K, e4[j & 3]);
                     // kd_s - kcoef_s = zeta delta^2 (alpha_s K^(zeta-1) - alpha_s)
