@@ -62,8 +62,9 @@ def parse():
     ap.add_argument("--mlp-cells", type=int, default=16,
                     help="separate training cells of the workload's kind")
     ap.add_argument("--mlp-epochs", type=int, default=10)
-    ap.add_argument("--mlp-hidden", type=int, default=256,
-                    help="hidden width H of each member (D -> H -> H -> 1)")
+    ap.add_argument("--mlp-hidden", type=int, default=0,
+                    help="hidden width H of each member (D -> H -> H -> 1); 0: 256 for "
+                         "D <= 512 (the carbon network), 128 above")
     ap.add_argument("--gate-ev", type=float, default=0.005)
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: shard ONE structure over the ranks by central-site ranges "
@@ -197,7 +198,8 @@ def mixed_leg(B, eng, blocks, keys, w, a, ext, dist, plain_ms):
     import torch
     from turbogap_b200 import learned
     t0 = time.time()
-    mlps = [B.Mlp(b.hypers.device_dim, a.mlp_hidden, 4, seed=100 + i) for i, b in enumerate(blocks)]
+    hidden = [a.mlp_hidden or (256 if b.hypers.device_dim <= 512 else 128) for b in blocks]
+    mlps = [B.Mlp(b.hypers.device_dim, hidden[i], 4, seed=100 + i) for i, b in enumerate(blocks)]
     kind = "CH" if len(blocks) > 1 else "C"
     cells = learned.training_cells(kind, a.mlp_cells, seed=w.seed * 100 + 61)
     data = learned.collect(B, mlps, keys, cells, a.mlp_samples, dt=w.dt, stride=2, seed=17)
@@ -247,8 +249,8 @@ def mixed_leg(B, eng, blocks, keys, w, a, ext, dist, plain_ms):
                            "rmse_f_mev_per_A": 1e3 * err_after[1], "gated_sites": err_after[2]},
         "reference": "exact bf16x3 GPU path at the same configurations (the benchmark "
                      "structure is not in the training data)",
-        "mlp": f"4 members x (D -> {a.mlp_hidden} -> {a.mlp_hidden} -> 1, SiLU) per block, bf16 "
-               f"GEMMs, fp32 accumulation",
+        "mlp": f"4 members x (D -> H -> H -> 1, SiLU) per block, H = {hidden}, bf16 GEMMs, "
+               f"fp32 accumulation",
         "training": {"samples": [m.n_samples() for m in mlps], "protocol":
                      f"exact GAP NVE MD of {data['cells']} separate {kind} cells, 216-4096 "
                      f"atoms, 300-5000 K, a snapshot every 2 steps", "data": data,

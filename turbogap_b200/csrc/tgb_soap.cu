@@ -785,6 +785,16 @@ struct ForceShape {
     // dead by then: the warp's area is the larger of the two
     static constexpr int GAREA = NLM * GS;
     static constexpr int WARP_FLOATS = BAREA > GAREA ? BAREA : GAREA;
+    // Gamma rows of slot k (lm 32k .. 32k + 31) may be stored as soon as slot k is
+    // done when they end below the first B_l that slot k + 1 reads
+    // (l = floor(sqrt(32 (k + 1)))); true for every shape compiled here.
+    static constexpr int isqrt(int v) { int r = 0; while ((r + 1) * (r + 1) <= v) ++r; return r; }
+    static constexpr bool gamma_over_b_ok() {
+        for (int k = 0; k + 1 < SLOTS; ++k)
+            if ((32 * (k + 1)) * GS > isqrt(32 * (k + 1)) * BSTRIDE) return false;
+        return true;
+    }
+    static constexpr bool GAMMA_EARLY = gamma_over_b_ok();
     static_assert(AMAX % 4 == 0, "float4 reads of Gamma need alpha_max % 4 == 0");
 };
 
@@ -927,10 +937,10 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
             lk[k] = l;
         }
         const float *cg = I.c + (size_t)site * NT * NLM;
-        float gv[Sh::SLOTS][NT];
-#pragma unroll
-        for (int k = 0; k < Sh::SLOTS; ++k) {
-            if (lmk[k] >= NLM) continue;
+        // One slot (32 lm) at a time, 16 live accumulators per lane: a slot's Gamma
+        // rows go over the B_l of the smallest l, which no later slot reads, once
+        // the whole warp has finished reading B for the slot (gamma_over_b_ok).
+        auto slot_gamma = [&](int k, float (&gv)[NT]) {
             float cr[NT];
 #pragma unroll
             for (int n2 = 0; n2 < NT; ++n2) cr[n2] = cg[n2 * NLM + lmk[k]];
@@ -945,17 +955,32 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                     v += b.x * cr[4 * j] + b.y * cr[4 * j + 1] + b.z * cr[4 * j + 2] +
                          b.w * cr[4 * j + 3];
                 }
-                gv[k][n] = v;
+                gv[n] = v;
             }
-        }
-        __syncwarp();   // every lane is done with B: Gamma goes over it
-#pragma unroll
-        for (int k = 0; k < Sh::SLOTS; ++k) {
-            if (lmk[k] >= NLM) continue;
+        };
+        auto store_gamma = [&](int k, const float (&gv)[NT]) {
 #pragma unroll
             for (int n0 = 0; n0 < NT; n0 += 4)
                 *reinterpret_cast<float4 *>(gam + lmk[k] * Sh::GS + n0) =
-                    make_float4(gv[k][n0], gv[k][n0 + 1], gv[k][n0 + 2], gv[k][n0 + 3]);
+                    make_float4(gv[n0], gv[n0 + 1], gv[n0 + 2], gv[n0 + 3]);
+        };
+        if constexpr (Sh::GAMMA_EARLY) {
+#pragma unroll
+            for (int k = 0; k < Sh::SLOTS; ++k) {
+                float gv[NT];
+                if (lmk[k] < NLM) slot_gamma(k, gv);
+                __syncwarp();   // the warp is done with this slot's B_l
+                if (lmk[k] < NLM) store_gamma(k, gv);
+            }
+        } else {
+            float gv[Sh::SLOTS][NT];
+#pragma unroll
+            for (int k = 0; k < Sh::SLOTS; ++k)
+                if (lmk[k] < NLM) slot_gamma(k, gv[k]);
+            __syncwarp();   // every lane is done with B: Gamma goes over it
+#pragma unroll
+            for (int k = 0; k < Sh::SLOTS; ++k)
+                if (lmk[k] < NLM) store_gamma(k, gv[k]);
         }
         __syncwarp();
         // pairs: lane per pair (the self pair, first in the list, is the -sum)
