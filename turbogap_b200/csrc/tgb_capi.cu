@@ -1646,6 +1646,7 @@ struct Engine {
         } else {
             TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
         }
+        TGB_TRY(launch_pair_species(n, nl, species.p, n, st));
         TGB_MARK(log, PASS_NEIGH, st);
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, site_beg, site_end, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
@@ -1661,6 +1662,7 @@ struct Engine {
             auto &r = runs[k];
             cudaStream_t sk = (fork && k > 0) ? side[k - 1] : st;
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            S.nsp = nl.nsp;
             if (r->mix)
                 TGB_TRY(evaluate_block_mixed(*r->b, *r->w, *r->mix, S, n, f.p, en.p, vir.p, err.p,
                                              sk, log));
@@ -1741,11 +1743,13 @@ struct Engine {
             p = pos_sc.p;
         }
         TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+        TGB_TRY(launch_pair_species(n, nl, species.p, n, st));
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(en.p, 0, sizeof(double) * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            S.nsp = nl.nsp;
             TGB_TRY(autotune_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
         }
         TGB_CUDA(cudaStreamSynchronize(st));
@@ -2378,6 +2382,7 @@ struct BatchEngine {
     DBuf<BatchStruct> sdev;
     DBuf<char> scan_tmp;
     DBuf<unsigned> err;
+    DBuf<signed char> nsp;     // per-pair neighbour species (launch_pair_species)
     BatchNL nl;
     std::vector<std::unique_ptr<BlockRun>> runs;
     std::vector<int> n_atoms_h;
@@ -2396,11 +2401,13 @@ struct BatchEngine {
             for (auto &r : runs) pin_tiles(*r->b, *r->w, pinned_tile());
         if (!autotune_enabled()) return TG_OK;
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        TGB_TRY(launch_pair_species(nl.pstart + n, nl.cap, nl.nbr, species.p, n, nsp.p, st));
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
         TGB_CUDA(cudaMemsetAsync(en.p, 0, sizeof(double) * n, st));
         TGB_CUDA(cudaMemsetAsync(vir.p, 0, sizeof(double) * 9, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            S.nsp = nsp.p;
             TGB_TRY(autotune_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st));
         }
         TGB_CUDA(cudaStreamSynchronize(st));
@@ -2410,6 +2417,7 @@ struct BatchEngine {
     int compute_ef(EventLog *log = nullptr) {
         TGB_MARK(log, -1, st);
         TGB_TRY(batch_nl_build(nl, pos.p, rcut, st));
+        TGB_TRY(launch_pair_species(nl.pstart + n, nl.cap, nl.nbr, species.p, n, nsp.p, st));
         TGB_MARK(log, PASS_NEIGH, st);
         k_energy_e0<<<grid_for(n), 256, 0, st>>>(n, species.p, e0.p, nz, 0, n, en.p);
         TGB_CUDA(cudaMemsetAsync(f.p, 0, sizeof(double) * 3 * n, st));
@@ -2417,6 +2425,7 @@ struct BatchEngine {
         TGB_CUDA(cudaMemsetAsync(vir_s.p, 0, sizeof(double) * 9 * ns, st));
         for (auto &r : runs) {
             SiteArgs S{r->n_sites, r->sites.p, r->sites.p, nl.pstart, nl.nbr, nl.xyz, species.p};
+            S.nsp = nsp.p;
             TGB_TRY(evaluate_block(*r->b, *r->w, S, n, f.p, en.p, vir.p, err.p, st, log,
                                    atom_struct.p, vir_s.p));
         }
@@ -2447,6 +2456,7 @@ struct BatchEngine {
         const int64_t cap = P + P / 4 + 64;
         TGB_TRY(nbr.ensure(cap));
         TGB_TRY(xyz.ensure(3 * (size_t)cap));
+        TGB_TRY(nsp.ensure(cap));
         nl.nbr = nbr.p;
         nl.xyz = xyz.p;
         nl.cap = cap;

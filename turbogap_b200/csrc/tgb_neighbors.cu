@@ -8,6 +8,8 @@
 
 #include "tgb_neighbors.cuh"
 
+#include <algorithm>
+
 #include <cub/device/device_scan.cuh>
 
 namespace tgb {
@@ -602,9 +604,11 @@ int NeighborList::reserve(int ns, int nsc, int64_t pair_cap, const CellGrid &g) 
     }
     if (pair_cap > cap) {
         dev_free(nbr); dev_free(rjs); dev_free(xyz);
+        dev_free(nsp);
         TGB_TRY(dev_alloc(&nbr, pair_cap));
         TGB_TRY(dev_alloc(&rjs, pair_cap));
         TGB_TRY(dev_alloc(&xyz, 3 * pair_cap));
+        TGB_TRY(dev_alloc(&nsp, pair_cap));
         cap = pair_cap;
     }
     if (!err) TGB_TRY(dev_alloc(&err, 1));
@@ -627,6 +631,7 @@ void NeighborList::release() {
     dev_free(n_neigh); dev_free(pstart); dev_free(cell_xyz); dev_free(cell_atoms);
     dev_free(cell_count); dev_free(cell_start); dev_free(cell_fill); dev_free(nbr);
     dev_free(rjs); dev_free(xyz); dev_free(scan_tmp); dev_free(err); dev_free(cell_pos);
+    dev_free(nsp);
     *this = NeighborList{};
 }
 
@@ -707,6 +712,38 @@ __global__ void k_skin_check(int n, const double *__restrict__ pos,
 }
 
 }  // namespace
+
+namespace {
+__global__ void k_pair_species(const int64_t *__restrict__ pend, int64_t cap,
+                               const int *__restrict__ nbr, const int *__restrict__ species,
+                               int n_atoms, signed char *__restrict__ nsp) {
+    const int64_t P = min(*pend, cap);
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int j = nbr[p];
+        nsp[p] = (signed char)species[j < n_atoms ? j : j % n_atoms];
+    }
+}
+}  // namespace
+
+int launch_pair_species(const int64_t *pend, int64_t cap, const int *nbr, const int *species,
+                        int n_atoms, signed char *nsp, cudaStream_t st) {
+    if (!nsp || cap <= 0 || n_atoms <= 0) return TG_OK;
+    int dev = 0, n_sm = 0;
+    TGB_CUDA(cudaGetDevice(&dev));
+    TGB_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t want = (cap + 255) / 256;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)n_sm * 16));
+    k_pair_species<<<grid, 256, 0, st>>>(pend, cap, nbr, species, n_atoms, nsp);
+    TGB_CUDA(cudaGetLastError());
+    return TG_OK;
+}
+
+int launch_pair_species(int n_sites, const NeighborList &nl, const int *species, int n_atoms,
+                        cudaStream_t st) {
+    if (n_sites <= 0) return TG_OK;
+    return launch_pair_species(nl.pstart + n_sites, nl.cap, nl.nbr, species, n_atoms, nl.nsp, st);
+}
 
 int launch_nl_refresh(int n_sites, const double *pos, const Box &bx, const NeighborList &nl,
                       const int *when, cudaStream_t st) {

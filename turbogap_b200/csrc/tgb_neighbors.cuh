@@ -55,6 +55,9 @@ struct NeighborList {
     double *rjs = nullptr;
     double *xyz = nullptr;
     double *cell_pos = nullptr;   // optional: positions in cell order (coalesced candidate reads)
+    // global species id of each pair's neighbour (launch_pair_species), so the
+    // SOAP passes stream it instead of gathering species[neighbour]
+    signed char *nsp = nullptr;
     void *scan_tmp = nullptr;
     size_t scan_bytes = 0;
     unsigned *err = nullptr;
@@ -90,6 +93,14 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
 // neighbors.f90:544-590): refresh distances of the kept pairs while *when is 0;
 // after the list phase restart the displacement sums if the list was rebuilt;
 // after the integrator raise *when once |displacement|^2 > thresh.
+// nsp[p] = species[neighbour of pair p mod n_atoms] for every pair of the list
+// (the pair count read on the device from pstart[n_sites], capped at nl.cap).
+int launch_pair_species(int n_sites, const NeighborList &nl, const int *species, int n_atoms,
+                        cudaStream_t st);
+// The same over raw arrays: pend = &pstart[n_sites] (the pair count), cap pairs at most.
+int launch_pair_species(const int64_t *pend, int64_t cap, const int *nbr, const int *species,
+                        int n_atoms, signed char *nsp, cudaStream_t st);
+
 int launch_nl_refresh(int n_sites, const double *pos, const Box &bx, const NeighborList &nl,
                       const int *when, cudaStream_t st);
 int launch_skin_reset(int n, const int *when, double *disp, long long *counters, cudaStream_t st);

@@ -547,8 +547,7 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         int s = -1;
         if (base + t < np) {
             const int64_t p = p0 + base + t;
-            const int ja = fold_index(S.nbr[p], P.n_atoms);
-            s = zlookup(P, S.species[ja]);
+            s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[fold_index(S.nbr[p], P.n_atoms)]);
             const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
                         z = (float)S.xyz[3 * p + 2];
             const float r = sqrtf(x * x + y * y + z * z);
@@ -988,7 +987,7 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         for (int pp = 1 + lane; pp < np; pp += 32) {
             const int64_t p = p0 + pp;
             const int ja = fold_index(S.nbr[p], P.n_atoms);
-            const int s = zlookup(P, S.species[ja]);
+            const int s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[ja]);
             const double X = S.xyz[3 * p], Yy = S.xyz[3 * p + 1], Z = S.xyz[3 * p + 2];
             const float x = (float)X, y = (float)Yy, z = (float)Z;
             const float r = sqrtf(x * x + y * y + z * z);
@@ -1385,8 +1384,8 @@ __global__ void __launch_bounds__(128, 2)
                 for (int k = 0; k <= 40; ++k) ax[k] = 0.f;   // [40]: the valid flag
                 if (pp < np) {
                     const int64_t p = p0 + pp;
-                    const int ja = fold_index(S.nbr[p], P.n_atoms);
-                    const int s = zlookup(P, S.species[ja]);
+                    const int s = zlookup(P, S.nsp ? (int)S.nsp[p]
+                                                   : S.species[fold_index(S.nbr[p], P.n_atoms)]);
                     const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
                                 z = (float)S.xyz[3 * p + 2];
                     const float r = sqrtf(x * x + y * y + z * z);

@@ -51,6 +51,9 @@ struct SiteArgs {
     const double *xyz;       // (3, P) MIC vectors r_j - r_i
     const int *species;      // global species id per unit-cell atom
     int ahead = 0;           // set by the launchers: sites in flight at once (L2 prefetch distance)
+    // optional: the global species id of each pair's neighbour (streamed instead of
+    // gathering species[neighbour])
+    const signed char *nsp = nullptr;
 };
 
 // Descriptor entries on the device run in the internal order d = l * NP + pi
