@@ -69,6 +69,27 @@ def test_local_property_matches_oracle(gpu, offset, compressed):
     assert len(far) > 0 and not der[far].any()
 
 
+def test_local_property_species_multiplicity(gpu):
+    """A property block with carbon in both descriptor species (species
+    multiplicity 2): each pair's dV/dr adds both species' terms."""
+    from test_gpu_parity import multiplicity_hypers
+    h = multiplicity_hypers()
+    blk = sparse_block(h, 200, seed=97, sigma_alpha=0.002, n_structs=2)
+    gpu.soap_backend_begin(blk, key=905)
+    st = random_structure(216, 12.91, 1.2, seed=98)
+    nl = neighbor_data(st, h.rcut_max)
+    nn, idx = _kept(st, h, nl)
+    q, sder, _ = O.get_soap(O.HypersC(h), nn, np.ones((len(idx), 2), np.int32), nl["rjs"][idx],
+                            nl["xyz"][idx], derivatives=True)
+    vals, der = gpu.get_local_property(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"],
+                                       nl["xyz"], st.species, st.species, v0=0.0)
+    Vo, Do = O.local_property_predict(q, blk.Qs, blk.alphas, 0.0, blk.delta, blk.zeta, sder, nn)
+    assert np.abs(vals - Vo).max() < 1e-7
+    full = np.zeros((len(nl["rjs"]), 3))
+    full[idx] = Do
+    assert np.abs(der - full).max() < 1e-6 * max(1.0, np.abs(full).max())
+
+
 @pytest.mark.parametrize("zeta", [4.0, 2.5])
 def test_soap_dipole_matches_oracle(gpu, zeta):
     """get_soap_dipole (gap.f90:261-398): the self pair's gradient of a dipole

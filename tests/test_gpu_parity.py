@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from _util import O, neighbor_data, oracle_descriptors, sparse_block
-from turbogap_b200.hypers import carbon_hypers, ch_hypers
+from turbogap_b200.hypers import SoapTurboHypers, carbon_hypers, ch_hypers
 from turbogap_b200.synth import maxwell_velocities, random_structure
 
 pytestmark = pytest.mark.gpu
@@ -168,6 +168,49 @@ def test_engine_parity_two_species(gpu, ch_blocks):
     assert np.abs(e - eo).max() < E_TOL
     assert np.abs(f - fo).max() < F_TOL
     assert np.abs(v - vo).max() < V_TOL * np.abs(vo).max()
+    eng.close()
+
+
+def multiplicity_hypers(central=0):
+    """Carbon (species 1) in both descriptor species of one block (species
+    multiplicity 2, gap_interface.f90:180-199), each with its own cutoff,
+    widths and central weight."""
+    return SoapTurboHypers(species_z=[1, 1], alpha_max=[8, 8], l_max=8, rcut_hard=[3.7, 2.9],
+                           buffer=[0.5, 0.4], atom_sigma_r=[0.5, 0.35], atom_sigma_t=[0.5, 0.4],
+                           central_weight=[1.0, 0.6], central_species=central)
+
+
+def test_descriptor_parity_species_multiplicity(gpu):
+    h = multiplicity_hypers()
+    blk = sparse_block(h, 200, seed=23, n_structs=2)
+    gpu.soap_backend_begin(blk, key=231)
+    st = random_structure(216, 12.91, 1.2, seed=1001)
+    nl = neighbor_data(st, h.rcut_max)
+    q = gpu.get_soap(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"], nl["xyz"], st.species,
+                     st.species, h.dim)
+    qo, _, _ = oracle_descriptors(st, h, nl)
+    assert np.abs(q - qo).max() < Q_TOL
+    # the two descriptor species see the same atoms through different hypers
+    half = h.alpha_max[0]
+    assert np.abs(qo[:, : half * (half + 1) // 2]).max() > 0.0
+
+
+def test_engine_parity_species_multiplicity(gpu):
+    """C/H structure, a C-centred block with C in both descriptor species: H
+    atoms are invisible to it; energies, forces and the virial against the oracle."""
+    L = (300 / 0.12) ** (1 / 3)
+    h = multiplicity_hypers(central=1)
+    blk = sparse_block(h, 400, seed=24, n_atoms=300, L=L, d_min=1.0, h_fraction=0.25,
+                       n_structs=3)
+    gpu.soap_backend_begin(blk, key=232)
+    st = random_structure(300, L, 1.0, seed=25, h_fraction=0.25)
+    eo, fo, vo, _ = O.evaluate(st.positions, st.species, st.box, [blk])
+    eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [232])
+    e, f, v = eng.compute()
+    assert np.abs(e - eo).max() < E_TOL
+    assert np.abs(f - fo).max() < F_TOL
+    assert np.abs(v - vo).max() < V_TOL * np.abs(vo).max()
+    assert (st.species == 2).any() and not f[st.species == 2].any()   # H is invisible to it
     eng.close()
 
 

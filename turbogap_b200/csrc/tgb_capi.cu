@@ -72,7 +72,8 @@ struct Block {
     int KD = 0;   // stored kd row: [hi | lo] (bf16x3) or [hi]; GEMM 2 reads hi twice
     double delta = 1.0, zeta = 1.0, rcut_max = 0.0;
     int zeta_int = 0;
-    signed char zmap[kMaxZ];
+    signed char zmap[kMaxZ], zmap2[kMaxZ];   // first and second descriptor species of a global id
+    int n_inst = 1;                          // 2 when a global species appears twice
     DBuf<float> table, selfR;
     DBuf<float4> table_fd;   // the descriptor's (f, f') interval copy
     DBuf<__nv_bfloat16> QsA, QsT;
@@ -101,6 +102,8 @@ struct Block {
         P.ns = ns; P.amax = amax; P.lmax = lmax; P.ntot = ntot; P.nlm = nlm; P.dim = dim;
         P.nsplit = nsplit; P.K1 = K1; P.tw = tw; P.n_atoms = n_atoms;
         std::memcpy(P.zmap, zmap, sizeof(zmap));
+        std::memcpy(P.zmap2, zmap2, sizeof(zmap2));
+        P.n_inst = n_inst;
         for (int s = 0; s < ns; ++s) {
             P.rcut[s] = (float)hh.rcut_hard[s];
             P.tab_h[s] = (float)(hh.rcut_hard[s] / kTableIntervals);
@@ -859,9 +862,6 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
                   "species id %d outside 1..%d", hh.species_z[s], kMaxZ - 1);
         TGB_CHECK(hh.rcut_hard[s] > 0.0 && hh.sigma_r[s] > 0.0 && hh.sigma_t[s] > 0.0, TG_ERR_ARG,
                   "rcut and atom sigmas must be positive");
-        for (int s2 = 0; s2 < s; ++s2)
-            TGB_CHECK(hh.species_z[s2] != hh.species_z[s], TG_ERR_ARG,
-                      "repeated species in one block (multiplicity > 1) is not supported on the device");
     }
     b->ns = hh.ns;
     b->amax = hh.alpha_max[0];
@@ -906,8 +906,21 @@ int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, 
         b->zeta_int = 0;
         b->zeta = zeta;
     }
-    for (int z = 0; z < kMaxZ; ++z) b->zmap[z] = -1;
-    for (int s = hh.ns - 1; s >= 0; --s) b->zmap[hh.species_z[s]] = (signed char)s;
+    // species multiplicity (gap_interface.f90:180-199): a global species listed
+    // twice feeds both descriptor species, each with its own hypers. The device
+    // shapes have at most two species, so two matches is the most there can be.
+    for (int z = 0; z < kMaxZ; ++z) b->zmap[z] = b->zmap2[z] = -1;
+    b->n_inst = 1;
+    for (int s = 0; s < hh.ns; ++s) {
+        const int z = hh.species_z[s];
+        if (b->zmap[z] < 0) {
+            b->zmap[z] = (signed char)s;
+        } else {
+            TGB_CHECK(b->zmap2[z] < 0, TG_ERR_ARG, "species %d listed more than twice in one block", z);
+            b->zmap2[z] = (signed char)s;
+            b->n_inst = 2;
+        }
+    }
     TGB_TRY(b->table.ensure((size_t)hh.ns * (kTableIntervals + 1) * b->tw));
     TGB_TRY(b->selfR.ensure((size_t)hh.ns * b->amax));
     TGB_TRY(b->QsA.ensure((size_t)b->Mpad * b->K1));

@@ -416,9 +416,19 @@ __device__ __forceinline__ void prefetch_force_site(const SiteArgs &S, const For
     }
 }
 
-// Descriptor species of a global species id, -1 when the block does not see it.
-__device__ __forceinline__ int zlookup(const SoapParams &P, int z) {
-    return (z >= 0 && z < kMaxZ) ? (int)P.zmap[z] : -1;
+// Descriptor species of a global species id (its first match, or with inst 1
+// its second), -1 when the block does not see it.
+__device__ __forceinline__ int zlookup(const SoapParams &P, int z, int inst = 0) {
+    if (z < 0 || z >= kMaxZ) return -1;
+    return inst == 0 ? (int)P.zmap[z] : (int)P.zmap2[z];
+}
+
+// Under species multiplicity a site's list is walked once per match as one run
+// of virtual pairs 1 .. n_inst (np - 1): virtual pair v >= np is list pair
+// v - np + 1 of the second match. Returns the list position and sets inst.
+__device__ __forceinline__ int virtual_pair(int v, int np, int &inst) {
+    inst = v >= np;
+    return inst ? v - np + 1 : v;
 }
 
 // Real spherical harmonics of unit u into Y[l*l + l + m] (m = -l..l), by the
@@ -493,7 +503,9 @@ struct DescShape {
 // Power spectrum and |p| in FP64. RAW (compressed blocks, P.raw): the power
 // spectrum goes to O.praw in FP64 for the compression pass, and the kernel stops
 // there; a separate instantiation, so the uncompressed kernels keep their code.
-template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
+// MULT: the block has species multiplicity (P.n_inst = 2); its own
+// instantiation, so blocks without it keep their code and registers.
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false, bool MULT = false>
 __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
     k_soap_expand(SoapParams P, SiteArgs S, DescOut O) {
     using Sh = DescShape<NS, AMAX, LMAX, TILE>;
@@ -541,13 +553,18 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
 #pragma unroll
         for (int k = 0; k < Sh::SLOTS; ++k) acc[n][k] = 0.f;
 
-    // the self pair (first of the list) is not part of the chunks
-    for (int base = 1; base < np; base += Sh::CHUNK) {
+    // the self pair (first of the list) is not part of the chunks; under species
+    // multiplicity the list is walked once per match (virtual pairs)
+    const int npv = MULT ? 2 * np - 1 : np;
+    for (int base = 1; base < npv; base += Sh::CHUNK) {
         const int t = lane;
         int s = -1;
-        if (base + t < np) {
-            const int64_t p = p0 + base + t;
-            s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[fold_index(S.nbr[p], P.n_atoms)]);
+        if (base + t < npv) {
+            int inst = 0;
+            int64_t p = p0 + base + t;
+            if constexpr (MULT) p = p0 + virtual_pair(base + t, np, inst);
+            s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[fold_index(S.nbr[p], P.n_atoms)],
+                        inst);
             const float x = (float)S.xyz[3 * p], y = (float)S.xyz[3 * p + 1],
                         z = (float)S.xyz[3 * p + 2];
             const float r = sqrtf(x * x + y * y + z * z);
@@ -572,7 +589,7 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         }
         pspec[t] = s;
         __syncwarp();
-        const int cnt = min(Sh::CHUNK, np - base);
+        const int cnt = min(Sh::CHUNK, npv - base);
         for (int tt = 0; tt < cnt; ++tt) {
             const int ss = pspec[tt];
             if (ss < 0) continue;
@@ -601,7 +618,9 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         }
         __syncwarp();
     }
-    // c to shared (FP64, layout [n][lm]) with the central term, and to global (fp32)
+    // c to shared (FP64, layout [n][lm]) with the central term, and to global (fp32);
+    // (under multiplicity the central atom's second descriptor species too)
+    const int scen2 = MULT ? zlookup(P, S.species[catom], 1) : -1;
     double *cs = reinterpret_cast<double *>(Ys);
 #pragma unroll
     for (int n = 0; n < NT; ++n)
@@ -609,8 +628,8 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
         for (int k = 0; k < Sh::SLOTS; ++k)
             if (lmk[k] < NLM) {
                 double v = (double)acc[n][k];
-                if (lmk[k] == 0 && scen >= 0 && n / AMAX == scen)
-                    v += (double)P.self_R[scen * AMAX + n % AMAX];
+                if (lmk[k] == 0 && (n / AMAX == scen || n / AMAX == scen2))
+                    v += (double)P.self_R[n];   // [ns][amax]: species n / AMAX, radial n % AMAX
                 cs[n * Sh::CS + lmk[k]] = v;
                 O.c[((size_t)site * NT + n) * NLM + lmk[k]] = (float)v;
             }
@@ -802,7 +821,8 @@ struct ForceShape {
 // on the fly: F_j -= dE_i/dr_j, F_i += dE_i/dr_j, virial += 1/2 (f x + x f).
 // RAW (compressed blocks, P.raw): I.g already holds dE/dp, from the compression's
 // adjoint; a separate instantiation, so the uncompressed kernels keep their code.
-template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
+// MULT: species multiplicity, as in k_soap_expand.
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false, bool MULT = false>
 __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TILE))
     k_soap_force(SoapParams P, SiteArgs S, ForceIn I, ForceOut O) {
     using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
@@ -982,12 +1002,16 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
                 if (lmk[k] < NLM) store_gamma(k, gv[k]);
         }
         __syncwarp();
-        // pairs: lane per pair (the self pair, first in the list, is the -sum)
+        // pairs: lane per pair (the self pair, first in the list, is the -sum),
+        // once per species match
         double fs[3] = {0, 0, 0};
-        for (int pp = 1 + lane; pp < np; pp += 32) {
-            const int64_t p = p0 + pp;
+        const int npv = MULT ? 2 * np - 1 : np;   // virtual pairs: once per species match
+        for (int pv = 1 + lane; pv < npv; pv += 32) {
+            int inst = 0;
+            int64_t p = p0 + pv;
+            if constexpr (MULT) p = p0 + virtual_pair(pv, np, inst);
             const int ja = fold_index(S.nbr[p], P.n_atoms);
-            const int s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[ja]);
+            const int s = zlookup(P, S.nsp ? (int)S.nsp[p] : S.species[ja], inst);
             const double X = S.xyz[3 * p], Yy = S.xyz[3 * p + 1], Z = S.xyz[3 * p + 2];
             const float x = (float)X, y = (float)Yy, z = (float)Z;
             const float r = sqrtf(x * x + y * y + z * z);
@@ -1075,10 +1099,16 @@ __global__ void __launch_bounds__(32 * soap_tile_warps(TILE), soap_tile_minb(TIL
             atomicAdd(&O.forces[3 * (size_t)ja], (double)fx);
             atomicAdd(&O.forces[3 * (size_t)ja + 1], (double)fy);
             atomicAdd(&O.forces[3 * (size_t)ja + 2], (double)fz);
-            if (O.pair_grad) {   // d E_i / d r_j = -f_pair
-                O.pair_grad[3 * p] = -(double)fx;
-                O.pair_grad[3 * p + 1] = -(double)fy;
-                O.pair_grad[3 * p + 2] = -(double)fz;
+            if (O.pair_grad) {   // d E_i / d r_j = -f_pair (summed over species matches)
+                if constexpr (MULT) {
+                    O.pair_grad[3 * p] -= (double)fx;
+                    O.pair_grad[3 * p + 1] -= (double)fy;
+                    O.pair_grad[3 * p + 2] -= (double)fz;
+                } else {
+                    O.pair_grad[3 * p] = -(double)fx;
+                    O.pair_grad[3 * p + 1] = -(double)fy;
+                    O.pair_grad[3 * p + 2] = -(double)fz;
+                }
             }
             fs[0] -= fx; fs[1] -= fy; fs[2] -= fz;
             // virial += 1/2 (f x + x f), packed xx yy zz xy xz yz
@@ -1723,50 +1753,50 @@ static int resident_warps(K kernel, int threads, size_t smem, int *out) {
     return TG_OK;
 }
 
-template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false, bool MULT = false>
 static int expand_impl(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st) {
     using Sh = DescShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX, TILE, RAW>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_expand<NS, AMAX, LMAX, TILE, RAW, MULT>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     static int resident = 0;   // sites in flight at once: the L2 prefetch distance
     if (!resident)
-        TGB_TRY(resident_warps(k_soap_expand<NS, AMAX, LMAX, TILE, RAW>, 32 * Sh::WARPS, smem,
+        TGB_TRY(resident_warps(k_soap_expand<NS, AMAX, LMAX, TILE, RAW, MULT>, 32 * Sh::WARPS, smem,
                                &resident));
     SiteArgs S2 = S;
     S2.ahead = resident;
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     if (grid > 0)
-        k_soap_expand<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S2, O);
+        k_soap_expand<NS, AMAX, LMAX, TILE, RAW, MULT><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S2, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
 
-template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false>
+template <int NS, int AMAX, int LMAX, int TILE, bool RAW = false, bool MULT = false>
 static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st) {
     using Sh = ForceShape<NS, AMAX, LMAX, TILE>;
     const size_t smem = sizeof(float) * Sh::WARP_FLOATS * Sh::WARPS;
     static bool attr = false;
     if (!attr) {
-        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX, TILE, RAW>,
+        TGB_CUDA(cudaFuncSetAttribute(k_soap_force<NS, AMAX, LMAX, TILE, RAW, MULT>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
     static int resident = 0;   // sites in flight at once: the L2 prefetch distance
     if (!resident)
-        TGB_TRY(resident_warps(k_soap_force<NS, AMAX, LMAX, TILE, RAW>, 32 * Sh::WARPS, smem,
+        TGB_TRY(resident_warps(k_soap_force<NS, AMAX, LMAX, TILE, RAW, MULT>, 32 * Sh::WARPS, smem,
                                &resident));
     ForceIn I2 = I;
     I2.ahead = resident;
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     *nblk = grid;
     if (grid > 0)
-        k_soap_force<NS, AMAX, LMAX, TILE, RAW><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I2, O);
+        k_soap_force<NS, AMAX, LMAX, TILE, RAW, MULT><<<grid, 32 * Sh::WARPS, smem, st>>>(P, S, I2, O);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
@@ -1782,13 +1812,19 @@ static int expand_tiles(const SoapParams &P, const SiteArgs &S, const DescOut &O
     }
 }
 
+// A block with species multiplicity runs tile 0 whatever the tile asked for.
 template <int NS, int AMAX, int LMAX>
 static int expand_tile(const SoapParams &P, const SiteArgs &S, const DescOut &O, cudaStream_t st,
                        int tile) {
-    if (P.raw) {
-        TGB_CHECK(O.praw != nullptr, TG_ERR_ARG, "a compressed block needs DescOut::praw");
-        return expand_tiles<NS, AMAX, LMAX, true>(P, S, O, st, tile);
+    TGB_CHECK(!P.raw || O.praw != nullptr, TG_ERR_ARG, "a compressed block needs DescOut::praw");
+    if (P.n_inst > 1) {
+        if constexpr (NS == 2)
+            return P.raw ? expand_impl<NS, AMAX, LMAX, 0, true, true>(P, S, O, st)
+                         : expand_impl<NS, AMAX, LMAX, 0, false, true>(P, S, O, st);
+        set_error("species multiplicity needs two descriptor species");
+        return TG_ERR_ARG;
     }
+    if (P.raw) return expand_tiles<NS, AMAX, LMAX, true>(P, S, O, st, tile);
     return expand_tiles<NS, AMAX, LMAX, false>(P, S, O, st, tile);
 }
 
@@ -1816,7 +1852,7 @@ static int force_mma_impl(const SoapParams &P, const SiteArgs &S, const ForceIn 
 }
 
 bool soap_force_mma_supported(const SoapParams &P) {
-    return !P.raw && P.amax == 8 && P.lmax == 8 && (P.ns == 1 || P.ns == 2);
+    return !P.raw && P.n_inst == 1 && P.amax == 8 && P.lmax == 8 && (P.ns == 1 || P.ns == 2);
 }
 
 static int launch_soap_force_mma(const SoapParams &P, const SiteArgs &S, const ForceIn &I,
@@ -1844,8 +1880,16 @@ static int force_tiles(const SoapParams &P, const SiteArgs &S, const ForceIn &I,
 template <int NS, int AMAX, int LMAX>
 static int force_tile(const SoapParams &P, const SiteArgs &S, const ForceIn &I, const ForceOut &O,
                       int *nblk, cudaStream_t st, int tile) {
+    TGB_CHECK(P.raw || (I.qoff && P.muf && P.g0f), TG_ERR_ARG,
+              "the force pass needs qoff, muf and g0f");
+    if (P.n_inst > 1) {
+        if constexpr (NS == 2)
+            return P.raw ? force_impl<NS, AMAX, LMAX, 0, true, true>(P, S, I, O, nblk, st)
+                         : force_impl<NS, AMAX, LMAX, 0, false, true>(P, S, I, O, nblk, st);
+        set_error("species multiplicity needs two descriptor species");
+        return TG_ERR_ARG;
+    }
     if (P.raw) return force_tiles<NS, AMAX, LMAX, true>(P, S, I, O, nblk, st, tile);
-    TGB_CHECK(I.qoff && P.muf && P.g0f, TG_ERR_ARG, "the force pass needs qoff, muf and g0f");
     return force_tiles<NS, AMAX, LMAX, false>(P, S, I, O, nblk, st, tile);
 }
 

@@ -38,6 +38,11 @@ struct SoapParams {
     // to fill_to); 0 means the whole row K1. The mixed form writes nsplit 1 and
     // fills to its network's padded input length.
     int fill_to = 0;
+    // Species multiplicity (one global species in two descriptor species of the
+    // block, gap_interface.f90:180-199): zmap2 gives the second match or -1, and
+    // n_inst = 2 makes the pair passes run over the lists once per match.
+    int n_inst = 1;
+    signed char zmap2[kMaxZ];
 };
 
 // Per-launch site addressing: site i reads CSR row site_row[i] of the pair
@@ -130,7 +135,8 @@ struct ForceOut {
     const int *atom_struct = nullptr;
     double *vir_struct = nullptr;   // [n_structs][9]
     // optional (local properties): d E_site / d r_j per pair of the site lists,
-    // (3, P) in list order; the self pair gets d E_site / d r_site
+    // (3, P) in list order; the self pair gets d E_site / d r_site. Under species
+    // multiplicity a pair's matches add into it, so the caller zeroes it first.
     double *pair_grad = nullptr;
 };
 
