@@ -82,8 +82,11 @@ def test_adam_step_matches_oracle(gpu):
     m.close()
 
 
-def test_predict_matches_oracle_ensemble(gpu):
-    D, H, nm = 324, 256, 4
+# layer 2 as: one block-diagonal launch per tile column (H = 256), one dense
+# block-diagonal GEMM (4 x 64 and 2 x 128: every member in one column tile), and
+# one launch per member (4 x 128)
+@pytest.mark.parametrize("D,H,nm", [(324, 256, 4), (324, 64, 4), (1224, 128, 2), (324, 128, 4)])
+def test_predict_matches_oracle_ensemble(gpu, D, H, nm):
     m = gpu.Mlp(D, H, nm, seed=3)
     Dp = m.layout()["Dp"]
     members = [M.Params.random(D, Dp, H, seed=20 + k) for k in range(nm)]
@@ -102,8 +105,13 @@ def test_predict_matches_oracle_ensemble(gpu):
         Es.append(se * E + mu_e)
         Gs.append(se / sx * G[:, :D])
     Es, Gs = np.array(Es), np.array(Gs)
-    assert np.max(np.abs(em - Es.mean(0))) < 2e-4 * se
-    assert np.max(np.abs(es - Es.std(0))) < 2e-4 * se
+    # The oracle rounds to bf16 where the GPU does, so nearly every row agrees to
+    # fp32 accumulation order (about 1e-8). An activation that lands on a bf16
+    # rounding boundary can round the other way and move its row by one bf16 step
+    # of one hidden unit (about 5e-4 here); such rows are rare.
+    de, ds = np.abs(em - Es.mean(0)), np.abs(es - Es.std(0))
+    assert np.mean(de < 1e-5 * se) > 0.98 and np.mean(ds < 1e-5 * se) > 0.98
+    assert de.max() < 2e-3 * se and ds.max() < 2e-3 * se
     assert rel(gm, Gs.mean(0)) < 2e-3
     m.close()
 

@@ -247,7 +247,8 @@ __global__ void k_refresh_infer(const float *__restrict__ P, MlpLayout L, int k,
                                 bf16 *__restrict__ W1Tcat, bf16 *__restrict__ W2cat,
                                 bf16 *__restrict__ W2Tcat, float *__restrict__ b1cat,
                                 float *__restrict__ b2cat, float *__restrict__ w3cat,
-                                float *__restrict__ b3cat) {
+                                float *__restrict__ b3cat, bf16 *__restrict__ W2d,
+                                bf16 *__restrict__ W2Td) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t n1 = (int64_t)L.H * L.Dp, n2 = (int64_t)L.H * L.H;
     const int HH = nm * L.H;
@@ -257,6 +258,10 @@ __global__ void k_refresh_infer(const float *__restrict__ P, MlpLayout L, int k,
         const bf16 v = __float2bfloat16_rn(P[L.oW2 + q]);
         W2cat[((size_t)k * L.H + r) * L.H + c] = v;
         W2Tcat[((size_t)k * L.H + c) * L.H + r] = v;
+        if (W2d) {   // member k's diagonal block; the rest was zeroed
+            W2d[((size_t)k * L.H + r) * HH + k * L.H + c] = v;
+            W2Td[((size_t)k * L.H + c) * HH + k * L.H + r] = v;
+        }
     } else if (i < n1) {
         const int r = (int)(i / L.Dp), c = (int)(i % L.Dp);
         const bf16 v = __float2bfloat16_rn(c < L.D ? P[L.oW1 + i] * inv_sx : 0.f);
@@ -413,6 +418,16 @@ struct MlpTrainWork {
     }
 };
 
+// Layer 2 and its adjoint as one GEMM each over a dense block-diagonal weight
+// (every member's hidden columns in one column tile) when the members' columns
+// are not whole tiles but all of them fit one: one launch instead of one per
+// member, and every epilogue warp busy. The layer-2 epilogue's row partials then
+// come one per 64-column group, H / 64 of them per member.
+static bool mlp_dense_l2(const Mlp &m) {
+    const int HH = m.n_members * m.L.H;
+    return m.L.H % kGemmBN != 0 && HH <= kGemmBN && m.L.H % (kGemmBN / kGemmMlpEpiGroups) == 0;
+}
+
 struct MlpInferWork {
     int cap = 0;
     // binding of the current plans
@@ -425,7 +440,10 @@ struct MlpInferWork {
     Plan p1, p4;
     std::vector<Plan> p2, p3;
 
-    int npart(const Mlp &m) const { return gemm_n_tiles(m.L.H) * kGemmMlpEpiGroups; }
+    int npart(const Mlp &m) const {
+        return mlp_dense_l2(m) ? m.L.H / (kGemmBN / kGemmMlpEpiGroups)
+                               : gemm_n_tiles(m.L.H) * kGemmMlpEpiGroups;
+    }
 
     int ensure(Mlp &m, int rows) {
         if (rows > cap) {
@@ -449,11 +467,24 @@ struct MlpInferWork {
         TGB_TRY(plan_store(p1, HS.p, rows, 2 * HH, 2 * HH));
         // layer 2 and its adjoint: one block-diagonal launch over all members when a
         // member's columns are whole tiles, else one launch per member
-        const bool bd = H % kGemmBN == 0;
-        const int nl = bd ? 1 : nm;
+        const bool bd = H % kGemmBN == 0, dense = mlp_dense_l2(m);
+        const int nl = (bd || dense) ? 1 : nm;
         p2.assign(nl, Plan{});
         p3.assign(nl, Plan{});
-        if (bd) {
+        if (dense) {
+            TGB_TRY(plan(p2[0], HS.p, rows, 2 * HH, m.W2d, HH, HH, HH, nullptr, 0));
+            p2[0].ep.mode = EPI_MLP_L2;
+            p2[0].ep.p0 = m.b2cat;
+            p2[0].ep.p1 = m.w3cat;
+            p2[0].ep.rowpart = part.p;
+            p2[0].ep.rowpart_ld = nm * np;
+            TGB_TRY(plan_store(p2[0], U2.p, rows, HH, HH));
+            TGB_TRY(plan(p3[0], U2.p, rows, HH, m.W2Td, HH, HH, HH, nullptr, 0));
+            p3[0].ep.mode = EPI_MLP_L2B;
+            p3[0].ep.in_b = HS.p + HH;
+            p3[0].ep.ldi = 2 * HH;
+            TGB_TRY(plan_store(p3[0], U1.p, rows, HH, HH));
+        } else if (bd) {
             // the A maps span every member's columns: tile column j reads K range [j H, j H + H)
             TGB_TRY(plan(p2[0], HS.p, rows, 2 * HH, m.W2cat, HH, H, H, nullptr, 0));
             TGB_TRY(make_tma_bf16(&p2[0].a, HS.p, rows, HH, 2 * HH, kGemmBM));
@@ -472,7 +503,7 @@ struct MlpInferWork {
             p3[0].ep.ldi = 2 * HH;
             TGB_TRY(plan_store(p3[0], U1.p, rows, HH, HH));
         }
-        for (int k = 0; k < nm && !bd; ++k) {
+        for (int k = 0; k < nm && !bd && !dense; ++k) {
             TGB_TRY(plan(p2[k], HS.p + k * H, rows, 2 * HH, m.W2b[k], H, H, H, nullptr, 0));
             p2[k].ep.mode = EPI_MLP_L2;
             p2[k].ep.p0 = m.b2cat + k * H;
@@ -536,6 +567,8 @@ int mlp_create(int dim, int hidden, int n_members, unsigned long long seed, Mlp 
     if (rc == TG_OK) rc = dev_alloc(&m->W1Tcat, HH * L.Dp);
     if (rc == TG_OK) rc = dev_alloc(&m->W2cat, HH * L.H);
     if (rc == TG_OK) rc = dev_alloc(&m->W2Tcat, HH * L.H);
+    if (rc == TG_OK && mlp_dense_l2(*m)) rc = dev_alloc(&m->W2d, HH * HH);
+    if (rc == TG_OK && mlp_dense_l2(*m)) rc = dev_alloc(&m->W2Td, HH * HH);
     if (rc == TG_OK) rc = dev_alloc(&m->b1cat, HH);
     if (rc == TG_OK) rc = dev_alloc(&m->b2cat, HH);
     if (rc == TG_OK) rc = dev_alloc(&m->w3cat, HH);
@@ -573,6 +606,7 @@ void mlp_destroy(Mlp *m) {
     for (auto *v : {&m->W1b, &m->W1Tb, &m->W2b, &m->W2Tb})
         for (auto &p : *v) dev_free(p);
     dev_free(m->W1cat); dev_free(m->W1Tcat); dev_free(m->W2cat); dev_free(m->W2Tcat);
+    dev_free(m->W2d); dev_free(m->W2Td);
     dev_free(m->b1cat); dev_free(m->b2cat);
     dev_free(m->w3cat); dev_free(m->b3cat); dev_free(m->dx); dev_free(m->dg); dev_free(m->de);
     dev_free(m->err);
@@ -593,11 +627,16 @@ static int refresh_infer(Mlp &m, cudaStream_t st) {
     const MlpLayout &L = m.L;
     const double sx = m.sx > 0 ? m.sx : 1.0, sE = m.sE > 0 ? m.sE : 1.0;
     const int64_t n = (int64_t)L.H * L.Dp + L.H + (int64_t)L.H * L.H;
+    if (m.W2d) {
+        const size_t hh = (size_t)m.n_members * L.H;
+        TGB_CUDA(cudaMemsetAsync(m.W2d, 0, sizeof(bf16) * hh * hh, st));
+        TGB_CUDA(cudaMemsetAsync(m.W2Td, 0, sizeof(bf16) * hh * hh, st));
+    }
     for (int k = 0; k < m.n_members; ++k) {
         k_refresh_infer<<<blocks_for(n), 256, 0, st>>>(m.P[k], L, k, m.n_members, (float)(1.0 / sx),
                                                        (float)sE, (float)m.muE, m.W1cat, m.W1Tcat,
                                                        m.W2cat, m.W2Tcat, m.b1cat, m.b2cat,
-                                                       m.w3cat, m.b3cat);
+                                                       m.w3cat, m.b3cat, m.W2d, m.W2Td);
         TGB_CUDA(cudaGetLastError());
     }
     m.infer_ready = true;

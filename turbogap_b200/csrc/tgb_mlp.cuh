@@ -53,6 +53,9 @@ struct Mlp {
     // inference weights of all members (refreshed after training / set)
     __nv_bfloat16 *W1cat = nullptr, *W1Tcat = nullptr;   // [nm H][Dp], [Dp][nm H]
     __nv_bfloat16 *W2cat = nullptr, *W2Tcat = nullptr;   // [nm H][H]: W2, W2^T of member k at row k H
+    // [nm H][nm H] block-diagonal W2 and W2^T (zero off the members' blocks), for
+    // ensembles whose hidden layers fit one GEMM column tile (mlp_dense_l2)
+    __nv_bfloat16 *W2d = nullptr, *W2Td = nullptr;
     float *b1cat = nullptr, *b2cat = nullptr, *w3cat = nullptr, *b3cat = nullptr;
     bool infer_ready = false;
     MlpTrainWork *tw = nullptr;

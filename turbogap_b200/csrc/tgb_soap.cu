@@ -1588,12 +1588,15 @@ __global__ void __launch_bounds__(128, 2)
     }
 }
 
+// Grid-strided over the per-CTA partials; every block adds its sums into out
+// (as do the reductions of other blocks' passes into the same virial).
 __global__ void k_virial_reduce(const double *__restrict__ vpart, int nblk, double *out) {
     const int q = threadIdx.y;   // 9 components
     double s = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += 32) s += vpart[(size_t)b * 9 + q];
+    for (int b = blockIdx.x * 32 + threadIdx.x; b < nblk; b += 32 * gridDim.x)
+        s += vpart[(size_t)b * 9 + q];
     s = warp_sum(s);
-    if (threadIdx.x == 0) atomicAdd(out + q, s);   // blocks may reduce concurrently
+    if (threadIdx.x == 0) atomicAdd(out + q, s);
 }
 
 // ===================== SOAP compression =====================================
@@ -1922,7 +1925,9 @@ int launch_soap_force(const SoapParams &P, const SiteArgs &S, const ForceIn &I, 
 
 int launch_virial_reduce(const double *vpart, int nblk, double *virial_out, cudaStream_t st) {
     if (nblk <= 0) return TG_OK;
-    k_virial_reduce<<<1, dim3(32, 9), 0, st>>>(vpart, nblk, virial_out);
+    // about 128 partials per block (four per lane), at most 1024 blocks
+    const int grid = std::min(1024, (nblk + 127) / 128);
+    k_virial_reduce<<<grid, dim3(32, 9), 0, st>>>(vpart, nblk, virial_out);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
