@@ -172,39 +172,44 @@ struct PairSink {
     }
 };
 
-// Cell-list search (neighbors.f90:409-472), one warp per atom: self first, then
-// the cells k3 (z) outer, j3, i3 inner with the reference's skips for 1- and
-// 2-cell axes, each cell in descending atom index. The candidates of the (up to)
-// 27 cells form one flattened sequence in that order; lanes test 32 consecutive
-// candidates at a time and emit the accepted ones in sequence order (ballot +
-// prefix popcount), so the pairs come out exactly in the reference's order.
+// Cell-list search (neighbors.f90:409-472): per atom, self first, then the cells
+// k3 (z) outer, j3, i3 inner with the reference's skips for 1- and 2-cell axes,
+// each cell in descending atom index. The candidates of the (up to) 27 cells form
+// one flattened sequence in that order; lanes test 32 consecutive candidates at a
+// time and emit the accepted ones in sequence order (ballot + prefix popcount),
+// so the pairs come out exactly in the reference's order.
+// One warp per cell: the candidates of the cell's neighbourhood are staged in
+// shared memory once (CAP at a time; a larger neighbourhood is staged again per
+// atom, round by round) and walked for each of the cell's atoms in turn, so their
+// positions and indices are read from global memory once per cell.
 // Three uses, as in the batched search: count (pstart and slots unset), count
 // into slot rows (slots > 0: pair e of site i at row i * slots + e while e <
 // slots, *ovf set past it), and fill at pstart (only when *gate is set, if given).
-__global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box bx, CellGrid g,
-                                double rcut, const int *__restrict__ do_list,
-                                const int *__restrict__ cell_xyz, const int *__restrict__ cell_start,
-                                const int *__restrict__ cell_count,
-                                const int *__restrict__ cell_atoms,
-                                const double *__restrict__ cell_pos, int *__restrict__ n_neigh,
-                                const int64_t *__restrict__ pstart, int64_t cap,
-                                int *__restrict__ nbr, double *__restrict__ rjs,
-                                double *__restrict__ xyz, unsigned *err,
-                                const int *__restrict__ when, int slots = 0,
-                                int *__restrict__ ovf = nullptr,
-                                const int *__restrict__ gate = nullptr) {
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n_sites || (when && !*when) || (gate && !*gate)) return;
+constexpr int kNlCellWarps = 4, kNlCellCap = 256;   // 28 KB of staging per CTA
+
+template <int WARPS, int CAP>
+__global__ void __launch_bounds__(32 * WARPS)
+    k_nl_cells_cell(int ncells, const double *__restrict__ pos, Box bx, CellGrid g, double rcut,
+                    const int *__restrict__ do_list, const int *__restrict__ cell_xyz,
+                    const int *__restrict__ cell_start, const int *__restrict__ cell_count,
+                    const int *__restrict__ cell_atoms, const double *__restrict__ cell_pos,
+                    int *__restrict__ n_neigh, const int64_t *__restrict__ pstart, int64_t cap,
+                    int *__restrict__ nbr, double *__restrict__ rjs, double *__restrict__ xyz,
+                    unsigned *err, const int *__restrict__ when, int slots, int *__restrict__ ovf,
+                    const int *__restrict__ gate) {
+    __shared__ double sx[WARPS][CAP], sy[WARPS][CAP], sz[WARPS][CAP];
+    __shared__ int sk[WARPS][CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int cell = blockIdx.x * WARPS + w;
+    if (cell >= ncells || (when && !*when) || (gate && !*gate)) return;
+    const int na = cell_count[cell];
+    if (na == 0) return;
+    const int c0 = cell_start[cell];
     const bool slotted = !pstart && slots > 0;
     const bool writes = pstart || slotted;
-    if (do_list && !do_list[i]) {
-        if (!pstart && lane == 0) n_neigh[i] = 0;
-        return;
-    }
-    const int i2 = 1 + cell_xyz[3 * i], j2 = 1 + cell_xyz[3 * i + 1], k2 = 1 + cell_xyz[3 * i + 2];
+    const int a0 = cell_atoms[c0];
+    const int i2 = 1 + cell_xyz[3 * a0], j2 = 1 + cell_xyz[3 * a0 + 1], k2 = 1 + cell_xyz[3 * a0 + 2];
     const int mx = g.mx, my = g.my, mz = g.mz;
-    // lane c < 27: cell (k3, j3, i3) = (k2-1 + c/9, j2-1 + (c/3)%3, i2-1 + c%3)
     int cstart = 0, ccount = 0;
     if (lane < 27) {
         const int k3 = k2 - 1 + lane / 9, j3 = j2 - 1 + (lane / 3) % 3, i3 = i2 - 1 + lane % 3;
@@ -218,7 +223,6 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
             ccount = cell_count[c];
         }
     }
-    // inclusive scan of the cell counts over lanes
     int incl = ccount;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -226,83 +230,107 @@ __global__ void k_nl_cells_warp(int n_sites, const double *__restrict__ pos, Box
         if (lane >= o) incl += v;
     }
     const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    const int nround = (total + CAP - 1) / CAP;
     const double rc2 = rcut * rcut, rc2_lo = rc2 * (1.0 - 1e-12), rc2_hi = rc2 * (1.0 + 1e-12);
-    const int64_t base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
-    const int64_t lim = pstart ? cap : base + slots;
-    if (writes && lane == 0) {   // self pair first
-        if (base < lim) {
-            nbr[base] = i;
-            rjs[base] = 0.0;
-            xyz[3 * base] = 0.0;
-            xyz[3 * base + 1] = 0.0;
-            xyz[3 * base + 2] = 0.0;
-        } else {
-            atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+    int staged = -1;   // the round now in shared memory
+    for (int a = 0; a < na; ++a) {
+        const int i = cell_atoms[c0 + a];
+        if (do_list && !do_list[i]) {
+            if (!pstart && lane == 0) n_neigh[i] = 0;
+            continue;
         }
-    }
-    int count = 1;
-    for (int f0 = 0; f0 < total; f0 += 32) {   // warp-uniform trip count
-        const int f = f0 + lane;
-        const int fc = f < total ? f : total - 1;
-        // cell of candidate fc: c = #{cells with incl <= fc}, by fixed-step binary
-        // lifting so that every lane executes every shuffle
-        int c = 0;
-#pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-            const int probe = c + step - 1;
-            const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
-            if (probe < 27 && v <= fc) c += step;
-        }
-        const int cs = __shfl_sync(0xffffffffu, cstart, c);
-        const int before = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, ccount, c);
-        bool take = false;
-        int k = -1;
-        double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
-        if (f < total) {
-            const int slot = cs + (fc - before);
-            k = cell_atoms[slot];
-            if (k != i) {   // the same values from the cell-ordered copy when there is one
-                const double *pk = cell_pos ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
-                // minimum image as get_distance does it (orthorhombic: the cell path);
-                // the squared distance settles every candidate away from the cutoff,
-                // the correctly rounded sqrt decides the rest as the reference does
-                double d2 = 0.0;
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    const double L = bx.L[q];
-                    double v = f_modulo(pk[q] - pi[q], L);
-                    if (v > L / 2.0) v = v - L;
-                    dist[q] = v;
-                    d2 = d2 + v * v;
-                }
-                if (d2 < rc2_lo) {
-                    take = true;
-                    if (writes) d = sqrt(d2);
-                } else if (d2 <= rc2_hi) {
-                    d = sqrt(d2);
-                    take = d < rcut;
-                }
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, take);
-        if (writes && take) {
-            const int64_t p = base + count + __popc(m & ((1u << lane) - 1u));
-            if (p < lim) {
-                nbr[p] = k;
-                rjs[p] = d;
-                xyz[3 * p] = dist[0];
-                xyz[3 * p + 1] = dist[1];
-                xyz[3 * p + 2] = dist[2];
-            } else if (slotted) {
-                *ovf = 1;   // the filling search makes this build
+        const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+        const int64_t base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
+        const int64_t lim = pstart ? cap : base + slots;
+        if (writes && lane == 0) {   // self pair first
+            if (base < lim) {
+                nbr[base] = i;
+                rjs[base] = 0.0;
+                xyz[3 * base] = 0.0;
+                xyz[3 * base + 1] = 0.0;
+                xyz[3 * base + 2] = 0.0;
             } else {
                 atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
             }
         }
-        count += __popc(m);
+        int count = 1;
+        for (int r = 0; r < nround; ++r) {
+            const int f_beg = r * CAP, f_end = min(total, f_beg + CAP);
+            if (staged != r) {
+                __syncwarp();   // every lane is done with the previous round
+                for (int f0 = f_beg; f0 < f_end; f0 += 32) {   // warp-uniform trip count
+                    const int f = f0 + lane;
+                    const int fc = f < f_end ? f : f_end - 1;
+                    int c = 0;   // cell of candidate fc (binary lifting, every lane shuffles)
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int probe = c + step - 1;
+                        const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
+                        if (probe < 27 && v <= fc) c += step;
+                    }
+                    const int cs = __shfl_sync(0xffffffffu, cstart, c);
+                    const int before = __shfl_sync(0xffffffffu, incl, c) -
+                                       __shfl_sync(0xffffffffu, ccount, c);
+                    if (f < f_end) {
+                        const int slot = cs + (fc - before);
+                        const int k = cell_atoms[slot];
+                        const double *pk = cell_pos ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
+                        sk[w][f - f_beg] = k;
+                        sx[w][f - f_beg] = pk[0];
+                        sy[w][f - f_beg] = pk[1];
+                        sz[w][f - f_beg] = pk[2];
+                    }
+                }
+                __syncwarp();
+                staged = r;
+            }
+            for (int f0 = f_beg; f0 < f_end; f0 += 32) {   // warp-uniform trip count
+                const int f = f0 + lane;
+                bool take = false;
+                int k = -1;
+                double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
+                if (f < f_end) {
+                    k = sk[w][f - f_beg];
+                    if (k != i) {
+                        const double pk[3] = {sx[w][f - f_beg], sy[w][f - f_beg], sz[w][f - f_beg]};
+                        double d2 = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            const double L = bx.L[q];
+                            double v = f_modulo(pk[q] - pi[q], L);
+                            if (v > L / 2.0) v = v - L;
+                            dist[q] = v;
+                            d2 = d2 + v * v;
+                        }
+                        if (d2 < rc2_lo) {
+                            take = true;
+                            if (writes) d = sqrt(d2);
+                        } else if (d2 <= rc2_hi) {
+                            d = sqrt(d2);
+                            take = d < rcut;
+                        }
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, take);
+                if (writes && take) {
+                    const int64_t p = base + count + __popc(m & ((1u << lane) - 1u));
+                    if (p < lim) {
+                        nbr[p] = k;
+                        rjs[p] = d;
+                        xyz[3 * p] = dist[0];
+                        xyz[3 * p + 1] = dist[1];
+                        xyz[3 * p + 2] = dist[2];
+                    } else if (slotted) {
+                        *ovf = 1;   // the filling search makes this build
+                    } else {
+                        atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+                    }
+                }
+                count += __popc(m);
+            }
+        }
+        if (!pstart && lane == 0) n_neigh[i] = count;
     }
-    if (!pstart && lane == 0) n_neigh[i] = count;
 }
 
 // Slot rows to the compact arrays (a warp per site), unless a row overflowed.
@@ -777,8 +805,9 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     const int gw = (int)(((int64_t)n_sites * 32 + TB - 1) / TB);   // one warp per site
     const bool one_pass = use_cells && nl.slots > 0 && nl.cap > 0;
     if (one_pass) TGB_CUDA(cudaMemsetAsync(nl.ovf, 0, sizeof(int), st));
+    const int ncells = use_cells ? g.mx * g.my * g.mz : 0;
+    const int gcell = (ncells + kNlCellWarps - 1) / kNlCellWarps;   // one warp per cell
     if (use_cells) {
-        const int ncells = g.mx * g.my * g.mz;
         TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
         TGB_CUDA(cudaMemsetAsync(nl.cell_fill, 0, sizeof(int) * ncells, st));
         k_cell_assign<<<gb, TB, 0, st>>>(n_sites, pos, bx, g, nl.cell_xyz, nl.cell_count, when);
@@ -791,12 +820,11 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
                                                            nl.cell_atoms, when);
         if (nl.cell_pos)
             k_cell_gather_pos<<<gb, TB, 0, st>>>(n_sites, nl.cell_atoms, pos, nl.cell_pos, when);
-        k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                           nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
-                                           nl.n_neigh, nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
-                                           one_pass ? nl.srjs : nullptr,
-                                           one_pass ? nl.sxyz : nullptr, nl.err, when,
-                                           one_pass ? nl.slots : 0, nl.ovf);
+        k_nl_cells_cell<kNlCellWarps, kNlCellCap><<<gcell, 32 * kNlCellWarps, 0, st>>>(
+            ncells, pos, bx, g, rcut, do_list, nl.cell_xyz, nl.cell_start, nl.cell_count,
+            nl.cell_atoms, nl.cell_pos, nl.n_neigh, nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
+            one_pass ? nl.srjs : nullptr, one_pass ? nl.sxyz : nullptr, nl.err, when,
+            one_pass ? nl.slots : 0, nl.ovf, nullptr);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nullptr,
                                       nl.cap, nullptr, nullptr, nullptr, nl.err);
@@ -811,10 +839,10 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
                                             nl.srjs, nl.sxyz, nl.ovf, when, nl.cap, nl.nbr, nl.rjs,
                                             nl.xyz, nl.err);
         // the filling search: always in the two-pass build, after an overflow in the other
-        k_nl_cells_warp<<<gw, TB, 0, st>>>(n_sites, pos, bx, g, rcut, do_list, nl.cell_xyz,
-                                           nl.cell_start, nl.cell_count, nl.cell_atoms, nl.cell_pos,
-                                           nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
-                                           nl.err, when, 0, nullptr, one_pass ? nl.ovf : nullptr);
+        k_nl_cells_cell<kNlCellWarps, kNlCellCap><<<gcell, 32 * kNlCellWarps, 0, st>>>(
+            ncells, pos, bx, g, rcut, do_list, nl.cell_xyz, nl.cell_start, nl.cell_count,
+            nl.cell_atoms, nl.cell_pos, nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.rjs, nl.xyz,
+            nl.err, when, 0, nullptr, one_pass ? nl.ovf : nullptr);
     } else {
         k_nl_brute<<<gb, TB, 0, st>>>(n_sites, n_sc, pos, bx, rcut, do_list, nl.n_neigh, nl.pstart,
                                       nl.cap, nl.nbr, nl.rjs, nl.xyz, nl.err);
