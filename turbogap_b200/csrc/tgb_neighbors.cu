@@ -178,14 +178,65 @@ struct PairSink {
 // one flattened sequence in that order; lanes test 32 consecutive candidates at a
 // time and emit the accepted ones in sequence order (ballot + prefix popcount),
 // so the pairs come out exactly in the reference's order.
-// One warp per cell: the candidates of the cell's neighbourhood are staged in
-// shared memory once (CAP at a time; a larger neighbourhood is staged again per
-// atom, round by round) and walked for each of the cell's atoms in turn, so their
-// positions and indices are read from global memory once per cell.
+// One CTA per cell: its warps stage the candidates of the cell's neighbourhood in
+// shared memory together (CAP at a time), and warp w lists the cell's atoms w,
+// w + WARPS, ... from there, so candidate positions and indices are read from
+// global memory once per cell instead of once per atom.
 // Three uses, as in the batched search: count (pstart and slots unset), count
 // into slot rows (slots > 0: pair e of site i at row i * slots + e while e <
 // slots, *ovf set past it), and fill at pstart (only when *gate is set, if given).
-constexpr int kNlCellWarps = 4, kNlCellCap = 256;   // 28 KB of staging per CTA
+constexpr int kNlCellWarps = 4, kNlCellCap = 256;   // 7 KB of staging per CTA
+
+// The 27 neighbour cells' candidate ranges (lane c < 27) and their inclusive
+// prefix sum over the warp; the flattened candidate f of a warp lies in the cell
+// found by binary lifting over the prefix sums.
+struct CellWalk {
+    int cstart, ccount, incl, total;
+    __device__ __forceinline__ void scan(int lane) {
+        incl = ccount;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        total = __shfl_sync(0xffffffffu, incl, 31);
+    }
+    // slot in cell_atoms of candidate fc (every lane of the warp calls it)
+    __device__ __forceinline__ int slot_of(int fc) const {
+        int c = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            const int probe = c + step - 1;
+            const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
+            if (probe < 27 && v <= fc) c += step;
+        }
+        const int cs = __shfl_sync(0xffffffffu, cstart, c);
+        const int before = __shfl_sync(0xffffffffu, incl, c) - __shfl_sync(0xffffffffu, ccount, c);
+        return cs + (fc - before);
+    }
+};
+
+// Candidates [f_beg, f_end) of the walk into shared memory, warp w taking every
+// WARPS-th group of 32 (positions from the cell-ordered copy when there is one).
+template <int WARPS>
+__device__ __forceinline__ void stage_candidates(const CellWalk &cw, int f_beg, int f_end, int w,
+                                                 int lane, const int *__restrict__ cell_atoms,
+                                                 const double *__restrict__ cell_pos,
+                                                 const double *__restrict__ pos, int *sk,
+                                                 double *sx, double *sy, double *sz) {
+    for (int f0 = f_beg + 32 * w; f0 < f_end; f0 += 32 * WARPS) {   // warp-uniform trip count
+        const int f = f0 + lane;
+        const int slot = cw.slot_of(f < f_end ? f : f_end - 1);
+        if (f < f_end) {
+            const int k = cell_atoms[slot];
+            const double *pk = cell_pos ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
+            sk[f - f_beg] = k;
+            sx[f - f_beg] = pk[0];
+            sy[f - f_beg] = pk[1];
+            sz[f - f_beg] = pk[2];
+        }
+    }
+}
 
 template <int WARPS, int CAP>
 __global__ void __launch_bounds__(32 * WARPS)
@@ -197,10 +248,10 @@ __global__ void __launch_bounds__(32 * WARPS)
                     int *__restrict__ nbr, double *__restrict__ rjs, double *__restrict__ xyz,
                     unsigned *err, const int *__restrict__ when, int slots, int *__restrict__ ovf,
                     const int *__restrict__ gate) {
-    __shared__ double sx[WARPS][CAP], sy[WARPS][CAP], sz[WARPS][CAP];
-    __shared__ int sk[WARPS][CAP];
+    __shared__ double sx[CAP], sy[CAP], sz[CAP];
+    __shared__ int sk[CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int cell = blockIdx.x * WARPS + w;
+    const int cell = blockIdx.x;   // every exit before the loop is CTA-uniform
     if (cell >= ncells || (when && !*when) || (gate && !*gate)) return;
     const int na = cell_count[cell];
     if (na == 0) return;
@@ -210,7 +261,7 @@ __global__ void __launch_bounds__(32 * WARPS)
     const int a0 = cell_atoms[c0];
     const int i2 = 1 + cell_xyz[3 * a0], j2 = 1 + cell_xyz[3 * a0 + 1], k2 = 1 + cell_xyz[3 * a0 + 2];
     const int mx = g.mx, my = g.my, mz = g.mz;
-    int cstart = 0, ccount = 0;
+    CellWalk cw{0, 0, 0, 0};
     if (lane < 27) {
         const int k3 = k2 - 1 + lane / 9, j3 = j2 - 1 + (lane / 3) % 3, i3 = i2 - 1 + lane % 3;
         bool skip = false;
@@ -219,80 +270,62 @@ __global__ void __launch_bounds__(32 * WARPS)
         skip |= (mx == 1 && i3 != 1) || (mx == 2 && i2 == 1 && i3 == 0) || (mx == 2 && i2 == 2 && i3 == 3);
         if (!skip) {
             const int c = imod(i3 - 1, mx) + imod(j3 - 1, my) * mx + imod(k3 - 1, mz) * mx * my;
-            cstart = cell_start[c];
-            ccount = cell_count[c];
+            cw.cstart = cell_start[c];
+            cw.ccount = cell_count[c];
         }
     }
-    int incl = ccount;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    cw.scan(lane);
+    const int total = cw.total;
     const int nround = (total + CAP - 1) / CAP;
     const double rc2 = rcut * rcut, rc2_lo = rc2 * (1.0 - 1e-12), rc2_hi = rc2 * (1.0 + 1e-12);
-    int staged = -1;   // the round now in shared memory
-    for (int a = 0; a < na; ++a) {
-        const int i = cell_atoms[c0 + a];
-        if (do_list && !do_list[i]) {
-            if (!pstart && lane == 0) n_neigh[i] = 0;
-            continue;
-        }
-        const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
-        const int64_t base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
-        const int64_t lim = pstart ? cap : base + slots;
-        if (writes && lane == 0) {   // self pair first
-            if (base < lim) {
-                nbr[base] = i;
-                rjs[base] = 0.0;
-                xyz[3 * base] = 0.0;
-                xyz[3 * base + 1] = 0.0;
-                xyz[3 * base + 2] = 0.0;
-            } else {
-                atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+    if (nround == 1) {
+        stage_candidates<WARPS>(cw, 0, total, w, lane, cell_atoms, cell_pos, pos, sk, sx, sy, sz);
+        __syncthreads();
+    }
+    for (int ag = 0; ag < na; ag += WARPS) {   // CTA-uniform trip count
+        const int a = ag + w;
+        const int i = a < na ? cell_atoms[c0 + a] : -1;
+        const bool listed = i >= 0 && !(do_list && !do_list[i]);   // warp-uniform
+        if (i >= 0 && !listed && !pstart && lane == 0) n_neigh[i] = 0;
+        double pi[3] = {0.0, 0.0, 0.0};
+        int64_t base = 0, lim = 0;
+        if (listed) {
+            pi[0] = pos[3 * (size_t)i];
+            pi[1] = pos[3 * (size_t)i + 1];
+            pi[2] = pos[3 * (size_t)i + 2];
+            base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
+            lim = pstart ? cap : base + slots;
+            if (writes && lane == 0) {   // self pair first
+                if (base < lim) {
+                    nbr[base] = i;
+                    rjs[base] = 0.0;
+                    xyz[3 * base] = 0.0;
+                    xyz[3 * base + 1] = 0.0;
+                    xyz[3 * base + 2] = 0.0;
+                } else {
+                    atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+                }
             }
         }
         int count = 1;
-        for (int r = 0; r < nround; ++r) {
+        for (int r = 0; r < nround; ++r) {   // CTA-uniform trip count
             const int f_beg = r * CAP, f_end = min(total, f_beg + CAP);
-            if (staged != r) {
-                __syncwarp();   // every lane is done with the previous round
-                for (int f0 = f_beg; f0 < f_end; f0 += 32) {   // warp-uniform trip count
-                    const int f = f0 + lane;
-                    const int fc = f < f_end ? f : f_end - 1;
-                    int c = 0;   // cell of candidate fc (binary lifting, every lane shuffles)
-#pragma unroll
-                    for (int step = 16; step >= 1; step >>= 1) {
-                        const int probe = c + step - 1;
-                        const int v = __shfl_sync(0xffffffffu, incl, probe < 31 ? probe : 31);
-                        if (probe < 27 && v <= fc) c += step;
-                    }
-                    const int cs = __shfl_sync(0xffffffffu, cstart, c);
-                    const int before = __shfl_sync(0xffffffffu, incl, c) -
-                                       __shfl_sync(0xffffffffu, ccount, c);
-                    if (f < f_end) {
-                        const int slot = cs + (fc - before);
-                        const int k = cell_atoms[slot];
-                        const double *pk = cell_pos ? cell_pos + 3 * (size_t)slot : pos + 3 * (size_t)k;
-                        sk[w][f - f_beg] = k;
-                        sx[w][f - f_beg] = pk[0];
-                        sy[w][f - f_beg] = pk[1];
-                        sz[w][f - f_beg] = pk[2];
-                    }
-                }
-                __syncwarp();
-                staged = r;
+            if (nround > 1) {   // a large neighbourhood: staged again, round by round
+                __syncthreads();   // every warp is done with the previous round
+                stage_candidates<WARPS>(cw, f_beg, f_end, w, lane, cell_atoms, cell_pos, pos, sk, sx,
+                                        sy, sz);
+                __syncthreads();
             }
+            if (!listed) continue;
             for (int f0 = f_beg; f0 < f_end; f0 += 32) {   // warp-uniform trip count
                 const int f = f0 + lane;
                 bool take = false;
                 int k = -1;
                 double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
                 if (f < f_end) {
-                    k = sk[w][f - f_beg];
+                    k = sk[f - f_beg];
                     if (k != i) {
-                        const double pk[3] = {sx[w][f - f_beg], sy[w][f - f_beg], sz[w][f - f_beg]};
+                        const double pk[3] = {sx[f - f_beg], sy[f - f_beg], sz[f - f_beg]};
                         double d2 = 0.0;
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
@@ -329,7 +362,7 @@ __global__ void __launch_bounds__(32 * WARPS)
                 count += __popc(m);
             }
         }
-        if (!pstart && lane == 0) n_neigh[i] = count;
+        if (listed && !pstart && lane == 0) n_neigh[i] = count;
     }
 }
 
@@ -806,7 +839,7 @@ int nl_build(NeighborList &nl, int n_sites, int n_sc, const double *pos, const B
     const bool one_pass = use_cells && nl.slots > 0 && nl.cap > 0;
     if (one_pass) TGB_CUDA(cudaMemsetAsync(nl.ovf, 0, sizeof(int), st));
     const int ncells = use_cells ? g.mx * g.my * g.mz : 0;
-    const int gcell = (ncells + kNlCellWarps - 1) / kNlCellWarps;   // one warp per cell
+    const int gcell = ncells;   // one CTA per cell
     if (use_cells) {
         TGB_CUDA(cudaMemsetAsync(nl.cell_count, 0, sizeof(int) * ncells, st));
         TGB_CUDA(cudaMemsetAsync(nl.cell_fill, 0, sizeof(int) * ncells, st));
@@ -935,7 +968,7 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
                            double rcut, int *__restrict__ n_neigh,
                            const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
                            double *__restrict__ xyz, unsigned *err, int slots,
-                           int *__restrict__ ovf, const int *__restrict__ gate) {
+                           int *__restrict__ ovf, const int *__restrict__ gate, int skip_cells) {
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= n || (gate && !*gate)) return;
@@ -943,6 +976,7 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
     const bool slotted = !pstart && slots > 0;
     const bool writes = pstart || slotted;
     const BatchStruct b = st[atom_struct[i]];
+    if (skip_cells && b.mode == 0) return;   // k_bnl_cell lists the atoms of cell structures
     const double pi[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
     const double invL[3] = {1.0 / b.L[0], 1.0 / b.L[1], 1.0 / b.L[2]};
     // candidate segments: lane c < 27 describes cell c (mode 0); mode 1 has one
@@ -1046,6 +1080,121 @@ __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStr
     if (!pstart && lane == 0) n_neigh[i] = count;
 }
 
+// The cell structures' atoms by cell: one CTA per cell stages the candidates of
+// the cell's 27-cell neighbourhood (the walk order of k_bnl_warp) in shared memory,
+// CAP at a time, and warp w lists the cell's atoms w, w + WARPS, ... from there,
+// with the tests and the three uses of k_bnl_warp.
+template <int WARPS, int CAP>
+__global__ void __launch_bounds__(32 * WARPS)
+    k_bnl_cell(int n_cells, const double *__restrict__ pos, const BatchStruct *__restrict__ st,
+               const int *__restrict__ atom_struct, const int *__restrict__ cell_start,
+               const int *__restrict__ cell_count, const int *__restrict__ cell_atoms,
+               const double *__restrict__ cell_pos, double rcut, int *__restrict__ n_neigh,
+               const int64_t *__restrict__ pstart, int64_t cap, int *__restrict__ nbr,
+               double *__restrict__ xyz, unsigned *err, int slots, int *__restrict__ ovf,
+               const int *__restrict__ gate) {
+    __shared__ double sx[CAP], sy[CAP], sz[CAP];
+    __shared__ int sk[CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int cell = blockIdx.x;   // every exit before the loop is CTA-uniform
+    if (cell >= n_cells || (gate && !*gate)) return;
+    const int na = cell_count[cell];
+    if (na == 0) return;
+    const int c0 = cell_start[cell];
+    const bool slotted = !pstart && slots > 0;
+    const bool writes = pstart || slotted;
+    const BatchStruct b = st[atom_struct[cell_atoms[c0]]];
+    const double invL[3] = {1.0 / b.L[0], 1.0 / b.L[1], 1.0 / b.L[2]};
+    CellWalk cw{0, 0, 0, 0};
+    if (lane < 27) {
+        const int ci = cell - b.coff;
+        const int cx = ci / (b.m[1] * b.m[2]), cy = (ci / b.m[2]) % b.m[1], cz = ci % b.m[2];
+        const int x = (cx + lane / 9 - 1 + b.m[0]) % b.m[0];
+        const int y = (cy + (lane / 3) % 3 - 1 + b.m[1]) % b.m[1];
+        const int z = (cz + lane % 3 - 1 + b.m[2]) % b.m[2];
+        const int c = b.coff + (x * b.m[1] + y) * b.m[2] + z;
+        cw.cstart = cell_start[c];
+        cw.ccount = cell_count[c];
+    }
+    cw.scan(lane);
+    const int total = cw.total;
+    const int nround = (total + CAP - 1) / CAP;
+    const double rc2 = rcut * rcut;
+    if (nround == 1) {
+        stage_candidates<WARPS>(cw, 0, total, w, lane, cell_atoms, cell_pos, pos, sk, sx, sy, sz);
+        __syncthreads();
+    }
+    for (int ag = 0; ag < na; ag += WARPS) {   // CTA-uniform trip count
+        const int a = ag + w;
+        const int i = a < na ? cell_atoms[c0 + a] : -1;   // warp-uniform
+        double pi[3] = {0.0, 0.0, 0.0};
+        int64_t base = 0, lim = 0;
+        if (i >= 0) {
+            pi[0] = pos[3 * (size_t)i];
+            pi[1] = pos[3 * (size_t)i + 1];
+            pi[2] = pos[3 * (size_t)i + 2];
+            base = pstart ? pstart[i] : (slotted ? (int64_t)i * slots : 0);
+            lim = pstart ? cap : base + slots;
+            if (writes && lane == 0) {   // self pair first
+                if (base < lim) {
+                    nbr[base] = i;
+                    xyz[3 * base] = 0.0;
+                    xyz[3 * base + 1] = 0.0;
+                    xyz[3 * base + 2] = 0.0;
+                } else {
+                    atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+                }
+            }
+        }
+        int count = 1;
+        for (int r = 0; r < nround; ++r) {   // CTA-uniform trip count
+            const int f_beg = r * CAP, f_end = min(total, f_beg + CAP);
+            if (nround > 1) {   // a large neighbourhood: staged again, round by round
+                __syncthreads();   // every warp is done with the previous round
+                stage_candidates<WARPS>(cw, f_beg, f_end, w, lane, cell_atoms, cell_pos, pos, sk, sx,
+                                        sy, sz);
+                __syncthreads();
+            }
+            if (i < 0) continue;
+            for (int f0 = f_beg; f0 < f_end; f0 += 32) {   // warp-uniform trip count
+                const int f = f0 + lane;
+                bool take = false;
+                int k = -1;
+                double dist[3] = {0.0, 0.0, 0.0};
+                if (f < f_end) {
+                    k = sk[f - f_beg];
+                    const double pk[3] = {sx[f - f_beg], sy[f - f_beg], sz[f - f_beg]};
+                    double d2 = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        double v = pk[q] - pi[q];
+                        v -= b.L[q] * rint(v * invL[q]);   // minimum image, as in k_bnl_warp
+                        dist[q] = v;
+                        d2 += v * v;
+                    }
+                    take = k != i && d2 < rc2;
+                }
+                const unsigned msk = __ballot_sync(0xffffffffu, take);
+                if (writes && take) {
+                    const int64_t p = base + count + __popc(msk & ((1u << lane) - 1u));
+                    if (p < lim) {
+                        nbr[p] = k;
+                        xyz[3 * p] = dist[0];
+                        xyz[3 * p + 1] = dist[1];
+                        xyz[3 * p + 2] = dist[2];
+                    } else if (slotted) {
+                        *ovf = 1;   // the fallback search fills this build
+                    } else {
+                        atomicOr(err, (unsigned)DEV_ERR_NEIGH_CAPACITY);
+                    }
+                }
+                count += __popc(msk);
+            }
+        }
+        if (i >= 0 && !pstart && lane == 0) n_neigh[i] = count;
+    }
+}
+
 // Slot rows to the compact arrays (a warp per atom), unless a row overflowed.
 __global__ void k_bnl_compact(int n, int slots, const int *__restrict__ n_neigh,
                               const int64_t *__restrict__ pstart, const int *__restrict__ snbr,
@@ -1087,11 +1236,18 @@ int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st)
     }
     const bool one_pass = nl.slots > 0 && nl.cap > 0;
     if (one_pass) TGB_CUDA(cudaMemsetAsync(nl.ovf, 0, sizeof(int), st));
+    // atoms of cell structures by cell, the others (images) by atom
+    const int gcell = nl.n_cells;   // one CTA per cell
+    if (nl.n_cells > 0)
+        k_bnl_cell<kNlCellWarps, kNlCellCap><<<gcell, 32 * kNlCellWarps, 0, st>>>(
+            nl.n_cells, pos, nl.st, nl.atom_struct, nl.cell_start, nl.cell_count, nl.cell_atoms,
+            nl.cell_pos, rcut, nl.n_neigh, nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
+            one_pass ? nl.sxyz : nullptr, nl.err, one_pass ? nl.slots : 0, nl.ovf, nullptr);
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
                                   nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
                                   nullptr, nl.cap, one_pass ? nl.snbr : nullptr,
                                   one_pass ? nl.sxyz : nullptr, nl.err, one_pass ? nl.slots : 0,
-                                  nl.ovf, nullptr);
+                                  nl.ovf, nullptr, nl.n_cells > 0);
     k_pstart_zero<<<1, 1, 0, st>>>(nl.pstart);
     size_t bytes = nl.scan_bytes;
     TGB_CUDA(cub::DeviceScan::InclusiveSum(nl.scan_tmp, bytes, nl.n_neigh, nl.pstart + 1, n, st));
@@ -1099,10 +1255,15 @@ int batch_nl_build(BatchNL &nl, const double *pos, double rcut, cudaStream_t st)
         k_bnl_compact<<<gw, TB, 0, st>>>(n, nl.slots, nl.n_neigh, nl.pstart, nl.snbr, nl.sxyz,
                                          nl.ovf, nl.cap, nl.nbr, nl.xyz, nl.err);
     // the filling search: always in the two-pass build, after an overflow in the other
+    if (nl.n_cells > 0)
+        k_bnl_cell<kNlCellWarps, kNlCellCap><<<gcell, 32 * kNlCellWarps, 0, st>>>(
+            nl.n_cells, pos, nl.st, nl.atom_struct, nl.cell_start, nl.cell_count, nl.cell_atoms,
+            nl.cell_pos, rcut, nl.n_neigh, nl.pstart, nl.cap, nl.nbr, nl.xyz, nl.err, 0, nullptr,
+            one_pass ? nl.ovf : nullptr);
     k_bnl_warp<<<gw, TB, 0, st>>>(n, pos, nl.st, nl.atom_struct, nl.cell_id, nl.cell_start,
                                   nl.cell_count, nl.cell_atoms, nl.cell_pos, rcut, nl.n_neigh,
                                   nl.pstart, nl.cap, nl.nbr, nl.xyz, nl.err, 0, nullptr,
-                                  one_pass ? nl.ovf : nullptr);
+                                  one_pass ? nl.ovf : nullptr, nl.n_cells > 0);
     TGB_CUDA(cudaGetLastError());
     return TG_OK;
 }
