@@ -39,12 +39,14 @@ def test_site_range_shares_sum_to_whole(gpu, ch):
     assert np.abs(e - eo).max() < 1e-6 and np.abs(f - fo).max() < 1e-6
     for world in (2, 3):
         es, fs, vs = np.zeros_like(e), np.zeros_like(f), np.zeros_like(v)
+        pairs = 0
         for rank in range(world):
             beg, end = site_range(st.n, world, rank)
             eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [301, 302],
                              e0_by_species=e0)
             eng.set_site_range(beg, end)
             er, fr, vr = eng.compute()
+            pairs += eng.n_pairs()   # each rank lists its own sites only
             assert np.all(er[:beg] == 0.0) and np.all(er[end:] == 0.0)
             # the oracle computes the same share (its site_range argument)
             eq, fq, vq, _ = O.evaluate(st.positions, st.species, st.box, list(ch), e0=e0,
@@ -54,6 +56,7 @@ def test_site_range_shares_sum_to_whole(gpu, ch):
             fs += fr
             vs += vr
             eng.close()
+        assert pairs == full.n_pairs()
         assert np.abs(es - e).max() < 1e-9
         assert np.abs(fs - f).max() < 1e-9
         assert np.abs(vs - v).max() < 1e-9 * np.abs(v).max()

@@ -455,18 +455,19 @@ int autotune_block(Block &b, Workspace &w, const SiteArgs &S, int n_atoms, doubl
 // one thread per site: MLP sites get epart = E / delta^2 and kdsum = 0 (their g
 // rows already hold dE/dq - g0, so that the force pass's g0 + g is the MLP's
 // dE/dq); gated sites are appended to gidx
+// One thread per (row, energy tile), so the stores of consecutive threads are
+// consecutive; the thread of tile 0 also gates its row.
 __global__ void k_mlp_mix(int n, int n_et, const double *__restrict__ emean,
                           const double *__restrict__ estd, double gate, double inv_delta2,
                           double *__restrict__ epart, double *__restrict__ kdsum,
                           int *__restrict__ gidx, int *__restrict__ gcount) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= n) return;
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)n * n_et) return;
+    const int row = (int)(e / n_et), t = (int)(e - (size_t)row * n_et);
     const bool gated = !(estd[row] <= gate);   // a NaN spread is gated too
-    if (gated) gidx[atomicAdd(gcount, 1)] = row;
-    for (int t = 0; t < n_et; ++t) {
-        epart[(size_t)row * n_et + t] = (!gated && t == 0) ? emean[row] * inv_delta2 : 0.0;
-        kdsum[(size_t)row * n_et + t] = 0.0;
-    }
+    if (gated && t == 0) gidx[atomicAdd(gcount, 1)] = row;
+    epart[e] = (!gated && t == 0) ? emean[row] * inv_delta2 : 0.0;
+    kdsum[e] = 0.0;
 }
 
 // compacted GEMM-1 operand rows of the gated sites and their delta.mu. The mixed
@@ -592,9 +593,9 @@ int evaluate_block_mixed(Block &b, Workspace &w, MixedRun &x, const SiteArgs &S,
     TGB_TRY(mlp_infer(*x.mlp, *x.iw, n, w.qsplit.p, b.K1, x.emean.p, x.estd.p, w.g.p, b.dim,
                       b.g0f.p, st));
     TGB_CUDA(cudaMemsetAsync(x.gcount.p, 0, sizeof(int), st));
-    k_mlp_mix<<<grid_for(n), 256, 0, st>>>(n, b.n_etiles, x.emean.p, x.estd.p, x.gate,
-                                           1.0 / (b.delta * b.delta), w.epart.p, w.kdsum.p,
-                                           x.gidx.p, x.gcount.p);
+    k_mlp_mix<<<grid_for((int64_t)n * b.n_etiles), 256, 0, st>>>(
+        n, b.n_etiles, x.emean.p, x.estd.p, x.gate, 1.0 / (b.delta * b.delta), w.epart.p, w.kdsum.p,
+        x.gidx.p, x.gcount.p);
     const unsigned gg = (unsigned)std::min(n, 1184);   // grid-stride over the gated rows
     k_gather_gated<<<gg, 128, 0, st>>>(x.gcount.p, x.gidx.p, b.dim, b.K1, b.nsplit, w.q.p,
                                       w.qoff.p, x.Qg.p, x.qoff_g.p);
@@ -1604,6 +1605,10 @@ struct Engine {
     DBuf<long long> nl_counts;           // rebuilds, evaluations
     std::vector<int> species_h;          // host copy, for the site lists
     int site_beg = 0, site_end = 0;      // central sites of this rank
+    // a rank's share of a sharded structure lists its own sites only: list flags
+    // (1 inside [site_beg, site_end)) for the neighbour search, unset for the whole
+    DBuf<int> do_list;
+    bool ranged = false;
     Comm *comm = nullptr;                // set: forces/energies/virial summed over ranks
     bool frame_prev = false;    // the last evaluation saw pos_prev (an MD step ran)
     double dt_prev = 0.0;
@@ -1652,12 +1657,13 @@ struct Engine {
         if (skin) {
             // neighbors_buffer > 0: rebuild only when the previous step asked for it,
             // otherwise refresh the kept pairs (decided on the device, inside the graph)
-            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st, nl_when.p));
+            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, ranged ? do_list.p : nullptr,
+                             st, nl_when.p));
             TGB_TRY(launch_nl_refresh(n, p, box, nl, nl_when.p, st));
             TGB_TRY(launch_skin_reset(n, nl_when.p, disp.p, nl_counts.p, st));
             TGB_CUDA(cudaMemsetAsync(nl_when.p, 0, sizeof(int), st));
         } else {
-            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, nullptr, st));
+            TGB_TRY(nl_build(nl, n, nsc, p, box, g, use_cells, rcut, ranged ? do_list.p : nullptr, st));
         }
         TGB_TRY(launch_pair_species(n, nl, species.p, n, st));
         TGB_MARK(log, PASS_NEIGH, st);
@@ -1703,6 +1709,13 @@ struct Engine {
     // central sites of each block within [site_beg, site_end); species never
     // change during MD
     int assign_sites() {
+        ranged = site_beg > 0 || site_end < n;
+        if (ranged) {
+            std::vector<int> flags(n, 0);
+            for (int i = site_beg; i < site_end; ++i) flags[i] = 1;
+            TGB_TRY(do_list.ensure(n));
+            TGB_CUDA(cudaMemcpyAsync(do_list.p, flags.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        }
         for (auto &run : runs) {
             const Block *b = run->b;
             std::vector<int> s;
