@@ -48,7 +48,9 @@ enum {
  * as filled by read_gap_hypers, src/read_files.f90:4633-5236). Per-species arrays
  * hold n_species entries; rcut_soft is rcut_hard - buffer (read_files.f90:5101-5108).
  * species_z[s] is the global species id (1-based position in the input deck's
- * species_types) that descriptor species s stands for. */
+ * species_types) that descriptor species s stands for. One id may appear twice
+ * (species multiplicity, gap_interface.f90:180-199): its atoms then feed both
+ * descriptor species, each with its own hyperparameters. */
 typedef struct {
     int32_t n_species;
     int32_t l_max;
