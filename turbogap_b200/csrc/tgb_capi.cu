@@ -10,6 +10,7 @@
 #include "tgb_soap.cuh"
 
 #include <cub/device/device_scan.cuh>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdlib>
@@ -244,6 +245,16 @@ __global__ void k_prep_alpha(const double *__restrict__ al, int M, int Mpad,
 // on the stream; the time since the previous mark is booked to that pass.
 enum Pass {
     PASS_NEIGH = 0, PASS_DESC, PASS_GEMM1, PASS_GEMM2, PASS_FORCE, PASS_INTEGRATE, PASS_MLP, N_PASS
+};
+
+// A host-side NVTX range over one C-ABI call, so that a profiler's timeline
+// (ncu --nvtx, nsys) shows which entry point launched which kernels. NVTX v3 is
+// header-only: without a tool attached a range costs a few nanoseconds.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 struct EventLog {
@@ -817,6 +828,7 @@ static int upload_compression(Block &b, const tg_soap_hypers &h) {
 
 int tg_soap_begin(int32_t block_key, const tg_soap_hypers *h, int32_t n_sparse, const double *Qs,
                   const double *alphas, double delta, double zeta, int32_t precision) {
+    NvtxRange nvtx_range("tg_soap_begin");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(!C.families.count(block_key), TG_ERR_ARG, "key %d already names a 2b/3b/core_pot family",
@@ -1175,6 +1187,7 @@ int tg_get_gap_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_ne
                     const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                     const int32_t *species_batch, const int32_t *species_all, double *energies0,
                     double *forces0, double *virial) {
+    NvtxRange nvtx_range("tg_get_gap_soap");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
@@ -1246,6 +1259,7 @@ int tg_family_begin(int32_t key, const tg_family *family) {
 int tg_get_family(int32_t key, int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0,
                   const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                   const int32_t *species_all, double *energies0, double *forces0, double *virial) {
+    NvtxRange nvtx_range("tg_get_family");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     auto fi = C.families.find(key);
@@ -1359,6 +1373,7 @@ int tg_get_local_property(int32_t n_total_sites, int32_t n_sites0, const int32_t
                           const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                           const int32_t *species_batch, const int32_t *species_all, double v0,
                           double *values, double *value_der, int32_t *n_central) {
+    NvtxRange nvtx_range("tg_get_local_property");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
@@ -1393,6 +1408,7 @@ int tg_get_soap_dipole(int32_t n_total_sites, int32_t n_sites0, const int32_t *n
                        const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                        const int32_t *species_batch, const int32_t *species_all, double *dipoles,
                        double *energies, int32_t *n_central) {
+    NvtxRange nvtx_range("tg_get_soap_dipole");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
@@ -1423,6 +1439,7 @@ int tg_get_soap(int32_t n_total_sites, int32_t n_sites0, const int32_t *n_neigh0
                 const int32_t *neighbors_list0, const double *rjs0, const double *xyz0,
                 const int32_t *species_batch, const int32_t *species_all, double *soap,
                 int32_t *n_central) {
+    NvtxRange nvtx_range("tg_get_soap");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(C.current, TG_ERR_STATE, "no block is open (call tg_soap_begin first)");
@@ -1459,6 +1476,7 @@ int tg_build_neighbors_list(int32_t n_sites_supercell, const double *positions, 
                             const int32_t *do_list, int64_t cap, int32_t *n_neigh,
                             int32_t *neighbors_list, double *rjs, double *thetas, double *phis,
                             double *xyz, int32_t *neighbor_species, int64_t *n_pairs) {
+    NvtxRange nvtx_range("tg_build_neighbors_list");
     TGB_TRY(need_ctx());
     Context &C = *g_ctx;
     TGB_CHECK(n_sites >= 1 && n_sites_supercell >= n_sites, TG_ERR_ARG, "bad site counts");
@@ -1807,6 +1825,7 @@ int tg_engine_create(int32_t n_atoms, const double *positions, const int32_t *sp
                      const double *c_box, int32_t n_blocks, const int32_t *block_keys,
                      const double *e0_by_species, int32_t n_species_total, double neighbors_buffer,
                      tg_engine **out) {
+    NvtxRange nvtx_range("tg_engine_create");
     TGB_TRY(need_ctx());
     TGB_CHECK(out && n_atoms >= 1 && n_blocks >= 1, TG_ERR_ARG, "bad engine arguments");
     Context &C = *g_ctx;
@@ -1964,12 +1983,14 @@ static int engine_errors(Engine &E) {
 }
 
 int tg_engine_compute_device(tg_engine *eh) {
+    NvtxRange nvtx_range("tg_engine_compute_device");
     TGB_CHECK(eh, TG_ERR_ARG, "null engine");
     eh->e.frame_prev = false;
     return eh->e.compute_ef();
 }
 
 int tg_engine_compute(tg_engine *eh, double *energies, double *forces, double *virial) {
+    NvtxRange nvtx_range("tg_engine_compute");
     TGB_CHECK(eh, TG_ERR_ARG, "null engine");
     Engine &E = eh->e;
     E.frame_prev = false;
@@ -1984,6 +2005,7 @@ int tg_engine_compute(tg_engine *eh, double *energies, double *forces, double *v
 }
 
 int tg_engine_md(tg_engine *eh, int32_t n_steps, double dt, double *e_pot, double *e_kin) {
+    NvtxRange nvtx_range("tg_engine_md");
     TGB_CHECK(eh, TG_ERR_ARG, "null engine");
     Engine &E = eh->e;
     for (int s = 0; s < n_steps; ++s) {
@@ -2127,6 +2149,7 @@ int tg_engine_n_pairs(tg_engine *eh, int64_t *n_pairs) {
 
 int tg_engine_profile(tg_engine *eh, int32_t n_steps, double dt, double *ms_per_pass,
                       int32_t *n_passes) {
+    NvtxRange nvtx_range("tg_engine_profile");
     TGB_CHECK(eh && ms_per_pass && n_steps >= 1, TG_ERR_ARG, "bad profile arguments");
     Engine &E = eh->e;
     double acc[N_PASS] = {0};
@@ -2258,6 +2281,7 @@ int tg_mlp_add_samples(tg_mlp *h, int32_t n, const float *delta, const double *e
 }
 
 int tg_mlp_add_engine_samples(tg_mlp *h, tg_engine *eh, int32_t block) {
+    NvtxRange nvtx_range("tg_mlp_add_engine_samples");
     TGB_CHECK(h && eh, TG_ERR_ARG, "null argument");
     Engine &E = eh->e;
     TGB_CHECK(block >= 0 && block < (int)E.runs.size(), TG_ERR_ARG, "block %d out of range", block);
@@ -2292,6 +2316,7 @@ int tg_mlp_n_samples(tg_mlp *h, int64_t *n) {
 
 int tg_mlp_train(tg_mlp *h, int32_t epochs, int32_t batch, double lr, double force_weight,
                  uint64_t seed, double *loss_per_epoch) {
+    NvtxRange nvtx_range("tg_mlp_train");
     TGB_TRY(need_ctx());
     TGB_CHECK(h, TG_ERR_ARG, "null MLP");
     return mlp_train(*h->m, epochs, batch, lr, force_weight, (unsigned long long)seed,
@@ -2309,6 +2334,7 @@ __global__ void k_rows_to_bf16(int n, int D, int Dp, const float *__restrict__ x
 
 int tg_mlp_predict(tg_mlp *h, int32_t n, const float *delta, double *energy_mean,
                    double *energy_std, double *dedq_mean) {
+    NvtxRange nvtx_range("tg_mlp_predict");
     TGB_TRY(need_ctx());
     TGB_CHECK(h && n >= 0 && (n == 0 || (delta && energy_mean)), TG_ERR_ARG, "bad arguments");
     if (n == 0) return TG_OK;
@@ -2526,6 +2552,7 @@ int tg_batch_create(int32_t n_structs, const int32_t *n_atoms, const double *pos
                     const int32_t *species, const double *boxes, int32_t n_blocks,
                     const int32_t *block_keys, const double *e0_by_species,
                     int32_t n_species_total, tg_batch **out) {
+    NvtxRange nvtx_range("tg_batch_create");
     TGB_TRY(need_ctx());
     TGB_CHECK(out && n_structs >= 1 && n_atoms && positions && species && boxes && n_blocks >= 1 &&
                   block_keys,
@@ -2657,6 +2684,7 @@ int tg_batch_set_positions(tg_batch *bh, const double *positions) {
 // Evaluation without copies out: the first call runs eagerly, later calls replay
 // one CUDA graph of the whole evaluation.
 int tg_batch_compute_device(tg_batch *bh) {
+    NvtxRange nvtx_range("tg_batch_compute_device");
     TGB_CHECK(bh, TG_ERR_ARG, "null batch");
     BatchEngine &E = bh->e;
     if (!E.graph) {
@@ -2678,6 +2706,7 @@ int tg_batch_compute_device(tg_batch *bh) {
 }
 
 int tg_batch_compute(tg_batch *bh, double *energies, double *forces, double *virials) {
+    NvtxRange nvtx_range("tg_batch_compute");
     TGB_CHECK(bh, TG_ERR_ARG, "null batch");
     BatchEngine &E = bh->e;
     TGB_TRY(tg_batch_compute_device(bh));
@@ -2699,6 +2728,7 @@ int tg_batch_stream(tg_batch *bh, void **stream) {
 }
 
 int tg_batch_profile(tg_batch *bh, int32_t n_evals, double *ms_per_pass, int32_t *n_passes) {
+    NvtxRange nvtx_range("tg_batch_profile");
     TGB_CHECK(bh && ms_per_pass && n_evals >= 1, TG_ERR_ARG, "bad profile arguments");
     BatchEngine &E = bh->e;
     double acc[N_PASS] = {0};
