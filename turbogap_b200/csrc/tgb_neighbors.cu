@@ -961,6 +961,8 @@ __global__ void k_bcell_sort(int ncells, const int *__restrict__ cell_start,
 // Three uses: count (pstart and slots unset), count into slot rows (slots > 0:
 // pair e of atom i at row i * slots + e while e < slots, *ovf set past it), and
 // fill the compact arrays at pstart (run only when *gate is set, if gate given).
+// With skip_cells set it lists only the atoms of image structures; k_bnl_cell
+// lists those of the cell structures.
 __global__ void k_bnl_warp(int n, const double *__restrict__ pos, const BatchStruct *__restrict__ st,
                            const int *__restrict__ atom_struct, const int *__restrict__ cell_id,
                            const int *__restrict__ cell_start, const int *__restrict__ cell_count,
