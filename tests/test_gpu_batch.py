@@ -70,3 +70,27 @@ def test_batch_list_builds_agree(gpu, monkeypatch, slots):
         assert np.max(np.abs(v - v1)) < 1e-9
     bat.close()
 
+
+
+def test_batch_dense_cell_rounds(gpu):
+    """A cell structure dense enough (0.25 atoms/A^3, 4 cells per axis) that each
+    cell's neighbourhood exceeds the 256 candidates the search stages at once,
+    batched with a small one: per-structure parity with the oracle."""
+    h = carbon_hypers()
+    blk = sparse_block(h, 300, seed=41)
+    gpu.soap_backend_begin(blk, key=4242)
+    cells = [synth.random_structure(850, 15.0, 1.0, seed=531),
+             synth.random_structure(64, 7.0, 1.2, seed=532)]
+    bat = gpu.Batch(cells, [4242])
+    e, f, v = bat.compute()
+    off = 0
+    for s, st in enumerate(cells):
+        eo, fo, vo, _ = O.evaluate(st.positions, st.species, st.box, [blk])
+        sl = slice(off, off + st.n)
+        assert np.max(np.abs(e[sl] - eo)) < E_TOL, s
+        assert np.max(np.abs(f[sl] - fo)) < F_TOL, s
+        # the virial per atom (its parity bound): a sum over about 50 000 pair
+        # terms whose forces carry the 1e-6 eV/A bound
+        assert np.max(np.abs(v[s] - vo)) / st.n < 1e-6, s
+        off += st.n
+    bat.close()

@@ -49,6 +49,9 @@ CASES = [
     ("supercell", lambda: random_structure(30, 6.0, 1.2, seed=4)),
     ("two_species", lambda: random_structure(300, (300 / 0.12) ** (1 / 3), 1.0, seed=11,
                                              h_fraction=0.25)),
+    # 4 cells per axis of 13 atoms each: a 27-cell neighbourhood of about 350
+    # candidates, more than the search stages at once (256), so it runs in rounds
+    ("dense_rounds", lambda: random_structure(850, 15.0, 1.0, seed=12)),
 ]
 
 
@@ -154,6 +157,20 @@ def ch_blocks(gpu):
     bH = sparse_block(ch_hypers(2), 300, seed=9, n_atoms=300, L=L, d_min=1.0, h_fraction=0.25,
                       n_structs=4)
     return bC, bH
+
+
+def test_engine_parity_dense_rounds(gpu, carbon_block):
+    """An engine on a structure dense enough that each cell's neighbourhood is
+    staged in rounds (about 350 candidates against the 256 staged at once)."""
+    st = random_structure(850, 15.0, 1.0, seed=12)
+    gpu.soap_backend_begin(carbon_block, key=101)
+    eo, fo, vo, _ = O.evaluate(st.positions, st.species, st.box, [carbon_block])
+    eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [101])
+    e, f, v = eng.compute()
+    assert np.abs(e - eo).max() < E_TOL
+    assert np.abs(f - fo).max() < F_TOL
+    assert np.abs(v - vo).max() / st.n < 1e-6   # the virial per atom (its parity bound)
+    eng.close()
 
 
 def test_engine_parity_two_species(gpu, ch_blocks):
