@@ -63,8 +63,7 @@ def parse():
                     help="separate training cells of the workload's kind")
     ap.add_argument("--mlp-epochs", type=int, default=10)
     ap.add_argument("--mlp-hidden", type=int, default=0,
-                    help="hidden width H of each member (D -> H -> H -> 1); 0: 256 for "
-                         "D <= 512 (the carbon network), 64 above")
+                    help="hidden width H of each member (D -> H -> H -> 1); 0: 64")
     ap.add_argument("--gate-ev", type=float, default=0.005)
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: shard ONE structure over the ranks by central-site ranges "
@@ -198,7 +197,7 @@ def mixed_leg(B, eng, blocks, keys, w, a, ext, dist, plain_ms):
     import torch
     from turbogap_b200 import learned
     t0 = time.time()
-    hidden = [a.mlp_hidden or (256 if b.hypers.device_dim <= 512 else 64) for b in blocks]
+    hidden = [a.mlp_hidden or 64 for b in blocks]
     mlps = [B.Mlp(b.hypers.device_dim, hidden[i], 4, seed=100 + i) for i, b in enumerate(blocks)]
     kind = "CH" if len(blocks) > 1 else "C"
     cells = learned.training_cells(kind, a.mlp_cells, seed=w.seed * 100 + 61)
