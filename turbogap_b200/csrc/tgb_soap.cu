@@ -1790,12 +1790,14 @@ static int force_impl(const SoapParams &P, const SiteArgs &S, const ForceIn &I, 
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    static int resident = 0;   // sites in flight at once: the L2 prefetch distance
+    static int resident = 0;   // sites in flight at once
     if (!resident)
         TGB_TRY(resident_warps(k_soap_force<NS, AMAX, LMAX, TILE, RAW, MULT>, 32 * Sh::WARPS, smem,
                                &resident));
     ForceIn I2 = I;
-    I2.ahead = resident;
+    // the L2 prefetch distance: a quarter of the sites in flight ahead: the rows arrive in L2 in time and
+    // stay there until used (measured: ch32k 0.552 -> 0.541 ms, ch1m unchanged)
+    I2.ahead = std::max(1, resident / 4);
     const int grid = (S.n_sites + Sh::WARPS - 1) / Sh::WARPS;
     *nblk = grid;
     if (grid > 0)
