@@ -339,7 +339,8 @@ int tg_engine_tiles(tg_engine *e, int32_t *tiles, int32_t n, int32_t *n_blocks);
  *      energies, forces and the virial (src/turbogap.f90:1876-1885).
  * tg_engine_set_site_range: this engine evaluates the central sites in
  *   [site_beg, site_end) (0-based) only; other sites' energies are zero (no e0),
- *   forces and virial hold this range's share. Default: every site.
+ *   forces and virial hold this range's share. The neighbour search lists the
+ *   range's sites only (other sites get empty lists). Default: every site.
  * tg_nccl_unique_id: 128 bytes for tg_engine_set_comm, made on one rank and
  *   sent to the others by the host (e.g. a torch.distributed broadcast).
  * tg_engine_set_comm: collective over n_ranks processes; afterwards every force
