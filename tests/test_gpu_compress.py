@@ -177,3 +177,28 @@ def test_repeated_entries_add(gpu):
     qo, _, _ = oracle_descriptors(st, h, nl)
     assert np.abs(out[0] - out[1]).max() < 1e-7
     assert np.abs(out[0] - qo).max() < Q_TOL and np.abs(out[1] - qo).max() < Q_TOL
+
+
+def test_compressed_species_multiplicity(gpu):
+    """A compressed block with carbon in both descriptor species (species
+    multiplicity with the compression's raw-spectrum instantiations): descriptors
+    and the engine's energies, forces and virial against the oracle."""
+    from test_gpu_parity import multiplicity_hypers
+    h = multiplicity_hypers(central=1)
+    h.compress = random_transformation(h.uncompressed_dim, 301, seed=86)
+    blk = sparse_block(h, 300, seed=87, n_atoms=300, L=L, d_min=1.0, h_fraction=0.25,
+                       n_structs=2)
+    gpu.soap_backend_begin(blk, key=1804)
+    st = synth.random_structure(300, L, 1.0, seed=88, h_fraction=0.25)
+    nl = neighbor_data(st, h.rcut_max)
+    q = gpu.get_soap(st.n, nl["n_neigh"], nl["neighbors_list"], nl["rjs"], nl["xyz"],
+                     st.species, st.species, h.dim)
+    qo, _, _ = oracle_descriptors(st, h, nl)
+    assert np.abs(q - qo).max() < Q_TOL
+    eo, fo, vo, _ = O.evaluate(st.positions, st.species, st.box, [blk])
+    eng = gpu.Engine(st.positions, st.species, st.masses, st.box, [1804])
+    e, f, v = eng.compute()
+    assert np.abs(e - eo).max() < E_TOL
+    assert np.abs(f - fo).max() < F_TOL
+    assert np.abs(v - vo).max() < V_TOL * np.abs(vo).max()
+    eng.close()
