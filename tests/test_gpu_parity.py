@@ -228,6 +228,15 @@ def test_engine_parity_species_multiplicity(gpu):
     assert np.abs(f - fo).max() < F_TOL
     assert np.abs(v - vo).max() < V_TOL * np.abs(vo).max()
     assert (st.species == 2).any() and not f[st.species == 2].any()   # H is invisible to it
+    # the mixed form on the multiplicity block: with a gate of 0 every site goes
+    # back to the exact kernel, through the single-bf16 descriptor of the mixed form
+    m = gpu.Mlp(h.device_dim, 64, 2, seed=5)
+    gpu.engine_set_mlp(eng, 0, m, gate_ev=0.0)
+    eg, fg, _ = eng.compute()
+    assert gpu.engine_mlp_stats(eng, 0)[0] == int(np.sum(st.species == 1))
+    assert np.abs(eg - e).max() < 1e-9 and np.abs(fg - f).max() < 1e-9
+    gpu.engine_set_mlp(eng, 0, None)
+    m.close()
     eng.close()
 
 
